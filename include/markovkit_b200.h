@@ -1,0 +1,174 @@
+/* markovkit_b200 — C ABI of the B200 resolvent / FSP engine.
+ *
+ * Plain pointers and sizes only. Vectors named d_* are device pointers (the caller owns
+ * them); h_* are host pointers. `stream` is a cudaStream_t passed as void* (NULL = the
+ * default stream). Every call returns an MK_* status; mk_last_error() describes the last
+ * failure on the calling thread. Handles own their device memory; *_destroy frees it.
+ * A generator and a multigrid only read the space and model they were created from, and
+ * copy what they need, so those may be destroyed afterwards.
+ *
+ * Each entry point names the MarkovKit interface it replaces (file:line in the reference).
+ */
+#ifndef MARKOVKIT_B200_H
+#define MARKOVKIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; the C++ facade maps them back to the reference's exception types */
+#define MK_OK 0
+#define MK_EINVAL 1     /* std::invalid_argument */
+#define MK_EOVERFLOW 2  /* std::overflow_error ("population state space is too large") */
+#define MK_ESINGULAR 3  /* std::runtime_error ("singular block") */
+#define MK_ENOMEM 4     /* device allocation failed */
+#define MK_ENOTCONV 5   /* solver stopped at max_iterations (result still returned) */
+#define MK_ENAN 6       /* non-finite residual */
+#define MK_ETIMEOUT 7   /* a bounded device wait gave up */
+#define MK_ECUDA 8      /* any other CUDA error */
+
+typedef struct mk_space_s *mk_space;
+typedef struct mk_model_s *mk_model;
+typedef struct mk_generator_s *mk_generator;
+typedef struct mk_multigrid_s *mk_multigrid;
+typedef struct mk_solver_s *mk_solver;
+
+const char *mk_last_error(void);
+int mk_version(void);
+
+/* ---- device memory helpers (for callers without their own CUDA runtime) ---- */
+int mk_device_alloc(size_t bytes, void **d_ptr);
+int mk_device_free(void *d_ptr);
+int mk_memcpy_h2d(void *d_dst, const void *h_src, size_t bytes, void *stream);
+int mk_memcpy_d2h(void *h_dst, const void *d_src, size_t bytes, void *stream);
+int mk_stream_synchronize(void *stream);
+
+/* ---- population state spaces: markovkit/rdme/population_space.hpp ---- */
+/* population_box(n_voxels, max_totals)          population_space.hpp:131-139 */
+int mk_space_create_box(int64_t n_voxels, int n_species, const int *max_totals, mk_space *out);
+/* population_sector(n_voxels, totals)           population_space.hpp:105-109 */
+int mk_space_create_sector(int64_t n_voxels, int n_species, const int *totals, mk_space *out);
+void mk_space_destroy(mk_space space);
+/* size(), n_sectors(), sector_begin(k), sector_totals(k)   population_space.hpp:141,156-159 */
+int mk_space_size(mk_space space, int64_t *n);
+int mk_space_n_sectors(mk_space space, int64_t *n_sectors);
+int mk_space_sector_begin(mk_space space, int64_t k, int64_t *begin);
+int mk_space_sector_totals(mk_space space, int64_t k, int *totals);
+/* find_sector(totals) -> k or -1                population_space.hpp:166-175 */
+int mk_space_find_sector(mk_space space, const int *totals, int64_t *k);
+/* sector_of(i)                                  population_space.hpp:161-164 */
+int mk_space_sector_of(mk_space space, int64_t i, int64_t *k);
+/* find(x) -> index or -1, operator[](i) on one voxel-major state (host)
+ *                                               population_space.hpp:142-150, :141 */
+int mk_space_find_host(mk_space space, const int *h_state, int64_t *index);
+int mk_space_state_host(mk_space space, int64_t i, int *h_state);
+/* batched, on the device: d_states is count x (n_voxels * n_species) ints, voxel-major */
+int mk_space_rank(mk_space space, const int *d_states, int64_t count, int64_t *d_index,
+                  void *stream);
+int mk_space_unrank(mk_space space, const int64_t *d_index, int64_t count, int *d_states,
+                    void *stream);
+
+/* ---- RDME models: markovkit/rdme/reaction_diffusion.hpp ---- */
+/* voxel_domain(grid<D>(dims, spacing), diffusivities) reaction_diffusion.hpp:23-49,
+ * with grid<D> = structured_grid_graph<D> (rdme/multigrid.hpp:20-21) */
+int mk_model_create_grid(int dim, const int64_t *dims, const double *spacing, int n_species,
+                         const double *diffusivities, mk_model *out);
+/* voxel_domain(graph, volumes, diffusivities) with an explicit symmetric graph (CSR)
+ *                                               reaction_diffusion.hpp:29-40 */
+int mk_model_create_graph(int64_t n_voxels, const int64_t *nbr_ptr, const int64_t *nbr_idx,
+                          const double *nbr_weight, const double *volumes, int n_species,
+                          const double *diffusivities, mk_model *out);
+/* the local reactions {change, rate(counts, volume)} of reaction_diffusion::reactions
+ * (reaction_diffusion.hpp:62-67), tabulated by the caller: rates[r][c][tuple] is the rate of
+ * reaction r in a voxel of volume class c whose counts n_s (0 <= n_s <= tuple_max[s]) have
+ * tuple index sum_s n_s * prod_{s' > s} (tuple_max[s'] + 1). voxel_class may be NULL when
+ * n_volume_classes == 1. */
+int mk_model_set_reactions(mk_model model, int n_reactions, const int *change,
+                           const int *tuple_max, int n_volume_classes, const int *voxel_class,
+                           const double *rates);
+int mk_model_n_voxels(mk_model model, int64_t *n_voxels);
+void mk_model_destroy(mk_model model);
+
+/* ---- the generator: markovkit/generator.hpp ---- */
+/* generator(space, model, boundary)             generator.hpp:27-44; absorbing = 1 or 0 */
+int mk_generator_create(mk_space space, mk_model model, int absorbing, mk_generator *out);
+void mk_generator_destroy(mk_generator gen);
+int mk_generator_rows(mk_generator gen, int64_t *rows);
+/* exit_rates(), leak_rates()                    generator.hpp:55-59 */
+int mk_generator_exit_leak(mk_generator gen, double *d_exit, double *d_leak, void *stream);
+/* apply: y = Q x                                generator.hpp:62-70 */
+int mk_generator_apply(mk_generator gen, const double *d_x, double *d_y, void *stream);
+/* apply_shifted: y = shift x - Q x              generator.hpp:73-81 */
+int mk_generator_apply_shifted(mk_generator gen, double shift, const double *d_x, double *d_y,
+                               void *stream);
+int mk_generator_apply_f32(mk_generator gen, const float *d_x, float *d_y, void *stream);
+int mk_generator_apply_shifted_f32(mk_generator gen, float shift, const float *d_x, float *d_y,
+                                   void *stream);
+
+/* ---- sector multigrid: markovkit/rdme/multigrid.hpp ---- */
+typedef struct {
+    int pre_sweeps;       /* multigrid_options, multigrid.hpp:125-134 */
+    int post_sweeps;
+    double jacobi_weight;
+    int64_t coarsest_size;
+    int max_levels;
+    int coarse_cycles;
+    int sweep_growth;
+    int smoother;  /* 0 weighted Jacobi (reference default), 1 red-black Gauss-Seidel */
+    int precision; /* 0 FP64, 1 FP32 (use inside flexible GMRES) */
+} mk_multigrid_options;
+void mk_multigrid_options_default(mk_multigrid_options *opt);
+/* sector_multigrid(domain, box, shift, options) multigrid.hpp:377-384; a single-sector
+ * space gives population_multigrid (multigrid.hpp:145-179) */
+int mk_multigrid_create(mk_space space, mk_model model, double shift,
+                        const mk_multigrid_options *opt, mk_multigrid *out);
+void mk_multigrid_destroy(mk_multigrid mg);
+/* apply(b, x): one cycle per sector             multigrid.hpp:397-403 */
+int mk_multigrid_apply(mk_multigrid mg, const double *d_b, double *d_x, void *stream);
+/* max_levels()                                  multigrid.hpp:389-395 */
+int mk_multigrid_max_levels(mk_multigrid mg, int *levels);
+int mk_multigrid_depth(mk_multigrid mg, int *depth);
+int mk_multigrid_level_size(mk_multigrid mg, int depth, int64_t *n);
+/* population_transfer restrict / prolong between depth d and d+1 (multigrid.hpp:100-111)
+ * and apply_system at depth d (multigrid.hpp:196), FP64 */
+int mk_multigrid_restrict(mk_multigrid mg, int depth, const double *d_fine, double *d_coarse,
+                          void *stream);
+int mk_multigrid_prolong(mk_multigrid mg, int depth, const double *d_coarse, double *d_fine,
+                         void *stream);
+int mk_multigrid_apply_system(mk_multigrid mg, int depth, const double *d_x, double *d_y,
+                              void *stream);
+
+/* ---- GMRES: num::gmres(A, [M], b, x, options) (call sites tests/test_rdme.cpp:238-249) ---- */
+typedef struct {
+    double tolerance;       /* absolute, on ||b - A x||_2 */
+    int64_t max_iterations; /* Arnoldi steps in total */
+    int restart;
+    int flexible;           /* FGMRES; forced on with an FP32 preconditioner */
+} mk_gmres_options;
+typedef struct {
+    int64_t iterations;
+    double residual; /* recomputed true residual norm */
+    int converged;
+    int status;
+} mk_solver_result;
+void mk_gmres_options_default(mk_gmres_options *opt);
+/* a resident solver for A = shift I - Q (shifted_generator, generator.hpp:116-133),
+ * preconditioned by mg (NULL: plain GMRES); it keeps the Krylov workspace on the device */
+int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,
+                     const mk_gmres_options *opt, mk_solver *out);
+void mk_solver_destroy(mk_solver solver);
+/* x is the initial guess on entry and the solution on return (device vectors) */
+int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_result *result,
+                    void *stream);
+/* the same with host vectors: copies in, solves, copies out */
+int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
+                         mk_solver_result *result, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MARKOVKIT_B200_H */

@@ -1,0 +1,22 @@
+"""markovkit_b200: MarkovKit's RDME resolvent solve and Krylov FSP on NVIDIA B200.
+
+The compute lives in libmarkovkit_b200.so (hand-written sm_100a CUDA behind the C ABI of
+include/markovkit_b200.h). This package is the Python mirror of the reference API over it.
+"""
+
+from .api import (  # noqa: F401
+    generator,
+    gmres,
+    gmres_options,
+    grid,
+    local_reaction,
+    multigrid_options,
+    population_box,
+    population_sector,
+    reaction_diffusion,
+    sector_multigrid,
+    shifted_generator,
+    solver,
+    voxel_domain,
+)
+from .inputs import dirichlet_rhs, uniform01, uniform_rhs  # noqa: F401

@@ -1,0 +1,159 @@
+"""ctypes bindings of the C ABI in include/markovkit_b200.h.
+
+The shared library is built in-tree (markovkit_b200/build.py). There is no fallback: if it
+is missing or fails to load, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libmarkovkit_b200.so"
+
+MK_OK = 0
+MK_EINVAL = 1
+MK_EOVERFLOW = 2
+MK_ESINGULAR = 3
+MK_ENOMEM = 4
+MK_ENOTCONV = 5
+MK_ENAN = 6
+MK_ETIMEOUT = 7
+MK_ECUDA = 8
+
+
+class MkError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class InvalidArgument(MkError, ValueError):
+    pass
+
+
+class OverflowErrorMk(MkError, OverflowError):
+    pass
+
+
+_EXC = {MK_EINVAL: InvalidArgument, MK_EOVERFLOW: OverflowErrorMk}
+
+
+class MultigridOptions(C.Structure):
+    _fields_ = [
+        ("pre_sweeps", C.c_int),
+        ("post_sweeps", C.c_int),
+        ("jacobi_weight", C.c_double),
+        ("coarsest_size", C.c_int64),
+        ("max_levels", C.c_int),
+        ("coarse_cycles", C.c_int),
+        ("sweep_growth", C.c_int),
+        ("smoother", C.c_int),
+        ("precision", C.c_int),
+    ]
+
+
+class GmresOptions(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double),
+        ("max_iterations", C.c_int64),
+        ("restart", C.c_int),
+        ("flexible", C.c_int),
+    ]
+
+
+class SolverResult(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int64),
+        ("residual", C.c_double),
+        ("converged", C.c_int),
+        ("status", C.c_int),
+    ]
+
+
+P = C.c_void_p
+I64 = C.c_int64
+I64P = C.POINTER(C.c_int64)
+IP = C.POINTER(C.c_int)
+DP = C.POINTER(C.c_double)
+
+# name: (restype, argtypes)
+SIGNATURES = {
+    "mk_last_error": (C.c_char_p, []),
+    "mk_version": (C.c_int, []),
+    "mk_device_alloc": (C.c_int, [C.c_size_t, C.POINTER(P)]),
+    "mk_device_free": (C.c_int, [P]),
+    "mk_memcpy_h2d": (C.c_int, [P, P, C.c_size_t, P]),
+    "mk_memcpy_d2h": (C.c_int, [P, P, C.c_size_t, P]),
+    "mk_stream_synchronize": (C.c_int, [P]),
+    "mk_space_create_box": (C.c_int, [I64, C.c_int, IP, C.POINTER(P)]),
+    "mk_space_create_sector": (C.c_int, [I64, C.c_int, IP, C.POINTER(P)]),
+    "mk_space_destroy": (None, [P]),
+    "mk_space_size": (C.c_int, [P, I64P]),
+    "mk_space_n_sectors": (C.c_int, [P, I64P]),
+    "mk_space_sector_begin": (C.c_int, [P, I64, I64P]),
+    "mk_space_sector_totals": (C.c_int, [P, I64, IP]),
+    "mk_space_find_sector": (C.c_int, [P, IP, I64P]),
+    "mk_space_sector_of": (C.c_int, [P, I64, I64P]),
+    "mk_space_find_host": (C.c_int, [P, IP, I64P]),
+    "mk_space_state_host": (C.c_int, [P, I64, IP]),
+    "mk_space_rank": (C.c_int, [P, P, I64, P, P]),
+    "mk_space_unrank": (C.c_int, [P, P, I64, P, P]),
+    "mk_model_create_grid": (C.c_int, [C.c_int, I64P, DP, C.c_int, DP, C.POINTER(P)]),
+    "mk_model_create_graph": (C.c_int, [I64, I64P, I64P, DP, DP, C.c_int, DP, C.POINTER(P)]),
+    "mk_model_set_reactions": (C.c_int, [P, C.c_int, IP, IP, C.c_int, IP, DP]),
+    "mk_model_n_voxels": (C.c_int, [P, I64P]),
+    "mk_model_destroy": (None, [P]),
+    "mk_generator_create": (C.c_int, [P, P, C.c_int, C.POINTER(P)]),
+    "mk_generator_destroy": (None, [P]),
+    "mk_generator_rows": (C.c_int, [P, I64P]),
+    "mk_generator_exit_leak": (C.c_int, [P, P, P, P]),
+    "mk_generator_apply": (C.c_int, [P, P, P, P]),
+    "mk_generator_apply_shifted": (C.c_int, [P, C.c_double, P, P, P]),
+    "mk_generator_apply_f32": (C.c_int, [P, P, P, P]),
+    "mk_generator_apply_shifted_f32": (C.c_int, [P, C.c_float, P, P, P]),
+    "mk_multigrid_options_default": (None, [C.POINTER(MultigridOptions)]),
+    "mk_multigrid_create": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
+    "mk_multigrid_destroy": (None, [P]),
+    "mk_multigrid_apply": (C.c_int, [P, P, P, P]),
+    "mk_multigrid_max_levels": (C.c_int, [P, IP]),
+    "mk_multigrid_depth": (C.c_int, [P, IP]),
+    "mk_multigrid_level_size": (C.c_int, [P, C.c_int, I64P]),
+    "mk_multigrid_restrict": (C.c_int, [P, C.c_int, P, P, P]),
+    "mk_multigrid_prolong": (C.c_int, [P, C.c_int, P, P, P]),
+    "mk_multigrid_apply_system": (C.c_int, [P, C.c_int, P, P, P]),
+    "mk_gmres_options_default": (None, [C.POINTER(GmresOptions)]),
+    "mk_solver_create": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.POINTER(P)]),
+    "mk_solver_destroy": (None, [P]),
+    "mk_solver_solve": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
+    "mk_solver_solve_host": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
+}
+
+_lib: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """Load the in-tree library once and attach every declared signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise MkError(MK_ECUDA, f"{LIB_PATH.name} is not built; run markovkit_b200/build.py")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, allow: tuple[int, ...] = ()) -> int:
+    if rc == MK_OK or rc in allow:
+        return rc
+    msg = load().mk_last_error().decode(errors="replace")
+    raise _EXC.get(rc, MkError)(rc, msg)
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)

@@ -1,0 +1,1241 @@
+// Host side of the B200 resolvent engine (see engine.hpp).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <map>
+#include <numeric>
+
+namespace mkb {
+
+void check_cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) {
+        return;
+    }
+    const int code = (e == cudaErrorMemoryAllocation) ? kENoMem : kECuda;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------------------
+// binomials and spaces
+
+Binomials::Binomials(int jmax_, int qmax_) : jmax(jmax_), qmax(qmax_) {
+    host.assign(static_cast<std::size_t>(jmax + 1) * (qmax + 1), 0);
+    auto at = [&](int j, int q) -> std::int64_t & {
+        return host[static_cast<std::size_t>(j) * (qmax + 1) + q];
+    };
+    for (int q = 0; q <= qmax; ++q) {
+        at(0, q) = 1;
+        for (int j = 1; j <= std::min(q, jmax); ++j) {
+            const std::int64_t a = at(j - 1, q - 1), b = (j <= q - 1) ? at(j, q - 1) : 0;
+            at(j, q) = (a >= kSaturated || b >= kSaturated || a + b >= kSaturated) ? kSaturated
+                                                                                  : a + b;
+        }
+    }
+    dev.upload(host);
+}
+
+std::vector<SectorDesc> layout_sectors(int V, int S, const std::vector<std::vector<int>> &totals,
+                                       const Binomials &B, std::int64_t *total_size) {
+    std::vector<SectorDesc> out;
+    std::int64_t begin = 0;
+    const BinomTable bt = B.host_view();
+    for (const auto &t : totals) {
+        SectorDesc sec;
+        std::int64_t comp[kMaxSpecies] = {};
+        std::int64_t size = 1;
+        int mol = 0;
+        for (int s = 0; s < S; ++s) {
+            sec.total[s] = t[s];
+            sec.mol_offset[s] = mol;
+            mol += t[s];
+            comp[s] = binom(bt, t[s] + V - 1, t[s]);
+            if (comp[s] >= kSaturated || size > std::numeric_limits<std::int64_t>::max() / comp[s]) {
+                throw Error(kEOverflow, "population state space is too large");
+            }
+            size *= comp[s];
+        }
+        sec.n_mol = mol;
+        std::int64_t stride = 1;
+        for (int s = S - 1; s >= 0; --s) {
+            sec.stride[s] = stride;
+            stride *= comp[s];
+        }
+        sec.begin = begin;
+        sec.size = size;
+        for (int r = 0; r < kMaxReactions; ++r) {
+            sec.src[r] = -1;
+            sec.dst[r] = -1;
+        }
+        if (begin > std::numeric_limits<std::int64_t>::max() - size) {
+            throw Error(kEOverflow, "population state space is too large");
+        }
+        begin += size;
+        out.push_back(sec);
+    }
+    *total_size = begin;
+    return out;
+}
+
+std::unique_ptr<Space> Space::make(int V, const std::vector<int> &limits, bool is_box) {
+    const int S = static_cast<int>(limits.size());
+    if (V < 1 || S < 1) {
+        throw Error(kEInval, "population state space needs a voxel and a species");
+    }
+    if (S > kMaxSpecies) {
+        throw Error(kEInval, "at most 4 species are supported");
+    }
+    for (int t : limits) {
+        if (t < 0) {
+            throw Error(kEInval, "species totals must be nonnegative");
+        }
+    }
+    auto sp = std::make_unique<Space>();
+    sp->V = V;
+    sp->S = S;
+    sp->is_box = is_box;
+    sp->limits = limits;
+    sp->max_total = *std::max_element(limits.begin(), limits.end());
+    sp->max_mol = std::accumulate(limits.begin(), limits.end(), 0);
+    sp->binom = std::make_shared<Binomials>(sp->max_total + 1, V + sp->max_total + 1);
+    std::vector<std::vector<int>> totals;
+    if (is_box) {
+        std::vector<int> t(S, 0);
+        // mixed radix, species 0 most significant (population_space.hpp:166-189)
+        while (true) {
+            totals.push_back(t);
+            int s = S - 1;
+            while (s >= 0 && t[s] == limits[s]) {
+                t[s] = 0;
+                --s;
+            }
+            if (s < 0) {
+                break;
+            }
+            ++t[s];
+        }
+    } else {
+        totals.push_back(limits);
+    }
+    sp->sectors = layout_sectors(V, S, totals, *sp->binom, &sp->n);
+    sp->d_sectors.upload(sp->sectors);
+    sp->d_limits.upload(limits);
+    return sp;
+}
+
+int Space::find_sector(const int *totals) const {
+    if (!is_box) {
+        for (int s = 0; s < S; ++s) {
+            if (totals[s] != limits[s]) {
+                return -1;
+            }
+        }
+        return 0;
+    }
+    int k = 0;
+    for (int s = 0; s < S; ++s) {
+        if (totals[s] < 0 || totals[s] > limits[s]) {
+            return -1;
+        }
+        k = k * (limits[s] + 1) + totals[s];
+    }
+    return k;
+}
+
+int Space::sector_of(std::int64_t i) const {
+    auto it = std::upper_bound(sectors.begin(), sectors.end(), i,
+                               [](std::int64_t v, const SectorDesc &s) { return v < s.begin; });
+    return static_cast<int>(it - sectors.begin()) - 1;
+}
+
+std::int64_t Space::rank(const int *state) const {
+    int totals[kMaxSpecies] = {};
+    for (int v = 0; v < V; ++v) {
+        for (int s = 0; s < S; ++s) {
+            const int c = state[static_cast<std::int64_t>(v) * S + s];
+            if (c < 0) {
+                return -1;
+            }
+            totals[s] += c;
+        }
+    }
+    const int k = find_sector(totals);
+    if (k < 0) {
+        return -1;
+    }
+    const SectorDesc &sec = sectors[k];
+    const BinomTable B = binom->host_view();
+    std::vector<int> u;
+    std::int64_t local = 0;
+    for (int s = 0; s < S; ++s) {
+        u.clear();
+        for (int v = V - 1; v >= 0; --v) {
+            for (int q = 0; q < state[static_cast<std::int64_t>(v) * S + s]; ++q) {
+                u.push_back(V - 1 - v);
+            }
+        }
+        local += rank_species(B, u.data(), static_cast<int>(u.size())) * sec.stride[s];
+    }
+    return sec.begin + local;
+}
+
+void Space::unrank(std::int64_t i, int *state) const {
+    std::fill(state, state + static_cast<std::int64_t>(V) * S, 0);
+    if (i < 0 || i >= n) {
+        throw Error(kEInval, "state index out of range");
+    }
+    const SectorDesc &sec = sectors[sector_of(i)];
+    std::int64_t rank[kMaxSpecies];
+    split_local(sec, S, i - sec.begin, rank);
+    std::vector<int> u(std::max(max_total, 1));
+    const BinomTable B = binom->host_view();
+    for (int s = 0; s < S; ++s) {
+        unrank_species(B, rank[s], sec.total[s], V, u.data());
+        for (int p = 0; p < sec.total[s]; ++p) {
+            ++state[static_cast<std::int64_t>(V - 1 - u[p]) * S + s];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// models
+
+int Model::ntuple() const {
+    int n = 1;
+    for (int t : tmax) {
+        n *= (t + 1);
+    }
+    return n;
+}
+
+std::unique_ptr<Model> Model::grid(int dim, const std::int64_t *dims, const double *spacing,
+                                   const std::vector<double> &diff) {
+    if (dim < 1 || dim > 3) {
+        throw Error(kEInval, "grid dimension must be 1, 2 or 3");
+    }
+    auto m = std::make_unique<Model>();
+    m->has_grid = true;
+    m->dim = dim;
+    std::int64_t V = 1, stride[3] = {1, 1, 1};
+    for (int a = 0; a < dim; ++a) {
+        if (dims[a] < 1 || !(spacing[a] > 0.0)) {
+            throw Error(kEInval, "grid dimensions and spacings must be positive");
+        }
+        m->dims[a] = dims[a];
+        m->spacing[a] = spacing[a];
+        stride[a] = V;
+        V *= dims[a];
+    }
+    if (V > (std::int64_t(1) << 30)) {
+        throw Error(kEInval, "too many voxels");
+    }
+    m->V = static_cast<int>(V);
+    m->S = static_cast<int>(diff.size());
+    m->diff = diff;
+    double volume = 1.0;
+    for (int a = 0; a < dim; ++a) {
+        volume *= spacing[a];
+    }
+    m->volumes.assign(m->V, volume);
+    m->nbr_ptr.assign(m->V + 1, 0);
+    // axis 0 fastest; neighbours axis by axis, the lower one first; weight = face area / h
+    for (std::int64_t v = 0; v < V; ++v) {
+        std::int64_t rem = v;
+        std::int64_t c[3] = {0, 0, 0};
+        for (int a = 0; a < dim; ++a) {
+            c[a] = rem % dims[a];
+            rem /= dims[a];
+        }
+        for (int a = 0; a < dim; ++a) {
+            double face = 1.0;
+            for (int b = 0; b < dim; ++b) {
+                if (b != a) {
+                    face *= spacing[b];
+                }
+            }
+            const double w = face / spacing[a];
+            if (c[a] > 0) {
+                m->nbr_idx.push_back(static_cast<int>(v - stride[a]));
+                m->nbr_w.push_back(w);
+            }
+            if (c[a] + 1 < dims[a]) {
+                m->nbr_idx.push_back(static_cast<int>(v + stride[a]));
+                m->nbr_w.push_back(w);
+            }
+        }
+        m->nbr_ptr[v + 1] = static_cast<int>(m->nbr_idx.size());
+    }
+    return m;
+}
+
+void Model::validate() const {
+    if (V < 1 || S < 1 || S > kMaxSpecies) {
+        throw Error(kEInval, "model needs 1..4 species and a voxel");
+    }
+    if (static_cast<int>(nbr_ptr.size()) != V + 1 || static_cast<int>(volumes.size()) != V ||
+        static_cast<int>(diff.size()) != S) {
+        throw Error(kEInval, "model arrays have the wrong sizes");
+    }
+    for (double v : volumes) {
+        if (!(v > 0.0) || !std::isfinite(v)) {
+            throw Error(kEInval, "voxel_domain: volumes must be positive");
+        }
+    }
+    if (R > kMaxReactions) {
+        throw Error(kEInval, "at most 16 local reactions are supported");
+    }
+    if (R > 0) {
+        if (static_cast<int>(change.size()) != R * S || static_cast<int>(tmax.size()) != S ||
+            static_cast<std::int64_t>(rates.size()) !=
+                static_cast<std::int64_t>(R) * nvc * ntuple()) {
+            throw Error(kEInval, "reaction tables have the wrong sizes");
+        }
+        if (nvc > 1 && static_cast<int>(vclass.size()) != V) {
+            throw Error(kEInval, "one volume class per voxel");
+        }
+    }
+}
+
+template <typename T>
+void ModelTables<T>::build(const Model &m, double diff_scale, bool with_reactions, bool absorbing) {
+    m.validate();
+    const int V = m.V;
+    h_nbr_ptr = m.nbr_ptr;
+    h_nbr_idx = m.nbr_idx;
+    const std::size_t E = h_nbr_idx.size();
+    h_in_coef.assign(E, T(0));
+    h_deg_coef.assign(V, T(0));
+    for (int v = 0; v < V; ++v) {
+        double deg = 0.0;
+        for (int e = m.nbr_ptr[v]; e < m.nbr_ptr[v + 1]; ++e) {
+            const int w = m.nbr_idx[e];
+            if (w < 0 || w >= V) {
+                throw Error(kEInval, "voxel graph edge out of range");
+            }
+            deg += m.nbr_w[e] / m.volumes[v];
+            // the reverse edge w -> v carries the in-jump
+            double wr = -1.0;
+            for (int f = m.nbr_ptr[w]; f < m.nbr_ptr[w + 1]; ++f) {
+                if (m.nbr_idx[f] == v) {
+                    wr = m.nbr_w[f];
+                    break;
+                }
+            }
+            if (wr < 0.0) {
+                throw Error(kEInval, "voxel graph must list every edge in both directions");
+            }
+            h_in_coef[e] = static_cast<T>(wr / m.volumes[w]);
+        }
+        h_deg_coef[v] = static_cast<T>(deg);
+    }
+    h_vparity.assign(V, 0);
+    if (m.has_grid) {
+        for (int v = 0; v < V; ++v) {
+            std::int64_t rem = v, sum = 0;
+            for (int a = 0; a < m.dim; ++a) {
+                sum += rem % m.dims[a];
+                rem /= m.dims[a];
+            }
+            h_vparity[v] = static_cast<unsigned char>(sum & 1);
+        }
+    }
+    ModelView<T> mv;
+    mv.V = V;
+    mv.S = m.S;
+    mv.absorbing = absorbing ? 1 : 0;
+    for (int s = 0; s < m.S; ++s) {
+        mv.diff[s] = static_cast<T>(m.diff[s] * diff_scale);
+    }
+    h_vclass.clear();
+    h_rate.clear();
+    if (with_reactions && m.R > 0) {
+        mv.R = m.R;
+        mv.nvc = m.nvc;
+        mv.ntuple = m.ntuple();
+        int stride = 1;
+        for (int s = m.S - 1; s >= 0; --s) {
+            mv.tmax[s] = m.tmax[s];
+            mv.tstride[s] = stride;
+            stride *= m.tmax[s] + 1;
+        }
+        h_rate.resize(m.rates.size());
+        for (std::size_t k = 0; k < m.rates.size(); ++k) {
+            const double a = m.rates[k];
+            h_rate[k] = static_cast<T>((a > 0.0 && std::isfinite(a)) ? a : 0.0);
+        }
+        if (m.nvc > 1) {
+            h_vclass = m.vclass;
+        }
+        for (int r = 0; r < m.R; ++r) {
+            bool nonneg = true, nonpos = true, fits = true;
+            int t_neg = 0;
+            for (int s = 0; s < m.S; ++s) {
+                const int c = m.change[r * m.S + s];
+                nonneg = nonneg && c >= 0;
+                nonpos = nonpos && c <= 0;
+                fits = fits && -c <= m.tmax[s];
+                t_neg += (c < 0 ? -c : 0) * mv.tstride[s];
+                mv.change[r][s] = c;
+            }
+            auto rate_at = [&](int vc, int tuple) {
+                return m.rates[(static_cast<std::size_t>(r) * m.nvc + vc) * mv.ntuple + tuple];
+            };
+            if (nonneg) {
+                mv.nonneg_mask |= 1U << r;
+                double total = 0.0;
+                for (int v = 0; v < V; ++v) {
+                    const double a = rate_at(m.nvc > 1 ? m.vclass[v] : 0, 0);
+                    total += (a > 0.0 && std::isfinite(a)) ? a : 0.0;
+                }
+                mv.empty_total[r] = static_cast<T>(total);
+            }
+            if (nonpos && fits) {
+                for (int vc = 0; vc < m.nvc; ++vc) {
+                    if (rate_at(vc, t_neg) > 0.0) {
+                        mv.heavy_mask |= 1U << r;
+                    }
+                }
+            }
+        }
+    }
+    nbr_ptr.upload(h_nbr_ptr);
+    nbr_idx.upload(h_nbr_idx);
+    in_coef.upload(h_in_coef);
+    deg_coef.upload(h_deg_coef);
+    vparity.upload(h_vparity);
+    vclass.upload(h_vclass);
+    rate.upload(h_rate);
+
+    host = mv;
+    host.nbr_ptr = h_nbr_ptr.data();
+    host.nbr_idx = h_nbr_idx.data();
+    host.in_coef = h_in_coef.data();
+    host.deg_coef = h_deg_coef.data();
+    host.vparity = h_vparity.data();
+    host.vclass = h_vclass.empty() ? nullptr : h_vclass.data();
+    host.rate = h_rate.empty() ? nullptr : h_rate.data();
+    dev = mv;
+    dev.nbr_ptr = nbr_ptr.get();
+    dev.nbr_idx = nbr_idx.get();
+    dev.in_coef = in_coef.get();
+    dev.deg_coef = deg_coef.get();
+    dev.vparity = vparity.get();
+    dev.vclass = h_vclass.empty() ? nullptr : vclass.get();
+    dev.rate = h_rate.empty() ? nullptr : rate.get();
+}
+
+template struct ModelTables<double>;
+template struct ModelTables<float>;
+
+// ---------------------------------------------------------------------------------------
+// operator levels and the generator
+
+void OperatorLevel::finalize(const Model &m, bool with_reactions, bool is_box_like,
+                             const std::vector<int> &box_limits) {
+    (void)is_box_like;
+    (void)box_limits;
+    std::map<std::vector<int>, int> by_totals;
+    int max_mol = 0;
+    for (std::size_t k = 0; k < sectors.size(); ++k) {
+        by_totals[std::vector<int>(sectors[k].total, sectors[k].total + S)] = static_cast<int>(k);
+        max_mol = std::max(max_mol, sectors[k].n_mol);
+    }
+    mol_cap = mol_cap_for(max_mol);
+    if (mol_cap < 0) {
+        throw Error(kEInval, "more than 64 molecules per state are not supported on the device");
+    }
+    const ModelView<double> &mv = t64.host;
+    for (auto &sec : sectors) {
+        sec.heavy = 0;
+        for (int r = 0; r < kMaxReactions; ++r) {
+            sec.src[r] = -1;
+            sec.dst[r] = -1;
+        }
+        if (!with_reactions) {
+            continue;
+        }
+        for (int r = 0; r < m.R; ++r) {
+            std::vector<int> up(S), down(S);
+            for (int s = 0; s < S; ++s) {
+                up[s] = sec.total[s] + m.change[r * S + s];
+                down[s] = sec.total[s] - m.change[r * S + s];
+            }
+            auto it = by_totals.find(up);
+            sec.dst[r] = it == by_totals.end() ? -1 : it->second;
+            it = by_totals.find(down);
+            sec.src[r] = it == by_totals.end() ? -1 : it->second;
+            if (((mv.heavy_mask >> r) & 1U) && sec.src[r] >= 0) {
+                sec.heavy = 1;
+            }
+        }
+    }
+    tiles.clear();
+    for (std::size_t k = 0; k < sectors.size(); ++k) {
+        const SectorDesc &sec = sectors[k];
+        const int rows = sec.heavy ? kWarpRows : kRowBlock;
+        for (std::int64_t l = 0; l < sec.size; l += rows) {
+            Tile t;
+            t.local0 = l;
+            t.sector = static_cast<int>(k);
+            t.kind = sec.heavy ? 1 : 0;
+            t.count = static_cast<int>(std::min<std::int64_t>(rows, sec.size - l));
+            tiles.push_back(t);
+        }
+    }
+    if (tiles.size() > 0x7fffffffULL) {
+        throw Error(kEInval, "space too large for one launch");
+    }
+    d_sectors.upload(sectors);
+    d_tiles.upload(tiles);
+}
+
+template <typename T>
+RowParams<T> OperatorLevel::params() const {
+    RowParams<T> p;
+    p.B = binom->device_view();
+    p.sectors = d_sectors.get();
+    p.tiles = d_tiles.get();
+    if constexpr (std::is_same_v<T, double>) {
+        p.md = t64.dev;
+    } else {
+        p.md = t32.dev;
+    }
+    p.n_tiles = static_cast<int>(tiles.size());
+    return p;
+}
+
+template <typename T>
+void OperatorLevel::run(RowMode mode, const RowParams<T> &p, cudaStream_t stream) const {
+    check_cuda(launch_rows<T>(mode, mol_cap, p, stream), "row kernel launch");
+}
+
+template RowParams<double> OperatorLevel::params<double>() const;
+template RowParams<float> OperatorLevel::params<float>() const;
+template void OperatorLevel::run<double>(RowMode, const RowParams<double> &, cudaStream_t) const;
+template void OperatorLevel::run<float>(RowMode, const RowParams<float> &, cudaStream_t) const;
+
+Generator::Generator(const Space &sp, const Model &model, bool absorbing_)
+    : space(&sp), absorbing(absorbing_) {
+    model.validate();
+    if (model.V != sp.V || model.S != sp.S) {
+        throw Error(kEInval, "model and space disagree on voxels or species");
+    }
+    if (model.R > 0) {
+        for (int s = 0; s < sp.S; ++s) {
+            if (model.tmax[s] < sp.limits[s]) {
+                throw Error(kEInval, "reaction rates must be tabulated up to the space's totals");
+            }
+        }
+    }
+    op.V = sp.V;
+    op.S = sp.S;
+    op.n = sp.n;
+    op.sectors = sp.sectors;
+    op.binom = sp.binom;
+    op.t64.build(model, 1.0, true, absorbing);
+    op.t32.build(model, 1.0, true, absorbing);
+    op.finalize(model, true, sp.is_box, sp.limits);
+}
+
+template <typename T>
+void Generator::apply(RowMode mode, T shift, const T *x, const T *b, T *y, T *aux,
+                      cudaStream_t stream) const {
+    RowParams<T> p = op.params<T>();
+    p.shift = shift;
+    p.x = x;
+    p.b = b;
+    p.y = y;
+    p.aux = aux;
+    op.run<T>(mode, p, stream);
+}
+
+template void Generator::apply<double>(RowMode, double, const double *, const double *, double *,
+                                       double *, cudaStream_t) const;
+template void Generator::apply<float>(RowMode, float, const float *, const float *, float *,
+                                      float *, cudaStream_t) const;
+
+// ---------------------------------------------------------------------------------------
+// multigrid
+
+namespace {
+
+template <typename T>
+__global__ void axpy_t_kernel(T a, const T *x, T *y, std::int64_t n) {
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        y[i] += a * x[i];
+    }
+}
+
+template <typename T>
+void axpy_t(T a, const T *x, T *y, std::int64_t n, cudaStream_t stream) {
+    if (n == 0) {
+        return;
+    }
+    const std::int64_t want = (n + 255) / 256;
+    const auto blocks = static_cast<unsigned>(std::min<std::int64_t>(want, 148 * 8));
+    axpy_t_kernel<T><<<blocks, 256, 0, stream>>>(a, x, y, n);
+    check_cuda(cudaGetLastError(), "axpy");
+}
+
+// dense inverse by Gauss-Jordan with partial pivoting; false when singular
+bool invert_dense(std::vector<double> &A, int n, std::vector<double> &inv) {
+    inv.assign(static_cast<std::size_t>(n) * n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        inv[static_cast<std::size_t>(i) * n + i] = 1.0;
+    }
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        for (int i = k + 1; i < n; ++i) {
+            if (std::abs(A[static_cast<std::size_t>(i) * n + k]) >
+                std::abs(A[static_cast<std::size_t>(p) * n + k])) {
+                p = i;
+            }
+        }
+        if (A[static_cast<std::size_t>(p) * n + k] == 0.0) {
+            return false;
+        }
+        if (p != k) {
+            for (int j = 0; j < n; ++j) {
+                std::swap(A[static_cast<std::size_t>(k) * n + j], A[static_cast<std::size_t>(p) * n + j]);
+                std::swap(inv[static_cast<std::size_t>(k) * n + j],
+                          inv[static_cast<std::size_t>(p) * n + j]);
+            }
+        }
+        const double d = A[static_cast<std::size_t>(k) * n + k];
+        for (int j = 0; j < n; ++j) {
+            A[static_cast<std::size_t>(k) * n + j] /= d;
+            inv[static_cast<std::size_t>(k) * n + j] /= d;
+        }
+        for (int i = 0; i < n; ++i) {
+            if (i == k) {
+                continue;
+            }
+            const double f = A[static_cast<std::size_t>(i) * n + k];
+            if (f == 0.0) {
+                continue;
+            }
+            for (int j = 0; j < n; ++j) {
+                A[static_cast<std::size_t>(i) * n + j] -= f * A[static_cast<std::size_t>(k) * n + j];
+                inv[static_cast<std::size_t>(i) * n + j] -= f * inv[static_cast<std::size_t>(k) * n + j];
+            }
+        }
+    }
+    return true;
+}
+
+template <int MAXM>
+void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vector<double> &A) {
+    const SectorDesc &sec = op.sectors[slot];
+    const auto n = static_cast<int>(sec.size);
+    A.assign(static_cast<std::size_t>(n) * n, 0.0);
+    const BinomTable B = op.binom->host_view();
+    for (int i = 0; i < n; ++i) {
+        RowState<MAXM> st;
+        load_state<MAXM>(B, sec, op.S, op.V, i, st);
+        double exit = 0.0, leak = 0.0;
+        visit_row<double, MAXM>(B, op.sectors.data(), sec, op.t64.host, i, st, true, 0, 1, exit,
+                                leak, [&](std::int64_t j, double a) {
+                                    A[static_cast<std::size_t>(i) * n + (j - sec.begin)] -= a;
+                                });
+        A[static_cast<std::size_t>(i) * n + i] += shift + exit;
+    }
+}
+
+} // namespace
+
+Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
+                     const MultigridOptions &o)
+    : opt(o), shift(shift_), n(space.n), binom(space.binom) {
+    if (!(shift > 0.0)) {
+        throw Error(kEInval, "population_multigrid: shift must be positive");
+    }
+    model.validate();
+    if (!model.has_grid) {
+        throw Error(kEInval, "sector_multigrid needs a structured grid");
+    }
+    if (model.V != space.V || model.S != space.S) {
+        throw Error(kEInval, "model and space disagree on voxels or species");
+    }
+    if (opt.smoother < 0 || opt.smoother > 1 || opt.precision < 0 || opt.precision > 1) {
+        throw Error(kEInval, "unknown smoother or precision");
+    }
+    const int S = space.S;
+    std::vector<double> h_lgf(space.max_total + 2);
+    for (std::size_t k = 0; k < h_lgf.size(); ++k) {
+        h_lgf[k] = std::lgamma(static_cast<double>(k) + 1.0);
+    }
+    lgf.upload(h_lgf);
+
+    // depth 0: every sector of the space, on the model's own grid
+    std::vector<std::vector<int>> totals;
+    std::vector<int> box_of;
+    for (std::size_t k = 0; k < space.sectors.size(); ++k) {
+        totals.emplace_back(space.sectors[k].total, space.sectors[k].total + S);
+        box_of.push_back(static_cast<int>(k));
+    }
+    std::int64_t dims[3] = {model.dims[0], model.dims[1], model.dims[2]};
+    double spacing[3] = {model.spacing[0], model.spacing[1], model.spacing[2]};
+    double scale = 1.0;
+    for (int d = 0; !totals.empty(); ++d) {
+        auto L = std::make_unique<Level>();
+        auto grid_model = Model::grid(model.dim, dims, spacing, model.diff);
+        L->op.V = grid_model->V;
+        L->op.S = S;
+        L->op.binom = binom;
+        L->op.sectors = layout_sectors(grid_model->V, S, totals, *binom, &L->op.n);
+        L->op.t64.build(*grid_model, scale, false, true);
+        L->op.t32.build(*grid_model, scale, false, true);
+        L->pre = opt.pre_sweeps + d * opt.sweep_growth;
+        L->post = opt.post_sweeps + d * opt.sweep_growth;
+        L->box_sector = box_of;
+
+        // coarsen (markovkit/rdme/multigrid.hpp:25-42)
+        bool can_coarsen = false, odd = false;
+        std::int64_t cdims[3] = {dims[0], dims[1], dims[2]};
+        double cspacing[3] = {spacing[0], spacing[1], spacing[2]};
+        for (int a = 0; a < model.dim; ++a) {
+            if (dims[a] == 1) {
+                continue;
+            }
+            if (dims[a] % 2 != 0) {
+                odd = true;
+                break;
+            }
+            cdims[a] /= 2;
+            cspacing[a] *= 2.0;
+            can_coarsen = true;
+        }
+        can_coarsen = can_coarsen && !odd;
+        const int levels_left = opt.max_levels - d;
+
+        std::vector<std::vector<int>> next_totals;
+        std::vector<int> next_box;
+        for (std::size_t k = 0; k < totals.size(); ++k) {
+            SectorDesc &sec = L->op.sectors[k];
+            const bool terminal =
+                sec.size <= opt.coarsest_size || levels_left <= 1 || !can_coarsen;
+            if (terminal) {
+                sec.terminal = static_cast<int>(L->h_term.size());
+                TerminalBlock tb;
+                tb.begin = sec.begin;
+                tb.n = static_cast<int>(sec.size);
+                if (sec.size > 8192) {
+                    throw Error(kEInval, "terminal multigrid block larger than 8192 states");
+                }
+                L->h_term.push_back(tb);
+            } else {
+                sec.coarse = static_cast<int>(next_totals.size());
+                next_totals.push_back(totals[k]);
+                next_box.push_back(box_of[k]);
+            }
+        }
+        L->op.finalize(*grid_model, false, false, {});
+
+        // dense inverses of the terminal blocks, from the same matrix-free rows
+        std::vector<double> inv_all, A, inv;
+        for (std::size_t k = 0; k < L->op.sectors.size(); ++k) {
+            const SectorDesc &sec = L->op.sectors[k];
+            if (sec.terminal < 0) {
+                continue;
+            }
+            switch (L->op.mol_cap) {
+            case 4:
+                assemble_terminal<4>(L->op, static_cast<int>(k), shift, A);
+                break;
+            case 16:
+                assemble_terminal<16>(L->op, static_cast<int>(k), shift, A);
+                break;
+            default:
+                assemble_terminal<64>(L->op, static_cast<int>(k), shift, A);
+                break;
+            }
+            if (!invert_dense(A, static_cast<int>(sec.size), inv)) {
+                throw Error(kESingular, "population_multigrid: singular block");
+            }
+            L->h_term[sec.terminal].inv_offset = static_cast<std::int64_t>(inv_all.size());
+            inv_all.insert(inv_all.end(), inv.begin(), inv.end());
+        }
+        L->d_term.upload(L->h_term);
+        L->inv64.upload(inv_all);
+        std::vector<float> inv_f(inv_all.begin(), inv_all.end());
+        L->inv32.upload(inv_f);
+
+        if (!next_totals.empty()) {
+            // parent voxel of every fine voxel (multigrid.hpp:56-65)
+            auto coarse_model = Model::grid(model.dim, cdims, cspacing, model.diff);
+            std::vector<int> parent(grid_model->V);
+            std::vector<int> children(coarse_model->V, 0);
+            for (int v = 0; v < grid_model->V; ++v) {
+                std::int64_t rem = v, cv = 0, cstride = 1;
+                for (int a = 0; a < model.dim; ++a) {
+                    std::int64_t c = rem % dims[a];
+                    rem /= dims[a];
+                    if (dims[a] > 1) {
+                        c /= 2;
+                    }
+                    cv += c * cstride;
+                    cstride *= cdims[a];
+                }
+                parent[v] = static_cast<int>(cv);
+                ++children[cv];
+            }
+            std::vector<double> log_children(coarse_model->V);
+            for (int a = 0; a < coarse_model->V; ++a) {
+                log_children[a] = std::log(static_cast<double>(children[a]));
+            }
+            L->parent.upload(parent);
+            L->log_children.upload(log_children);
+        }
+        levels.push_back(std::move(L));
+        totals = next_totals;
+        box_of = next_box;
+        for (int a = 0; a < 3; ++a) {
+            dims[a] = cdims[a];
+            spacing[a] = cspacing[a];
+        }
+        scale *= 2.0;
+    }
+    max_depth = static_cast<int>(levels.size());
+
+    // work vectors in the preconditioner's precision
+    for (std::size_t d = 0; d < levels.size(); ++d) {
+        Level &L = *levels[d];
+        const std::size_t nd = static_cast<std::size_t>(L.op.n);
+        const std::size_t nc = d + 1 < levels.size() ? static_cast<std::size_t>(levels[d + 1]->op.n) : 0;
+        if (opt.precision == 0) {
+            L.rhs64.resize(nd);
+            L.x64.resize(nd);
+            L.tmp64.resize(nd);
+            L.r64.resize(nd);
+            if (opt.coarse_cycles > 1 && nc) {
+                L.acc64.resize(nc);
+                L.crhs64.resize(nc);
+            }
+        } else {
+            L.rhs32.resize(nd);
+            L.x32.resize(nd);
+            L.tmp32.resize(nd);
+            L.r32.resize(nd);
+            if (opt.coarse_cycles > 1 && nc) {
+                L.acc32.resize(nc);
+                L.crhs32.resize(nc);
+            }
+        }
+    }
+}
+
+int Multigrid::levels_of_sector(int k) const {
+    int count = 0;
+    for (const auto &L : levels) {
+        if (std::find(L->box_sector.begin(), L->box_sector.end(), k) != L->box_sector.end()) {
+            ++count;
+        }
+    }
+    return count;
+}
+
+template <typename T>
+T *Multigrid::buf(Level &L, int which) {
+    if constexpr (std::is_same_v<T, double>) {
+        switch (which) {
+        case 0:
+            return L.rhs64.get();
+        case 1:
+            return L.x64.get();
+        case 2:
+            return L.tmp64.get();
+        case 3:
+            return L.r64.get();
+        case 4:
+            return L.acc64.get();
+        default:
+            return L.crhs64.get();
+        }
+    } else {
+        switch (which) {
+        case 0:
+            return L.rhs32.get();
+        case 1:
+            return L.x32.get();
+        case 2:
+            return L.tmp32.get();
+        case 3:
+            return L.r32.get();
+        case 4:
+            return L.acc32.get();
+        default:
+            return L.crhs32.get();
+        }
+    }
+}
+
+// one cycle of every sector at depth d from a zero initial guess
+// (markovkit/rdme/multigrid.hpp:201-228); returns the buffer holding x
+template <typename T>
+T *Multigrid::cycle(int d, cudaStream_t stream) {
+    Level &L = *levels[d];
+    const T *rhs = buf<T>(L, 0);
+    T *x = buf<T>(L, 1);
+    T *tmp = buf<T>(L, 2);
+    T *r = buf<T>(L, 3);
+    const std::int64_t nd = L.op.n;
+    RowParams<T> p = L.op.params<T>();
+    p.shift = static_cast<T>(shift);
+    p.omega = static_cast<T>(opt.jacobi_weight);
+
+    if (opt.smoother == 0) {
+        if (L.pre > 0) {
+            p.b = rhs;
+            p.y = x;
+            L.op.run<T>(kJacobiZero, p, stream);
+            for (int k = 1; k < L.pre; ++k) {
+                p.x = x;
+                p.b = rhs;
+                p.y = tmp;
+                L.op.run<T>(kJacobi, p, stream);
+                std::swap(x, tmp);
+            }
+        } else {
+            check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
+        }
+    } else {
+        check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
+        for (int k = 0; k < L.pre; ++k) {
+            for (int c = 0; c < 2; ++c) {
+                p.b = rhs;
+                p.y = x;
+                p.colour = c;
+                L.op.run<T>(kGaussSeidel, p, stream);
+            }
+        }
+    }
+
+    Level *C = d + 1 < max_depth ? levels[d + 1].get() : nullptr;
+    if (C) {
+        check_cuda(cudaMemsetAsync(buf<T>(*C, 0), 0, C->op.n * sizeof(T), stream), "memset");
+        p.tv.Vc = C->op.V;
+        p.tv.parent = L.parent.get();
+        p.tv.log_children = L.log_children.get();
+        p.tv.lgf = lgf.get();
+        p.tv.coarse_sectors = C->op.d_sectors.get();
+        p.coarse = buf<T>(*C, 0);
+    }
+    p.x = x;
+    p.b = rhs;
+    p.aux = r;
+    L.op.run<T>(kResidualRestrict, p, stream);
+    if (!L.h_term.empty()) {
+        const T *inv;
+        if constexpr (std::is_same_v<T, double>) {
+            inv = L.inv64.get();
+        } else {
+            inv = L.inv32.get();
+        }
+        check_cuda(launch_terminal<T>(L.d_term.get(), static_cast<int>(L.h_term.size()), inv, r,
+                                      x, stream),
+                   "terminal solve");
+    }
+    if (C) {
+        T *cx = nullptr;
+        if (opt.coarse_cycles <= 1) {
+            cx = cycle<T>(d + 1, stream);
+        } else {
+            T *acc = buf<T>(L, 4), *crhs = buf<T>(L, 5);
+            const std::size_t bytes = C->op.n * sizeof(T);
+            check_cuda(cudaMemcpyAsync(crhs, buf<T>(*C, 0), bytes, cudaMemcpyDeviceToDevice, stream),
+                       "copy");
+            T *e = cycle<T>(d + 1, stream);
+            check_cuda(cudaMemcpyAsync(acc, e, bytes, cudaMemcpyDeviceToDevice, stream), "copy");
+            for (int c = 1; c < opt.coarse_cycles; ++c) {
+                RowParams<T> pc = C->op.params<T>();
+                pc.shift = static_cast<T>(shift);
+                pc.x = acc;
+                pc.b = crhs;
+                pc.y = buf<T>(*C, 0);
+                C->op.run<T>(kResidual, pc, stream);
+                e = cycle<T>(d + 1, stream);
+                axpy_t<T>(T(1), e, acc, C->op.n, stream);
+            }
+            cx = acc;
+        }
+        p.coarse = cx;
+        p.y = x;
+        L.op.run<T>(kProlongAdd, p, stream);
+    }
+
+    if (opt.smoother == 0) {
+        for (int k = 0; k < L.post; ++k) {
+            p.x = x;
+            p.b = rhs;
+            p.y = tmp;
+            L.op.run<T>(kJacobi, p, stream);
+            std::swap(x, tmp);
+        }
+    } else {
+        for (int k = 0; k < L.post; ++k) {
+            for (int c = 1; c >= 0; --c) {
+                p.b = rhs;
+                p.y = x;
+                p.colour = c;
+                L.op.run<T>(kGaussSeidel, p, stream);
+            }
+        }
+    }
+    // keep the result in x's own buffer so the caller's view of the level stays fixed
+    if (x != buf<T>(L, 1)) {
+        check_cuda(cudaMemcpyAsync(buf<T>(L, 1), x, nd * sizeof(T), cudaMemcpyDeviceToDevice,
+                                   stream),
+                   "copy");
+    }
+    return buf<T>(L, 1);
+}
+
+void Multigrid::transfer(int d, int direction, const double *in, double *out,
+                         cudaStream_t stream) {
+    if (d < 0 || d + 1 >= max_depth) {
+        throw Error(kEInval, "no coarser level below this depth");
+    }
+    Level &L = *levels[d];
+    Level &C = *levels[d + 1];
+    RowParams<double> p = L.op.params<double>();
+    p.tv.Vc = C.op.V;
+    p.tv.parent = L.parent.get();
+    p.tv.log_children = L.log_children.get();
+    p.tv.lgf = lgf.get();
+    p.tv.coarse_sectors = C.op.d_sectors.get();
+    if (direction == 0) {
+        check_cuda(cudaMemsetAsync(out, 0, C.op.n * sizeof(double), stream), "memset");
+        p.x = in;
+        p.coarse = out;
+        L.op.run<double>(kRestrict, p, stream);
+    } else {
+        p.coarse = const_cast<double *>(in);
+        p.y = out;
+        L.op.run<double>(kProlong, p, stream);
+    }
+}
+
+void Multigrid::apply_system(int d, const double *x, double *y, cudaStream_t stream) {
+    if (d < 0 || d >= max_depth) {
+        throw Error(kEInval, "no such multigrid level");
+    }
+    Level &L = *levels[d];
+    RowParams<double> p = L.op.params<double>();
+    p.shift = shift;
+    p.x = x;
+    p.y = y;
+    L.op.run<double>(kApplyShifted, p, stream);
+}
+
+void Multigrid::apply(const double *b, double *x, cudaStream_t stream) {
+    Level &L0 = *levels[0];
+    const std::size_t n0 = static_cast<std::size_t>(L0.op.n);
+    if (opt.precision == 0) {
+        check_cuda(cudaMemcpyAsync(L0.rhs64.get(), b, n0 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   stream),
+                   "copy");
+        double *out = cycle<double>(0, stream);
+        check_cuda(cudaMemcpyAsync(x, out, n0 * sizeof(double), cudaMemcpyDeviceToDevice, stream),
+                   "copy");
+    } else {
+        check_cuda(convert<double, float>(b, L0.rhs32.get(), static_cast<std::int64_t>(n0), stream),
+                   "convert");
+        float *out = cycle<float>(0, stream);
+        check_cuda(convert<float, double>(out, x, static_cast<std::int64_t>(n0), stream), "convert");
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// (F)GMRES
+
+Krylov::Krylov(std::int64_t n_, int m_, bool flexible_) : n(n_), m(m_), flexible(flexible_) {
+    if (m < 1) {
+        throw Error(kEInval, "restart must be positive");
+    }
+    ld = (n + 31) / 32 * 32;
+    V.resize(static_cast<std::size_t>(ld) * (m + 1));
+    if (flexible) {
+        Z.resize(static_cast<std::size_t>(ld) * m);
+    }
+    w.resize(ld);
+    r.resize(ld);
+    t.resize(ld);
+    partials.resize(static_cast<std::size_t>(kDotBlocks) * kMaxFusedBasis);
+    const std::size_t H = static_cast<std::size_t>(m + 1) * m;
+    small.resize(H + 6 * (m + 1) + 16);
+    double *p = small.get();
+    st.m = m;
+    st.H = p;
+    p += H;
+    st.cs = p;
+    p += m + 1;
+    st.sn = p;
+    p += m + 1;
+    st.g = p;
+    p += m + 1;
+    st.y = p;
+    p += m + 1;
+    st.h1 = p;
+    p += m + 1;
+    st.h2 = p;
+    p += m + 1;
+    st.hn = p++;
+    st.inv_hn = p++;
+    st.beta = p++;
+    st.report = p;
+    check_cuda(cudaMallocHost(reinterpret_cast<void **>(&report_host), 4 * sizeof(double)),
+               "cudaMallocHost");
+}
+
+Krylov::~Krylov() {
+    if (report_host) {
+        cudaFreeHost(report_host);
+    }
+}
+
+namespace {
+
+// out[k] = <V_k, w> for k < K, any K
+void gs_dots(const Krylov &ws, int K, double *w, double *out, cudaStream_t stream) {
+    for (int c0 = 0; c0 < K; c0 += kMaxFusedBasis) {
+        const int kc = std::min(kMaxFusedBasis, K - c0);
+        check_cuda(cgs_pass(0, ws.V.get() + c0 * ws.ld, ws.ld, kc, w, ws.n, nullptr,
+                            ws.partials.get(), out + c0, stream),
+                   "cgs");
+    }
+}
+
+// w -= V coef; then out = V^T w (mode 1) or out[0] = <w, w> (mode 2)
+void gs_update(const Krylov &ws, int mode, int K, double *w, const double *coef, double *out,
+               cudaStream_t stream) {
+    if (K <= kMaxFusedBasis) {
+        check_cuda(cgs_pass(mode, ws.V.get(), ws.ld, K, w, ws.n, coef, ws.partials.get(), out,
+                            stream),
+                   "cgs");
+        return;
+    }
+    for (int c0 = 0; c0 < K; c0 += kMaxFusedBasis) {
+        const int kc = std::min(kMaxFusedBasis, K - c0);
+        check_cuda(cgs_pass(3, ws.V.get() + c0 * ws.ld, ws.ld, kc, w, ws.n, coef + c0,
+                            ws.partials.get(), nullptr, stream),
+                   "cgs");
+    }
+    if (mode == 1) {
+        gs_dots(ws, K, w, out, stream);
+    } else {
+        check_cuda(dot(w, w, ws.n, ws.partials.get(), out, stream), "dot");
+    }
+}
+
+void read_report(const Krylov &ws, cudaStream_t stream) {
+    check_cuda(cudaMemcpyAsync(ws.report_host, ws.st.report, 4 * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream),
+               "report");
+    check_cuda(cudaStreamSynchronize(stream), "sync");
+}
+
+} // namespace
+
+SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double *b, double *x,
+                   const GmresOptions &opt, Krylov &ws, cudaStream_t stream) {
+    SolverResult res;
+    const std::int64_t n = A.op.n;
+    if (ws.n != n) {
+        throw Error(kEInval, "workspace size does not match the system");
+    }
+    if (M && M->n != n) {
+        throw Error(kEInval, "preconditioner size does not match the system");
+    }
+    const bool flexible = opt.flexible || (M && M->opt.precision != 0);
+    if (flexible && !ws.flexible) {
+        throw Error(kEInval, "flexible GMRES needs a flexible workspace");
+    }
+    const int m = std::min(ws.m, std::max(1, opt.restart));
+    const double tol = opt.tolerance;
+
+    auto true_residual = [&]() {
+        A.apply<double>(kResidual, shift, x, b, ws.r.get(), nullptr, stream);
+        check_cuda(dot(ws.r.get(), ws.r.get(), n, ws.partials.get(), ws.st.beta, stream), "dot");
+        check_cuda(arnoldi_start(ws.st, stream), "arnoldi");
+        read_report(ws, stream);
+        return ws.report_host[0];
+    };
+
+    double beta = true_residual();
+    res.residual = beta;
+    if (!std::isfinite(beta)) {
+        res.status = kENan;
+        return res;
+    }
+    if (beta <= tol) {
+        res.converged = 1;
+        return res;
+    }
+    while (res.iterations < opt.max_iterations) {
+        check_cuda(scale_copy(ws.r.get(), ws.st.beta, ws.V.get(), n, stream), "scale");
+        int k = 0;
+        bool nan = false;
+        for (int j = 0; j < m && res.iterations < opt.max_iterations; ++j) {
+            double *vj = ws.V.get() + j * ws.ld;
+            double *z = vj;
+            if (M) {
+                z = flexible ? ws.Z.get() + j * ws.ld : ws.t.get();
+                M->apply(vj, z, stream);
+            }
+            A.apply<double>(kApplyShifted, shift, z, nullptr, ws.w.get(), nullptr, stream);
+            const int K = j + 1;
+            gs_dots(ws, K, ws.w.get(), ws.st.h1, stream);
+            gs_update(ws, 1, K, ws.w.get(), ws.st.h1, ws.st.h2, stream);
+            gs_update(ws, 2, K, ws.w.get(), ws.st.h2, ws.st.hn, stream);
+            check_cuda(arnoldi_column(ws.st, j, stream), "arnoldi");
+            ++res.iterations;
+            k = j + 1;
+            read_report(ws, stream);
+            const double est = ws.report_host[0];
+            if (!std::isfinite(est) || !std::isfinite(ws.report_host[1])) {
+                nan = true;
+                break;
+            }
+            if (est <= tol || ws.report_host[2] != 0.0) {
+                break;
+            }
+            if (j + 1 < m) {
+                check_cuda(scale_copy(ws.w.get(), ws.st.inv_hn, ws.V.get() + (j + 1) * ws.ld, n,
+                                      stream),
+                           "scale");
+            }
+        }
+        if (nan) {
+            res.status = kENan;
+            res.residual = std::numeric_limits<double>::quiet_NaN();
+            return res;
+        }
+        check_cuda(arnoldi_solve(ws.st, k, stream), "arnoldi");
+        if (flexible && M) {
+            check_cuda(multi_axpy(ws.Z.get(), ws.ld, k, ws.st.y, x, n, stream), "update");
+        } else if (M) {
+            check_cuda(multi_combine(ws.V.get(), ws.ld, k, ws.st.y, ws.t.get(), n, stream), "update");
+            M->apply(ws.t.get(), ws.w.get(), stream);
+            check_cuda(axpy(1.0, ws.w.get(), x, n, stream), "update");
+        } else {
+            check_cuda(multi_axpy(ws.V.get(), ws.ld, k, ws.st.y, x, n, stream), "update");
+        }
+        beta = true_residual();
+        res.residual = beta;
+        if (!std::isfinite(beta)) {
+            res.status = kENan;
+            return res;
+        }
+        if (beta <= tol) {
+            res.converged = 1;
+            return res;
+        }
+    }
+    res.status = kENotConv;
+    return res;
+}
+
+} // namespace mkb

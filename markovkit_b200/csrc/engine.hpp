@@ -1,0 +1,282 @@
+// Host side of the B200 resolvent engine: population spaces, RDME models, the matrix-free
+// generator, the sector multigrid hierarchy and (flexible) GMRES. Everything here owns device
+// memory and launches the sm_100a kernels of row_kernels.cu and krylov.cu on a caller stream.
+#pragma once
+
+#include "krylov.cuh"
+#include "row_kernels.cuh"
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace mkb {
+
+// status codes, shared with the C ABI (include/markovkit_b200.h)
+enum Status : int {
+    kOk = 0,
+    kEInval = 1,
+    kEOverflow = 2,
+    kESingular = 3,
+    kENoMem = 4,
+    kENotConv = 5,
+    kENan = 6,
+    kETimeout = 7,
+    kECuda = 8,
+};
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &what) : std::runtime_error(what), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char *what);
+
+template <typename T>
+class DeviceArray {
+  public:
+    DeviceArray() = default;
+    explicit DeviceArray(std::size_t n) { resize(n); }
+    ~DeviceArray() { release(); }
+    DeviceArray(const DeviceArray &) = delete;
+    DeviceArray &operator=(const DeviceArray &) = delete;
+    DeviceArray(DeviceArray &&o) noexcept : p_(o.p_), n_(o.n_) {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    DeviceArray &operator=(DeviceArray &&o) noexcept {
+        if (this != &o) {
+            release();
+            p_ = o.p_;
+            n_ = o.n_;
+            o.p_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    void resize(std::size_t n) {
+        release();
+        if (n > 0) {
+            check_cuda(cudaMalloc(reinterpret_cast<void **>(&p_), n * sizeof(T)), "cudaMalloc");
+            n_ = n;
+        }
+    }
+    void upload(const std::vector<T> &h) {
+        resize(h.size());
+        if (!h.empty()) {
+            check_cuda(cudaMemcpy(p_, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice),
+                       "upload");
+        }
+    }
+    [[nodiscard]] T *get() const { return p_; }
+    [[nodiscard]] std::size_t size() const { return n_; }
+
+  private:
+    void release() {
+        if (p_) {
+            cudaFree(p_);
+        }
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T *p_ = nullptr;
+    std::size_t n_ = 0;
+};
+
+// C(q, j), 0 <= j <= jmax, 0 <= q <= qmax, on host and device (saturating at 2^62)
+struct Binomials {
+    int jmax = 0, qmax = 0;
+    std::vector<std::int64_t> host;
+    DeviceArray<std::int64_t> dev;
+    Binomials(int jmax, int qmax);
+    [[nodiscard]] BinomTable host_view() const { return {host.data(), jmax, qmax}; }
+    [[nodiscard]] BinomTable device_view() const { return {dev.get(), jmax, qmax}; }
+};
+constexpr std::int64_t kSaturated = std::int64_t(1) << 62;
+
+// Every sector of a box (0 <= t_s <= max_s, mixed-radix order, species 0 most significant,
+// markovkit/rdme/population_space.hpp:131-196) or a single sector (:105-127).
+struct Space {
+    int V = 0, S = 0;
+    bool is_box = true;
+    std::vector<int> limits; // box: max totals; sector: totals
+    std::vector<SectorDesc> sectors;
+    std::int64_t n = 0;
+    int max_total = 0; // largest total of one species
+    int max_mol = 0;   // largest molecules in one state
+    std::shared_ptr<Binomials> binom;
+    DeviceArray<SectorDesc> d_sectors;
+    DeviceArray<int> d_limits;
+
+    static std::unique_ptr<Space> make(int V, const std::vector<int> &limits, bool is_box);
+    [[nodiscard]] int find_sector(const int *totals) const;
+    [[nodiscard]] std::int64_t rank(const int *state) const; // -1: not in the space
+    void unrank(std::int64_t i, int *state) const;
+    [[nodiscard]] int sector_of(std::int64_t i) const;
+};
+
+// sectors with the given totals on V voxels, numbered contiguously from 0 in list order
+std::vector<SectorDesc> layout_sectors(int V, int S, const std::vector<std::vector<int>> &totals,
+                                       const Binomials &B, std::int64_t *total_size);
+
+// An RDME model: a symmetric voxel graph, volumes, diffusivities and local reactions whose
+// rates are tabulated over count tuples 0..tmax_s (markovkit/rdme/reaction_diffusion.hpp).
+struct Model {
+    int V = 0, S = 0;
+    std::vector<int> nbr_ptr, nbr_idx;
+    std::vector<double> nbr_w, volumes, diff;
+    bool has_grid = false;
+    int dim = 0;
+    std::int64_t dims[3] = {1, 1, 1};
+    double spacing[3] = {1.0, 1.0, 1.0};
+    int R = 0;
+    std::vector<int> change; // R x S
+    std::vector<int> tmax;   // S
+    int nvc = 1;
+    std::vector<int> vclass; // V (empty: one class)
+    std::vector<double> rates; // R x nvc x ntuple
+
+    [[nodiscard]] int ntuple() const;
+    static std::unique_ptr<Model> grid(int dim, const std::int64_t *dims, const double *spacing,
+                                       const std::vector<double> &diff);
+    void validate() const;
+};
+
+// host + device tables of one voxel graph and model in one precision
+template <typename T>
+struct ModelTables {
+    std::vector<int> h_nbr_ptr, h_nbr_idx, h_vclass;
+    std::vector<T> h_in_coef, h_deg_coef, h_rate;
+    std::vector<unsigned char> h_vparity;
+    DeviceArray<int> nbr_ptr, nbr_idx, vclass;
+    DeviceArray<T> in_coef, deg_coef, rate;
+    DeviceArray<unsigned char> vparity;
+    ModelView<T> host, dev;
+    void build(const Model &m, double diff_scale, bool with_reactions, bool absorbing);
+};
+
+// A level space with one model: the unit the row kernels run over.
+struct OperatorLevel {
+    int V = 0, S = 0;
+    std::int64_t n = 0;
+    int mol_cap = 4;
+    std::vector<SectorDesc> sectors;
+    DeviceArray<SectorDesc> d_sectors;
+    std::vector<Tile> tiles;
+    DeviceArray<Tile> d_tiles;
+    ModelTables<double> t64;
+    ModelTables<float> t32;
+    std::shared_ptr<Binomials> binom;
+
+    // sector couplings (src/dst/heavy) for the model's reactions, then tiles and uploads
+    void finalize(const Model &m, bool with_reactions, bool is_box_like,
+                  const std::vector<int> &box_limits);
+    template <typename T>
+    [[nodiscard]] RowParams<T> params() const;
+    template <typename T>
+    void run(RowMode mode, const RowParams<T> &p, cudaStream_t stream) const;
+};
+
+struct Generator {
+    const Space *space = nullptr;
+    OperatorLevel op;
+    bool absorbing = true;
+    std::int64_t n_jumps_cache = -1;
+    Generator(const Space &space, const Model &model, bool absorbing);
+    template <typename T>
+    void apply(RowMode mode, T shift, const T *x, const T *b, T *y, T *aux,
+               cudaStream_t stream) const;
+};
+
+struct MultigridOptions {
+    int pre_sweeps = 2;
+    int post_sweeps = 2;
+    double jacobi_weight = 2.0 / 3.0;
+    std::int64_t coarsest_size = 4;
+    int max_levels = 32;
+    int coarse_cycles = 1;
+    int sweep_growth = 0;
+    int smoother = 0;  // 0 weighted Jacobi (the reference's default), 1 red-black Gauss-Seidel
+    int precision = 0; // 0 FP64, 1 FP32 preconditioner
+};
+
+// sector_multigrid (markovkit/rdme/multigrid.hpp:136-408): one geometric V-cycle per
+// population sector on the diffusion-only operator, all sectors of a depth in one launch.
+struct Multigrid {
+    struct Level {
+        OperatorLevel op;
+        int pre = 2, post = 2;
+        // transfer to the next level
+        DeviceArray<int> parent;
+        DeviceArray<double> log_children;
+        // dense terminal blocks of sectors that stop here
+        std::vector<TerminalBlock> h_term;
+        DeviceArray<TerminalBlock> d_term;
+        DeviceArray<double> inv64;
+        DeviceArray<float> inv32;
+        // work vectors (precision of the preconditioner)
+        DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
+        DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
+        std::vector<int> box_sector; // box sector of each slot
+    };
+    MultigridOptions opt;
+    double shift = 0.0;
+    std::int64_t n = 0;
+    int max_depth = 0;
+    std::vector<std::unique_ptr<Level>> levels;
+    DeviceArray<double> lgf;
+    std::shared_ptr<Binomials> binom;
+
+    Multigrid(const Space &space, const Model &model, double shift, const MultigridOptions &opt);
+    // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
+    void apply(const double *b, double *x, cudaStream_t stream);
+    [[nodiscard]] int n_levels() const { return static_cast<int>(levels.size()); }
+    [[nodiscard]] int levels_of_sector(int k) const;
+    // FP64 hooks on one depth: population_transfer restrict (direction 0) or prolong (1)
+    // between depth d and d + 1, and y = (shift I - Q_d) x on depth d
+    void transfer(int d, int direction, const double *in, double *out, cudaStream_t stream);
+    void apply_system(int d, const double *x, double *y, cudaStream_t stream);
+
+  private:
+    template <typename T>
+    T *cycle(int d, cudaStream_t stream);
+    template <typename T>
+    T *buf(Level &L, int which);
+};
+
+struct GmresOptions {
+    double tolerance = 1e-8; // absolute, on the Euclidean residual norm
+    std::int64_t max_iterations = 1000;
+    int restart = 30;
+    int flexible = 0; // keep Z_j = M v_j (required for the FP32 preconditioner)
+};
+
+struct SolverResult {
+    std::int64_t iterations = 0;
+    double residual = 0.0;
+    int converged = 0;
+    int status = kOk;
+};
+
+// workspace of restarted (F)GMRES for one system size
+struct Krylov {
+    std::int64_t n = 0, ld = 0;
+    int m = 0;
+    bool flexible = false;
+    DeviceArray<double> V, Z, w, r, t, partials, small;
+    ArnoldiState st;
+    double *report_host = nullptr; // pinned
+    Krylov(std::int64_t n, int m, bool flexible);
+    ~Krylov();
+    Krylov(const Krylov &) = delete;
+    Krylov &operator=(const Krylov &) = delete;
+};
+
+// right-preconditioned restarted GMRES (Saad Alg. 9.5) or FGMRES (Alg. 9.6) on
+// A = shift I - Q with classical Gram-Schmidt and one re-orthogonalisation
+SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double *b, double *x,
+                   const GmresOptions &opt, Krylov &ws, cudaStream_t stream);
+
+} // namespace mkb

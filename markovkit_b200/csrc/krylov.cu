@@ -1,0 +1,295 @@
+// sm_100a Krylov kernels. All are HBM-bound streaming passes over the Arnoldi basis.
+#include "krylov.cuh"
+
+#include <cmath>
+
+namespace mkb {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+    }
+    return v;
+}
+
+// reduce KMAX per-thread accumulators over the block; write partials[k * gridDim.x + block]
+template <int KMAX>
+__device__ __forceinline__ void block_partials(double (&acc)[KMAX], int K, double *partials) {
+    __shared__ double red[kDotThreads / 32][KMAX];
+    const int warp = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        if (k < K) {
+            const double v = warp_sum(acc[k]);
+            if (lane == 0) {
+                red[warp][k] = v;
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = static_cast<int>(threadIdx.x); k < K; k += blockDim.x) {
+        double s = 0.0;
+        for (int wi = 0; wi < kDotThreads / 32; ++wi) {
+            s += red[wi][k];
+        }
+        partials[static_cast<std::int64_t>(k) * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// mode 0: dots; mode 1: update then dots; mode 2: update then norm^2
+template <int KMAX, int MODE>
+__global__ void __launch_bounds__(kDotThreads)
+    cgs_kernel(const double *__restrict__ V, std::int64_t ld, int K, double *__restrict__ w,
+               std::int64_t n, const double *__restrict__ coef, double *__restrict__ partials) {
+    double c[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        c[k] = (MODE != 0 && k < K) ? coef[k] : 0.0;
+    }
+    double acc[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+        acc[k] = 0.0;
+    }
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        double v[KMAX];
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            v[k] = k < K ? __ldcs(V + k * ld + i) : 0.0;
+        }
+        double wi = w[i];
+        if constexpr (MODE != 0) {
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {
+                wi -= c[k] * v[k];
+            }
+            w[i] = wi;
+        }
+        if constexpr (MODE == 2) {
+            acc[0] += wi * wi;
+        } else if constexpr (MODE == 0 || MODE == 1) {
+#pragma unroll
+            for (int k = 0; k < KMAX; ++k) {
+                acc[k] += v[k] * wi;
+            }
+        }
+    }
+    if constexpr (MODE != 3) {
+        block_partials<KMAX>(acc, MODE == 2 ? 1 : K, partials);
+    }
+}
+
+// out[k] = sum_b partials[k * nb + b], one warp per k, fixed order
+__global__ void finalize_kernel(const double *partials, int nb, int K, double *out) {
+    const int warp = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    for (int k = warp; k < K; k += blockDim.x >> 5) {
+        double s = 0.0;
+        for (int b = lane; b < nb; b += 32) {
+            s += partials[static_cast<std::int64_t>(k) * nb + b];
+        }
+        s = warp_sum(s);
+        if (lane == 0) {
+            out[k] = s;
+        }
+    }
+}
+
+template <int KMAX, int MODE>
+cudaError_t launch_cgs(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
+                       const double *coef, double *partials, double *out, cudaStream_t stream) {
+    cgs_kernel<KMAX, MODE><<<kDotBlocks, kDotThreads, 0, stream>>>(V, ld, K, w, n, coef, partials);
+    if (MODE != 3) {
+        finalize_kernel<<<1, 1024, 0, stream>>>(partials, kDotBlocks, MODE == 2 ? 1 : K, out);
+    }
+    return cudaGetLastError();
+}
+
+template <int MODE>
+cudaError_t launch_cgs_k(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
+                         const double *coef, double *partials, double *out, cudaStream_t stream) {
+    if (K <= 4) {
+        return launch_cgs<4, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+    }
+    if (K <= 8) {
+        return launch_cgs<8, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+    }
+    if (K <= 16) {
+        return launch_cgs<16, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+    }
+    return launch_cgs<32, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+}
+
+__global__ void scale_copy_kernel(const double *x, const double *scale, double *y, std::int64_t n) {
+    const double a = *scale;
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        y[i] = x[i] * a;
+    }
+}
+
+template <bool ACCUMULATE>
+__global__ void multi_axpy_kernel(const double *V, std::int64_t ld, int K, const double *coef,
+                                  double *y, std::int64_t n) {
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        double s = ACCUMULATE ? y[i] : 0.0;
+        for (int k = 0; k < K; ++k) {
+            s += coef[k] * V[k * ld + i];
+        }
+        y[i] = s;
+    }
+}
+
+__global__ void axpy_kernel(double a, const double *x, double *y, std::int64_t n) {
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        y[i] += a * x[i];
+    }
+}
+
+template <typename A, typename B>
+__global__ void convert_kernel(const A *x, B *y, std::int64_t n) {
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        y[i] = static_cast<B>(x[i]);
+    }
+}
+
+unsigned stream_blocks(std::int64_t n) {
+    const std::int64_t want = (n + 255) / 256;
+    return static_cast<unsigned>(want < 148 * 8 ? (want > 0 ? want : 1) : 148 * 8);
+}
+
+__global__ void arnoldi_start_kernel(ArnoldiState s) {
+    const double norm = sqrt(*s.beta);
+    for (int i = 0; i <= s.m; ++i) {
+        s.g[i] = 0.0;
+    }
+    s.g[0] = norm;
+    *s.beta = norm > 0.0 ? 1.0 / norm : 0.0;
+    s.report[0] = norm;
+    s.report[1] = norm;
+    s.report[2] = 0.0;
+}
+
+__global__ void arnoldi_column_kernel(ArnoldiState s, int j) {
+    const int ld = s.m + 1;
+    double *col = s.H + static_cast<std::int64_t>(j) * ld;
+    for (int i = 0; i <= j; ++i) {
+        col[i] = s.h1[i] + s.h2[i];
+    }
+    const double hn = sqrt(*s.hn);
+    col[j + 1] = hn;
+    for (int i = 0; i < j; ++i) {
+        const double a = col[i], c = col[i + 1];
+        col[i] = s.cs[i] * a + s.sn[i] * c;
+        col[i + 1] = -s.sn[i] * a + s.cs[i] * c;
+    }
+    const double a = col[j], c = col[j + 1];
+    const double denom = hypot(a, c);
+    s.cs[j] = denom > 0.0 ? a / denom : 1.0;
+    s.sn[j] = denom > 0.0 ? c / denom : 0.0;
+    col[j] = denom;
+    col[j + 1] = 0.0;
+    s.g[j + 1] = -s.sn[j] * s.g[j];
+    s.g[j] = s.cs[j] * s.g[j];
+    *s.inv_hn = hn > 0.0 ? 1.0 / hn : 0.0;
+    s.report[0] = fabs(s.g[j + 1]);
+    s.report[1] = hn;
+    s.report[2] = (hn > 0.0 && isfinite(hn)) ? 0.0 : 1.0;
+}
+
+__global__ void arnoldi_solve_kernel(ArnoldiState s, int k) {
+    const int ld = s.m + 1;
+    for (int i = k - 1; i >= 0; --i) {
+        double v = s.g[i];
+        for (int t = i + 1; t < k; ++t) {
+            v -= s.H[static_cast<std::int64_t>(t) * ld + i] * s.y[t];
+        }
+        s.y[i] = v / s.H[static_cast<std::int64_t>(i) * ld + i];
+    }
+}
+
+} // namespace
+
+cudaError_t cgs_pass(int mode, const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
+                     const double *coef, double *partials, double *out, cudaStream_t stream) {
+    if (K < 1 || K > kMaxFusedBasis) {
+        return cudaErrorInvalidValue;
+    }
+    switch (mode) {
+    case 0:
+        return launch_cgs_k<0>(V, ld, K, w, n, coef, partials, out, stream);
+    case 1:
+        return launch_cgs_k<1>(V, ld, K, w, n, coef, partials, out, stream);
+    case 2:
+        return launch_cgs_k<2>(V, ld, K, w, n, coef, partials, out, stream);
+    case 3:
+        return launch_cgs_k<3>(V, ld, K, w, n, coef, partials, out, stream);
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t dot(const double *a, const double *b, std::int64_t n, double *partials, double *out,
+                cudaStream_t stream) {
+    // <a, b> as a one-vector "basis" pass
+    return launch_cgs<4, 0>(a, n, 1, const_cast<double *>(b), n, nullptr, partials, out, stream);
+}
+
+cudaError_t scale_copy(const double *x, const double *scale, double *y, std::int64_t n,
+                       cudaStream_t stream) {
+    scale_copy_kernel<<<stream_blocks(n), 256, 0, stream>>>(x, scale, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t multi_axpy(const double *V, std::int64_t ld, int K, const double *coef, double *y,
+                       std::int64_t n, cudaStream_t stream) {
+    multi_axpy_kernel<true><<<stream_blocks(n), 256, 0, stream>>>(V, ld, K, coef, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t multi_combine(const double *V, std::int64_t ld, int K, const double *coef, double *y,
+                          std::int64_t n, cudaStream_t stream) {
+    multi_axpy_kernel<false><<<stream_blocks(n), 256, 0, stream>>>(V, ld, K, coef, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t axpy(double a, const double *x, double *y, std::int64_t n, cudaStream_t stream) {
+    axpy_kernel<<<stream_blocks(n), 256, 0, stream>>>(a, x, y, n);
+    return cudaGetLastError();
+}
+
+template <typename A, typename B>
+cudaError_t convert(const A *x, B *y, std::int64_t n, cudaStream_t stream) {
+    convert_kernel<A, B><<<stream_blocks(n), 256, 0, stream>>>(x, y, n);
+    return cudaGetLastError();
+}
+template cudaError_t convert<double, float>(const double *, float *, std::int64_t, cudaStream_t);
+template cudaError_t convert<float, double>(const float *, double *, std::int64_t, cudaStream_t);
+
+cudaError_t arnoldi_start(const ArnoldiState &s, cudaStream_t stream) {
+    arnoldi_start_kernel<<<1, 1, 0, stream>>>(s);
+    return cudaGetLastError();
+}
+
+cudaError_t arnoldi_column(const ArnoldiState &s, int j, cudaStream_t stream) {
+    arnoldi_column_kernel<<<1, 1, 0, stream>>>(s, j);
+    return cudaGetLastError();
+}
+
+cudaError_t arnoldi_solve(const ArnoldiState &s, int k, cudaStream_t stream) {
+    arnoldi_solve_kernel<<<1, 1, 0, stream>>>(s, k);
+    return cudaGetLastError();
+}
+
+} // namespace mkb

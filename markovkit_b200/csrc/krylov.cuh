@@ -1,0 +1,65 @@
+// Krylov building blocks on sm_100a: fused classical Gram-Schmidt passes, norms, vector
+// updates and the small Hessenberg / Givens state of (F)GMRES. Reductions are two-stage with
+// a fixed grid and fixed summation order, so results are bitwise reproducible run to run.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mkb {
+
+constexpr int kDotBlocks = 148 * 4; // one wave of 4 blocks per SM
+constexpr int kDotThreads = 256;
+constexpr int kMaxFusedBasis = 32;  // basis vectors handled by the fused CGS kernels
+
+// partials[k * kDotBlocks + block] for k < K, then out[k] = sum over blocks (fixed order)
+//   mode 0: out[k] = <V_k, w>
+//   mode 1: w -= sum_k coef[k] V_k, then out[k] = <V_k, w_new>
+//   mode 2: w -= sum_k coef[k] V_k, then out[0] = <w_new, w_new>
+//   mode 3: w -= sum_k coef[k] V_k only
+// K <= kMaxFusedBasis; longer bases are processed in chunks by the caller.
+cudaError_t cgs_pass(int mode, const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
+                     const double *coef, double *partials, double *out, cudaStream_t stream);
+
+// out[0] = <a, b>
+cudaError_t dot(const double *a, const double *b, std::int64_t n, double *partials, double *out,
+                cudaStream_t stream);
+
+// y = x * (*scale)           (scale read on the device)
+cudaError_t scale_copy(const double *x, const double *scale, double *y, std::int64_t n,
+                       cudaStream_t stream);
+// y += sum_k coef[k] V_k     (coef read on the device)
+cudaError_t multi_axpy(const double *V, std::int64_t ld, int K, const double *coef, double *y,
+                       std::int64_t n, cudaStream_t stream);
+// y = sum_k coef[k] V_k
+cudaError_t multi_combine(const double *V, std::int64_t ld, int K, const double *coef, double *y,
+                          std::int64_t n, cudaStream_t stream);
+// y = a x + y with a host scalar
+cudaError_t axpy(double a, const double *x, double *y, std::int64_t n, cudaStream_t stream);
+template <typename A, typename B>
+cudaError_t convert(const A *x, B *y, std::int64_t n, cudaStream_t stream);
+
+// Hessenberg / Givens state of one restart cycle, in device memory
+struct ArnoldiState {
+    double *H = nullptr;      // (m + 1) x m, column-major: H[j * (m + 1) + i]
+    double *cs = nullptr;     // m
+    double *sn = nullptr;     // m
+    double *g = nullptr;      // m + 1
+    double *y = nullptr;      // m
+    double *h1 = nullptr;     // m + 1: first Gram-Schmidt coefficients
+    double *h2 = nullptr;     // m + 1: second (re-orthogonalisation) coefficients
+    double *hn = nullptr;     // 1: <w, w> after the second pass
+    double *inv_hn = nullptr; // 1
+    double *beta = nullptr;   // 1: <r, r> on entry, then 1 / ||r||
+    double *report = nullptr; // 4: |g_{j+1}|, ||w||, breakdown flag, spare
+    int m = 0;
+};
+
+// g = (||r||, 0, ...), beta <- 1/||r|| (reads beta = <r, r>)
+cudaError_t arnoldi_start(const ArnoldiState &s, cudaStream_t stream);
+// fold column j (h1 + h2, sqrt(hn)) into H, rotate, update g; report |g_{j+1}|
+cudaError_t arnoldi_column(const ArnoldiState &s, int j, cudaStream_t stream);
+// y = H_k^{-1} g_k (upper triangular, k columns)
+cudaError_t arnoldi_solve(const ArnoldiState &s, int k, cudaStream_t stream);
+
+} // namespace mkb

@@ -1,0 +1,83 @@
+// Launch interface of the row kernels: every pass of the generator and of the multigrid
+// smoothers is one launch over a tile list that covers a level space.
+#pragma once
+
+#include "generator_row.cuh"
+#include <cuda_runtime.h>
+
+namespace mkb {
+
+// A tile is a block's work: `count` consecutive states of one sector, one per thread
+// (kind 0), or one per warp for rows with all-voxel in-jumps (kind 1).
+struct Tile {
+    std::int64_t local0 = 0;
+    int sector = 0;
+    int kind = 0;
+    int count = 0;
+    int pad = 0;
+};
+constexpr int kRowBlock = 256;
+constexpr int kWarpRows = kRowBlock / 32;
+
+enum RowMode : int {
+    kApplyQ = 0,          // y = Q x
+    kApplyShifted,        // y = shift x - Q x
+    kResidual,            // y = b - (shift x - Q x)
+    kJacobiZero,          // y = omega b / (shift + exit)       (a Jacobi sweep from x = 0)
+    kJacobi,              // y = x + omega (b - A x) / (shift + exit)
+    kGaussSeidel,         // x_i = (b_i + in_i) / (shift + exit_i) for states of one colour
+    kExitLeak,            // y = exit, aux = leak
+    kResidualRestrict,    // r = b - A x; coarse[c(i)] += r (or aux = r on terminal sectors)
+    kProlongAdd,          // y += weight * coarse[c(i)]
+    kDiagonal,            // y = shift + exit
+    kRestrict,            // coarse[c(i)] += x_i                (population_transfer::restrict)
+    kProlong,             // y_i = weight_i * coarse[c(i)]      (population_transfer::prolong)
+    kRowModeCount
+};
+
+template <typename T>
+struct RowParams {
+    BinomTable B;
+    const SectorDesc *sectors = nullptr;
+    const Tile *tiles = nullptr;
+    ModelView<T> md;
+    TransferView tv;
+    const T *x = nullptr;
+    const T *b = nullptr;
+    T *y = nullptr;
+    T *aux = nullptr;
+    T *coarse = nullptr;
+    T shift = 0;
+    T omega = 0;
+    int colour = 0;
+    int n_tiles = 0;
+};
+
+// max molecules per state the kernels are instantiated for
+constexpr int kMolCaps[] = {4, 16, 64};
+int mol_cap_for(int n_mol);
+
+template <typename T>
+cudaError_t launch_rows(RowMode mode, int mol_cap, const RowParams<T> &p, cudaStream_t stream);
+
+struct TerminalBlock {
+    std::int64_t begin = 0;      // first row in the level space
+    std::int64_t inv_offset = 0; // offset of the n x n inverse
+    int n = 0;
+    int pad = 0;
+};
+
+// x[begin + p] += sum_q inv[p][q] r[begin + q] for every terminal block
+template <typename T>
+cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, const T *inv, const T *r,
+                            T *x, cudaStream_t stream);
+
+// bit-exact state indexing on the device
+cudaError_t launch_unrank(const BinomTable &B, const SectorDesc *sectors, int n_sectors, int S,
+                          int V, const std::int64_t *index, std::int64_t count, int *states,
+                          cudaStream_t stream);
+cudaError_t launch_rank(const BinomTable &B, const SectorDesc *sectors, int n_sectors,
+                        const int *max_totals, int is_box, int S, int V, const int *states,
+                        std::int64_t count, std::int64_t *index, cudaStream_t stream);
+
+} // namespace mkb
