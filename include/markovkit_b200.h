@@ -19,6 +19,10 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 /* status codes; the C++ facade maps them back to the reference's exception types */
 #define MK_OK 0
 #define MK_EINVAL 1     /* std::invalid_argument */
@@ -160,12 +164,18 @@ void mk_gmres_options_default(mk_gmres_options *opt);
 int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,
                      const mk_gmres_options *opt, mk_solver *out);
 void mk_solver_destroy(mk_solver solver);
+/* change the absolute tolerance of a resident solver (e.g. 1e-10 * ||b|| per right-hand side) */
+int mk_solver_set_tolerance(mk_solver solver, double tolerance);
 /* x is the initial guess on entry and the solution on return (device vectors) */
 int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_result *result,
                     void *stream);
 /* the same with host vectors: copies in, solves, copies out */
 int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
                          mk_solver_result *result, void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }

@@ -125,6 +125,7 @@ SIGNATURES = {
     "mk_gmres_options_default": (None, [C.POINTER(GmresOptions)]),
     "mk_solver_create": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.POINTER(P)]),
     "mk_solver_destroy": (None, [P]),
+    "mk_solver_set_tolerance": (C.c_int, [P, C.c_double]),
     "mk_solver_solve": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
     "mk_solver_solve_host": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
 }

@@ -410,6 +410,9 @@ class solver(_Handle):
         opts = options if options is not None else gmres_options()
         check(load().mk_solver_create(A.Q._h, A.shift(), M._h if M is not None else None, C.byref(opts), C.byref(self._h)))
 
+    def set_tolerance(self, tolerance: float) -> None:
+        check(load().mk_solver_set_tolerance(self._h, float(tolerance)))
+
     def solve(self, b, x, stream=None) -> solver_result:
         r = SolverResult()
         check(load().mk_solver_solve(self._h, _ptr(b), _ptr(x), C.byref(r), _stream(stream)), allow=(_lib.MK_ENOTCONV,))

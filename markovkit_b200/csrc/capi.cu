@@ -506,6 +506,14 @@ int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,
 
 void mk_solver_destroy(mk_solver solver) { delete solver; }
 
+int mk_solver_set_tolerance(mk_solver solver, double tolerance) {
+    return guarded([&] {
+        MK_REQUIRE(solver, "null solver");
+        MK_REQUIRE(tolerance >= 0.0, "tolerance must be nonnegative");
+        solver->opt.tolerance = tolerance;
+    });
+}
+
 static int fill_result(const SolverResult &r, mk_solver_result *out) {
     if (out) {
         out->iterations = r.iterations;

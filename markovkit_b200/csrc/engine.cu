@@ -20,64 +20,6 @@ void check_cuda(cudaError_t e, const char *what) {
 // ---------------------------------------------------------------------------------------
 // binomials and spaces
 
-Binomials::Binomials(int jmax_, int qmax_) : jmax(jmax_), qmax(qmax_) {
-    host.assign(static_cast<std::size_t>(jmax + 1) * (qmax + 1), 0);
-    auto at = [&](int j, int q) -> std::int64_t & {
-        return host[static_cast<std::size_t>(j) * (qmax + 1) + q];
-    };
-    for (int q = 0; q <= qmax; ++q) {
-        at(0, q) = 1;
-        for (int j = 1; j <= std::min(q, jmax); ++j) {
-            const std::int64_t a = at(j - 1, q - 1), b = (j <= q - 1) ? at(j, q - 1) : 0;
-            at(j, q) = (a >= kSaturated || b >= kSaturated || a + b >= kSaturated) ? kSaturated
-                                                                                  : a + b;
-        }
-    }
-    dev.upload(host);
-}
-
-std::vector<SectorDesc> layout_sectors(int V, int S, const std::vector<std::vector<int>> &totals,
-                                       const Binomials &B, std::int64_t *total_size) {
-    std::vector<SectorDesc> out;
-    std::int64_t begin = 0;
-    const BinomTable bt = B.host_view();
-    for (const auto &t : totals) {
-        SectorDesc sec;
-        std::int64_t comp[kMaxSpecies] = {};
-        std::int64_t size = 1;
-        int mol = 0;
-        for (int s = 0; s < S; ++s) {
-            sec.total[s] = t[s];
-            sec.mol_offset[s] = mol;
-            mol += t[s];
-            comp[s] = binom(bt, t[s] + V - 1, t[s]);
-            if (comp[s] >= kSaturated || size > std::numeric_limits<std::int64_t>::max() / comp[s]) {
-                throw Error(kEOverflow, "population state space is too large");
-            }
-            size *= comp[s];
-        }
-        sec.n_mol = mol;
-        std::int64_t stride = 1;
-        for (int s = S - 1; s >= 0; --s) {
-            sec.stride[s] = stride;
-            stride *= comp[s];
-        }
-        sec.begin = begin;
-        sec.size = size;
-        for (int r = 0; r < kMaxReactions; ++r) {
-            sec.src[r] = -1;
-            sec.dst[r] = -1;
-        }
-        if (begin > std::numeric_limits<std::int64_t>::max() - size) {
-            throw Error(kEOverflow, "population state space is too large");
-        }
-        begin += size;
-        out.push_back(sec);
-    }
-    *total_size = begin;
-    return out;
-}
-
 std::unique_ptr<Space> Space::make(int V, const std::vector<int> &limits, bool is_box) {
     const int S = static_cast<int>(limits.size());
     if (V < 1 || S < 1) {
@@ -99,26 +41,9 @@ std::unique_ptr<Space> Space::make(int V, const std::vector<int> &limits, bool i
     sp->max_total = *std::max_element(limits.begin(), limits.end());
     sp->max_mol = std::accumulate(limits.begin(), limits.end(), 0);
     sp->binom = std::make_shared<Binomials>(sp->max_total + 1, V + sp->max_total + 1);
-    std::vector<std::vector<int>> totals;
-    if (is_box) {
-        std::vector<int> t(S, 0);
-        // mixed radix, species 0 most significant (population_space.hpp:166-189)
-        while (true) {
-            totals.push_back(t);
-            int s = S - 1;
-            while (s >= 0 && t[s] == limits[s]) {
-                t[s] = 0;
-                --s;
-            }
-            if (s < 0) {
-                break;
-            }
-            ++t[s];
-        }
-    } else {
-        totals.push_back(limits);
-    }
-    sp->sectors = layout_sectors(V, S, totals, *sp->binom, &sp->n);
+    const std::vector<std::vector<int>> totals =
+        is_box ? box_totals(limits) : std::vector<std::vector<int>>{limits};
+    sp->sectors = layout_sectors(V, S, totals, sp->binom->host_view(), &sp->n);
     sp->d_sectors.upload(sp->sectors);
     sp->d_limits.upload(limits);
     return sp;
@@ -201,228 +126,25 @@ void Space::unrank(std::int64_t i, int *state) const {
 // ---------------------------------------------------------------------------------------
 // models
 
-int Model::ntuple() const {
-    int n = 1;
-    for (int t : tmax) {
-        n *= (t + 1);
-    }
-    return n;
-}
-
-std::unique_ptr<Model> Model::grid(int dim, const std::int64_t *dims, const double *spacing,
-                                   const std::vector<double> &diff) {
-    if (dim < 1 || dim > 3) {
-        throw Error(kEInval, "grid dimension must be 1, 2 or 3");
-    }
-    auto m = std::make_unique<Model>();
-    m->has_grid = true;
-    m->dim = dim;
-    std::int64_t V = 1, stride[3] = {1, 1, 1};
-    for (int a = 0; a < dim; ++a) {
-        if (dims[a] < 1 || !(spacing[a] > 0.0)) {
-            throw Error(kEInval, "grid dimensions and spacings must be positive");
-        }
-        m->dims[a] = dims[a];
-        m->spacing[a] = spacing[a];
-        stride[a] = V;
-        V *= dims[a];
-    }
-    if (V > (std::int64_t(1) << 30)) {
-        throw Error(kEInval, "too many voxels");
-    }
-    m->V = static_cast<int>(V);
-    m->S = static_cast<int>(diff.size());
-    m->diff = diff;
-    double volume = 1.0;
-    for (int a = 0; a < dim; ++a) {
-        volume *= spacing[a];
-    }
-    m->volumes.assign(m->V, volume);
-    m->nbr_ptr.assign(m->V + 1, 0);
-    // axis 0 fastest; neighbours axis by axis, the lower one first; weight = face area / h
-    for (std::int64_t v = 0; v < V; ++v) {
-        std::int64_t rem = v;
-        std::int64_t c[3] = {0, 0, 0};
-        for (int a = 0; a < dim; ++a) {
-            c[a] = rem % dims[a];
-            rem /= dims[a];
-        }
-        for (int a = 0; a < dim; ++a) {
-            double face = 1.0;
-            for (int b = 0; b < dim; ++b) {
-                if (b != a) {
-                    face *= spacing[b];
-                }
-            }
-            const double w = face / spacing[a];
-            if (c[a] > 0) {
-                m->nbr_idx.push_back(static_cast<int>(v - stride[a]));
-                m->nbr_w.push_back(w);
-            }
-            if (c[a] + 1 < dims[a]) {
-                m->nbr_idx.push_back(static_cast<int>(v + stride[a]));
-                m->nbr_w.push_back(w);
-            }
-        }
-        m->nbr_ptr[v + 1] = static_cast<int>(m->nbr_idx.size());
-    }
-    return m;
-}
-
-void Model::validate() const {
-    if (V < 1 || S < 1 || S > kMaxSpecies) {
-        throw Error(kEInval, "model needs 1..4 species and a voxel");
-    }
-    if (static_cast<int>(nbr_ptr.size()) != V + 1 || static_cast<int>(volumes.size()) != V ||
-        static_cast<int>(diff.size()) != S) {
-        throw Error(kEInval, "model arrays have the wrong sizes");
-    }
-    for (double v : volumes) {
-        if (!(v > 0.0) || !std::isfinite(v)) {
-            throw Error(kEInval, "voxel_domain: volumes must be positive");
-        }
-    }
-    if (R > kMaxReactions) {
-        throw Error(kEInval, "at most 16 local reactions are supported");
-    }
-    if (R > 0) {
-        if (static_cast<int>(change.size()) != R * S || static_cast<int>(tmax.size()) != S ||
-            static_cast<std::int64_t>(rates.size()) !=
-                static_cast<std::int64_t>(R) * nvc * ntuple()) {
-            throw Error(kEInval, "reaction tables have the wrong sizes");
-        }
-        if (nvc > 1 && static_cast<int>(vclass.size()) != V) {
-            throw Error(kEInval, "one volume class per voxel");
-        }
-    }
-}
-
 template <typename T>
 void ModelTables<T>::build(const Model &m, double diff_scale, bool with_reactions, bool absorbing) {
-    m.validate();
-    const int V = m.V;
-    h_nbr_ptr = m.nbr_ptr;
-    h_nbr_idx = m.nbr_idx;
-    const std::size_t E = h_nbr_idx.size();
-    h_in_coef.assign(E, T(0));
-    h_deg_coef.assign(V, T(0));
-    for (int v = 0; v < V; ++v) {
-        double deg = 0.0;
-        for (int e = m.nbr_ptr[v]; e < m.nbr_ptr[v + 1]; ++e) {
-            const int w = m.nbr_idx[e];
-            if (w < 0 || w >= V) {
-                throw Error(kEInval, "voxel graph edge out of range");
-            }
-            deg += m.nbr_w[e] / m.volumes[v];
-            // the reverse edge w -> v carries the in-jump
-            double wr = -1.0;
-            for (int f = m.nbr_ptr[w]; f < m.nbr_ptr[w + 1]; ++f) {
-                if (m.nbr_idx[f] == v) {
-                    wr = m.nbr_w[f];
-                    break;
-                }
-            }
-            if (wr < 0.0) {
-                throw Error(kEInval, "voxel graph must list every edge in both directions");
-            }
-            h_in_coef[e] = static_cast<T>(wr / m.volumes[w]);
-        }
-        h_deg_coef[v] = static_cast<T>(deg);
-    }
-    h_vparity.assign(V, 0);
-    if (m.has_grid) {
-        for (int v = 0; v < V; ++v) {
-            std::int64_t rem = v, sum = 0;
-            for (int a = 0; a < m.dim; ++a) {
-                sum += rem % m.dims[a];
-                rem /= m.dims[a];
-            }
-            h_vparity[v] = static_cast<unsigned char>(sum & 1);
-        }
-    }
-    ModelView<T> mv;
-    mv.V = V;
-    mv.S = m.S;
-    mv.absorbing = absorbing ? 1 : 0;
-    for (int s = 0; s < m.S; ++s) {
-        mv.diff[s] = static_cast<T>(m.diff[s] * diff_scale);
-    }
-    h_vclass.clear();
-    h_rate.clear();
-    if (with_reactions && m.R > 0) {
-        mv.R = m.R;
-        mv.nvc = m.nvc;
-        mv.ntuple = m.ntuple();
-        int stride = 1;
-        for (int s = m.S - 1; s >= 0; --s) {
-            mv.tmax[s] = m.tmax[s];
-            mv.tstride[s] = stride;
-            stride *= m.tmax[s] + 1;
-        }
-        h_rate.resize(m.rates.size());
-        for (std::size_t k = 0; k < m.rates.size(); ++k) {
-            const double a = m.rates[k];
-            h_rate[k] = static_cast<T>((a > 0.0 && std::isfinite(a)) ? a : 0.0);
-        }
-        if (m.nvc > 1) {
-            h_vclass = m.vclass;
-        }
-        for (int r = 0; r < m.R; ++r) {
-            bool nonneg = true, nonpos = true, fits = true;
-            int t_neg = 0;
-            for (int s = 0; s < m.S; ++s) {
-                const int c = m.change[r * m.S + s];
-                nonneg = nonneg && c >= 0;
-                nonpos = nonpos && c <= 0;
-                fits = fits && -c <= m.tmax[s];
-                t_neg += (c < 0 ? -c : 0) * mv.tstride[s];
-                mv.change[r][s] = c;
-            }
-            auto rate_at = [&](int vc, int tuple) {
-                return m.rates[(static_cast<std::size_t>(r) * m.nvc + vc) * mv.ntuple + tuple];
-            };
-            if (nonneg) {
-                mv.nonneg_mask |= 1U << r;
-                double total = 0.0;
-                for (int v = 0; v < V; ++v) {
-                    const double a = rate_at(m.nvc > 1 ? m.vclass[v] : 0, 0);
-                    total += (a > 0.0 && std::isfinite(a)) ? a : 0.0;
-                }
-                mv.empty_total[r] = static_cast<T>(total);
-            }
-            if (nonpos && fits) {
-                for (int vc = 0; vc < m.nvc; ++vc) {
-                    if (rate_at(vc, t_neg) > 0.0) {
-                        mv.heavy_mask |= 1U << r;
-                    }
-                }
-            }
-        }
-    }
-    nbr_ptr.upload(h_nbr_ptr);
-    nbr_idx.upload(h_nbr_idx);
-    in_coef.upload(h_in_coef);
-    deg_coef.upload(h_deg_coef);
-    vparity.upload(h_vparity);
-    vclass.upload(h_vclass);
-    rate.upload(h_rate);
-
-    host = mv;
-    host.nbr_ptr = h_nbr_ptr.data();
-    host.nbr_idx = h_nbr_idx.data();
-    host.in_coef = h_in_coef.data();
-    host.deg_coef = h_deg_coef.data();
-    host.vparity = h_vparity.data();
-    host.vclass = h_vclass.empty() ? nullptr : h_vclass.data();
-    host.rate = h_rate.empty() ? nullptr : h_rate.data();
-    dev = mv;
+    h.build(m, diff_scale, with_reactions, absorbing);
+    nbr_ptr.upload(h.nbr_ptr);
+    nbr_idx.upload(h.nbr_idx);
+    in_coef.upload(h.in_coef);
+    deg_coef.upload(h.deg_coef);
+    vparity.upload(h.vparity);
+    vclass.upload(h.vclass);
+    rate.upload(h.rate);
+    host = h.view;
+    dev = h.view;
     dev.nbr_ptr = nbr_ptr.get();
     dev.nbr_idx = nbr_idx.get();
     dev.in_coef = in_coef.get();
     dev.deg_coef = deg_coef.get();
     dev.vparity = vparity.get();
-    dev.vclass = h_vclass.empty() ? nullptr : vclass.get();
-    dev.rate = h_rate.empty() ? nullptr : rate.get();
+    dev.vclass = h.vclass.empty() ? nullptr : vclass.get();
+    dev.rate = h.rate.empty() ? nullptr : rate.get();
 }
 
 template struct ModelTables<double>;
@@ -431,45 +153,12 @@ template struct ModelTables<float>;
 // ---------------------------------------------------------------------------------------
 // operator levels and the generator
 
-void OperatorLevel::finalize(const Model &m, bool with_reactions, bool is_box_like,
-                             const std::vector<int> &box_limits) {
-    (void)is_box_like;
-    (void)box_limits;
-    std::map<std::vector<int>, int> by_totals;
-    int max_mol = 0;
-    for (std::size_t k = 0; k < sectors.size(); ++k) {
-        by_totals[std::vector<int>(sectors[k].total, sectors[k].total + S)] = static_cast<int>(k);
-        max_mol = std::max(max_mol, sectors[k].n_mol);
-    }
-    mol_cap = mol_cap_for(max_mol);
+void OperatorLevel::finalize(const Model &m, bool with_reactions) {
+    mol_cap = mol_cap_for(max_molecules(sectors));
     if (mol_cap < 0) {
         throw Error(kEInval, "more than 64 molecules per state are not supported on the device");
     }
-    const ModelView<double> &mv = t64.host;
-    for (auto &sec : sectors) {
-        sec.heavy = 0;
-        for (int r = 0; r < kMaxReactions; ++r) {
-            sec.src[r] = -1;
-            sec.dst[r] = -1;
-        }
-        if (!with_reactions) {
-            continue;
-        }
-        for (int r = 0; r < m.R; ++r) {
-            std::vector<int> up(S), down(S);
-            for (int s = 0; s < S; ++s) {
-                up[s] = sec.total[s] + m.change[r * S + s];
-                down[s] = sec.total[s] - m.change[r * S + s];
-            }
-            auto it = by_totals.find(up);
-            sec.dst[r] = it == by_totals.end() ? -1 : it->second;
-            it = by_totals.find(down);
-            sec.src[r] = it == by_totals.end() ? -1 : it->second;
-            if (((mv.heavy_mask >> r) & 1U) && sec.src[r] >= 0) {
-                sec.heavy = 1;
-            }
-        }
-    }
+    couple_sectors<double>(sectors, S, m, t64.host, with_reactions);
     tiles.clear();
     for (std::size_t k = 0; k < sectors.size(); ++k) {
         const SectorDesc &sec = sectors[k];
@@ -535,7 +224,7 @@ Generator::Generator(const Space &sp, const Model &model, bool absorbing_)
     op.binom = sp.binom;
     op.t64.build(model, 1.0, true, absorbing);
     op.t32.build(model, 1.0, true, absorbing);
-    op.finalize(model, true, sp.is_box, sp.limits);
+    op.finalize(model, true);
 }
 
 template <typename T>
@@ -685,7 +374,7 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
         L->op.V = grid_model->V;
         L->op.S = S;
         L->op.binom = binom;
-        L->op.sectors = layout_sectors(grid_model->V, S, totals, *binom, &L->op.n);
+        L->op.sectors = layout_sectors(grid_model->V, S, totals, binom->host_view(), &L->op.n);
         L->op.t64.build(*grid_model, scale, false, true);
         L->op.t32.build(*grid_model, scale, false, true);
         L->pre = opt.pre_sweeps + d * opt.sweep_growth;
@@ -693,22 +382,9 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
         L->box_sector = box_of;
 
         // coarsen (markovkit/rdme/multigrid.hpp:25-42)
-        bool can_coarsen = false, odd = false;
-        std::int64_t cdims[3] = {dims[0], dims[1], dims[2]};
-        double cspacing[3] = {spacing[0], spacing[1], spacing[2]};
-        for (int a = 0; a < model.dim; ++a) {
-            if (dims[a] == 1) {
-                continue;
-            }
-            if (dims[a] % 2 != 0) {
-                odd = true;
-                break;
-            }
-            cdims[a] /= 2;
-            cspacing[a] *= 2.0;
-            can_coarsen = true;
-        }
-        can_coarsen = can_coarsen && !odd;
+        std::int64_t cdims[3];
+        double cspacing[3];
+        const bool can_coarsen = coarsen_grid(model.dim, dims, spacing, cdims, cspacing);
         const int levels_left = opt.max_levels - d;
 
         std::vector<std::vector<int>> next_totals;
@@ -732,7 +408,7 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
                 next_box.push_back(box_of[k]);
             }
         }
-        L->op.finalize(*grid_model, false, false, {});
+        L->op.finalize(*grid_model, false);
 
         // dense inverses of the terminal blocks, from the same matrix-free rows
         std::vector<double> inv_all, A, inv;
@@ -765,27 +441,9 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
 
         if (!next_totals.empty()) {
             // parent voxel of every fine voxel (multigrid.hpp:56-65)
-            auto coarse_model = Model::grid(model.dim, cdims, cspacing, model.diff);
-            std::vector<int> parent(grid_model->V);
-            std::vector<int> children(coarse_model->V, 0);
-            for (int v = 0; v < grid_model->V; ++v) {
-                std::int64_t rem = v, cv = 0, cstride = 1;
-                for (int a = 0; a < model.dim; ++a) {
-                    std::int64_t c = rem % dims[a];
-                    rem /= dims[a];
-                    if (dims[a] > 1) {
-                        c /= 2;
-                    }
-                    cv += c * cstride;
-                    cstride *= cdims[a];
-                }
-                parent[v] = static_cast<int>(cv);
-                ++children[cv];
-            }
-            std::vector<double> log_children(coarse_model->V);
-            for (int a = 0; a < coarse_model->V; ++a) {
-                log_children[a] = std::log(static_cast<double>(children[a]));
-            }
+            std::vector<int> parent;
+            std::vector<double> log_children;
+            parent_map(model.dim, dims, cdims, parent, log_children);
             L->parent.upload(parent);
             L->log_children.upload(log_children);
         }

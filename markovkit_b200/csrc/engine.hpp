@@ -3,6 +3,7 @@
 // memory and launches the sm_100a kernels of row_kernels.cu and krylov.cu on a caller stream.
 #pragma once
 
+#include "host_model.hpp"
 #include "krylov.cuh"
 #include "row_kernels.cuh"
 
@@ -13,24 +14,6 @@
 #include <vector>
 
 namespace mkb {
-
-// status codes, shared with the C ABI (include/markovkit_b200.h)
-enum Status : int {
-    kOk = 0,
-    kEInval = 1,
-    kEOverflow = 2,
-    kESingular = 3,
-    kENoMem = 4,
-    kENotConv = 5,
-    kENan = 6,
-    kETimeout = 7,
-    kECuda = 8,
-};
-
-struct Error : std::runtime_error {
-    int code;
-    Error(int c, const std::string &what) : std::runtime_error(what), code(c) {}
-};
 
 void check_cuda(cudaError_t e, const char *what);
 
@@ -90,11 +73,12 @@ struct Binomials {
     int jmax = 0, qmax = 0;
     std::vector<std::int64_t> host;
     DeviceArray<std::int64_t> dev;
-    Binomials(int jmax, int qmax);
+    Binomials(int jmax_, int qmax_) : jmax(jmax_), qmax(qmax_), host(binomial_table(jmax_, qmax_)) {
+        dev.upload(host);
+    }
     [[nodiscard]] BinomTable host_view() const { return {host.data(), jmax, qmax}; }
     [[nodiscard]] BinomTable device_view() const { return {dev.get(), jmax, qmax}; }
 };
-constexpr std::int64_t kSaturated = std::int64_t(1) << 62;
 
 // Every sector of a box (0 <= t_s <= max_s, mixed-radix order, species 0 most significant,
 // markovkit/rdme/population_space.hpp:131-196) or a single sector (:105-127).
@@ -117,39 +101,10 @@ struct Space {
     [[nodiscard]] int sector_of(std::int64_t i) const;
 };
 
-// sectors with the given totals on V voxels, numbered contiguously from 0 in list order
-std::vector<SectorDesc> layout_sectors(int V, int S, const std::vector<std::vector<int>> &totals,
-                                       const Binomials &B, std::int64_t *total_size);
-
-// An RDME model: a symmetric voxel graph, volumes, diffusivities and local reactions whose
-// rates are tabulated over count tuples 0..tmax_s (markovkit/rdme/reaction_diffusion.hpp).
-struct Model {
-    int V = 0, S = 0;
-    std::vector<int> nbr_ptr, nbr_idx;
-    std::vector<double> nbr_w, volumes, diff;
-    bool has_grid = false;
-    int dim = 0;
-    std::int64_t dims[3] = {1, 1, 1};
-    double spacing[3] = {1.0, 1.0, 1.0};
-    int R = 0;
-    std::vector<int> change; // R x S
-    std::vector<int> tmax;   // S
-    int nvc = 1;
-    std::vector<int> vclass; // V (empty: one class)
-    std::vector<double> rates; // R x nvc x ntuple
-
-    [[nodiscard]] int ntuple() const;
-    static std::unique_ptr<Model> grid(int dim, const std::int64_t *dims, const double *spacing,
-                                       const std::vector<double> &diff);
-    void validate() const;
-};
-
 // host + device tables of one voxel graph and model in one precision
 template <typename T>
 struct ModelTables {
-    std::vector<int> h_nbr_ptr, h_nbr_idx, h_vclass;
-    std::vector<T> h_in_coef, h_deg_coef, h_rate;
-    std::vector<unsigned char> h_vparity;
+    HostTables<T> h;
     DeviceArray<int> nbr_ptr, nbr_idx, vclass;
     DeviceArray<T> in_coef, deg_coef, rate;
     DeviceArray<unsigned char> vparity;
@@ -171,8 +126,7 @@ struct OperatorLevel {
     std::shared_ptr<Binomials> binom;
 
     // sector couplings (src/dst/heavy) for the model's reactions, then tiles and uploads
-    void finalize(const Model &m, bool with_reactions, bool is_box_like,
-                  const std::vector<int> &box_limits);
+    void finalize(const Model &m, bool with_reactions);
     template <typename T>
     [[nodiscard]] RowParams<T> params() const;
     template <typename T>

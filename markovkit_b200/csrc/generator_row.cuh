@@ -17,6 +17,8 @@
 
 #include "population_index.cuh"
 
+#include <cmath>
+
 namespace mkb {
 
 template <typename T>

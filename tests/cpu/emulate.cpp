@@ -1,0 +1,196 @@
+// Test infrastructure: runs the product's shared host/device row logic
+// (markovkit_b200/csrc/generator_row.cuh, population_index.cuh, host_model.hpp) on the CPU,
+// one row at a time, so the non-GPU tests can check state indexing, the generator gather and
+// the multigrid transfer against the reference's golden vectors before any kernel runs.
+// Built by tests/cpu_emulator.py with g++ into a small shared library.
+#include "host_model.hpp"
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace mkb;
+
+namespace {
+
+struct Problem {
+    std::unique_ptr<Model> model;
+    std::vector<std::int64_t> binom;
+    BinomTable B;
+    std::vector<SectorDesc> sectors;
+    std::int64_t n = 0;
+    HostTables<double> t;
+};
+
+void write_err(char *err, const std::string &msg) {
+    if (err) {
+        std::strncpy(err, msg.c_str(), 255);
+        err[255] = '\0';
+    }
+}
+
+Problem make(int dim, const std::int64_t *dims, const double *spacing, int S, const double *D,
+             int R, const int *change, const int *tmax, const double *rates, int is_box,
+             const int *limits, int absorbing) {
+    Problem p;
+    p.model = Model::grid(dim, dims, spacing, std::vector<double>(D, D + S));
+    if (R > 0) {
+        p.model->R = R;
+        p.model->change.assign(change, change + R * S);
+        p.model->tmax.assign(tmax, tmax + S);
+        p.model->rates.assign(rates, rates + static_cast<std::size_t>(R) * p.model->ntuple());
+    }
+    const std::vector<int> lim(limits, limits + S);
+    const int max_total = *std::max_element(lim.begin(), lim.end());
+    p.binom = binomial_table(max_total + 1, p.model->V + max_total + 1);
+    p.B = {p.binom.data(), max_total + 1, p.model->V + max_total + 1};
+    const auto totals = is_box ? box_totals(lim) : std::vector<std::vector<int>>{lim};
+    p.sectors = layout_sectors(p.model->V, S, totals, p.B, &p.n);
+    p.t.build(*p.model, 1.0, true, absorbing != 0);
+    couple_sectors<double>(p.sectors, S, *p.model, p.t.view, true);
+    return p;
+}
+
+constexpr int kCap = 64;
+
+} // namespace
+
+extern "C" {
+
+// exit, leak, Q x and (shift I - Q) x for every state; returns the number of states
+std::int64_t emu_generator(int dim, const std::int64_t *dims, const double *spacing, int S,
+                           const double *D, int R, const int *change, const int *tmax,
+                           const double *rates, int is_box, const int *limits, int absorbing,
+                           double shift, const double *x, double *exit_out, double *leak_out,
+                           double *Qx, double *Ax, char *err) {
+    try {
+        Problem p = make(dim, dims, spacing, S, D, R, change, tmax, rates, is_box, limits, absorbing);
+        if (!x) {
+            return p.n;
+        }
+        for (const SectorDesc &sec : p.sectors) {
+            for (std::int64_t local = 0; local < sec.size; ++local) {
+                RowState<kCap> st;
+                load_state<kCap>(p.B, sec, S, p.model->V, local, st);
+                double e = 0.0, l = 0.0, in = 0.0;
+                visit_row<double, kCap>(p.B, p.sectors.data(), sec, p.t.view, local, st, true, 0,
+                                        1, e, l, [&](std::int64_t j, double a) {
+                                            if (j < 0 || j >= p.n) {
+                                                throw Error(kEInval, "in-jump source out of range");
+                                            }
+                                            in += a * x[j];
+                                        });
+                const std::int64_t i = sec.begin + local;
+                exit_out[i] = e;
+                leak_out[i] = l;
+                Qx[i] = in - e * x[i];
+                Ax[i] = (shift + e) * x[i] - in;
+            }
+        }
+        return p.n;
+    } catch (const std::exception &e) {
+        write_err(err, e.what());
+        return -1;
+    }
+}
+
+// states (n x V*S, voxel-major) of every index by the product's unrank, and the product's
+// rank of each of them
+std::int64_t emu_states(int V, int S, const int *limits, int is_box, int *states,
+                        std::int64_t *ranks, char *err) {
+    try {
+        const std::vector<int> lim(limits, limits + S);
+        const int max_total = *std::max_element(lim.begin(), lim.end());
+        auto table = binomial_table(max_total + 1, V + max_total + 1);
+        const BinomTable B{table.data(), max_total + 1, V + max_total + 1};
+        const auto totals = is_box ? box_totals(lim) : std::vector<std::vector<int>>{lim};
+        std::int64_t n = 0;
+        const auto sectors = layout_sectors(V, S, totals, B, &n);
+        if (!states) {
+            return n;
+        }
+        for (const SectorDesc &sec : sectors) {
+            for (std::int64_t local = 0; local < sec.size; ++local) {
+                RowState<kCap> st;
+                load_state<kCap>(B, sec, S, V, local, st);
+                int *out = states + (sec.begin + local) * static_cast<std::int64_t>(V) * S;
+                std::fill(out, out + static_cast<std::int64_t>(V) * S, 0);
+                std::int64_t r = sec.begin;
+                for (int s = 0; s < S; ++s) {
+                    for (int q = 0; q < sec.total[s]; ++q) {
+                        ++out[static_cast<std::int64_t>(V - 1 - st.u[sec.mol_offset[s] + q]) * S + s];
+                    }
+                    r += rank_species(B, st.u + sec.mol_offset[s], sec.total[s]) * sec.stride[s];
+                }
+                ranks[sec.begin + local] = r;
+            }
+        }
+        return n;
+    } catch (const std::exception &e) {
+        write_err(err, e.what());
+        return -1;
+    }
+}
+
+// population_transfer of one sector between a grid and its coarsening:
+// Pc = prolong(c), Rg = restrict(g); returns the fine size (coarse size in *n_coarse)
+std::int64_t emu_transfer(int dim, const std::int64_t *dims, const double *spacing, int S,
+                          const int *totals, const double *c, const double *g, double *Pc,
+                          double *Rg, std::int64_t *n_coarse, char *err) {
+    try {
+        std::int64_t cdims[3];
+        double cspacing[3];
+        if (!coarsen_grid(dim, dims, spacing, cdims, cspacing)) {
+            throw Error(kEInval, "grid cannot be coarsened");
+        }
+        std::int64_t Vf = 1, Vc = 1;
+        for (int a = 0; a < dim; ++a) {
+            Vf *= dims[a];
+            Vc *= cdims[a];
+        }
+        const std::vector<int> t(totals, totals + S);
+        const int max_total = *std::max_element(t.begin(), t.end());
+        auto table = binomial_table(max_total + 1, static_cast<int>(Vf) + max_total + 1);
+        const BinomTable B{table.data(), max_total + 1, static_cast<int>(Vf) + max_total + 1};
+        std::int64_t nf = 0, nc = 0;
+        auto fine = layout_sectors(static_cast<int>(Vf), S, {t}, B, &nf);
+        auto coarse = layout_sectors(static_cast<int>(Vc), S, {t}, B, &nc);
+        fine[0].coarse = 0;
+        *n_coarse = nc;
+        if (!c) {
+            return nf;
+        }
+        std::vector<int> parent;
+        std::vector<double> log_children, lgf(max_total + 2);
+        parent_map(dim, dims, cdims, parent, log_children);
+        for (std::size_t k = 0; k < lgf.size(); ++k) {
+            lgf[k] = std::lgamma(static_cast<double>(k) + 1.0);
+        }
+        TransferView tv;
+        tv.Vc = static_cast<int>(Vc);
+        tv.parent = parent.data();
+        tv.log_children = log_children.data();
+        tv.lgf = lgf.data();
+        tv.coarse_sectors = coarse.data();
+        std::fill(Rg, Rg + nc, 0.0);
+        for (std::int64_t i = 0; i < nf; ++i) {
+            RowState<kCap> st;
+            load_state<kCap>(B, fine[0], S, static_cast<int>(Vf), i, st);
+            double w = 0.0;
+            const std::int64_t ci =
+                coarse_index<kCap>(B, tv, fine[0], S, static_cast<int>(Vf), st, &w);
+            if (ci < 0 || ci >= nc) {
+                throw Error(kEInval, "coarse index out of range");
+            }
+            Pc[i] = w * c[ci];
+            Rg[ci] += g[i];
+        }
+        return nf;
+    } catch (const std::exception &e) {
+        write_err(err, e.what());
+        return -1;
+    }
+}
+
+} // extern "C"
