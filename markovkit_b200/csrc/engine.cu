@@ -32,6 +32,9 @@ std::unique_ptr<Space> Space::make(int V, const std::vector<int> &limits, bool i
         if (t < 0) {
             throw Error(kEInval, "species totals must be nonnegative");
         }
+        if (t > kHostIndexCap) {
+            throw Error(kEInval, "species totals above 1024 are not supported");
+        }
     }
     auto sp = std::make_unique<Space>();
     sp->V = V;
@@ -91,16 +94,17 @@ std::int64_t Space::rank(const int *state) const {
     }
     const SectorDesc &sec = sectors[k];
     const BinomTable B = binom->host_view();
-    std::vector<int> u;
+    std::vector<int> buf(kHostIndexCap);
+    auto &u = *reinterpret_cast<int(*)[kHostIndexCap]>(buf.data());
     std::int64_t local = 0;
     for (int s = 0; s < S; ++s) {
-        u.clear();
+        int n = 0;
         for (int v = V - 1; v >= 0; --v) {
             for (int q = 0; q < state[static_cast<std::int64_t>(v) * S + s]; ++q) {
-                u.push_back(V - 1 - v);
+                u[n++] = V - 1 - v;
             }
         }
-        local += rank_species(B, u.data(), static_cast<int>(u.size())) * sec.stride[s];
+        local += rank_species<kHostIndexCap>(B, u, n) * sec.stride[s];
     }
     return sec.begin + local;
 }
@@ -113,10 +117,11 @@ void Space::unrank(std::int64_t i, int *state) const {
     const SectorDesc &sec = sectors[sector_of(i)];
     std::int64_t rank[kMaxSpecies];
     split_local(sec, S, i - sec.begin, rank);
-    std::vector<int> u(std::max(max_total, 1));
+    std::vector<int> buf(kHostIndexCap);
+    auto &u = *reinterpret_cast<int(*)[kHostIndexCap]>(buf.data());
     const BinomTable B = binom->host_view();
     for (int s = 0; s < S; ++s) {
-        unrank_species(B, rank[s], sec.total[s], V, u.data());
+        unrank_species<kHostIndexCap>(B, rank[s], sec.total[s], V, u);
         for (int p = 0; p < sec.total[s]; ++p) {
             ++state[static_cast<std::int64_t>(V - 1 - u[p]) * S + s];
         }
@@ -154,20 +159,25 @@ template struct ModelTables<float>;
 // operator levels and the generator
 
 void OperatorLevel::finalize(const Model &m, bool with_reactions) {
-    mol_cap = mol_cap_for(max_molecules(sectors));
+    if (n >= (std::int64_t(1) << 31)) {
+        throw Error(kEInval, "state spaces of 2^31 states or more are not supported on the device");
+    }
+    mol_cap = mol_cap_for(S, max_species_total(sectors));
     if (mol_cap < 0) {
-        throw Error(kEInval, "more than 64 molecules per state are not supported on the device");
+        throw Error(kEInval, "more than 64 molecules of one species per state are not supported");
     }
     couple_sectors<double>(sectors, S, m, t64.host, with_reactions);
     tiles.clear();
     for (std::size_t k = 0; k < sectors.size(); ++k) {
         const SectorDesc &sec = sectors[k];
-        const int rows = sec.heavy ? kWarpRows : kRowBlock;
+        // heavy rows: a warp each, or a whole block each when the sector has few of them
+        const int kind = sec.heavy ? (sec.size <= 4 * 148 ? 2 : 1) : 0;
+        const int rows = kind == 0 ? kRowBlock : (kind == 1 ? kWarpRows : 1);
         for (std::int64_t l = 0; l < sec.size; l += rows) {
             Tile t;
             t.local0 = l;
             t.sector = static_cast<int>(k);
-            t.kind = sec.heavy ? 1 : 0;
+            t.kind = kind;
             t.count = static_cast<int>(std::min<std::int64_t>(rows, sec.size - l));
             tiles.push_back(t);
         }
@@ -196,7 +206,7 @@ RowParams<T> OperatorLevel::params() const {
 
 template <typename T>
 void OperatorLevel::run(RowMode mode, const RowParams<T> &p, cudaStream_t stream) const {
-    check_cuda(launch_rows<T>(mode, mol_cap, p, stream), "row kernel launch");
+    check_cuda(launch_rows<T>(mode, S, mol_cap, p, stream), "row kernel launch");
 }
 
 template RowParams<double> OperatorLevel::params<double>() const;
@@ -315,17 +325,17 @@ bool invert_dense(std::vector<double> &A, int n, std::vector<double> &inv) {
     return true;
 }
 
-template <int MAXM>
+// the terminal block of one sector, dense, from the same matrix-free rows (host, generic shape)
 void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vector<double> &A) {
     const SectorDesc &sec = op.sectors[slot];
     const auto n = static_cast<int>(sec.size);
     A.assign(static_cast<std::size_t>(n) * n, 0.0);
     const BinomTable B = op.binom->host_view();
+    auto st = std::make_unique<RowState<kMaxSpecies, 64>>();
     for (int i = 0; i < n; ++i) {
-        RowState<MAXM> st;
-        load_state<MAXM>(B, sec, op.S, op.V, i, st);
+        load_state<kMaxSpecies, 64>(B, sec, op.S, op.V, i, *st);
         double exit = 0.0, leak = 0.0;
-        visit_row<double, MAXM>(B, op.sectors.data(), sec, op.t64.host, i, st, true, 0, 1, exit,
+        visit_row<double, kMaxSpecies, 64>(B, op.sectors.data(), sec, op.t64.host, i, *st, true, 0, 1, exit,
                                 leak, [&](std::int64_t j, double a) {
                                     A[static_cast<std::size_t>(i) * n + (j - sec.begin)] -= a;
                                 });
@@ -417,17 +427,7 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
             if (sec.terminal < 0) {
                 continue;
             }
-            switch (L->op.mol_cap) {
-            case 4:
-                assemble_terminal<4>(L->op, static_cast<int>(k), shift, A);
-                break;
-            case 16:
-                assemble_terminal<16>(L->op, static_cast<int>(k), shift, A);
-                break;
-            default:
-                assemble_terminal<64>(L->op, static_cast<int>(k), shift, A);
-                break;
-            }
+            assemble_terminal(L->op, static_cast<int>(k), shift, A);
             if (!invert_dense(A, static_cast<int>(sec.size), inv)) {
                 throw Error(kESingular, "population_multigrid: singular block");
             }
@@ -688,21 +688,64 @@ void Multigrid::apply_system(int d, const double *x, double *y, cudaStream_t str
     L.op.run<double>(kApplyShifted, p, stream);
 }
 
+// The cycle works only on the hierarchy's own buffers, so it is captured once into a CUDA
+// graph (about six launches per level) and replayed on the caller's stream.
+void Multigrid::ensure_graph() {
+    if (graph_exec_) {
+        return;
+    }
+    cudaStream_t cap = nullptr;
+    check_cuda(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream");
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        try {
+            if (opt.precision == 0) {
+                cycle<double>(0, cap);
+            } else {
+                cycle<float>(0, cap);
+            }
+        } catch (...) {
+            cudaStreamEndCapture(cap, &graph);
+            if (graph) {
+                cudaGraphDestroy(graph);
+            }
+            cudaStreamDestroy(cap);
+            throw;
+        }
+        e = cudaStreamEndCapture(cap, &graph);
+    }
+    cudaStreamDestroy(cap);
+    check_cuda(e, "multigrid graph capture");
+    e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    check_cuda(e, "multigrid graph instantiate");
+}
+
+Multigrid::~Multigrid() {
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+    }
+}
+
 void Multigrid::apply(const double *b, double *x, cudaStream_t stream) {
     Level &L0 = *levels[0];
     const std::size_t n0 = static_cast<std::size_t>(L0.op.n);
+    ensure_graph();
     if (opt.precision == 0) {
         check_cuda(cudaMemcpyAsync(L0.rhs64.get(), b, n0 * sizeof(double), cudaMemcpyDeviceToDevice,
                                    stream),
                    "copy");
-        double *out = cycle<double>(0, stream);
-        check_cuda(cudaMemcpyAsync(x, out, n0 * sizeof(double), cudaMemcpyDeviceToDevice, stream),
+        check_cuda(cudaGraphLaunch(graph_exec_, stream), "multigrid graph launch");
+        check_cuda(cudaMemcpyAsync(x, L0.x64.get(), n0 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   stream),
                    "copy");
     } else {
         check_cuda(convert<double, float>(b, L0.rhs32.get(), static_cast<std::int64_t>(n0), stream),
                    "convert");
-        float *out = cycle<float>(0, stream);
-        check_cuda(convert<float, double>(out, x, static_cast<std::int64_t>(n0), stream), "convert");
+        check_cuda(cudaGraphLaunch(graph_exec_, stream), "multigrid graph launch");
+        check_cuda(convert<float, double>(L0.x32.get(), x, static_cast<std::int64_t>(n0), stream),
+                   "convert");
     }
 }
 
@@ -744,11 +787,20 @@ Krylov::Krylov(std::int64_t n_, int m_, bool flexible_) : n(n_), m(m_), flexible
     st.inv_hn = p++;
     st.beta = p++;
     st.report = p;
-    check_cuda(cudaMallocHost(reinterpret_cast<void **>(&report_host), 4 * sizeof(double)),
+    // slot 0: true residuals; slots 1 and 2: the two Arnoldi steps in flight
+    check_cuda(cudaMallocHost(reinterpret_cast<void **>(&report_host), 12 * sizeof(double)),
                "cudaMallocHost");
+    for (auto &e : step_done) {
+        check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    }
 }
 
 Krylov::~Krylov() {
+    for (auto &e : step_done) {
+        if (e) {
+            cudaEventDestroy(e);
+        }
+    }
     if (report_host) {
         cudaFreeHost(report_host);
     }
@@ -836,7 +888,8 @@ SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double 
         check_cuda(scale_copy(ws.r.get(), ws.st.beta, ws.V.get(), n, stream), "scale");
         int k = 0;
         bool nan = false;
-        for (int j = 0; j < m && res.iterations < opt.max_iterations; ++j) {
+        // one Arnoldi step on the stream; its residual estimate lands in pinned slot j % 2
+        auto enqueue = [&](int j) {
             double *vj = ws.V.get() + j * ws.ld;
             double *z = vj;
             if (M) {
@@ -849,23 +902,45 @@ SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double 
             gs_update(ws, 1, K, ws.w.get(), ws.st.h1, ws.st.h2, stream);
             gs_update(ws, 2, K, ws.w.get(), ws.st.h2, ws.st.hn, stream);
             check_cuda(arnoldi_column(ws.st, j, stream), "arnoldi");
-            ++res.iterations;
-            k = j + 1;
-            read_report(ws, stream);
-            const double est = ws.report_host[0];
-            if (!std::isfinite(est) || !std::isfinite(ws.report_host[1])) {
-                nan = true;
-                break;
-            }
-            if (est <= tol || ws.report_host[2] != 0.0) {
-                break;
-            }
+            double *slot = ws.report_host + 4 * (1 + (j & 1));
+            check_cuda(cudaMemcpyAsync(slot, ws.st.report, 4 * sizeof(double),
+                                       cudaMemcpyDeviceToHost, stream),
+                       "report");
+            check_cuda(cudaEventRecord(ws.step_done[j & 1], stream), "event");
             if (j + 1 < m) {
                 check_cuda(scale_copy(ws.w.get(), ws.st.inv_hn, ws.V.get() + (j + 1) * ws.ld, n,
                                       stream),
                            "scale");
             }
+        };
+        // Step j + 1 is enqueued before the host waits for step j's estimate, so the host's
+        // launch work overlaps the device's. When step j converges, step j + 1 has run but is
+        // not used: the solve below takes the first k = j + 1 columns, and step j + 1 touched
+        // only H's column j + 1 and g[j + 1..j + 2].
+        const std::int64_t base = res.iterations; // steps taken in earlier restart cycles
+        int enqueued = 0;
+        if (base + 1 <= opt.max_iterations) {
+            enqueue(0);
+            enqueued = 1;
         }
+        for (int j = 0; j < m && j < enqueued; ++j) {
+            if (j + 1 < m && base + j + 2 <= opt.max_iterations) {
+                enqueue(j + 1);
+                ++enqueued;
+            }
+            check_cuda(cudaEventSynchronize(ws.step_done[j & 1]), "sync");
+            const double *rep = ws.report_host + 4 * (1 + (j & 1));
+            ++res.iterations;
+            k = j + 1;
+            if (!std::isfinite(rep[0]) || !std::isfinite(rep[1])) {
+                nan = true;
+                break;
+            }
+            if (rep[0] <= tol || rep[2] != 0.0) {
+                break;
+            }
+        }
+        check_cuda(cudaStreamSynchronize(stream), "sync");
         if (nan) {
             res.status = kENan;
             res.residual = std::numeric_limits<double>::quiet_NaN();

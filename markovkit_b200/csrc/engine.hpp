@@ -80,6 +80,8 @@ struct Binomials {
     [[nodiscard]] BinomTable device_view() const { return {dev.get(), jmax, qmax}; }
 };
 
+constexpr int kHostIndexCap = 1024; // largest species total the host rank/unrank accept
+
 // Every sector of a box (0 <= t_s <= max_s, mixed-radix order, species 0 most significant,
 // markovkit/rdme/population_space.hpp:131-196) or a single sector (:105-127).
 struct Space {
@@ -184,6 +186,9 @@ struct Multigrid {
     std::shared_ptr<Binomials> binom;
 
     Multigrid(const Space &space, const Model &model, double shift, const MultigridOptions &opt);
+    ~Multigrid();
+    Multigrid(const Multigrid &) = delete;
+    Multigrid &operator=(const Multigrid &) = delete;
     // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
     void apply(const double *b, double *x, cudaStream_t stream);
     [[nodiscard]] int n_levels() const { return static_cast<int>(levels.size()); }
@@ -198,6 +203,8 @@ struct Multigrid {
     T *cycle(int d, cudaStream_t stream);
     template <typename T>
     T *buf(Level &L, int which);
+    void ensure_graph();
+    cudaGraphExec_t graph_exec_ = nullptr;
 };
 
 struct GmresOptions {
@@ -221,7 +228,8 @@ struct Krylov {
     bool flexible = false;
     DeviceArray<double> V, Z, w, r, t, partials, small;
     ArnoldiState st;
-    double *report_host = nullptr; // pinned
+    double *report_host = nullptr; // pinned, 3 slots of 4
+    cudaEvent_t step_done[2] = {nullptr, nullptr};
     Krylov(std::int64_t n, int m, bool flexible);
     ~Krylov();
     Krylov(const Krylov &) = delete;

@@ -1,6 +1,7 @@
 // One row of the RDME generator, matrix-free: the exit rate, leak rate and every in-jump of
 // a state, computed from its unranked molecule lists. Shared by the sm_100a kernels (gather
-// SpMV, residuals, smoothers) and by host set-up (dense terminal blocks).
+// SpMV, residuals, smoothers) and by host set-up (dense terminal blocks) and the tests' CPU
+// emulation.
 //
 // Semantics follow markovkit/rdme/reaction_diffusion.hpp:82-118 and generator.hpp:27-44:
 //  * a molecule of species s jumps from voxel v along edge e at rate n * D_s * w_e / vol_v;
@@ -12,7 +13,11 @@
 // The reference scatters each column (generator.hpp:62-81); this gathers each row, so
 //   (s I - Q x)_i = (s + exit_i) x_i - sum_{j -> i} rate_{j->i} x_j.
 // In-jumps of reactions whose source can sit in any empty voxel (deaths, annihilations)
-// fan in from all V voxels; those rows are split across a warp's lanes ("heavy" rows).
+// fan in from all V voxels; those rows are split across a warp's or a block's threads
+// ("heavy" rows).
+//
+// NS (species) and TMAX (molecules of one species) are compile-time bounds of the state's
+// molecule lists; species s < NS with s >= S carry no molecules.
 #pragma once
 
 #include "population_index.cuh"
@@ -52,173 +57,124 @@ MK_HD T load_ro(const T *p) {
 #endif
 }
 
-template <typename T>
-MK_HD int load_ro_i(const int *p) {
-#if defined(__CUDA_ARCH__)
-    return __ldg(p);
-#else
-    return *p;
-#endif
+// The compiled state shapes: (species S, largest species total `cap`) -> (NS, TMAX); calls
+// f.template operator()<NS, TMAX>(). Shared by the kernel launches and the CPU emulation so
+// both run the same instantiation.
+template <typename F>
+inline auto with_shape(int S, int cap, F &&f) {
+    if (S == 1) {
+        if (cap <= 2) {
+            return f.template operator()<1, 2>();
+        }
+        if (cap <= 4) {
+            return f.template operator()<1, 4>();
+        }
+        if (cap <= 16) {
+            return f.template operator()<1, 16>();
+        }
+        return f.template operator()<1, 64>();
+    }
+    if (S == 2) {
+        if (cap <= 1) {
+            return f.template operator()<2, 1>();
+        }
+        if (cap <= 2) {
+            return f.template operator()<2, 2>();
+        }
+        if (cap <= 4) {
+            return f.template operator()<2, 4>();
+        }
+        return f.template operator()<2, 16>();
+    }
+    if (cap <= 4) {
+        return f.template operator()<kMaxSpecies, 4>();
+    }
+    return f.template operator()<kMaxSpecies, 16>();
 }
 
-// the unranked state of one row
-template <int MAXM>
+// the unranked state of one row: species s's molecules u[s][0..total_s), ascending.
+// Index arithmetic inside a level space is 32-bit: level spaces hold fewer than 2^31 states.
+template <int NS, int TMAX>
 struct RowState {
-    int u[MAXM];                       // molecule lists, species-major, ascending per species
-    std::int64_t rank[kMaxSpecies];    // per-species rank inside the sector
+    int u[NS][TMAX];
+    int rank[NS]; // per-species rank inside the sector
 };
 
-template <int MAXM>
+template <int NS>
+MK_HD void split_species(const SectorDesc &sec, int S, std::int64_t local, int (&rank)[NS]) {
+    int rem = static_cast<int>(local);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if (s + 1 >= S) {
+            rank[s] = s + 1 == S ? rem : 0;
+        } else {
+            const int stride = static_cast<int>(sec.stride[s]);
+            int q = static_cast<int>(static_cast<double>(rem) * sec.inv_stride[s]);
+            q -= (q * stride > rem) ? 1 : 0;
+            q += ((q + 1) * stride <= rem) ? 1 : 0;
+            rank[s] = q;
+            rem -= q * stride;
+        }
+    }
+}
+
+template <int NS, int TMAX>
 MK_HD void load_state(const BinomTable &B, const SectorDesc &sec, int S, int V, std::int64_t local,
-                      RowState<MAXM> &st) {
-    split_local(sec, S, local, st.rank);
-    for (int s = 0; s < S; ++s) {
-        unrank_species(B, st.rank[s], sec.total[s], V, st.u + sec.mol_offset[s]);
+                      RowState<NS, TMAX> &st) {
+    split_species<NS>(sec, S, local, st.rank);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        unrank_species<TMAX>(B, st.rank[s], s < S ? sec.total[s] : 0, V, st.u[s]);
     }
 }
 
 // checkerboard colour of a state: parity of the sum over molecules of their voxel's colour
-template <typename T, int MAXM>
-MK_HD int state_colour(const ModelView<T> &md, const SectorDesc &sec, const RowState<MAXM> &st) {
+template <typename T, int NS, int TMAX>
+MK_HD int state_colour(const ModelView<T> &md, const SectorDesc &sec, const RowState<NS, TMAX> &st) {
     int c = 0;
-    for (int p = 0; p < sec.n_mol; ++p) {
-        c ^= md.vparity[md.V - 1 - st.u[p]];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        MK_UNROLL_MOL
+        for (int p = 0; p < TMAX; ++p) {
+            if (p < sec.total[s]) {
+                c ^= md.vparity[md.V - 1 - st.u[s][p]];
+            }
+        }
     }
     return c;
+}
+
+// global index of the source state of reaction r's in-jump at voxel uu (source sector ss)
+template <typename T, int NS, int TMAX>
+MK_HD int reaction_source(const BinomTable &B, const ModelView<T> &md, const SectorDesc &sec,
+                          const SectorDesc &ss, const RowState<NS, TMAX> &st, int r, int uu) {
+    int src = static_cast<int>(ss.begin);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int c = md.change[r][s];
+        const int rs = c == 0 ? st.rank[s]
+                              : static_cast<int>(rank_modified<TMAX>(B, st.u[s], sec.total[s],
+                                                                     uu, -c));
+        src += rs * static_cast<int>(ss.stride[s]);
+    }
+    return src;
 }
 
 // Visit the row: acc(source_index, rate) for every in-jump; adds into exit and leak.
 // light: the exit/leak terms and the in-jumps that start in occupied voxels.
 // [lane, V) step nlanes: the all-voxel loop of heavy reactions.
-template <typename T, int MAXM, bool WANT_IN = true, typename Acc>
+template <typename T, int NS, int TMAX, bool WANT_IN = true, typename Acc>
 MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const SectorDesc &sec,
-                     const ModelView<T> &md, std::int64_t local, const RowState<MAXM> &st,
+                     const ModelView<T> &md, std::int64_t local, const RowState<NS, TMAX> &st,
                      bool light, int lane, int nlanes, T &exit, T &leak, Acc &&acc) {
-    const int V = md.V, S = md.S, R = md.R;
+    const int V = md.V, R = md.R;
     if (light) {
-        // distinct occupied voxels across species, ascending in u
-        int d[MAXM];
-        int nd = 0;
-        for (int p = 0; p < sec.n_mol; ++p) {
-            const int val = st.u[p];
-            int pos = nd;
-            bool seen = false;
-            for (int q = 0; q < nd; ++q) {
-                if (d[q] == val) {
-                    seen = true;
-                    break;
-                }
-            }
-            if (seen) {
-                continue;
-            }
-            while (pos > 0 && d[pos - 1] > val) {
-                d[pos] = d[pos - 1];
-                --pos;
-            }
-            d[pos] = val;
-            ++nd;
-        }
-        T esub[kMaxReactions];
-        for (int r = 0; r < R; ++r) {
-            esub[r] = T(0);
-        }
-        for (int q = 0; q < nd; ++q) {
-            const int uu = d[q];
-            const int v = V - 1 - uu;
-            int n[kMaxSpecies];
-            int ti = 0;
-            for (int s = 0; s < S; ++s) {
-                n[s] = count_of(st.u + sec.mol_offset[s], sec.total[s], uu);
-                ti += n[s] * md.tstride[s];
-            }
-            // diffusion: out of v, and into v from each neighbour
-            const int e0 = load_ro_i<int>(md.nbr_ptr + v), e1 = load_ro_i<int>(md.nbr_ptr + v + 1);
-            for (int s = 0; s < S; ++s) {
-                if (n[s] == 0) {
-                    continue;
-                }
-                const int *us = st.u + sec.mol_offset[s];
-                const int ts = sec.total[s];
-                exit += T(n[s]) * md.diff[s] * load_ro(md.deg_coef + v);
-                if (!WANT_IN) {
-                    continue;
-                }
-                for (int e = e0; e < e1; ++e) {
-                    const int w = load_ro_i<int>(md.nbr_idx + e);
-                    const int uw = V - 1 - w;
-                    const int nw = count_of(us, ts, uw);
-                    const T rate = T(nw + 1) * md.diff[s] * load_ro(md.in_coef + e);
-                    const std::int64_t r2 = rank_replace(B, us, ts, uu, uw);
-                    acc(sec.begin + local + (r2 - st.rank[s]) * sec.stride[s], rate);
-                }
-            }
-            if (R == 0) {
-                continue;
-            }
-            const int vc = md.vclass ? load_ro_i<int>(md.vclass + v) : 0;
-            for (int r = 0; r < R; ++r) {
-                const T *rrow = md.rate + (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple;
-                bool valid = true;
-                for (int s = 0; s < S; ++s) {
-                    valid = valid && (n[s] + md.change[r][s] >= 0);
-                }
-                if (valid) {
-                    const T a = load_ro(rrow + ti);
-                    if (a > T(0)) {
-                        if (sec.dst[r] >= 0) {
-                            exit += a;
-                        } else {
-                            leak += a;
-                            if (md.absorbing) {
-                                exit += a;
-                            }
-                        }
-                    }
-                }
-                if ((md.nonneg_mask >> r) & 1U) {
-                    const T a0 = load_ro(rrow);
-                    esub[r] += a0 > T(0) ? a0 : T(0);
-                }
-                if (!WANT_IN || ((md.heavy_mask >> r) & 1U) || sec.src[r] < 0) {
-                    continue;
-                }
-                int tm = 0;
-                bool ok = true;
-                for (int s = 0; s < S; ++s) {
-                    const int m = n[s] - md.change[r][s];
-                    ok = ok && m >= 0 && m <= md.tmax[s];
-                    tm += m * md.tstride[s];
-                }
-                if (!ok) {
-                    continue;
-                }
-                const T a = load_ro(rrow + tm);
-                if (!(a > T(0))) {
-                    continue;
-                }
-                const SectorDesc &ss = sectors[sec.src[r]];
-                std::int64_t src = ss.begin;
-                for (int s = 0; s < S; ++s) {
-                    const std::int64_t rs =
-                        md.change[r][s] == 0
-                            ? st.rank[s]
-                            : rank_modified(B, st.u + sec.mol_offset[s], sec.total[s], uu,
-                                            -md.change[r][s]);
-                    src += rs * ss.stride[s];
-                }
-                acc(src, a);
-            }
-        }
-        // reactions that fire from the empty voxels: the all-empty total minus occupied voxels
+        // reactions firing from empty voxels: the all-empty total, corrected per occupied voxel
         for (int r = 0; r < R; ++r) {
             if (!((md.nonneg_mask >> r) & 1U)) {
                 continue;
             }
-            const T E = md.empty_total[r] - esub[r];
-            if (!(E > T(0))) {
-                continue;
-            }
+            const T E = md.empty_total[r];
             if (sec.dst[r] >= 0) {
                 exit += E;
             } else {
@@ -228,45 +184,128 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                 }
             }
         }
+        // each distinct occupied voxel once: (species s, position p) is its first occurrence
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            MK_UNROLL_MOL
+            for (int p = 0; p < TMAX; ++p) {
+                if (p >= sec.total[s]) {
+                    continue;
+                }
+                const int uu = st.u[s][p];
+                if (p > 0 && st.u[s][p - 1] == uu) {
+                    continue;
+                }
+                bool seen = false;
+#pragma unroll
+                for (int s2 = 0; s2 < s; ++s2) {
+                    seen = seen || count_of<TMAX>(st.u[s2], sec.total[s2], uu) > 0;
+                }
+                if (seen) {
+                    continue;
+                }
+                const int v = V - 1 - uu;
+                int n[NS];
+                int ti = 0;
+#pragma unroll
+                for (int s2 = 0; s2 < NS; ++s2) {
+                    n[s2] = count_of<TMAX>(st.u[s2], sec.total[s2], uu);
+                    ti += n[s2] * md.tstride[s2];
+                }
+                // diffusion: out of v, and into v from each neighbour
+                const int e0 = load_ro(md.nbr_ptr + v), e1 = load_ro(md.nbr_ptr + v + 1);
+                const T deg = load_ro(md.deg_coef + v);
+#pragma unroll
+                for (int s3 = 0; s3 < NS; ++s3) {
+                    if (n[s3] == 0) {
+                        continue;
+                    }
+                    exit += T(n[s3]) * md.diff[s3] * deg;
+                    if constexpr (WANT_IN) {
+                        for (int e = e0; e < e1; ++e) {
+                            const int uw = V - 1 - load_ro(md.nbr_idx + e);
+                            const int nw = count_of<TMAX>(st.u[s3], sec.total[s3], uw);
+                            const T rate = T(nw + 1) * md.diff[s3] * load_ro(md.in_coef + e);
+                            const int r2 = static_cast<int>(
+                                rank_replace<TMAX>(B, st.u[s3], sec.total[s3], uu, uw));
+                            acc(static_cast<int>(sec.begin + local) +
+                                    (r2 - st.rank[s3]) * static_cast<int>(sec.stride[s3]),
+                                rate);
+                        }
+                    }
+                }
+                if (R == 0) {
+                    continue;
+                }
+                const int vc = md.vclass ? load_ro(md.vclass + v) : 0;
+                for (int r = 0; r < R; ++r) {
+                    const T *rrow =
+                        md.rate + (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple;
+                    bool valid = true;
+                    int tm = 0;
+                    bool ok = true;
+#pragma unroll
+                    for (int s4 = 0; s4 < NS; ++s4) {
+                        valid = valid && n[s4] + md.change[r][s4] >= 0;
+                        const int m = n[s4] - md.change[r][s4];
+                        ok = ok && m >= 0 && m <= md.tmax[s4];
+                        tm += m * md.tstride[s4];
+                    }
+                    // out of this voxel; and it is not one of the empty voxels counted above
+                    T a = valid ? load_ro(rrow + ti) : T(0);
+                    if ((md.nonneg_mask >> r) & 1U) {
+                        a -= load_ro(rrow);
+                    }
+                    if (sec.dst[r] >= 0) {
+                        exit += a;
+                    } else {
+                        leak += a;
+                        if (md.absorbing) {
+                            exit += a;
+                        }
+                    }
+                    if constexpr (WANT_IN) {
+                        if (((md.heavy_mask >> r) & 1U) || sec.src[r] < 0 || !ok) {
+                            continue;
+                        }
+                        const T ain = load_ro(rrow + tm);
+                        if (ain > T(0)) {
+                            acc(reaction_source<T, NS, TMAX>(B, md, sec, sectors[sec.src[r]], st,
+                                                             r, uu),
+                                ain);
+                        }
+                    }
+                }
+            }
+        }
     }
     // heavy reactions: a source in every voxel
-    if (!WANT_IN) {
-        return;
-    }
-    for (int r = 0; r < R; ++r) {
-        if (!((md.heavy_mask >> r) & 1U) || sec.src[r] < 0) {
-            continue;
-        }
-        const SectorDesc &ss = sectors[sec.src[r]];
-        for (int v = lane; v < V; v += nlanes) {
-            const int uu = V - 1 - v;
-            int tm = 0;
-            bool ok = true;
-            for (int s = 0; s < S; ++s) {
-                const int m =
-                    count_of(st.u + sec.mol_offset[s], sec.total[s], uu) - md.change[r][s];
-                ok = ok && m >= 0 && m <= md.tmax[s];
-                tm += m * md.tstride[s];
-            }
-            if (!ok) {
+    if constexpr (WANT_IN) {
+        for (int r = 0; r < R; ++r) {
+            if (!((md.heavy_mask >> r) & 1U) || sec.src[r] < 0) {
                 continue;
             }
-            const int vc = md.vclass ? load_ro_i<int>(md.vclass + v) : 0;
-            const T a =
-                load_ro(md.rate + (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple + tm);
-            if (!(a > T(0))) {
-                continue;
+            const SectorDesc &ss = sectors[sec.src[r]];
+            for (int v = lane; v < V; v += nlanes) {
+                const int uu = V - 1 - v;
+                int tm = 0;
+                bool ok = true;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const int m = count_of<TMAX>(st.u[s], sec.total[s], uu) - md.change[r][s];
+                    ok = ok && m >= 0 && m <= md.tmax[s];
+                    tm += m * md.tstride[s];
+                }
+                if (!ok) {
+                    continue;
+                }
+                const int vc = md.vclass ? load_ro(md.vclass + v) : 0;
+                const T a = load_ro(md.rate +
+                                    (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple + tm);
+                if (a > T(0)) {
+                    acc(reaction_source<T, NS, TMAX>(B, md, sec, ss, st, r, uu), a);
+                }
             }
-            std::int64_t src = ss.begin;
-            for (int s = 0; s < S; ++s) {
-                const std::int64_t rs =
-                    md.change[r][s] == 0
-                        ? st.rank[s]
-                        : rank_modified(B, st.u + sec.mol_offset[s], sec.total[s], uu,
-                                        -md.change[r][s]);
-                src += rs * ss.stride[s];
-            }
-            acc(src, a);
         }
     }
 }
@@ -285,50 +324,56 @@ struct TransferView {
     const SectorDesc *coarse_sectors = nullptr;
 };
 
-// the coarse index of a fine state and (optionally) its prolongation weight
-template <int MAXM>
+// the coarse index of a fine state and (optionally) its prolongation weight; the coarse
+// molecule list is ranked without sorting: an element of value w at sorted position q adds
+// C(w + q, q + 1), q = (#smaller) + (#equal ones before it)
+template <int NS, int TMAX>
 MK_HD std::int64_t coarse_index(const BinomTable &B, const TransferView &tv, const SectorDesc &fine,
-                                int S, int Vf, const RowState<MAXM> &st, double *weight) {
+                                int Vf, const RowState<NS, TMAX> &st, double *weight) {
     const SectorDesc &cs = tv.coarse_sectors[fine.coarse];
     std::int64_t index = cs.begin;
     double logw = 0.0;
-    for (int s = 0; s < S; ++s) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
         const int t = fine.total[s];
-        const int *u = st.u + fine.mol_offset[s];
-        int cu[MAXM];
-        for (int p = 0; p < t; ++p) {
-            const int a = load_ro_i<int>(tv.parent + (Vf - 1 - u[p]));
-            int val = tv.Vc - 1 - a;
-            int pos = p;
-            while (pos > 0 && cu[pos - 1] > val) {
-                cu[pos] = cu[pos - 1];
-                --pos;
-            }
-            cu[pos] = val;
+        int cu[TMAX];
+        MK_UNROLL_MOL
+        for (int p = 0; p < TMAX; ++p) {
+            cu[p] = p < t ? tv.Vc - 1 - load_ro(tv.parent + (Vf - 1 - st.u[s][p])) : 0;
         }
-        index += rank_species(B, cu, t) * cs.stride[s];
-        if (weight) {
-            for (int p = 0; p < t;) {
-                int q = p;
-                while (q < t && u[q] == u[p]) {
-                    ++q;
-                }
-                logw -= load_ro(tv.lgf + (q - p));
-                p = q;
+        std::int64_t r = 0;
+        MK_UNROLL_MOL
+        for (int p = 0; p < TMAX; ++p) {
+            if (p >= t) {
+                continue;
             }
-            for (int p = 0; p < t;) {
-                int q = p;
-                while (q < t && cu[q] == cu[p]) {
-                    ++q;
+            int q = 0, equal_before = 0, equal_total = 0;
+            MK_UNROLL_MOL
+            for (int k = 0; k < TMAX; ++k) {
+                if (k < t) {
+                    q += cu[k] < cu[p] ? 1 : 0;
+                    equal_before += (k < p && cu[k] == cu[p]) ? 1 : 0;
+                    equal_total += cu[k] == cu[p] ? 1 : 0;
                 }
-                const int a = tv.Vc - 1 - cu[p];
-                logw += load_ro(tv.lgf + (q - p)) - (q - p) * load_ro(tv.log_children + a);
-                p = q;
+            }
+            q += equal_before;
+            r += binom(B, cu[p] + q, q + 1);
+            if (weight) {
+                if (equal_before == 0) {
+                    // first copy of a coarse value: lgamma(c_a + 1) - c_a log(children_a)
+                    logw += load_ro(tv.lgf + equal_total) -
+                            equal_total * load_ro(tv.log_children + (tv.Vc - 1 - cu[p]));
+                }
+                if (p == 0 || st.u[s][p - 1] != st.u[s][p]) {
+                    // first copy of a fine value: - lgamma(n_v + 1)
+                    logw -= load_ro(tv.lgf + count_of<TMAX>(st.u[s], t, st.u[s][p]));
+                }
             }
         }
+        index += r * cs.stride[s];
     }
     if (weight) {
-        *weight = exp(logw);
+        *weight = std::exp(logw);
     }
     return index;
 }

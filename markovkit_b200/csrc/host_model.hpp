@@ -101,6 +101,7 @@ inline std::vector<SectorDesc> layout_sectors(int V, int S,
         std::int64_t stride = 1;
         for (int s = S - 1; s >= 0; --s) {
             sec.stride[s] = stride;
+            sec.inv_stride[s] = 1.0 / static_cast<double>(stride);
             stride *= comp[s];
         }
         sec.begin = begin;
@@ -449,10 +450,13 @@ inline void parent_map(int dim, const std::int64_t *dims, const std::int64_t *cd
     }
 }
 
-inline int max_molecules(const std::vector<SectorDesc> &sectors) {
+// the largest total of one species in any sector (sizes the kernels' molecule lists)
+inline int max_species_total(const std::vector<SectorDesc> &sectors) {
     int m = 0;
     for (const auto &s : sectors) {
-        m = std::max(m, s.n_mol);
+        for (int k = 0; k < kMaxSpecies; ++k) {
+            m = std::max(m, s.total[k]);
+        }
     }
     return m;
 }

@@ -1,214 +1,39 @@
-// sm_100a row kernels: the matrix-free generator gather and every multigrid pass built on it.
-// All of them are HBM-bound gathers (no dense contraction, so no tensor cores): each
-// thread unranks its state, visits its in-jumps and writes one value.
+// Dispatch of the row kernels (instantiated in row_kernels_f64.cu / row_kernels_f32.cu), the
+// dense terminal solve of the multigrid, and bit-exact state indexing on the device.
 #include "row_kernels.cuh"
 
 namespace mkb {
 
-int mol_cap_for(int n_mol) {
-    for (int cap : kMolCaps) {
-        if (n_mol <= cap) {
+int mol_cap_for(int n_species, int max_species_total) {
+    const int limit = n_species == 1 ? 64 : 16;
+    if (max_species_total > limit) {
+        return -1;
+    }
+    for (int cap : {1, 2, 4, 16, 64}) {
+        if (max_species_total <= cap) {
             return cap;
         }
     }
     return -1;
 }
 
+template <>
+cudaError_t launch_rows<double>(RowMode mode, int S, int cap, const RowParams<double> &p,
+                                cudaStream_t stream) {
+    RowParams<double> q = p;
+    q.mode = mode;
+    return launch_rows_f64(q, S, cap, stream);
+}
+
+template <>
+cudaError_t launch_rows<float>(RowMode mode, int S, int cap, const RowParams<float> &p,
+                               cudaStream_t stream) {
+    RowParams<float> q = p;
+    q.mode = mode;
+    return launch_rows_f32(q, S, cap, stream);
+}
+
 namespace {
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        v += __shfl_xor_sync(0xffffffffu, v, off);
-    }
-    return v;
-}
-
-template <typename T, int MAXM, int MODE>
-__device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDesc &sec,
-                                           std::int64_t local, const RowState<MAXM> &st, T exit,
-                                           T leak, T in) {
-    const std::int64_t i = sec.begin + local;
-    if constexpr (MODE == kApplyQ) {
-        p.y[i] = in - exit * p.x[i];
-    } else if constexpr (MODE == kApplyShifted) {
-        p.y[i] = (p.shift + exit) * p.x[i] - in;
-    } else if constexpr (MODE == kResidual) {
-        p.y[i] = p.b[i] - ((p.shift + exit) * p.x[i] - in);
-    } else if constexpr (MODE == kJacobiZero) {
-        p.y[i] = p.omega * p.b[i] / (p.shift + exit);
-    } else if constexpr (MODE == kJacobi) {
-        const T d = p.shift + exit;
-        const T xi = p.x[i];
-        p.y[i] = xi + p.omega * (p.b[i] - (d * xi - in)) / d;
-    } else if constexpr (MODE == kGaussSeidel) {
-        p.y[i] = (p.b[i] + in) / (p.shift + exit);
-    } else if constexpr (MODE == kExitLeak) {
-        p.y[i] = exit;
-        p.aux[i] = leak;
-    } else if constexpr (MODE == kResidualRestrict) {
-        const T r = p.b[i] - ((p.shift + exit) * p.x[i] - in);
-        if (sec.coarse >= 0) {
-            const std::int64_t c =
-                coarse_index<MAXM>(p.B, p.tv, sec, p.md.S, p.md.V, st, nullptr);
-            atomicAdd(p.coarse + c, r);
-        } else {
-            p.aux[i] = r;
-        }
-    } else if constexpr (MODE == kDiagonal) {
-        p.y[i] = p.shift + exit;
-    }
-}
-
-template <typename T, int MAXM, int MODE>
-__device__ __forceinline__ void transfer_row(const RowParams<T> &p, const SectorDesc &sec,
-                                             std::int64_t local, const RowState<MAXM> &st) {
-    const std::int64_t i = sec.begin + local;
-    if (sec.coarse < 0) {
-        if constexpr (MODE == kProlong) {
-            p.y[i] = T(0);
-        }
-        return;
-    }
-    if constexpr (MODE == kRestrict) {
-        const std::int64_t c = coarse_index<MAXM>(p.B, p.tv, sec, p.md.S, p.md.V, st, nullptr);
-        atomicAdd(p.coarse + c, p.x[i]);
-    } else {
-        double w = 0.0;
-        const std::int64_t c = coarse_index<MAXM>(p.B, p.tv, sec, p.md.S, p.md.V, st, &w);
-        if constexpr (MODE == kProlongAdd) {
-            p.y[i] += static_cast<T>(w) * p.coarse[c];
-        } else {
-            p.y[i] = static_cast<T>(w) * p.coarse[c];
-        }
-    }
-}
-
-template <typename T, int MAXM, int MODE>
-__global__ void __launch_bounds__(kRowBlock) row_kernel(const RowParams<T> p) {
-    __shared__ SectorDesc s_sec;
-    const Tile tile = p.tiles[blockIdx.x];
-    if (threadIdx.x == 0) {
-        s_sec = p.sectors[tile.sector];
-    }
-    __syncthreads();
-    const SectorDesc &sec = s_sec;
-    // in-place Gauss-Seidel reads x while other threads write it: plain loads there
-    const T *xs = (MODE == kGaussSeidel) ? p.y : p.x;
-
-    if (tile.kind == 0) {
-        if (static_cast<int>(threadIdx.x) >= tile.count) {
-            return;
-        }
-        const std::int64_t local = tile.local0 + threadIdx.x;
-        RowState<MAXM> st;
-        load_state<MAXM>(p.B, sec, p.md.S, p.md.V, local, st);
-        if constexpr (MODE == kProlongAdd || MODE == kProlong || MODE == kRestrict) {
-            transfer_row<T, MAXM, MODE>(p, sec, local, st);
-            return;
-        } else {
-            if constexpr (MODE == kGaussSeidel) {
-                if (state_colour<T, MAXM>(p.md, sec, st) != p.colour) {
-                    return;
-                }
-            }
-            T exit = T(0), leak = T(0), in = T(0);
-            if constexpr (MODE == kGaussSeidel) {
-                visit_row<T, MAXM>(p.B, p.sectors, sec, p.md, local, st, true, 0, 1, exit, leak,
-                                   [&](std::int64_t j, T a) { in += a * xs[j]; });
-            } else if constexpr (MODE == kJacobiZero || MODE == kExitLeak || MODE == kDiagonal) {
-                visit_row<T, MAXM, false>(p.B, p.sectors, sec, p.md, local, st, true, 0, 1, exit,
-                                          leak, [&](std::int64_t, T) {});
-            } else {
-                visit_row<T, MAXM>(p.B, p.sectors, sec, p.md, local, st, true, 0, 1, exit, leak,
-                                   [&](std::int64_t j, T a) { in += a * __ldg(xs + j); });
-            }
-            finish_row<T, MAXM, MODE>(p, sec, local, st, exit, leak, in);
-        }
-        return;
-    }
-
-    // one warp per row: lane 0 takes the light terms, all lanes split the voxel loop
-    const int warp = static_cast<int>(threadIdx.x) >> 5;
-    const int lane = static_cast<int>(threadIdx.x) & 31;
-    if (warp >= tile.count) {
-        return;
-    }
-    const std::int64_t local = tile.local0 + warp;
-    RowState<MAXM> st;
-    load_state<MAXM>(p.B, sec, p.md.S, p.md.V, local, st);
-    if constexpr (MODE == kProlongAdd || MODE == kProlong || MODE == kRestrict) {
-        if (lane == 0) {
-            transfer_row<T, MAXM, MODE>(p, sec, local, st);
-        }
-        return;
-    } else {
-        if constexpr (MODE == kGaussSeidel) {
-            if (state_colour<T, MAXM>(p.md, sec, st) != p.colour) {
-                return;
-            }
-        }
-        T exit = T(0), leak = T(0), in = T(0);
-        if constexpr (MODE == kGaussSeidel) {
-            visit_row<T, MAXM>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, 32, exit,
-                               leak, [&](std::int64_t j, T a) { in += a * xs[j]; });
-        } else if constexpr (MODE == kJacobiZero || MODE == kExitLeak || MODE == kDiagonal) {
-            visit_row<T, MAXM, false>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, 32,
-                                      exit, leak, [&](std::int64_t, T) {});
-        } else {
-            visit_row<T, MAXM>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, 32, exit,
-                               leak, [&](std::int64_t j, T a) { in += a * __ldg(xs + j); });
-        }
-        exit = warp_sum(exit);
-        leak = warp_sum(leak);
-        in = warp_sum(in);
-        if (lane == 0) {
-            finish_row<T, MAXM, MODE>(p, sec, local, st, exit, leak, in);
-        }
-    }
-}
-
-template <typename T, int MAXM, int MODE>
-cudaError_t launch_one(const RowParams<T> &p, cudaStream_t stream) {
-    if (p.n_tiles == 0) {
-        return cudaSuccess;
-    }
-    row_kernel<T, MAXM, MODE><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
-    return cudaGetLastError();
-}
-
-template <typename T, int MAXM>
-cudaError_t launch_mode(RowMode mode, const RowParams<T> &p, cudaStream_t stream) {
-    switch (mode) {
-    case kApplyQ:
-        return launch_one<T, MAXM, kApplyQ>(p, stream);
-    case kApplyShifted:
-        return launch_one<T, MAXM, kApplyShifted>(p, stream);
-    case kResidual:
-        return launch_one<T, MAXM, kResidual>(p, stream);
-    case kJacobiZero:
-        return launch_one<T, MAXM, kJacobiZero>(p, stream);
-    case kJacobi:
-        return launch_one<T, MAXM, kJacobi>(p, stream);
-    case kGaussSeidel:
-        return launch_one<T, MAXM, kGaussSeidel>(p, stream);
-    case kExitLeak:
-        return launch_one<T, MAXM, kExitLeak>(p, stream);
-    case kResidualRestrict:
-        return launch_one<T, MAXM, kResidualRestrict>(p, stream);
-    case kProlongAdd:
-        return launch_one<T, MAXM, kProlongAdd>(p, stream);
-    case kDiagonal:
-        return launch_one<T, MAXM, kDiagonal>(p, stream);
-    case kRestrict:
-        return launch_one<T, MAXM, kRestrict>(p, stream);
-    case kProlong:
-        return launch_one<T, MAXM, kProlong>(p, stream);
-    default:
-        return cudaErrorInvalidValue;
-    }
-}
 
 template <typename T>
 __global__ void terminal_kernel(const TerminalBlock *blocks, const T *inv, const T *r, T *x) {
@@ -236,6 +61,8 @@ __device__ int find_sector_of(const SectorDesc *sectors, int n_sectors, std::int
     return lo;
 }
 
+constexpr int kIndexCap = 64;
+
 __global__ void unrank_kernel(const BinomTable B, const SectorDesc *sectors, int n_sectors, int S,
                               int V, const std::int64_t *index, std::int64_t count, int *states) {
     const std::int64_t t = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x;
@@ -247,18 +74,21 @@ __global__ void unrank_kernel(const BinomTable B, const SectorDesc *sectors, int
         out[k] = 0;
     }
     const std::int64_t i = index[t];
+    if (i < 0) {
+        return;
+    }
     const int k = find_sector_of(sectors, n_sectors, i);
     const SectorDesc &sec = sectors[k];
-    if (i < 0 || i >= sec.begin + sec.size) {
+    if (i >= sec.begin + sec.size) {
         return;
     }
     std::int64_t rank[kMaxSpecies];
     split_local(sec, S, i - sec.begin, rank);
-    int u[64];
+    int u[kIndexCap];
     for (int s = 0; s < S; ++s) {
-        unrank_species(B, rank[s], sec.total[s], V, u);
-        for (int p = 0; p < sec.total[s]; ++p) {
-            out[static_cast<std::int64_t>(V - 1 - u[p]) * S + s] += 1;
+        unrank_species<kIndexCap>(B, rank[s], sec.total[s], V, u);
+        for (int q = 0; q < sec.total[s]; ++q) {
+            out[static_cast<std::int64_t>(V - 1 - u[q]) * S + s] += 1;
         }
     }
 }
@@ -305,9 +135,9 @@ __global__ void rank_kernel(const BinomTable B, const SectorDesc *sectors, int n
     }
     const SectorDesc &sec = sectors[k];
     std::int64_t local = 0;
-    int u[64];
+    int u[kIndexCap];
     for (int s = 0; s < S; ++s) {
-        if (totals[s] > 64) {
+        if (totals[s] > kIndexCap) {
             index[t] = -1;
             return;
         }
@@ -318,29 +148,12 @@ __global__ void rank_kernel(const BinomTable B, const SectorDesc *sectors, int n
                 u[n++] = V - 1 - v;
             }
         }
-        local += rank_species(B, u, n) * sec.stride[s];
+        local += rank_species<kIndexCap>(B, u, n) * sec.stride[s];
     }
     index[t] = sec.begin + local;
 }
 
 } // namespace
-
-template <typename T>
-cudaError_t launch_rows(RowMode mode, int mol_cap, const RowParams<T> &p, cudaStream_t stream) {
-    switch (mol_cap) {
-    case 4:
-        return launch_mode<T, 4>(mode, p, stream);
-    case 16:
-        return launch_mode<T, 16>(mode, p, stream);
-    case 64:
-        return launch_mode<T, 64>(mode, p, stream);
-    default:
-        return cudaErrorInvalidValue;
-    }
-}
-
-template cudaError_t launch_rows<double>(RowMode, int, const RowParams<double> &, cudaStream_t);
-template cudaError_t launch_rows<float>(RowMode, int, const RowParams<float> &, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, const T *inv, const T *r,

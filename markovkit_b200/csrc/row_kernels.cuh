@@ -51,14 +51,17 @@ struct RowParams {
     T omega = 0;
     int colour = 0;
     int n_tiles = 0;
+    int mode = kApplyShifted;
 };
 
-// max molecules per state the kernels are instantiated for
-constexpr int kMolCaps[] = {4, 16, 64};
-int mol_cap_for(int n_mol);
+// the largest species total the kernels handle: 64 with one species, 16 with more
+int mol_cap_for(int n_species, int max_species_total);
 
+// one pass over every tile; (S, cap) select the kernel's state shape
 template <typename T>
-cudaError_t launch_rows(RowMode mode, int mol_cap, const RowParams<T> &p, cudaStream_t stream);
+cudaError_t launch_rows(RowMode mode, int S, int cap, const RowParams<T> &p, cudaStream_t stream);
+cudaError_t launch_rows_f64(const RowParams<double> &p, int S, int cap, cudaStream_t stream);
+cudaError_t launch_rows_f32(const RowParams<float> &p, int S, int cap, cudaStream_t stream);
 
 struct TerminalBlock {
     std::int64_t begin = 0;      // first row in the level space

@@ -53,6 +53,7 @@ Problem make(int dim, const std::int64_t *dims, const double *spacing, int S, co
 }
 
 constexpr int kCap = 64;
+using State = RowState<kMaxSpecies, kCap>; // the generic shape: any species count up to 4
 
 } // namespace
 
@@ -69,25 +70,30 @@ std::int64_t emu_generator(int dim, const std::int64_t *dims, const double *spac
         if (!x) {
             return p.n;
         }
-        for (const SectorDesc &sec : p.sectors) {
-            for (std::int64_t local = 0; local < sec.size; ++local) {
-                RowState<kCap> st;
-                load_state<kCap>(p.B, sec, S, p.model->V, local, st);
-                double e = 0.0, l = 0.0, in = 0.0;
-                visit_row<double, kCap>(p.B, p.sectors.data(), sec, p.t.view, local, st, true, 0,
-                                        1, e, l, [&](std::int64_t j, double a) {
-                                            if (j < 0 || j >= p.n) {
-                                                throw Error(kEInval, "in-jump source out of range");
-                                            }
-                                            in += a * x[j];
-                                        });
-                const std::int64_t i = sec.begin + local;
-                exit_out[i] = e;
-                leak_out[i] = l;
-                Qx[i] = in - e * x[i];
-                Ax[i] = (shift + e) * x[i] - in;
+        // the state shape the device kernels use for this space
+        with_shape(S, max_species_total(p.sectors), [&]<int NS, int TMAX>() {
+            for (const SectorDesc &sec : p.sectors) {
+                for (std::int64_t local = 0; local < sec.size; ++local) {
+                    RowState<NS, TMAX> st;
+                    load_state<NS, TMAX>(p.B, sec, S, p.model->V, local, st);
+                    double e = 0.0, l = 0.0, in = 0.0;
+                    visit_row<double, NS, TMAX>(
+                        p.B, p.sectors.data(), sec, p.t.view, local, st, true, 0, 1, e, l,
+                        [&](std::int64_t j, double a) {
+                            if (j < 0 || j >= p.n) {
+                                throw Error(kEInval, "in-jump source out of range");
+                            }
+                            in += a * x[j];
+                        });
+                    const std::int64_t i = sec.begin + local;
+                    exit_out[i] = e;
+                    leak_out[i] = l;
+                    Qx[i] = in - e * x[i];
+                    Ax[i] = (shift + e) * x[i] - in;
+                }
             }
-        }
+            return 0;
+        });
         return p.n;
     } catch (const std::exception &e) {
         write_err(err, e.what());
@@ -112,16 +118,16 @@ std::int64_t emu_states(int V, int S, const int *limits, int is_box, int *states
         }
         for (const SectorDesc &sec : sectors) {
             for (std::int64_t local = 0; local < sec.size; ++local) {
-                RowState<kCap> st;
-                load_state<kCap>(B, sec, S, V, local, st);
+                State st;
+                load_state<kMaxSpecies, kCap>(B, sec, S, V, local, st);
                 int *out = states + (sec.begin + local) * static_cast<std::int64_t>(V) * S;
                 std::fill(out, out + static_cast<std::int64_t>(V) * S, 0);
                 std::int64_t r = sec.begin;
                 for (int s = 0; s < S; ++s) {
                     for (int q = 0; q < sec.total[s]; ++q) {
-                        ++out[static_cast<std::int64_t>(V - 1 - st.u[sec.mol_offset[s] + q]) * S + s];
+                        ++out[static_cast<std::int64_t>(V - 1 - st.u[s][q]) * S + s];
                     }
-                    r += rank_species(B, st.u + sec.mol_offset[s], sec.total[s]) * sec.stride[s];
+                    r += rank_species<kCap>(B, st.u[s], sec.total[s]) * sec.stride[s];
                 }
                 ranks[sec.begin + local] = r;
             }
@@ -174,18 +180,21 @@ std::int64_t emu_transfer(int dim, const std::int64_t *dims, const double *spaci
         tv.lgf = lgf.data();
         tv.coarse_sectors = coarse.data();
         std::fill(Rg, Rg + nc, 0.0);
-        for (std::int64_t i = 0; i < nf; ++i) {
-            RowState<kCap> st;
-            load_state<kCap>(B, fine[0], S, static_cast<int>(Vf), i, st);
-            double w = 0.0;
-            const std::int64_t ci =
-                coarse_index<kCap>(B, tv, fine[0], S, static_cast<int>(Vf), st, &w);
-            if (ci < 0 || ci >= nc) {
-                throw Error(kEInval, "coarse index out of range");
+        with_shape(S, max_total, [&]<int NS, int TMAX>() {
+            for (std::int64_t i = 0; i < nf; ++i) {
+                RowState<NS, TMAX> st;
+                load_state<NS, TMAX>(B, fine[0], S, static_cast<int>(Vf), i, st);
+                double w = 0.0;
+                const std::int64_t ci =
+                    coarse_index<NS, TMAX>(B, tv, fine[0], static_cast<int>(Vf), st, &w);
+                if (ci < 0 || ci >= nc) {
+                    throw Error(kEInval, "coarse index out of range");
+                }
+                Pc[i] = w * c[ci];
+                Rg[ci] += g[i];
             }
-            Pc[i] = w * c[ci];
-            Rg[ci] += g[i];
-        }
+            return 0;
+        });
         return nf;
     } catch (const std::exception &e) {
         write_err(err, e.what());
