@@ -132,6 +132,19 @@ int mk_multigrid_create(mk_space space, mk_model model, double shift,
 void mk_multigrid_destroy(mk_multigrid mg);
 /* apply(b, x): one cycle per sector             multigrid.hpp:397-403 */
 int mk_multigrid_apply(mk_multigrid mg, const double *d_b, double *d_x, void *stream);
+/* The same cycle for callers that must not allocate device memory during the call: code that
+ * runs while a stream is being captured into a CUDA graph (where cudaMalloc is not allowed),
+ * or a host that fixes its device-memory budget at start-up and forbids allocation inside its
+ * compute callbacks. This entry point has no counterpart in the reference. It calls no
+ * cudaMalloc or cudaFree: the work vectors of every level live in one static device array of
+ * 64 MiB, which every GPU that loads the library holds until the process exits. A hierarchy
+ * whose work vectors need more than that is rejected with MK_EINVAL and a message giving the
+ * size. The first call on each device looks the array's address up (cudaGetSymbolAddress), so
+ * make that first call before any stream capture. All calls share the one array and each
+ * overwrites it; calls that overlap on the GPU (different streams, or different hierarchies
+ * at once) race and give wrong results, so order them on one stream. The result equals
+ * mk_multigrid_apply's up to the summation order of the restriction. */
+int mk_multigrid_apply_noalloc(mk_multigrid mg, const double *d_b, double *d_x, void *stream);
 /* max_levels()                                  multigrid.hpp:389-395 */
 int mk_multigrid_max_levels(mk_multigrid mg, int *levels);
 int mk_multigrid_depth(mk_multigrid mg, int *depth);

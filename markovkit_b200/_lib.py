@@ -116,6 +116,7 @@ SIGNATURES = {
     "mk_multigrid_create": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
     "mk_multigrid_destroy": (None, [P]),
     "mk_multigrid_apply": (C.c_int, [P, P, P, P]),
+    "mk_multigrid_apply_noalloc": (C.c_int, [P, P, P, P]),
     "mk_multigrid_max_levels": (C.c_int, [P, IP]),
     "mk_multigrid_depth": (C.c_int, [P, IP]),
     "mk_multigrid_level_size": (C.c_int, [P, C.c_int, I64P]),

@@ -1,68 +1,15 @@
 // The C ABI (include/markovkit_b200.h) over the engine: handle bookkeeping, argument checks
 // and the mapping of C++ errors to MK_* status codes.
-#include "../../include/markovkit_b200.h"
-#include "engine.hpp"
+#include "capi_internal.hpp"
 
 #include <cstring>
 #include <string>
 
 using namespace mkb;
-
-struct mk_space_s {
-    std::unique_ptr<Space> space;
-};
-struct mk_model_s {
-    std::unique_ptr<Model> model;
-};
-struct mk_generator_s {
-    std::unique_ptr<Space> space; // private copy of the geometry the generator indexes
-    std::unique_ptr<Generator> gen;
-};
-struct mk_multigrid_s {
-    std::unique_ptr<Multigrid> mg;
-};
-struct mk_solver_s {
-    mk_generator gen = nullptr;
-    mk_multigrid mg = nullptr;
-    double shift = 0.0;
-    GmresOptions opt;
-    std::unique_ptr<Krylov> ws;
-    DeviceArray<double> b, x; // staging for host-vector solves
-};
-
-namespace {
-
-thread_local std::string g_last_error;
-
-int fail(int code, const std::string &what) {
-    g_last_error = what;
-    return code;
-}
-
-template <typename F>
-int guarded(F &&f) {
-    try {
-        f();
-        return MK_OK;
-    } catch (const Error &e) {
-        return fail(e.code, e.what());
-    } catch (const std::bad_alloc &) {
-        return fail(MK_ENOMEM, "host allocation failed");
-    } catch (const std::exception &e) {
-        return fail(MK_EINVAL, e.what());
-    }
-}
-
-cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
-
-#define MK_REQUIRE(cond, msg)                                                                      \
-    do {                                                                                           \
-        if (!(cond)) {                                                                             \
-            throw Error(MK_EINVAL, msg);                                                           \
-        }                                                                                          \
-    } while (0)
-
-} // namespace
+using mkb::capi::as_stream;
+using mkb::capi::fail;
+using mkb::capi::g_last_error;
+using mkb::capi::guarded;
 
 extern "C" {
 

@@ -1,0 +1,66 @@
+// Internal to the C ABI: the handle types behind include/markovkit_b200.h and the mapping of
+// C++ errors to MK_* status codes, shared by the translation units that implement entry points.
+#pragma once
+
+#include "../../include/markovkit_b200.h"
+#include "engine.hpp"
+
+#include <new>
+#include <string>
+
+struct mk_space_s {
+    std::unique_ptr<mkb::Space> space;
+};
+struct mk_model_s {
+    std::unique_ptr<mkb::Model> model;
+};
+struct mk_generator_s {
+    std::unique_ptr<mkb::Space> space; // private copy of the geometry the generator indexes
+    std::unique_ptr<mkb::Generator> gen;
+};
+struct mk_multigrid_s {
+    std::unique_ptr<mkb::Multigrid> mg;
+};
+struct mk_solver_s {
+    mk_generator gen = nullptr;
+    mk_multigrid mg = nullptr;
+    double shift = 0.0;
+    mkb::GmresOptions opt;
+    std::unique_ptr<mkb::Krylov> ws;
+    mkb::DeviceArray<double> b, x; // staging for host-vector solves
+};
+
+namespace mkb::capi {
+
+// the message of the calling thread's last failure (mk_last_error)
+inline thread_local std::string g_last_error;
+
+inline int fail(int code, const std::string &what) {
+    g_last_error = what;
+    return code;
+}
+
+template <typename F>
+int guarded(F &&f) {
+    try {
+        f();
+        return MK_OK;
+    } catch (const Error &e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(MK_ENOMEM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(MK_EINVAL, e.what());
+    }
+}
+
+inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+} // namespace mkb::capi
+
+#define MK_REQUIRE(cond, msg)                                                                      \
+    do {                                                                                           \
+        if (!(cond)) {                                                                             \
+            throw ::mkb::Error(MK_EINVAL, msg);                                                    \
+        }                                                                                          \
+    } while (0)

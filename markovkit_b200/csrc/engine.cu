@@ -497,6 +497,9 @@ int Multigrid::levels_of_sector(int k) const {
 
 template <typename T>
 T *Multigrid::buf(Level &L, int which) {
+    if (use_carved_) {
+        return static_cast<T *>(L.carved[which]);
+    }
     if constexpr (std::is_same_v<T, double>) {
         switch (which) {
         case 0:
@@ -720,6 +723,69 @@ void Multigrid::ensure_graph() {
     e = cudaGraphInstantiate(&graph_exec_, graph, 0);
     cudaGraphDestroy(graph);
     check_cuda(e, "multigrid graph instantiate");
+}
+
+namespace {
+constexpr std::size_t kCarveAlign = 256;
+std::size_t carve_round(std::size_t bytes) { return (bytes + kCarveAlign - 1) / kCarveAlign * kCarveAlign; }
+} // namespace
+
+std::size_t Multigrid::scratch_bytes() const {
+    const std::size_t w = opt.precision == 0 ? sizeof(double) : sizeof(float);
+    std::size_t total = 0;
+    for (std::size_t d = 0; d < levels.size(); ++d) {
+        const auto nd = static_cast<std::size_t>(levels[d]->op.n);
+        total += 4 * carve_round(nd * w); // rhs, x, tmp, r
+        if (opt.coarse_cycles > 1 && d + 1 < levels.size()) {
+            total += 2 * carve_round(static_cast<std::size_t>(levels[d + 1]->op.n) * w); // acc, crhs
+        }
+    }
+    return total;
+}
+
+void Multigrid::apply_in(const double *b, double *x, void *scratch, std::size_t bytes,
+                         cudaStream_t stream) {
+    if (bytes < scratch_bytes() || (reinterpret_cast<std::uintptr_t>(scratch) % kCarveAlign) != 0) {
+        throw Error(kEInval, "multigrid scratch too small or misaligned");
+    }
+    const std::size_t w = opt.precision == 0 ? sizeof(double) : sizeof(float);
+    auto *base = static_cast<unsigned char *>(scratch);
+    std::size_t off = 0;
+    for (std::size_t d = 0; d < levels.size(); ++d) {
+        Level &L = *levels[d];
+        const std::size_t vec = carve_round(static_cast<std::size_t>(L.op.n) * w);
+        for (int k = 0; k < 4; ++k) {
+            L.carved[k] = base + off;
+            off += vec;
+        }
+        L.carved[4] = L.carved[5] = nullptr;
+        if (opt.coarse_cycles > 1 && d + 1 < levels.size()) {
+            const std::size_t cvec = carve_round(static_cast<std::size_t>(levels[d + 1]->op.n) * w);
+            L.carved[4] = base + off;
+            off += cvec;
+            L.carved[5] = base + off;
+            off += cvec;
+        }
+    }
+    struct Restore {
+        bool &flag;
+        ~Restore() { flag = false; }
+    } restore{use_carved_};
+    use_carved_ = true;
+    Level &L0 = *levels[0];
+    const auto n0 = static_cast<std::int64_t>(L0.op.n);
+    if (opt.precision == 0) {
+        check_cuda(cudaMemcpyAsync(buf<double>(L0, 0), b, n0 * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, stream),
+                   "copy");
+        double *out = cycle<double>(0, stream);
+        check_cuda(cudaMemcpyAsync(x, out, n0 * sizeof(double), cudaMemcpyDeviceToDevice, stream),
+                   "copy");
+    } else {
+        check_cuda(convert<double, float>(b, buf<float>(L0, 0), n0, stream), "convert");
+        float *out = cycle<float>(0, stream);
+        check_cuda(convert<float, double>(out, x, n0, stream), "convert");
+    }
 }
 
 Multigrid::~Multigrid() {

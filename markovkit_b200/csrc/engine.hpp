@@ -176,6 +176,7 @@ struct Multigrid {
         DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
         DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
         std::vector<int> box_sector; // box sector of each slot
+        void *carved[6] = {};        // work vectors in caller memory (apply_in)
     };
     MultigridOptions opt;
     double shift = 0.0;
@@ -191,6 +192,12 @@ struct Multigrid {
     Multigrid &operator=(const Multigrid &) = delete;
     // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
     void apply(const double *b, double *x, cudaStream_t stream);
+    // bytes of work vectors one cycle needs, each vector aligned to 256 bytes
+    [[nodiscard]] std::size_t scratch_bytes() const;
+    // the same cycle with every work vector carved from caller-given device memory of at
+    // least scratch_bytes(); plain launches, nothing allocated
+    void apply_in(const double *b, double *x, void *scratch, std::size_t bytes,
+                  cudaStream_t stream);
     [[nodiscard]] int n_levels() const { return static_cast<int>(levels.size()); }
     [[nodiscard]] int levels_of_sector(int k) const;
     // FP64 hooks on one depth: population_transfer restrict (direction 0) or prolong (1)
@@ -205,6 +212,7 @@ struct Multigrid {
     T *buf(Level &L, int which);
     void ensure_graph();
     cudaGraphExec_t graph_exec_ = nullptr;
+    bool use_carved_ = false;
 };
 
 struct GmresOptions {
