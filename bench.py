@@ -235,8 +235,10 @@ def run_ours(args) -> dict | None:
         sampler = ClockSampler(_uuid(dev)) if precision == "fp32" else None
         if sampler:
             sampler.__enter__()
+        launches0 = mk.api.kernel_launches()
         lat, its, conv, xs = solve_all(solver, range(W, W + K))
         torch.cuda.synchronize()
+        launches = mk.api.kernel_launches() - launches0
         if sampler:
             sampler.__exit__(None, None, None)
         worst = max(true_rel(x, W + i) for i, x in enumerate(xs))
@@ -247,7 +249,8 @@ def run_ours(args) -> dict | None:
             total_ms = float(t.item())
         results[precision] = dict(
             lat=lat, its=its, converged=all(conv), worst_true_rel=worst, total_ms=total_ms,
-            clocks=sampler.summary() if sampler else None, M=M, solver=solver,
+            clocks=sampler.summary() if sampler else None, M=M, solver=solver, xs=xs,
+            launches=launches,
         )
         if precision == "fp32":
             # e2e through the C ABI with host buffers
@@ -261,12 +264,15 @@ def run_ours(args) -> dict | None:
                                   worst_true_rel=max(true_rel(x, W + i) for i, x in enumerate(xs_h)))
             # the same solution as the FP64 oracle path is checked below
 
-    # error of the FP32-MG solution against the FP64 path's solution on the first right-hand side
+    # error of each FP32-MG solution against the FP64 path's solution of the same right-hand side
     r32 = results["fp32"]
     r64 = results["fp64"]
+    err_vs_fp64 = max(
+        float(torch.linalg.norm(a - b64) / torch.linalg.norm(b64)) for a, b64 in zip(r32["xs"], r64["xs"])
+    )
 
     roof = roofline(mk, Q, M=results["fp32"]["M"], dev=dev, N=N)
-    launches = count_launches(results["fp32"])
+    launches = r32["launches"]
 
     if rank != 0:
         return None
@@ -299,6 +305,7 @@ def run_ours(args) -> dict | None:
         "latency_ms": {"p50": round(pct(50), 4), "p99": round(pct(99), 4)},
         "iterations": {"median": int(np.median(r32["its"])), "max": int(max(r32["its"]))},
         "worst_true_rel_residual": r32["worst_true_rel"],
+        "rel_error_vs_fp64_path": err_vs_fp64,
         "fp64_path": {
             "value": round(world * K / (r64["total_ms"] / 1e3), 3),
             "unit": "solves/s",
@@ -336,31 +343,53 @@ def _uuid(dev) -> str | None:
         return None
 
 
-def roofline(mk, Q, M, dev, N) -> dict:
-    """The generator SpMV (FP64 apply_shifted over the whole box), timed alone with CUDA events
-    on its launch stream: algorithmic bytes = N * (8 read + 8 write)."""
+def _time_apply(Q, N, dev, flush=None, reps=20) -> float:
+    """Average ms of one FP64 apply_shifted, CUDA events on its launch stream, each launch timed
+    on its own (L2 flushed before each when `flush` is given)."""
     import torch
 
     x = torch.rand(N, dtype=torch.float64, device=dev)
     y = torch.empty_like(x)
-    for _ in range(5):
+    for _ in range(3):
         Q.apply_shifted(1.0, x, y)
     torch.cuda.synchronize()
-    reps = 50
     stream = torch.cuda.current_stream()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    total = 0.0
     for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         Q.apply_shifted(1.0, x, y)
-    e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / reps
-    algo = N * 16
-    achieved = algo / (ms * 1e-3) / 1e9
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total / reps
+
+
+def roofline(mk, Q, M, dev, N) -> dict:
+    """The generator SpMV, the kernel the north star's roofline target names, on the 3-D
+    16^3-voxel box of cap 2 (8,394,753 states): FP64 apply_shifted, one compulsory read of x and
+    write of y, 16 bytes per state (134 MB per launch, larger than L2), L2 flushed before each
+    timed launch. The bench workload's own SpMV (16.8 MB, L2-resident) is reported beside it."""
+    import torch
+
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     pk = peaks()
+    w = WORKLOADS["birth_death_3d16"]
+    dom = mk.voxel_domain(mk.grid([16] * 3, [1 / 16] * 3), w["D"])
+    model = mk.reaction_diffusion(dom, [mk.local_reaction(c, f) for c, f in reactions_of(w)])
+    box = mk.population_box(4096, w["caps"])
+    Q3 = mk.generator(box, model, "absorbing")
+    N3 = box.size()
+    ms = _time_apply(Q3, N3, dev, flush)
+    algo = N3 * 16
+    achieved = algo / (ms * 1e-3) / 1e9
+    ms_w = _time_apply(Q, N, dev, None)
+    achieved_w = N * 16 / (ms_w * 1e-3) / 1e9
     return {
-        "kernel": "generator apply_shifted (FP64 gather SpMV, row_kernel<double,4,kApplyShifted>)",
+        "kernel": "generator apply_shifted, FP64 gather SpMV (row_kernel<double,1,2>), 3-D 16^3 box cap 2",
         "bound": "hbm",
         "achieved": round(achieved, 1),
         "peak": pk["hbm_gbs"],
@@ -370,19 +399,49 @@ def roofline(mk, Q, M, dev, N) -> dict:
         "traffic": None,
         "us_per_launch": round(ms * 1e3, 3),
         "algorithmic_bytes_per_launch": algo,
+        "workload_spmv": {"kernel": "row_kernel<double,2,1>", "us_per_launch": round(ms_w * 1e3, 3),
+                          "achieved_gbs": round(achieved_w, 1), "note": "16.8 MB per launch, L2-resident"},
     }
 
 
-def count_launches(r) -> int | None:
-    return None
+def _problem_args(w: dict) -> list[str]:
+    keys = {"dim": w["dim"], "cells": w["cells"], "cap": ",".join(str(c) for c in w["caps"]), "model": w["model"],
+            "shift": w["shift"], "D": w["D"][0]}
+    if len(w["D"]) > 1:
+        keys["D2"] = w["D"][1]
+    for k in ("birth", "death", "k"):
+        if k in w:
+            keys[k] = w[k]
+    return [f"{k}={v}" for k, v in keys.items()]
 
 
 def cpu_baseline(w) -> dict:
-    """Bounded sample of the same workload on this host's cores (the CPU port)."""
-    return {"value": None, "unit": "solves/s", "cores": None, "kind": "port", "sample": "not yet measured"}
+    """The matrix-free CPU port (oracle/_ref/mf_port, a restatement of the reference's path
+    validated against it) on this host's cores: full solves of the same workload, setup excluded."""
+    port = ROOT / "oracle" / "_ref" / "mf_port"
+    if not port.exists():
+        return {"value": None, "unit": "solves/s", "cores": None, "kind": "port", "sample": "oracle/_ref/mf_port not built"}
+    threads = os.cpu_count() or 1
+    solves = 2
+    args = [str(port), *_problem_args(w), f"rhs={w['rhs']}", f"seed={w['seed']}", "tol=1e-10",
+            f"restart={RESTART}", f"threads={threads}", f"solves={solves}"]
+    proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
+    if proc.returncode != 0:
+        return {"value": None, "unit": "solves/s", "cores": threads, "kind": "port", "sample": proc.stderr[-200:]}
+    m = json.loads(proc.stdout.strip().splitlines()[-1])
+    secs = sum(m["solve_ms"]) / 1e3
+    return {
+        "value": round(solves / secs, 5), "unit": "solves/s", "cores": m["threads"], "kind": "port",
+        "sample": f"{solves} full solves ({m['iterations']} MG-GMRES iterations each, true rel. residual "
+                  f"{m['true_rel_residual']:.2e}) after an untimed {m['setup_ms'] / 1e3:.1f} s set-up",
+    }
 
 
 def run_reference(args) -> None:
+    """The reference's own CPU path (MarkovKit headers + numerics shim, oracle/_ref/ref_driver),
+    single-threaded as the reference is. Its set-up (population_box, generator, sector_multigrid)
+    runs untimed once; one full solve gives the iteration count; each step is a bounded sample of
+    SAMPLE_ITERS Arnoldi iterations, and solves/sec = SAMPLE_ITERS / (iterations * step time)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -391,7 +450,36 @@ def run_reference(args) -> None:
     if not driver.exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver is not built"}))
         return
-    print(json.dumps({"impl": "reference", "unavailable": "not wired yet"}))
+    sample_iters = 6
+    K, W = args.steps, args.warmup
+    with tempfile.TemporaryDirectory() as tmp:
+        cmd = [str(driver), *_problem_args(w), f"rhs={w['rhs']}", f"seed={w['seed']}", "tol=1e-10",
+               f"restart={RESTART}", "do_apply=0", "do_plain=0", "warmup=1", f"solves={W + K}",
+               f"sample_iters={sample_iters}", f"out={tmp}"]
+        t0 = time.time()
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        wall = time.time() - t0
+    if proc.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": "ref_driver failed: " + proc.stderr[-200:].replace("\n", " ")}))
+        return
+    m = json.loads(proc.stdout.strip().splitlines()[-1])
+    its = m["full_solve_iterations"]
+    steps_ms = m["gmres_mg"]["solve_ms"][W:]
+    per_solve_s = (sum(steps_ms) / len(steps_ms)) / 1e3 * its / sample_iters
+    value = 1.0 / per_solve_s
+    sample = (f"each step: {sample_iters} of the {its} MG-GMRES iterations of a full solve, scaled; "
+              f"untimed set-up {(m['box_ms'] + m['generator_ms'] + m['mg_setup_ms']) / 1e3:.0f} s")
+    line = {
+        "metric": "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)",
+        "impl": "reference", "value": round(value, 5), "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": K, "warmup": W, "ms_per_step": round(per_solve_s * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded right-hand side",
+        "config": {"workload": w["workload"], "states": m["N"], "parallelism": "1 host thread"},
+        "cpu_baseline": {"value": round(value, 5), "unit": "solves/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": round(value, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(wall, 1),
+    }
+    print(json.dumps(line), flush=True)
 
 
 def main() -> None:

@@ -42,6 +42,8 @@ typedef struct mk_solver_s *mk_solver;
 
 const char *mk_last_error(void);
 int mk_version(void);
+/* kernels this library has launched in this process (a graph launch counts its kernel nodes) */
+int mk_kernel_launches(uint64_t *count);
 
 /* ---- device memory helpers (for callers without their own CUDA runtime) ---- */
 int mk_device_alloc(size_t bytes, void **d_ptr);

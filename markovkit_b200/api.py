@@ -382,6 +382,13 @@ class sector_multigrid(_Handle):
         return y
 
 
+def kernel_launches() -> int:
+    """Kernels the library has launched in this process (graph launches count their nodes)."""
+    v = C.c_uint64()
+    check(load().mk_kernel_launches(C.byref(v)))
+    return v.value
+
+
 def gmres_options(tolerance: float = 1e-8, max_iterations: int = 1000, restart: int = 30, flexible: bool = False) -> GmresOptions:
     o = GmresOptions()
     o.tolerance = float(tolerance)

@@ -17,6 +17,13 @@ const char *mk_last_error(void) { return g_last_error.c_str(); }
 
 int mk_version(void) { return 1; }
 
+int mk_kernel_launches(uint64_t *count) {
+    return guarded([&] {
+        MK_REQUIRE(count, "null argument");
+        *count = g_kernel_launches.load(std::memory_order_relaxed);
+    });
+}
+
 int mk_device_alloc(size_t bytes, void **d_ptr) {
     return guarded([&] {
         MK_REQUIRE(d_ptr, "null output pointer");

@@ -275,6 +275,7 @@ void axpy_t(T a, const T *x, T *y, std::int64_t n, cudaStream_t stream) {
     }
     const std::int64_t want = (n + 255) / 256;
     const auto blocks = static_cast<unsigned>(std::min<std::int64_t>(want, 148 * 8));
+    count_launches(1);
     axpy_t_kernel<T><<<blocks, 256, 0, stream>>>(a, x, y, n);
     check_cuda(cudaGetLastError(), "axpy");
 }
@@ -720,6 +721,17 @@ void Multigrid::ensure_graph() {
     }
     cudaStreamDestroy(cap);
     check_cuda(e, "multigrid graph capture");
+    std::size_t n_nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &n_nodes);
+    std::vector<cudaGraphNode_t> nodes(n_nodes);
+    cudaGraphGetNodes(graph, nodes.data(), &n_nodes);
+    graph_kernels_ = 0;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) {
+            ++graph_kernels_;
+        }
+    }
     e = cudaGraphInstantiate(&graph_exec_, graph, 0);
     cudaGraphDestroy(graph);
     check_cuda(e, "multigrid graph instantiate");
@@ -803,6 +815,7 @@ void Multigrid::apply(const double *b, double *x, cudaStream_t stream) {
                                    stream),
                    "copy");
         check_cuda(cudaGraphLaunch(graph_exec_, stream), "multigrid graph launch");
+        count_launches(graph_kernels_);
         check_cuda(cudaMemcpyAsync(x, L0.x64.get(), n0 * sizeof(double), cudaMemcpyDeviceToDevice,
                                    stream),
                    "copy");
@@ -810,6 +823,7 @@ void Multigrid::apply(const double *b, double *x, cudaStream_t stream) {
         check_cuda(convert<double, float>(b, L0.rhs32.get(), static_cast<std::int64_t>(n0), stream),
                    "convert");
         check_cuda(cudaGraphLaunch(graph_exec_, stream), "multigrid graph launch");
+        count_launches(graph_kernels_);
         check_cuda(convert<float, double>(L0.x32.get(), x, static_cast<std::int64_t>(n0), stream),
                    "convert");
     }

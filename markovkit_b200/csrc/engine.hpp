@@ -5,6 +5,7 @@
 
 #include "host_model.hpp"
 #include "krylov.cuh"
+#include "launch_count.hpp"
 #include "row_kernels.cuh"
 
 #include <cstdint>
@@ -212,6 +213,7 @@ struct Multigrid {
     T *buf(Level &L, int which);
     void ensure_graph();
     cudaGraphExec_t graph_exec_ = nullptr;
+    std::uint64_t graph_kernels_ = 0; // kernel nodes of the captured cycle
     bool use_carved_ = false;
 };
 

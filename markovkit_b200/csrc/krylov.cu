@@ -1,5 +1,6 @@
 // sm_100a Krylov kernels. All are HBM-bound streaming passes over the Arnoldi basis.
 #include "krylov.cuh"
+#include "launch_count.hpp"
 
 #include <cmath>
 
@@ -102,6 +103,7 @@ __global__ void finalize_kernel(const double *partials, int nb, int K, double *o
 template <int KMAX, int MODE>
 cudaError_t launch_cgs(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
                        const double *coef, double *partials, double *out, cudaStream_t stream) {
+    count_launches(MODE != 3 ? 2 : 1);
     cgs_kernel<KMAX, MODE><<<kDotBlocks, kDotThreads, 0, stream>>>(V, ld, K, w, n, coef, partials);
     if (MODE != 3) {
         finalize_kernel<<<1, 1024, 0, stream>>>(partials, kDotBlocks, MODE == 2 ? 1 : K, out);
@@ -248,29 +250,34 @@ cudaError_t dot(const double *a, const double *b, std::int64_t n, double *partia
 
 cudaError_t scale_copy(const double *x, const double *scale, double *y, std::int64_t n,
                        cudaStream_t stream) {
+    count_launches(1);
     scale_copy_kernel<<<stream_blocks(n), 256, 0, stream>>>(x, scale, y, n);
     return cudaGetLastError();
 }
 
 cudaError_t multi_axpy(const double *V, std::int64_t ld, int K, const double *coef, double *y,
                        std::int64_t n, cudaStream_t stream) {
+    count_launches(1);
     multi_axpy_kernel<true><<<stream_blocks(n), 256, 0, stream>>>(V, ld, K, coef, y, n);
     return cudaGetLastError();
 }
 
 cudaError_t multi_combine(const double *V, std::int64_t ld, int K, const double *coef, double *y,
                           std::int64_t n, cudaStream_t stream) {
+    count_launches(1);
     multi_axpy_kernel<false><<<stream_blocks(n), 256, 0, stream>>>(V, ld, K, coef, y, n);
     return cudaGetLastError();
 }
 
 cudaError_t axpy(double a, const double *x, double *y, std::int64_t n, cudaStream_t stream) {
+    count_launches(1);
     axpy_kernel<<<stream_blocks(n), 256, 0, stream>>>(a, x, y, n);
     return cudaGetLastError();
 }
 
 template <typename A, typename B>
 cudaError_t convert(const A *x, B *y, std::int64_t n, cudaStream_t stream) {
+    count_launches(1);
     convert_kernel<A, B><<<stream_blocks(n), 256, 0, stream>>>(x, y, n);
     return cudaGetLastError();
 }
@@ -278,16 +285,19 @@ template cudaError_t convert<double, float>(const double *, float *, std::int64_
 template cudaError_t convert<float, double>(const float *, double *, std::int64_t, cudaStream_t);
 
 cudaError_t arnoldi_start(const ArnoldiState &s, cudaStream_t stream) {
+    count_launches(1);
     arnoldi_start_kernel<<<1, 1, 0, stream>>>(s);
     return cudaGetLastError();
 }
 
 cudaError_t arnoldi_column(const ArnoldiState &s, int j, cudaStream_t stream) {
+    count_launches(1);
     arnoldi_column_kernel<<<1, 1, 0, stream>>>(s, j);
     return cudaGetLastError();
 }
 
 cudaError_t arnoldi_solve(const ArnoldiState &s, int k, cudaStream_t stream) {
+    count_launches(1);
     arnoldi_solve_kernel<<<1, 1, 0, stream>>>(s, k);
     return cudaGetLastError();
 }

@@ -1,5 +1,6 @@
 // Dispatch of the row kernels (instantiated in row_kernels_f64.cu / row_kernels_f32.cu), the
 // dense terminal solve of the multigrid, and bit-exact state indexing on the device.
+#include "launch_count.hpp"
 #include "row_kernels.cuh"
 
 namespace mkb {
@@ -161,6 +162,7 @@ cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, const T *
     if (n_blocks == 0) {
         return cudaSuccess;
     }
+    count_launches(1);
     terminal_kernel<T><<<n_blocks, 128, 0, stream>>>(blocks, inv, r, x);
     return cudaGetLastError();
 }
@@ -178,6 +180,7 @@ cudaError_t launch_unrank(const BinomTable &B, const SectorDesc *sectors, int n_
     }
     const int threads = 128;
     const auto blocks = static_cast<unsigned>((count + threads - 1) / threads);
+    count_launches(1);
     unrank_kernel<<<blocks, threads, 0, stream>>>(B, sectors, n_sectors, S, V, index, count,
                                                   states);
     return cudaGetLastError();
@@ -191,6 +194,7 @@ cudaError_t launch_rank(const BinomTable &B, const SectorDesc *sectors, int n_se
     }
     const int threads = 128;
     const auto blocks = static_cast<unsigned>((count + threads - 1) / threads);
+    count_launches(1);
     rank_kernel<<<blocks, threads, 0, stream>>>(B, sectors, n_sectors, max_totals, is_box, S, V,
                                                 states, count, index);
     return cudaGetLastError();

@@ -6,6 +6,7 @@
 // Instantiated per precision in row_kernels_f64.cu and row_kernels_f32.cu.
 #pragma once
 
+#include "launch_count.hpp"
 #include "row_kernels.cuh"
 
 namespace mkb {
@@ -196,6 +197,7 @@ cudaError_t launch_shape(const RowParams<T> &p, cudaStream_t stream) {
     if (p.n_tiles == 0) {
         return cudaSuccess;
     }
+    count_launches(1);
     row_kernel<T, NS, TMAX><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }

@@ -215,17 +215,29 @@ int run(const args &a) {
                 .max_iterations = static_cast<idx>(a.integer("maxit", 1000)),
                 .restart = static_cast<idx>(a.integer("restart", 30))};
             const long warmup = a.integer("warmup", 0), solves = a.integer("solves", 1);
+            // sample_iters > 0: after the warm-up solves, each timed solve stops after this many
+            // Arnoldi steps (a bounded sample of a full solve)
+            const long sample = a.integer("sample_iters", 0);
             std::vector<double> solve_ms;
             vec<real> x(N, 0.0);
-            num::solver_result result;
+            num::solver_result result, full;
             for (long s = 0; s < warmup + solves; ++s) {
                 std::fill(x.begin(), x.end(), 0.0);
+                num::gmres_options run = options;
+                if (sample > 0 && s >= warmup) {
+                    run.max_iterations = static_cast<idx>(sample);
+                }
                 t0 = clock_type::now();
-                result = num::gmres(A, M, b, x, options);
+                result = num::gmres(A, M, b, x, run);
                 const double t = ms_since(t0);
                 if (s >= warmup) {
                     solve_ms.push_back(t);
+                } else {
+                    full = result;
                 }
+            }
+            if (warmup > 0) {
+                meta << ",\"full_solve_iterations\":" << full.iterations;
             }
             vec<real> r(N, 0.0);
             A.apply(x, r);
