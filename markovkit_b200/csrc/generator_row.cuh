@@ -46,7 +46,31 @@ struct ModelView {
     int nvc = 1;
     unsigned heavy_mask = 0;  // reactions with in-jumps from empty voxels
     unsigned nonneg_mask = 0; // reactions that can fire from an empty voxel
+    // structured grid with one cell volume: neighbours and coefficients by arithmetic
+    int grid_dim = 0;         // 0: use the CSR lists above
+    int gdims[3] = {1, 1, 1};
+    int gstride[3] = {1, 1, 1};
+    float ginv[3] = {1, 1, 1}; // 1 / gdims for coordinate division
+    T axis_coef[3] = {};       // weight / volume of an edge along each axis
 };
+
+// q = v / d for 0 <= v < 2^24 from a float reciprocal and one correction
+MK_HD int div_small(int v, int d, float inv) {
+    int q = static_cast<int>(static_cast<float>(v) * inv);
+    q -= (q * d > v) ? 1 : 0;
+    q += ((q + 1) * d <= v) ? 1 : 0;
+    return q;
+}
+
+// coordinates of voxel v on a structured grid (axis 0 fastest)
+template <typename T>
+MK_HD void grid_coords(const ModelView<T> &md, int v, int (&c)[3]) {
+    const int q0 = div_small(v, md.gdims[0], md.ginv[0]);
+    c[0] = v - q0 * md.gdims[0];
+    const int q1 = div_small(q0, md.gdims[1], md.ginv[1]);
+    c[1] = q0 - q1 * md.gdims[1];
+    c[2] = q1;
+}
 
 template <typename T>
 MK_HD T load_ro(const T *p) {
@@ -160,6 +184,139 @@ MK_HD int reaction_source(const BinomTable &B, const ModelView<T> &md, const Sec
     return src;
 }
 
+// Diffusion of species s: each molecule's exit rate, and the in-jumps into its voxel from each
+// neighbour w (the source state has one molecule of that voxel moved to w). A run of equal
+// molecules is entered once per neighbour: from above through its last copy, from below
+// through its first. When the moved molecule keeps its place in the sorted list, the source
+// rank differs by C(u' + p, p + 1) - C(u + p, p + 1) for its position p; only a move past a
+// neighbouring molecule re-ranks the whole list (lists of up to two use a closed form).
+// On a structured grid the neighbours and edge coefficients are arithmetic, not loaded.
+template <typename T, int NS, int TMAX, bool WANT_IN, typename Acc>
+MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const SectorDesc &sec,
+                           const RowState<NS, TMAX> &st, int s, int row, T &exit, Acc &acc) {
+    const int t = sec.total[s];
+    const int V = md.V;
+    const T Ds = md.diff[s];
+    const int stride = static_cast<int>(sec.stride[s]);
+    const int(&u)[TMAX] = st.u[s];
+    auto one = [&](auto P) {
+        constexpr int p = decltype(P)::value;
+        if (p >= t) {
+            return;
+        }
+        const int uu = u[p];
+        const int v = V - 1 - uu;
+        const bool first = p == 0 || u[p > 0 ? p - 1 : 0] != uu;
+        const bool last = p + 1 >= t || u[p + 1 < TMAX ? p + 1 : p] != uu;
+        const int lo = p > 0 ? u[p > 0 ? p - 1 : 0] : -1;
+        const int hi = p + 1 < t ? u[p + 1 < TMAX ? p + 1 : p] : 0x7fffffff;
+        constexpr int J = p + 1 <= 4 ? p + 1 : 4;
+        // the in-jump from the neighbour whose reversed index is uw, with edge coefficient coef
+        auto in_jump = [&](int uw, T coef) {
+            const bool up = uw > uu;
+            if (up ? !last : !first) {
+                return;
+            }
+            const int nw = count_of<TMAX>(u, t, uw);
+            const T rate = T(nw + 1) * Ds * coef;
+            int delta;
+            if constexpr (TMAX <= 2) {
+                delta = static_cast<int>(rank_replace<TMAX>(B, u, t, uu, uw)) - st.rank[s];
+            } else if (up ? uw <= hi : uw >= lo) {
+                delta = static_cast<int>(binom_j<J>(uw + p) - binom_j<J>(uu + p));
+            } else {
+                delta = static_cast<int>(rank_replace<TMAX>(B, u, t, uu, uw)) - st.rank[s];
+            }
+            acc(row + delta * stride, rate);
+        };
+        if (md.grid_dim > 0) {
+            int c[3];
+            grid_coords(md, v, c);
+            T deg = T(0);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a >= md.grid_dim) {
+                    continue;
+                }
+                const bool has_lo = c[a] > 0, has_hi = c[a] + 1 < md.gdims[a];
+                deg += T((has_lo ? 1 : 0) + (has_hi ? 1 : 0)) * md.axis_coef[a];
+                if constexpr (WANT_IN) {
+                    // neighbour v - stride has reversed index uu + stride, v + stride uu - stride
+                    if (has_lo && (first || last)) {
+                        in_jump(uu + md.gstride[a], md.axis_coef[a]);
+                    }
+                    if (has_hi && (first || last)) {
+                        in_jump(uu - md.gstride[a], md.axis_coef[a]);
+                    }
+                }
+            }
+            exit += Ds * deg;
+            return;
+        }
+        exit += Ds * load_ro(md.deg_coef + v);
+        if constexpr (WANT_IN) {
+            if (!first && !last) {
+                return;
+            }
+            const int e0 = load_ro(md.nbr_ptr + v), e1 = load_ro(md.nbr_ptr + v + 1);
+            for (int e = e0; e < e1; ++e) {
+                in_jump(V - 1 - load_ro(md.nbr_idx + e), load_ro(md.in_coef + e));
+            }
+        }
+    };
+    if constexpr (TMAX <= 4) {
+        static_for<TMAX>(one);
+    } else {
+        // long lists: a plain loop over the CSR lists, re-ranking every in-jump
+        for (int p = 0; p < t; ++p) {
+            const int uu = u[p];
+            const int v = V - 1 - uu;
+            exit += Ds * load_ro(md.deg_coef + v);
+            if constexpr (WANT_IN) {
+                const bool first = p == 0 || u[p - 1] != uu;
+                const bool last = p + 1 >= t || u[p + 1] != uu;
+                const int e0 = load_ro(md.nbr_ptr + v), e1 = load_ro(md.nbr_ptr + v + 1);
+                for (int e = e0; e < e1; ++e) {
+                    const int uw = V - 1 - load_ro(md.nbr_idx + e);
+                    if (uw > uu ? !last : !first) {
+                        continue;
+                    }
+                    const int nw = count_of<TMAX>(u, t, uw);
+                    const T rate = T(nw + 1) * Ds * load_ro(md.in_coef + e);
+                    const int delta =
+                        static_cast<int>(rank_replace<TMAX>(B, u, t, uu, uw)) - st.rank[s];
+                    acc(row + delta * stride, rate);
+                }
+            }
+        }
+    }
+}
+
+// rank of the list with one more copy of `value`: an element left of the insertion point keeps
+// its position (A_i = C(u_i + i, i + 1)), one right of it moves up one (B_i = C(u_i + i + 1,
+// i + 2)); the new element lands after the b smaller ones. A and B are per-row constants.
+template <int TMAX>
+MK_HD std::int64_t rank_inserted(const int (&u)[TMAX], int t, const std::int64_t (&A)[TMAX],
+                                 const std::int64_t (&Bc)[TMAX], int value) {
+    std::int64_t r = 0;
+    int b = 0;
+#pragma unroll
+    for (int i = 0; i < TMAX; ++i) {
+        if (i < t) {
+            const bool left = u[i] < value;
+            r += left ? A[i] : Bc[i];
+            b += left ? 1 : 0;
+        }
+    }
+    std::int64_t mine = 0;
+    static_for<TMAX + 1>([&](auto Q) {
+        constexpr int q = decltype(Q)::value;
+        constexpr int J = q + 1 <= 4 ? q + 1 : 4;
+        mine = b == q ? binom_j<J>(value + q) : mine;
+    });
+    return r + mine;
+}
+
 // Visit the row: acc(source_index, rate) for every in-jump; adds into exit and leak.
 // light: the exit/leak terms and the in-jumps that start in occupied voxels.
 // [lane, V) step nlanes: the all-voxel loop of heavy reactions.
@@ -184,12 +341,18 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                 }
             }
         }
-        // each distinct occupied voxel once: (species s, position p) is its first occurrence
+        // diffusion, molecule by molecule: out of its voxel, and into it from each neighbour
+        const int row = static_cast<int>(sec.begin + local);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            diffusion_terms<T, NS, TMAX, WANT_IN>(B, md, sec, st, s, row, exit, acc);
+        }
+        // reactions: each distinct occupied voxel once, at the first occurrence (s, p) of it
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             MK_UNROLL_MOL
             for (int p = 0; p < TMAX; ++p) {
-                if (p >= sec.total[s]) {
+                if (R == 0 || p >= sec.total[s]) {
                     continue;
                 }
                 const int uu = st.u[s][p];
@@ -211,31 +374,6 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                 for (int s2 = 0; s2 < NS; ++s2) {
                     n[s2] = count_of<TMAX>(st.u[s2], sec.total[s2], uu);
                     ti += n[s2] * md.tstride[s2];
-                }
-                // diffusion: out of v, and into v from each neighbour
-                const int e0 = load_ro(md.nbr_ptr + v), e1 = load_ro(md.nbr_ptr + v + 1);
-                const T deg = load_ro(md.deg_coef + v);
-#pragma unroll
-                for (int s3 = 0; s3 < NS; ++s3) {
-                    if (n[s3] == 0) {
-                        continue;
-                    }
-                    exit += T(n[s3]) * md.diff[s3] * deg;
-                    if constexpr (WANT_IN) {
-                        for (int e = e0; e < e1; ++e) {
-                            const int uw = V - 1 - load_ro(md.nbr_idx + e);
-                            const int nw = count_of<TMAX>(st.u[s3], sec.total[s3], uw);
-                            const T rate = T(nw + 1) * md.diff[s3] * load_ro(md.in_coef + e);
-                            const int r2 = static_cast<int>(
-                                rank_replace<TMAX>(B, st.u[s3], sec.total[s3], uu, uw));
-                            acc(static_cast<int>(sec.begin + local) +
-                                    (r2 - st.rank[s3]) * static_cast<int>(sec.stride[s3]),
-                                rate);
-                        }
-                    }
-                }
-                if (R == 0) {
-                    continue;
                 }
                 const int vc = md.vclass ? load_ro(md.vclass + v) : 0;
                 for (int r = 0; r < R; ++r) {
@@ -286,6 +424,23 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                 continue;
             }
             const SectorDesc &ss = sectors[sec.src[r]];
+            // the source gains |change| molecules in the visited voxel; species with one more
+            // molecule use per-row insertion coefficients, others the general re-rank
+            std::int64_t A[NS][TMAX], Bc[NS][TMAX];
+            int fixed = static_cast<int>(ss.begin);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                if (md.change[r][s] == 0) {
+                    fixed += st.rank[s] * static_cast<int>(ss.stride[s]);
+                }
+                if constexpr (TMAX <= 3) {
+                    static_for<TMAX>([&](auto I) {
+                        constexpr int i = decltype(I)::value;
+                        A[s][i] = binom_j<i + 1>(st.u[s][i] + i);
+                        Bc[s][i] = binom_j<i + 2>(st.u[s][i] + i + 1);
+                    });
+                }
+            }
             for (int v = lane; v < V; v += nlanes) {
                 const int uu = V - 1 - v;
                 int tm = 0;
@@ -302,9 +457,26 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                 const int vc = md.vclass ? load_ro(md.vclass + v) : 0;
                 const T a = load_ro(md.rate +
                                     (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple + tm);
-                if (a > T(0)) {
-                    acc(reaction_source<T, NS, TMAX>(B, md, sec, ss, st, r, uu), a);
+                if (!(a > T(0))) {
+                    continue;
                 }
+                int src = fixed;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const int c = md.change[r][s];
+                    if (c == 0) {
+                        continue;
+                    }
+                    std::int64_t rs;
+                    if constexpr (TMAX <= 3) {
+                        rs = c == -1 ? rank_inserted<TMAX>(st.u[s], sec.total[s], A[s], Bc[s], uu)
+                                     : rank_modified<TMAX>(B, st.u[s], sec.total[s], uu, -c);
+                    } else {
+                        rs = rank_modified<TMAX>(B, st.u[s], sec.total[s], uu, -c);
+                    }
+                    src += static_cast<int>(rs) * static_cast<int>(ss.stride[s]);
+                }
+                acc(src, a);
             }
         }
     }

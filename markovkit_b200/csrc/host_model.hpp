@@ -345,6 +345,29 @@ struct HostTables {
                 }
             }
         }
+        // structured grid with one cell volume: the kernels find neighbours by arithmetic
+        bool uniform = m.has_grid && V < (1 << 24);
+        for (int v = 0; uniform && v < V; ++v) {
+            uniform = m.volumes[v] == m.volumes[0];
+        }
+        if (uniform) {
+            mv.grid_dim = m.dim;
+            int stride = 1;
+            for (int a = 0; a < 3; ++a) {
+                mv.gdims[a] = a < m.dim ? static_cast<int>(m.dims[a]) : 1;
+                mv.gstride[a] = stride;
+                mv.ginv[a] = 1.0f / static_cast<float>(mv.gdims[a]);
+                stride *= mv.gdims[a];
+                double face = 1.0;
+                for (int b = 0; b < m.dim; ++b) {
+                    if (b != a) {
+                        face *= m.spacing[b];
+                    }
+                }
+                mv.axis_coef[a] =
+                    a < m.dim ? static_cast<T>((face / m.spacing[a]) / m.volumes[0]) : T(0);
+            }
+        }
         view = mv;
         bind_host();
     }

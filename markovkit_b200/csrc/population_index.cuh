@@ -187,6 +187,14 @@ MK_HD std::int64_t rank_replace(const BinomTable &B, const int (&u)[TMAX], int t
     if constexpr (TMAX == 1) {
         // the only molecule moves: the new list is {u_add}
         return u_add;
+    } else if constexpr (TMAX == 2) {
+        // at most two molecules: the one that stays, o, and u_add, ranked in closed form
+        if (t < 2) {
+            return u_add;
+        }
+        const int o = u[0] == u_rm ? u[1] : u[0];
+        const int a = o < u_add ? o : u_add, b = o < u_add ? u_add : o;
+        return a + ((std::int64_t(b) * (b + 1)) >> 1);
     } else if constexpr (TMAX <= 4) {
         // branch-free for short lists: element i (not the removed copy a) lands at
         // i - [i > a] + [u_i >= u_add]; u_add lands after the b remaining smaller elements
@@ -245,6 +253,19 @@ MK_HD std::int64_t rank_replace(const BinomTable &B, const int (&u)[TMAX], int t
 template <int TMAX>
 MK_HD std::int64_t rank_modified(const BinomTable &B, const int (&u)[TMAX], int t, int value,
                                  int delta) {
+    if constexpr (TMAX <= 2) {
+        // lists of at most two molecules before and after: closed forms for one copy more/less
+        if (delta == 1) {
+            if (t == 0) {
+                return value;
+            }
+            const int a = u[0] < value ? u[0] : value, b = u[0] < value ? value : u[0];
+            return a + ((std::int64_t(b) * (b + 1)) >> 1);
+        }
+        if (delta == -1) {
+            return t == 2 ? (u[0] == value ? u[TMAX - 1] : u[0]) : 0;
+        }
+    }
     std::int64_t r = 0;
     int p = 0;
     int skip = delta < 0 ? -delta : 0;

@@ -32,7 +32,7 @@ void write_err(char *err, const std::string &msg) {
 
 Problem make(int dim, const std::int64_t *dims, const double *spacing, int S, const double *D,
              int R, const int *change, const int *tmax, const double *rates, int is_box,
-             const int *limits, int absorbing) {
+             const int *limits, int absorbing, int csr = 0) {
     Problem p;
     p.model = Model::grid(dim, dims, spacing, std::vector<double>(D, D + S));
     if (R > 0) {
@@ -47,6 +47,10 @@ Problem make(int dim, const std::int64_t *dims, const double *spacing, int S, co
     p.B = {p.binom.data(), max_total + 1, p.model->V + max_total + 1};
     const auto totals = is_box ? box_totals(lim) : std::vector<std::vector<int>>{lim};
     p.sectors = layout_sectors(p.model->V, S, totals, p.B, &p.n);
+    if (csr) {
+        // the same voxel graph given as explicit neighbour lists (the general-graph path)
+        p.model->has_grid = false;
+    }
     p.t.build(*p.model, 1.0, true, absorbing != 0);
     couple_sectors<double>(p.sectors, S, *p.model, p.t.view, true);
     return p;
@@ -64,9 +68,10 @@ std::int64_t emu_generator(int dim, const std::int64_t *dims, const double *spac
                            const double *D, int R, const int *change, const int *tmax,
                            const double *rates, int is_box, const int *limits, int absorbing,
                            double shift, const double *x, double *exit_out, double *leak_out,
-                           double *Qx, double *Ax, char *err) {
+                           double *Qx, double *Ax, char *err, int csr) {
     try {
-        Problem p = make(dim, dims, spacing, S, D, R, change, tmax, rates, is_box, limits, absorbing);
+        Problem p =
+            make(dim, dims, spacing, S, D, R, change, tmax, rates, is_box, limits, absorbing, csr);
         if (!x) {
             return p.n;
         }

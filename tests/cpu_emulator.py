@@ -41,7 +41,7 @@ def rate_table(reactions, tmax, volume):
     return out
 
 
-def generator(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=True, shift=0.0, x=None):
+def generator(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=True, shift=0.0, x=None, csr=False):
     L = lib()
     S = len(D)
     dims_a = np.array(list(dims) + [1] * (3 - dim), dtype=np.int64)
@@ -57,14 +57,14 @@ def generator(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=T
     fn = L.emu_generator
     fn.restype = C.c_int64
     args = [C.c_int(dim), _d(dims_a), _d(sp_a), C.c_int(S), _d(D_a), C.c_int(R), _d(change), _d(tmax), _d(rates), C.c_int(int(is_box)), _d(lim), C.c_int(int(absorbing)), C.c_double(shift)]
-    n = fn(*args, None, None, None, None, None, err)
+    n = fn(*args, None, None, None, None, None, err, C.c_int(int(csr)))
     if n < 0:
         raise ValueError(err.value.decode())
     if x is None:
         x = np.zeros(n)
     x = np.ascontiguousarray(x, dtype=np.float64)
     out = {k: np.zeros(n) for k in ("exit", "leak", "Qx", "Ax")}
-    n = fn(*args, _d(x), _d(out["exit"]), _d(out["leak"]), _d(out["Qx"]), _d(out["Ax"]), err)
+    n = fn(*args, _d(x), _d(out["exit"]), _d(out["leak"]), _d(out["Qx"]), _d(out["Ax"]), err, C.c_int(int(csr)))
     if n < 0:
         raise ValueError(err.value.decode())
     return out

@@ -25,9 +25,10 @@ def test_state_indexing_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", NAMES)
-def test_generator_rows_match_reference(name):
+@pytest.mark.parametrize("csr", [False, True], ids=["grid", "csr"])
+def test_generator_rows_match_reference(name, csr):
     c = gc.load(name)
-    out = emu.generator(c.dim, c.dims, c.spacing, c.diffusivities, c.reactions, c.caps, True, c.absorbing, c.shift, c.data["x"])
+    out = emu.generator(c.dim, c.dims, c.spacing, c.diffusivities, c.reactions, c.caps, True, c.absorbing, c.shift, c.data["x"], csr=csr)
     # exit and leak rates: sums of the same positive terms, in another order
     np.testing.assert_allclose(out["exit"], c.data["exit"], rtol=1e-14, atol=0)
     np.testing.assert_allclose(out["leak"], c.data["leak"], rtol=1e-14, atol=0)
