@@ -33,6 +33,7 @@ extern "C" {
 #define MK_ENAN 6       /* non-finite residual */
 #define MK_ETIMEOUT 7   /* a bounded device wait gave up */
 #define MK_ECUDA 8      /* any other CUDA error */
+#define MK_ETOLERANCE 9 /* std::runtime_error ("expv: the requested tolerance is too high") */
 
 typedef struct mk_space_s *mk_space;
 typedef struct mk_model_s *mk_model;
@@ -187,6 +188,71 @@ int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_
 /* the same with host vectors: copies in, solves, copies out */
 int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
                          mk_solver_result *result, void *stream);
+
+/* ---- Krylov FSP: solve_krylov_fsp(model, initial, final_time, options), markovkit/fsp.hpp ---- */
+/* krylov_fsp_options (fsp.hpp:190-202) with inside = box(bounds) (fsp.hpp:26-35); save_every
+ * has no counterpart: only the final distribution is kept */
+typedef struct {
+    double tolerance;        /* the probability that may leak by final_time */
+    double initial_step;
+    double step_growth;
+    double drop_probability;
+    double drop_derivative;
+    int layers;
+    int krylov_dim;          /* 1..30 */
+    int64_t max_steps;       /* attempts */
+    double krylov_tol;
+} mk_fsp_options;
+void mk_fsp_options_default(mk_fsp_options *opt);
+/* One instance. A reaction_network (markovkit/reaction_network.hpp:11-39) restricted to the
+ * box 0 <= x_s <= bounds[s], with its propensities tabulated by the caller over the box:
+ * rates[r * box_size + i] = rate of reaction r in the state with box index
+ * i = sum_s x_s * prod_{s' > s} (bounds[s'] + 1) (species 0 most significant). Jumps with a
+ * rate that is not > 0 do not exist, as in reaction_network::transitions. The initial state
+ * (a delta, fsp.hpp:209) must lie in the box. */
+typedef struct {
+    int n_species;           /* 1..4 */
+    int n_reactions;         /* 0..16 */
+    const int *bounds;       /* n_species */
+    const int *change;       /* n_reactions x n_species */
+    const double *rates;     /* n_reactions x box_size, host memory */
+    const int *initial;      /* n_species */
+    double final_time;
+    mk_fsp_options options;
+} mk_fsp_problem;
+typedef struct {
+    double time;             /* fsp_solution::times.back() */
+    int64_t attempts;
+    int64_t accepted;
+    int64_t support;         /* states in the final support */
+    int status;              /* MK_OK, MK_ENOTCONV (stopped before final_time), MK_ETOLERANCE, MK_ENAN */
+} mk_fsp_result;
+typedef struct mk_fsp_batch_s *mk_fsp_batch;
+/* the number of states in box(bounds) */
+int mk_fsp_box_size(int n_species, const int *bounds, int64_t *size);
+/* Uploads n instances (their rate tables included) and sizes the workspace. The instances
+ * run in one persistent kernel, largest box first, one thread block per instance at a time. */
+int mk_fsp_batch_create(int n, const mk_fsp_problem *problems, mk_fsp_batch *out);
+void mk_fsp_batch_destroy(mk_fsp_batch batch);
+/* total states over all boxes (the length of the output) and, unless h_offsets is NULL, the
+ * offset of each instance's box in it (n entries; instance k's box follows instance k-1's) */
+int mk_fsp_batch_output_size(mk_fsp_batch batch, int64_t *total, int64_t *h_offsets);
+/* block shape: threads per block (256 or 512) and number of blocks (0 = all that fit) */
+int mk_fsp_batch_set_shape(mk_fsp_batch batch, int threads, int blocks);
+int mk_fsp_batch_get_shape(mk_fsp_batch batch, int *threads, int *blocks);
+/* times every shape on `sample` evenly spaced instances (0 = all) and keeps the fastest */
+int mk_fsp_batch_autotune(mk_fsp_batch batch, int sample, void *stream);
+/* runs every instance; stream-ordered */
+int mk_fsp_batch_run(mk_fsp_batch batch, void *stream);
+/* the device array of final distributions (each over its box, in box order) */
+int mk_fsp_batch_device_output(mk_fsp_batch batch, const double **d_out);
+/* copies results and (unless h_out is NULL) the distributions to the host, synchronising the
+ * stream; returns the first instance's failing status, with mk_last_error naming it */
+int mk_fsp_batch_results(mk_fsp_batch batch, double *h_out, mk_fsp_result *results,
+                         void *stream);
+/* create, run, copy out, destroy: solve_krylov_fsp for each problem */
+int mk_fsp_krylov_batch(int n, const mk_fsp_problem *problems, double *h_out,
+                        mk_fsp_result *results, void *stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -20,6 +20,7 @@ MK_ENOTCONV = 5
 MK_ENAN = 6
 MK_ETIMEOUT = 7
 MK_ECUDA = 8
+MK_ETOLERANCE = 9
 
 
 class MkError(RuntimeError):
@@ -59,6 +60,43 @@ class GmresOptions(C.Structure):
         ("max_iterations", C.c_int64),
         ("restart", C.c_int),
         ("flexible", C.c_int),
+    ]
+
+
+class FspOptions(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double),
+        ("initial_step", C.c_double),
+        ("step_growth", C.c_double),
+        ("drop_probability", C.c_double),
+        ("drop_derivative", C.c_double),
+        ("layers", C.c_int),
+        ("krylov_dim", C.c_int),
+        ("max_steps", C.c_int64),
+        ("krylov_tol", C.c_double),
+    ]
+
+
+class FspProblem(C.Structure):
+    _fields_ = [
+        ("n_species", C.c_int),
+        ("n_reactions", C.c_int),
+        ("bounds", C.POINTER(C.c_int)),
+        ("change", C.POINTER(C.c_int)),
+        ("rates", C.POINTER(C.c_double)),
+        ("initial", C.POINTER(C.c_int)),
+        ("final_time", C.c_double),
+        ("options", FspOptions),
+    ]
+
+
+class FspResult(C.Structure):
+    _fields_ = [
+        ("time", C.c_double),
+        ("attempts", C.c_int64),
+        ("accepted", C.c_int64),
+        ("support", C.c_int64),
+        ("status", C.c_int),
     ]
 
 
@@ -130,6 +168,18 @@ SIGNATURES = {
     "mk_solver_set_tolerance": (C.c_int, [P, C.c_double]),
     "mk_solver_solve": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
     "mk_solver_solve_host": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
+    "mk_fsp_options_default": (None, [C.POINTER(FspOptions)]),
+    "mk_fsp_box_size": (C.c_int, [C.c_int, IP, I64P]),
+    "mk_fsp_batch_create": (C.c_int, [C.c_int, C.POINTER(FspProblem), C.POINTER(P)]),
+    "mk_fsp_batch_destroy": (None, [P]),
+    "mk_fsp_batch_output_size": (C.c_int, [P, I64P, I64P]),
+    "mk_fsp_batch_set_shape": (C.c_int, [P, C.c_int, C.c_int]),
+    "mk_fsp_batch_get_shape": (C.c_int, [P, IP, IP]),
+    "mk_fsp_batch_autotune": (C.c_int, [P, C.c_int, P]),
+    "mk_fsp_batch_run": (C.c_int, [P, P]),
+    "mk_fsp_batch_device_output": (C.c_int, [P, C.POINTER(P)]),
+    "mk_fsp_batch_results": (C.c_int, [P, DP, C.POINTER(FspResult), P]),
+    "mk_fsp_krylov_batch": (C.c_int, [C.c_int, C.POINTER(FspProblem), DP, C.POINTER(FspResult), P]),
 }
 
 _lib: C.CDLL | None = None

@@ -37,3 +37,52 @@ def uniform_rhs(seed: int, n: int) -> np.ndarray:
 
 def dirichlet_rhs(seed: int, n: int) -> np.ndarray:
     return _sequential_normalise(-np.log1p(-uniform01(seed, n)))
+
+
+def fsp_batch_instances(seed: int = 3, count: int = 512, final_time: float = 2.0,
+                        tolerance: float = 1e-8) -> list:
+    """Seeded Krylov-FSP instances of the batching workload: the first half birth-death
+    ({+1} at b, {-1} at d x; b ~ U(1, 20), d ~ U(0.05, 0.5), box bound ~ U{99..1999}, so 100 to
+    2000 states), the second half toggle switches ({+1,0} at a1 / (1 + y^n1), {0,+1} at
+    a2 / (1 + x^n2), unit degradation; a ~ U(20, 60), n ~ U(1.5, 3), bounds ~ U{50..300}).
+    Instance k draws u(seed, 8k + j), j < 6. All start from the delta at 0."""
+    u = uniform01(seed, 8 * count)
+    out = []
+    for k in range(count):
+        v = u[8 * k : 8 * k + 8]
+        if k < count // 2:
+            out.append({
+                "family": "birth_death",
+                "birth": 1.0 + 19.0 * v[0],
+                "death": 0.05 + 0.45 * v[1],
+                "bounds": [99 + int(1901 * v[2])],
+                "initial": [0],
+                "final_time": final_time,
+                "tolerance": tolerance,
+            })
+        else:
+            out.append({
+                "family": "toggle",
+                "a1": 20.0 + 40.0 * v[0],
+                "a2": 20.0 + 40.0 * v[1],
+                "n1": 1.5 + 1.5 * v[2],
+                "n2": 1.5 + 1.5 * v[3],
+                "bounds": [50 + int(251 * v[4]), 50 + int(251 * v[5])],
+                "initial": [0, 0],
+                "final_time": final_time,
+                "tolerance": tolerance,
+            })
+    return out
+
+
+def fsp_instance_line(inst: dict, krylov_tol: float = 1e-8, krylov_dim: int = 30) -> str:
+    """One instance in the line format of the oracle's Krylov-FSP driver."""
+    g = lambda x: repr(float(x))  # noqa: E731 - shortest round-trip decimal
+    if inst["family"] == "birth_death":
+        return " ".join(["birth_death", g(inst["birth"]), g(inst["death"]), str(inst["bounds"][0]),
+                         g(inst["final_time"]), g(inst["tolerance"]), g(krylov_tol), str(krylov_dim),
+                         str(inst["initial"][0])])
+    return " ".join(["toggle", g(inst["a1"]), g(inst["a2"]), g(inst["n1"]), g(inst["n2"]),
+                     str(inst["bounds"][0]), str(inst["bounds"][1]), g(inst["final_time"]),
+                     g(inst["tolerance"]), g(krylov_tol), str(krylov_dim), str(inst["initial"][0]),
+                     str(inst["initial"][1])])

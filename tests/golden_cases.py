@@ -76,4 +76,5 @@ def load(name: str) -> Case:
 
 
 def names() -> list[str]:
-    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+    """the resolvent fixtures (fsp_cases.npz holds the Krylov-FSP ones)"""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != "fsp_cases")
