@@ -225,6 +225,8 @@ typedef struct {
     int64_t attempts;
     int64_t accepted;
     int64_t support;         /* states in the final support */
+    int64_t substeps;        /* expv time steps over all attempts */
+    int64_t applies;         /* operator applies over all attempts */
     int status;              /* MK_OK, MK_ENOTCONV (stopped before final_time), MK_ETOLERANCE, MK_ENAN */
 } mk_fsp_result;
 typedef struct mk_fsp_batch_s *mk_fsp_batch;
@@ -237,7 +239,7 @@ void mk_fsp_batch_destroy(mk_fsp_batch batch);
 /* total states over all boxes (the length of the output) and, unless h_offsets is NULL, the
  * offset of each instance's box in it (n entries; instance k's box follows instance k-1's) */
 int mk_fsp_batch_output_size(mk_fsp_batch batch, int64_t *total, int64_t *h_offsets);
-/* block shape: threads per block (256 or 512) and number of blocks (0 = all that fit) */
+/* block shape: threads per block (128, 256 or 512) and number of blocks (0 = all that fit) */
 int mk_fsp_batch_set_shape(mk_fsp_batch batch, int threads, int blocks);
 int mk_fsp_batch_get_shape(mk_fsp_batch batch, int *threads, int *blocks);
 /* times every shape on `sample` evenly spaced instances (0 = all) and keeps the fastest */

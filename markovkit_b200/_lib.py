@@ -96,6 +96,8 @@ class FspResult(C.Structure):
         ("attempts", C.c_int64),
         ("accepted", C.c_int64),
         ("support", C.c_int64),
+        ("substeps", C.c_int64),
+        ("applies", C.c_int64),
         ("status", C.c_int),
     ]
 

@@ -22,7 +22,6 @@ struct mk_fsp_batch_s {
     mkb::DeviceArray<int> d_queue;
     mkb::DeviceArray<double> work;
     mkb::DeviceArray<int> iwork;
-    mkb::DeviceArray<unsigned char> flags;
     int workspace_blocks = 0;               // blocks the workspace holds
     int threads = 512;
     int blocks = 0;                         // 0: every block that fits
@@ -108,7 +107,6 @@ void ensure_workspace(mk_fsp_batch_s &b, int blocks) {
     }
     b.work.resize(static_cast<std::size_t>(blocks) * mkb::fsp_work_doubles(b.cap));
     b.iwork.resize(static_cast<std::size_t>(blocks) * mkb::fsp_work_ints(b.cap));
-    b.flags.resize(static_cast<std::size_t>(blocks) * b.cap);
     b.workspace_blocks = blocks;
 }
 
@@ -126,7 +124,6 @@ void launch(mk_fsp_batch_s &b, const mkb::FspInstance *d_inst, int n, int thread
     v.queue = b.d_queue.get();
     v.work = b.work.get();
     v.iwork = b.iwork.get();
-    v.flags = b.flags.get();
     v.cap = b.cap;
     mkb::check_cuda(mkb::launch_fsp_batch(v, threads, blocks, stream), "fsp kernel launch");
 }
@@ -184,6 +181,10 @@ int mk_fsp_batch_create(int n, const mk_fsp_problem *problems, mk_fsp_batch *out
             I.S = p.n_species;
             I.R = p.n_reactions;
             const std::int64_t box = box_size(p.n_species, p.bounds);
+            if (box * std::max(p.n_reactions, 1) >= (std::int64_t(1) << 31)) {
+                throw Error(MK_EOVERFLOW,
+                            where + "box size x reactions must stay below 2^31");
+            }
             I.box = static_cast<int>(box);
             std::int64_t stride = 1;
             for (int s = p.n_species - 1; s >= 0; --s) {
@@ -264,7 +265,8 @@ int mk_fsp_batch_output_size(mk_fsp_batch batch, int64_t *total, int64_t *h_offs
 int mk_fsp_batch_set_shape(mk_fsp_batch batch, int threads, int blocks) {
     return mkb::capi::guarded([&] {
         MK_REQUIRE(batch, "null argument");
-        MK_REQUIRE(threads == 256 || threads == 512, "fsp: threads must be 256 or 512");
+        MK_REQUIRE(threads == 128 || threads == 256 || threads == 512,
+                   "fsp: threads must be 128, 256 or 512");
         MK_REQUIRE(blocks >= 0, "fsp: blocks must be >= 0");
         batch->threads = threads;
         batch->blocks = blocks;
@@ -373,6 +375,8 @@ int mk_fsp_batch_results(mk_fsp_batch batch, double *h_out, mk_fsp_result *resul
             r.attempts = outcome[k].attempts;
             r.accepted = outcome[k].accepted;
             r.support = outcome[k].support;
+            r.substeps = outcome[k].substeps;
+            r.applies = outcome[k].applies;
             r.status = status_code(outcome[k].status);
             if (r.status != MK_OK && first_failure == MK_OK) {
                 first_failure = r.status;

@@ -12,12 +12,18 @@
 // expv is Sidje's Expokit controller as the numerics library is called (fsp.hpp:223): Krylov
 // dimension m, the augmented (m+2)-square Hessenberg, a Pade (6,6) exponential with scaling and
 // squaring, the two-term error estimate, safety factors 0.9 and 1.2, break-down below 1e-7.
-// The Arnoldi process orthogonalises by classical Gram-Schmidt with one re-orthogonalisation
-// (two block-wide multi-dot passes), and writes each new basis vector inside the next
-// operator apply, so a step reads the basis three times.
-// The support is a compact list of slots with a box-to-slot map: old states keep their order,
-// each ring's new states follow in box order, and dropped states are compacted out in order.
-// Vectors and reductions therefore cost the support's size, not the box's. Every loop is bounded.
+//
+// The support is a compact list of slots with a box-to-slot map, in the reference's order: an
+// expansion ring appends the new states in the order the reference discovers them (support
+// slot, then reaction; the first discoverer of a state wins, found with an atomic minimum over
+// candidate numbers), and dropped states are compacted out in order. Vectors and reductions
+// cost the support's size, not the box's.
+// One Arnoldi step is three block-wide phases: (1) the operator apply, which also writes the
+// basis vector V_j = p / ||p|| of the previous step and accumulates the first Gram-Schmidt
+// projections <V_i, Q V_j>; (2) the first subtraction fused with the second projections;
+// (3) the second subtraction fused with the norm. The small exponential's elimination runs on
+// two warps under a named barrier while the rest of the block waits once.
+// Every loop is bounded; no thread waits on another block.
 #include "fsp.cuh"
 #include "launch_count.hpp"
 
@@ -30,7 +36,8 @@ namespace {
 constexpr int kMaxWarps = 16;
 constexpr int kBasis = kFspMaxKrylov + 1;
 constexpr int kE = 32;               // side of the small dense matrices in shared memory
-constexpr int kDotChunk = 16;        // basis vectors per multi-dot pass
+constexpr int kDotChunk = 16;        // basis vectors per projection pass
+constexpr int kNoOwner = 0x7fffffff;
 constexpr int kSubstepLimit = 100000;
 constexpr std::int64_t kAttemptLimit = 1000000;
 
@@ -51,6 +58,9 @@ __device__ __forceinline__ double warp_max(double v) {
     }
     return v;
 }
+
+// barrier 1 over the first two warps only
+__device__ __forceinline__ void pair_barrier() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
 
 struct Shared {
     FspInstance in;
@@ -131,8 +141,7 @@ struct Ctx {
     const double *rate;
     double *V;             // kBasis vectors of stride cap
     double *prob, *w, *buf0, *buf1, *tmp;
-    int *b2s, *s2b, *itmp;
-    unsigned char *newflag;
+    int *b2s, *s2b, *itmp, *owner;
     std::int64_t cap;
 };
 
@@ -143,113 +152,81 @@ __device__ __forceinline__ void coords(const FspInstance &in, int i, int (&x)[kF
     }
 }
 
-// out = Q (src / div) over the n support slots, and v_out = src / div when v_out is given.
-// Q is absorbing: every valid positive jump out of a state counts in its exit rate.
-// ABS: out = the absolute row sums of Q instead (src unused), for the infinity norm.
-// Returns the block's sum of out^2 when NORM.
-template <int NT, bool ABS, bool NORM>
-__device__ double apply_q(Shared &sh, const Ctx &c, int n, const double *src, double div,
-                          double *v_out, double *out) {
+// Row k of Q applied to src: sum of in-jumps from supported states minus exit * src[k], or
+// with ABS the row's absolute sum (src unused). Every valid positive jump counts in the exit.
+template <bool ABS>
+__device__ __forceinline__ double row_apply(const Ctx &c, int k, const double *src) {
     const FspInstance &in = *c.in;
-    double sq = 0.0;
-    for (int k = threadIdx.x; k < n; k += NT) {
-        const int i = c.s2b[k];
-        int xi[kFspMaxSpecies];
-        coords(in, i, xi);
-        double acc = 0.0, ex = 0.0;
-        for (int r = 0; r < in.R; ++r) {
-            bool valid = true, inside = true;
-            int j = i;
+    const int i = c.s2b[k];
+    int xi[kFspMaxSpecies];
+    coords(in, i, xi);
+    double acc = 0.0, ex = 0.0;
+    for (int r = 0; r < in.R; ++r) {
+        bool valid = true, inside = true;
+        int j = i;
 #pragma unroll
-            for (int s = 0; s < kFspMaxSpecies; ++s) {
-                if (s < in.S) {
-                    const int ch = in.change[r][s];
-                    valid = valid && xi[s] + ch >= 0;
-                    const int xs = xi[s] - ch;
-                    inside = inside && xs >= 0 && xs <= in.bound[s];
-                    j -= ch * in.stride[s];
-                }
+        for (int s = 0; s < kFspMaxSpecies; ++s) {
+            if (s < in.S) {
+                const int ch = in.change[r][s];
+                valid = valid && xi[s] + ch >= 0;
+                const int xs = xi[s] - ch;
+                inside = inside && xs >= 0 && xs <= in.bound[s];
+                j -= ch * in.stride[s];
             }
-            const double a = c.rate[static_cast<std::int64_t>(r) * in.box + i];
-            if (a > 0.0 && valid) {
-                ex += a;
-            }
-            if (inside) {
-                const int sl = c.b2s[j];
-                if (sl >= 0) {
-                    const double aj = c.rate[static_cast<std::int64_t>(r) * in.box + j];
-                    if (aj > 0.0) {
-                        if constexpr (ABS) {
-                            acc += aj;
-                        } else {
-                            acc += aj * src[sl];
-                        }
+        }
+        const double a = c.rate[static_cast<std::int64_t>(r) * in.box + i];
+        if (a > 0.0 && valid) {
+            ex += a;
+        }
+        if (inside) {
+            const int sl = c.b2s[j];
+            if (sl >= 0) {
+                const double aj = c.rate[static_cast<std::int64_t>(r) * in.box + j];
+                if (aj > 0.0) {
+                    if constexpr (ABS) {
+                        acc += aj;
+                    } else {
+                        acc += aj * src[sl];
                     }
                 }
             }
         }
-        double y;
-        if constexpr (ABS) {
-            y = acc + ex;
-        } else {
-            const double self = src[k];
-            y = (acc - ex * self) / div;
-            if (v_out) {
-                v_out[k] = self / div;
-            }
-        }
-        out[k] = y;
-        if constexpr (NORM) {
-            sq += y * y;
-        }
     }
-    if constexpr (NORM) {
-        return block_reduce<NT, false>(sh, sq); // its barriers order the writes above
+    if constexpr (ABS) {
+        return acc + ex;
+    } else {
+        return acc - ex * src[k];
+    }
+}
+
+// out = Q src over the n slots
+template <int NT>
+__device__ void apply_plain(const Ctx &c, int n, const double *src, double *out) {
+    for (int k = threadIdx.x; k < n; k += NT) {
+        out[k] = row_apply<false>(c, k, src);
     }
     __syncthreads();
-    return 0.0;
 }
 
-template <int NT>
-__device__ double dot(Shared &sh, const double *a, const double *b, int n) {
-    double v = 0.0;
-    for (int k = threadIdx.x; k < n; k += NT) {
-        v += a[k] * b[k];
-    }
-    return block_reduce<NT, false>(sh, v);
-}
-
-// h[k] = <V_k, p> for k < K, kDotChunk basis vectors per pass over p
-template <int NT>
-__device__ void multi_dot(Shared &sh, const Ctx &c, int K, const double *p, int n, double *h) {
-    constexpr int W = NT / 32;
+// warp partial sums of acc[q] (basis vector k0 + q, below K) into sh.red
+__device__ __forceinline__ void stash_partials(Shared &sh, const double (&acc)[kDotChunk], int k0,
+                                               int K) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k0 = 0; k0 < K; k0 += kDotChunk) {
-        double acc[kDotChunk];
 #pragma unroll
-        for (int q = 0; q < kDotChunk; ++q) {
-            acc[q] = 0.0;
-        }
-        const double *Vk = c.V + static_cast<std::int64_t>(k0) * c.cap;
-        for (int e = threadIdx.x; e < n; e += NT) {
-            const double pe = p[e];
-#pragma unroll
-            for (int q = 0; q < kDotChunk; ++q) {
-                if (k0 + q < K) {
-                    acc[q] += Vk[q * c.cap + e] * pe;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kDotChunk; ++q) {
-            if (k0 + q < K) {
-                const double v = warp_sum(acc[q]);
-                if (lane == 0) {
-                    sh.red[warp * kE + k0 + q] = v;
-                }
+    for (int q = 0; q < kDotChunk; ++q) {
+        if (k0 + q < K) {
+            const double v = warp_sum(acc[q]);
+            if (lane == 0) {
+                sh.red[warp * kE + k0 + q] = v;
             }
         }
     }
+}
+
+// h[i] = sum over warps of the stashed partials, i < K, visible to every thread on return
+template <int NT>
+__device__ void finish_dots(Shared &sh, int K, double *h) {
+    constexpr int W = NT / 32;
     __syncthreads();
     if (static_cast<int>(threadIdx.x) < K) {
         double t = 0.0;
@@ -261,23 +238,108 @@ __device__ void multi_dot(Shared &sh, const Ctx &c, int K, const double *p, int 
     __syncthreads();
 }
 
-// p -= sum_{k<K} h[k] V_k; returns the block's sum of the new p^2 when NORM
-template <int NT, bool NORM>
-__device__ double multi_axpy(Shared &sh, const Ctx &c, int K, const double *h, double *p, int n) {
-    double sq = 0.0;
-    for (int e = threadIdx.x; e < n; e += NT) {
-        double v = p[e];
-        for (int k = 0; k < K; ++k) {
-            v -= h[k] * c.V[k * c.cap + e];
+__device__ __forceinline__ void zero(double (&acc)[kDotChunk]) {
+#pragma unroll
+    for (int q = 0; q < kDotChunk; ++q) {
+        acc[q] = 0.0;
+    }
+}
+
+// Arnoldi phase 1: V_j = src / div, out = Q V_j, sh.h1[i] = <V_i, out> for i <= j
+template <int NT>
+__device__ void arnoldi_apply(Shared &sh, const Ctx &c, int n, const double *src, double div,
+                              int j, double *out) {
+    const int K = j + 1;
+    double *Vj = c.V + static_cast<std::int64_t>(j) * c.cap;
+    double acc[kDotChunk];
+    zero(acc);
+    for (int k = threadIdx.x; k < n; k += NT) {
+        const double y = row_apply<false>(c, k, src) / div;
+        const double vk = src[k] / div;
+        Vj[k] = vk;
+        out[k] = y;
+#pragma unroll
+        for (int q = 0; q < kDotChunk; ++q) {
+            if (q < K) {
+                const double v = q == j ? vk : c.V[q * c.cap + k];
+                acc[q] += v * y;
+            }
         }
-        p[e] = v;
+    }
+    stash_partials(sh, acc, 0, K);
+    for (int k0 = kDotChunk; k0 < K; k0 += kDotChunk) {
+        zero(acc);
+        for (int k = threadIdx.x; k < n; k += NT) {
+            const double y = out[k];
+#pragma unroll
+            for (int q = 0; q < kDotChunk; ++q) {
+                if (k0 + q < K) {
+                    acc[q] += c.V[(k0 + q) * c.cap + k] * y;
+                }
+            }
+        }
+        stash_partials(sh, acc, k0, K);
+    }
+    finish_dots<NT>(sh, K, sh.h1);
+}
+
+// Arnoldi phase 2: out -= sum_i h1[i] V_i, then sh.h2[i] = <V_i, out>
+template <int NT>
+__device__ void arnoldi_reorthogonalise(Shared &sh, const Ctx &c, int n, int K, double *out) {
+    double acc[kDotChunk];
+    zero(acc);
+    for (int k = threadIdx.x; k < n; k += NT) {
+        double v = out[k];
+        for (int i = 0; i < K; ++i) {
+            v -= sh.h1[i] * c.V[i * c.cap + k];
+        }
+        out[k] = v;
+#pragma unroll
+        for (int q = 0; q < kDotChunk; ++q) {
+            if (q < K) {
+                acc[q] += c.V[q * c.cap + k] * v;
+            }
+        }
+    }
+    stash_partials(sh, acc, 0, K);
+    for (int k0 = kDotChunk; k0 < K; k0 += kDotChunk) {
+        zero(acc);
+        for (int k = threadIdx.x; k < n; k += NT) {
+            const double v = out[k];
+#pragma unroll
+            for (int q = 0; q < kDotChunk; ++q) {
+                if (k0 + q < K) {
+                    acc[q] += c.V[(k0 + q) * c.cap + k] * v;
+                }
+            }
+        }
+        stash_partials(sh, acc, k0, K);
+    }
+    finish_dots<NT>(sh, K, sh.h2);
+}
+
+// Arnoldi phase 3: out -= sum_i h2[i] V_i; returns ||out||^2
+template <int NT>
+__device__ double arnoldi_finish(Shared &sh, const Ctx &c, int n, int K, double *out) {
+    double sq = 0.0;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        double v = out[k];
+        for (int i = 0; i < K; ++i) {
+            v -= sh.h2[i] * c.V[i * c.cap + k];
+        }
+        out[k] = v;
         sq += v * v;
     }
-    if constexpr (NORM) {
-        return block_reduce<NT, false>(sh, sq);
+    return block_reduce<NT, false>(sh, sq);
+}
+
+template <int NT>
+__device__ double dot(Shared &sh, const double *a, const double *b, int n) {
+    double v = 0.0;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        v += a[k] * b[k];
     }
-    __syncthreads();
-    return 0.0;
+    return block_reduce<NT, false>(sh, v);
 }
 
 // C = A B for n x n matrices in shared memory (row-major, side kE)
@@ -294,8 +356,62 @@ __device__ void matmul(const double *A, const double *B, double *C, int n) {
     __syncthreads();
 }
 
-// sh.F = exp(sh.X) for an n x n matrix: Pade (6,6) with scaling and squaring; the rational
-// function is solved by Gauss-Jordan elimination with partial pivoting
+// F = Q^{-1} F by Gauss-Jordan elimination with partial pivoting (first largest pivot), on the
+// first two warps: thread j < 32 owns column j of Q, thread 32 + j column j of F. The pivot
+// row is swapped in by each column's owner; the factors come from warp 0 before the swap.
+template <int NT>
+__device__ void solve_pade(Shared &sh, int n) {
+    if (threadIdx.x < 64) {
+        const int lane = threadIdx.x & 31;
+        double *M = threadIdx.x < 32 ? sh.Q : sh.F;
+        for (int k = 0; k < n; ++k) {
+            if (threadIdx.x < 32) {
+                double a = (lane >= k && lane < n) ? fabs(sh.Q[lane * kE + k]) : -1.0;
+                int idx = lane;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    const double oa = __shfl_xor_sync(0xffffffffu, a, off);
+                    const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
+                    if (oa > a || (oa == a && oi < idx)) {
+                        a = oa;
+                        idx = oi;
+                    }
+                }
+                const int piv = idx;
+                const double pivot = sh.Q[piv * kE + k];
+                if (lane < n) {
+                    const int src = lane == k ? piv : (lane == piv ? k : lane);
+                    sh.fac[lane] = lane == k ? 0.0 : sh.Q[src * kE + k] / pivot;
+                }
+                if (lane == 0) {
+                    sh.i[0] = piv;
+                }
+            }
+            pair_barrier();
+            const int piv = sh.i[0];
+            if (lane < n) {
+                const double rk = M[piv * kE + lane];
+                M[piv * kE + lane] = M[k * kE + lane];
+                M[k * kE + lane] = rk;
+                for (int i = 0; i < n; ++i) {
+                    const double f = sh.fac[i];
+                    if (f != 0.0) {
+                        M[i * kE + lane] -= f * rk;
+                    }
+                }
+            }
+            pair_barrier();
+        }
+        if (threadIdx.x >= 32 && lane < n) {
+            for (int i = 0; i < n; ++i) {
+                sh.F[i * kE + lane] /= sh.Q[i * kE + i];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// sh.F = exp(sh.X) for an n x n matrix: Pade (6,6) with scaling and squaring
 template <int NT>
 __device__ void small_expm(Shared &sh, int n) {
     double rowmax = 0.0;
@@ -333,56 +449,13 @@ __device__ void small_expm(Shared &sh, int n) {
             sh.PW[i * kE + j] = v;
             sh.P[i * kE + j] += cf * v;
             sh.Q[i * kE + j] += sign * cf * v;
-        }
-        __syncthreads();
-    }
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e / n, j = e % n;
-        sh.F[i * kE + j] = sh.P[i * kE + j];
-    }
-    __syncthreads();
-    for (int k = 0; k < n; ++k) {
-        if (threadIdx.x == 0) {
-            int piv = k;
-            for (int i = k + 1; i < n; ++i) {
-                if (fabs(sh.Q[i * kE + k]) > fabs(sh.Q[piv * kE + k])) {
-                    piv = i;
-                }
-            }
-            sh.i[0] = piv;
-        }
-        __syncthreads();
-        const int piv = sh.i[0];
-        if (piv != k) {
-            for (int j = threadIdx.x; j < n; j += NT) {
-                double t = sh.Q[k * kE + j];
-                sh.Q[k * kE + j] = sh.Q[piv * kE + j];
-                sh.Q[piv * kE + j] = t;
-                t = sh.F[k * kE + j];
-                sh.F[k * kE + j] = sh.F[piv * kE + j];
-                sh.F[piv * kE + j] = t;
-            }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += NT) {
-            sh.fac[i] = i == k ? 0.0 : sh.Q[i * kE + k] / sh.Q[k * kE + k];
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < n * n; e += NT) {
-            const int i = e / n, j = e % n;
-            const double f = sh.fac[i];
-            if (f != 0.0) {
-                sh.Q[i * kE + j] -= f * sh.Q[k * kE + j];
-                sh.F[i * kE + j] -= f * sh.F[k * kE + j];
+            if (k == p) {
+                sh.F[i * kE + j] = sh.P[i * kE + j];
             }
         }
         __syncthreads();
     }
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e / n, j = e % n;
-        sh.F[i * kE + j] /= sh.Q[i * kE + i];
-    }
-    __syncthreads();
+    solve_pade<NT>(sh, n);
     for (int s = 0; s < squarings; ++s) {
         matmul<NT>(sh.F, sh.F, sh.T, n);
         for (int e = threadIdx.x; e < n * n; e += NT) {
@@ -399,18 +472,23 @@ __device__ double round_step(double step) {
     return ceil(step / s) * s;
 }
 
+struct Counters {
+    std::int64_t substeps = 0, applies = 0;
+};
+
 // c.w (n slots) <- exp(t Q) c.w; returns 0, or an FspOutcome status
 template <int NT>
-__device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double tol) {
+__device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double tol,
+                    Counters &cnt) {
     if (n == 0 || t == 0.0) {
         return 0;
     }
     const int m = min(max(m_req, 1), n);
-    apply_q<NT, true, false>(sh, c, n, nullptr, 1.0, nullptr, c.tmp);
     double rowmax = 0.0;
     for (int k = threadIdx.x; k < n; k += NT) {
-        rowmax = fmax(rowmax, c.tmp[k]);
+        rowmax = fmax(rowmax, row_apply<true>(c, k, nullptr));
     }
+    ++cnt.applies;
     const double anorm = fmax(block_reduce<NT, true>(sh, rowmax), 1e-300);
     constexpr int max_reject = 10;
     constexpr double btol = 1e-7, gamma = 0.9, delta = 1.2;
@@ -428,6 +506,7 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
         if (sub >= kSubstepLimit) {
             return 2;
         }
+        ++cnt.substeps;
         double t_step = fmin(t_out - t_now, t_new);
         const int hd = m + 2;
         for (int e = threadIdx.x; e < hd * hd; e += NT) {
@@ -439,17 +518,13 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
         double div = beta;
         double *out = c.buf0;
         for (int j = 0; j < m; ++j) {
-            // out = Q V_j, writing V_j = src / div on the way
-            apply_q<NT, false, false>(sh, c, n, src, div, c.V + static_cast<std::int64_t>(j) * c.cap,
-                                      out);
-            multi_dot<NT>(sh, c, j + 1, out, n, sh.h1);
-            multi_axpy<NT, false>(sh, c, j + 1, sh.h1, out, n);
-            multi_dot<NT>(sh, c, j + 1, out, n, sh.h2);
-            const double ss = multi_axpy<NT, true>(sh, c, j + 1, sh.h2, out, n);
+            arnoldi_apply<NT>(sh, c, n, src, div, j, out);
+            arnoldi_reorthogonalise<NT>(sh, c, n, j + 1, out);
             for (int i = threadIdx.x; i <= j; i += NT) {
                 sh.H[i * kE + j] = sh.h1[i] + sh.h2[i];
             }
-            const double s = sqrt(ss);
+            const double s = sqrt(arnoldi_finish<NT>(sh, c, n, j + 1, out));
+            ++cnt.applies;
             if (!(s == s)) {
                 return 3;
             }
@@ -457,24 +532,30 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
                 k1 = 0;
                 mb = j + 1;
                 t_step = t_out - t_now;
-                __syncthreads();
                 break;
             }
             if (threadIdx.x == 0) {
                 sh.H[(j + 1) * kE + j] = s;
             }
-            __syncthreads();
             src = out;
             div = s;
             out = out == c.buf0 ? c.buf1 : c.buf0;
         }
         double avnorm = 0.0;
         if (k1 != 0) {
+            // V_m = src / div, and ||Q V_m||
+            double *Vm = c.V + static_cast<std::int64_t>(m) * c.cap;
+            double sq = 0.0;
+            for (int k = threadIdx.x; k < n; k += NT) {
+                const double y = row_apply<false>(c, k, src) / div;
+                Vm[k] = src[k] / div;
+                sq += y * y;
+            }
+            ++cnt.applies;
             if (threadIdx.x == 0) {
                 sh.H[(m + 1) * kE + m] = 1.0;
             }
-            avnorm = sqrt(apply_q<NT, false, true>(sh, c, n, src, div,
-                                                   c.V + static_cast<std::int64_t>(m) * c.cap, out));
+            avnorm = sqrt(block_reduce<NT, false>(sh, sq));
         }
         double err_loc = 0.0, xm = 1.0 / m;
         for (int reject = 0;; ++reject) {
@@ -511,15 +592,16 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
             t_step = round_step(t_step);
         }
         const int used = mb + max(0, k1 - 1);
+        double sq = 0.0;
         for (int k = threadIdx.x; k < n; k += NT) {
             double v = 0.0;
             for (int j = 0; j < used; ++j) {
                 v += (beta * sh.F[j * kE]) * c.V[static_cast<std::int64_t>(j) * c.cap + k];
             }
             c.w[k] = v;
+            sq += v * v;
         }
-        __syncthreads();
-        beta = sqrt(dot<NT>(sh, c.w, c.w, n));
+        beta = sqrt(block_reduce<NT, false>(sh, sq));
         t_now += t_step;
         t_new = gamma * t_step * pow(t_step * tol / fmax(err_loc, 1e-300), xm);
         t_new = round_step(t_new);
@@ -533,45 +615,64 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
     return 0;
 }
 
-// add `layers` rings of neighbours inside the box to slots [0, n); returns the new n
+// the state reached from slot k by reaction r, if the jump exists, stays in the box and leads
+// outside the support
+__device__ __forceinline__ bool new_neighbour(const Ctx &c, int k, int r, int &j) {
+    const FspInstance &in = *c.in;
+    const int i = c.s2b[k];
+    if (!(c.rate[static_cast<std::int64_t>(r) * in.box + i] > 0.0)) {
+        return false;
+    }
+    int xi[kFspMaxSpecies];
+    coords(in, i, xi);
+    bool inside = true;
+    j = i;
+#pragma unroll
+    for (int s = 0; s < kFspMaxSpecies; ++s) {
+        if (s < in.S) {
+            const int y = xi[s] + in.change[r][s];
+            inside = inside && y >= 0 && y <= in.bound[s];
+            j += in.change[r][s] * in.stride[s];
+        }
+    }
+    return inside && c.b2s[j] < 0;
+}
+
+// add `layers` rings of neighbours inside the box to slots [0, n), in the reference's order;
+// returns the new n
 template <int NT>
 __device__ int expand(Shared &sh, const Ctx &c, int n) {
     const FspInstance &in = *c.in;
+    const int R = in.R;
     int f0 = 0, f1 = n;
-    for (int layer = 0; layer < in.layers; ++layer) {
-        for (int k = f0 + static_cast<int>(threadIdx.x); k < f1; k += NT) {
-            const int i = c.s2b[k];
-            int xi[kFspMaxSpecies];
-            coords(in, i, xi);
-            for (int r = 0; r < in.R; ++r) {
-                if (!(c.rate[static_cast<std::int64_t>(r) * in.box + i] > 0.0)) {
-                    continue;
-                }
-                bool inside = true;
-                int j = i;
-#pragma unroll
-                for (int s = 0; s < kFspMaxSpecies; ++s) {
-                    if (s < in.S) {
-                        const int y = xi[s] + in.change[r][s];
-                        inside = inside && y >= 0 && y <= in.bound[s];
-                        j += in.change[r][s] * in.stride[s];
-                    }
-                }
-                if (inside && c.b2s[j] < 0) {
-                    c.newflag[j] = 1;
-                }
+    for (int layer = 0; layer < in.layers && R > 0; ++layer) {
+        // candidate q = (slot - f0) * R + r; a state's first discoverer has the smallest q
+        const int L = (f1 - f0) * R;
+        for (int q = threadIdx.x; q < L; q += NT) {
+            int j;
+            if (new_neighbour(c, f0 + q / R, q % R, j)) {
+                atomicMin(&c.owner[j], q);
             }
         }
         __syncthreads();
         const int added = compact<NT>(
-            sh, in.box, [&](int j) { return c.newflag[j] != 0; },
-            [&](int j, int dest) {
+            sh, L,
+            [&](int q) {
+                int j;
+                return new_neighbour(c, f0 + q / R, q % R, j) && c.owner[j] == q;
+            },
+            [&](int q, int dest) {
+                int j;
+                new_neighbour(c, f0 + q / R, q % R, j);
                 const int slot = f1 + dest;
                 c.b2s[j] = slot;
                 c.s2b[slot] = j;
                 c.prob[slot] = 0.0;
-                c.newflag[j] = 0;
             });
+        for (int slot = f1 + static_cast<int>(threadIdx.x); slot < f1 + added; slot += NT) {
+            c.owner[c.s2b[slot]] = kNoOwner;
+        }
+        __syncthreads();
         f0 = f1;
         f1 += added;
         if (added == 0) {
@@ -582,7 +683,7 @@ __device__ int expand(Shared &sh, const Ctx &c, int n) {
 }
 
 template <int NT>
-__global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
+__global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchView v) {
     extern __shared__ double smem_raw[];
     Shared &sh = *reinterpret_cast<Shared *>(smem_raw);
     Ctx c;
@@ -599,7 +700,7 @@ __global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
     c.b2s = ib;
     c.s2b = ib + v.cap;
     c.itmp = ib + 2 * v.cap;
-    c.newflag = v.flags + static_cast<std::int64_t>(blockIdx.x) * v.cap;
+    c.owner = ib + 3 * v.cap;
 
     while (true) {
         if (threadIdx.x == 0) {
@@ -622,7 +723,7 @@ __global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
         c.rate = v.rates + in.rate_offset;
         for (int j = threadIdx.x; j < in.box; j += NT) {
             c.b2s[j] = -1;
-            c.newflag[j] = 0;
+            c.owner[j] = kNoOwner;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -634,6 +735,7 @@ __global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
         int n = 1;
         double t = 0.0, tau = in.initial_step;
         std::int64_t attempt = 0, accepted = 0;
+        Counters cnt;
         int status = 0;
         const std::int64_t limit = in.max_steps < kAttemptLimit ? in.max_steps : kAttemptLimit;
         for (; t < in.final_time && attempt < limit; ++attempt) {
@@ -643,7 +745,7 @@ __global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
                 c.w[k] = c.prob[k];
             }
             __syncthreads();
-            status = expv<NT>(sh, c, n, tau, in.krylov_dim, in.krylov_tol);
+            status = expv<NT>(sh, c, n, tau, in.krylov_dim, in.krylov_tol, cnt);
             if (status != 0) {
                 break;
             }
@@ -657,7 +759,8 @@ __global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
                 continue;
             }
             // dp = Q w; keep max(0, w); drop what is both unlikely and nearly constant
-            apply_q<NT, false, false>(sh, c, n, c.w, 1.0, nullptr, c.tmp);
+            apply_plain<NT>(c, n, c.w, c.tmp);
+            ++cnt.applies;
             for (int k = threadIdx.x; k < n; k += NT) {
                 c.prob[k] = fmax(0.0, c.w[k]);
             }
@@ -713,6 +816,8 @@ __global__ void __launch_bounds__(NT) fsp_kernel(const FspBatchView v) {
             o.attempts = attempt;
             o.accepted = accepted;
             o.support = n;
+            o.substeps = cnt.substeps;
+            o.applies = cnt.applies;
             o.status = status;
             v.outcome[in.index] = o;
         }
@@ -755,6 +860,8 @@ std::size_t fsp_shared_bytes() { return sizeof(Shared); }
 
 int fsp_blocks_per_sm(int threads) {
     switch (threads) {
+    case 128:
+        return blocks_per_sm_shape<128>();
     case 256:
         return blocks_per_sm_shape<256>();
     case 512:
@@ -770,6 +877,8 @@ cudaError_t launch_fsp_batch(const FspBatchView &v, int threads, int blocks,
         return cudaErrorInvalidValue;
     }
     switch (threads) {
+    case 128:
+        return launch_shape<128>(v, blocks, stream);
     case 256:
         return launch_shape<256>(v, blocks, stream);
     case 512:

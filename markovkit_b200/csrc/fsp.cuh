@@ -38,6 +38,8 @@ struct FspOutcome {
     std::int64_t attempts = 0;
     std::int64_t accepted = 0;
     std::int64_t support = 0;
+    std::int64_t substeps = 0;  // expv time steps
+    std::int64_t applies = 0;   // operator applies (Arnoldi steps and the extra ones)
     int status = 0; // 0 ok, 1 expv tolerance too high, 2 step limit, 3 non-finite
     int pad = 0;
 };
@@ -52,21 +54,20 @@ struct FspBatchView {
     // per-block workspace of `cap` states: Krylov basis and vectors, slot maps
     double *work = nullptr;
     int *iwork = nullptr;
-    unsigned char *flags = nullptr;
     std::int64_t cap = 0;
 };
 
 // block shapes the kernel is built for (threads per block); the autotuner picks one of these
 // and the number of blocks
-constexpr int kFspShapes[] = {256, 512};
+constexpr int kFspShapes[] = {128, 256, 512};
 
 // doubles and ints of per-block workspace for a capacity of `cap` states: the Krylov basis
-// (krylov_dim + 1 vectors) and five more vectors; the box-to-slot map, the slot list and a
-// compaction buffer
+// (krylov_dim + 1 vectors) and five more vectors; the box-to-slot map, the slot list, a
+// compaction buffer and the first-discoverer map of the expansion
 __host__ __device__ inline std::int64_t fsp_work_doubles(std::int64_t cap) {
     return (kFspMaxKrylov + 6) * cap;
 }
-__host__ __device__ inline std::int64_t fsp_work_ints(std::int64_t cap) { return 3 * cap; }
+__host__ __device__ inline std::int64_t fsp_work_ints(std::int64_t cap) { return 4 * cap; }
 std::size_t fsp_shared_bytes();
 
 // resident blocks per SM of the kernel with `threads` threads per block

@@ -94,6 +94,12 @@ def cases() -> dict:
     for k in (256, 257, 258):
         out[f"cfg_toggle_{k}"] = (network_of(inst[k]), inst[k]["initial"], inst[k]["final_time"],
                                   krylov_fsp_options(inside=box(inst[k]["bounds"]), tolerance=inst[k]["tolerance"]))
+    # a toggle whose box (63 x 244) cuts through a likely region: the leak budget forces tiny
+    # steps, so it stops at max_steps long before t = 2
+    k = 295
+    out[f"cfg_toggle_{k}_capped"] = (network_of(inst[k]), inst[k]["initial"], inst[k]["final_time"],
+                                     krylov_fsp_options(inside=box(inst[k]["bounds"]), tolerance=inst[k]["tolerance"],
+                                                        max_steps=300))
     return out
 
 
