@@ -16,6 +16,7 @@ struct mk_fsp_batch_s {
     std::vector<std::int64_t> out_offset;   // by instance
     std::int64_t total_box = 0;
     std::int64_t cap = 0;                   // largest box
+    int rmax = 0;                           // most reactions
     mkb::DeviceArray<mkb::FspInstance> d_inst;
     mkb::DeviceArray<double> d_rates, d_out;
     mkb::DeviceArray<mkb::FspOutcome> d_outcome;
@@ -105,13 +106,16 @@ void ensure_workspace(mk_fsp_batch_s &b, int blocks) {
     if (blocks <= b.workspace_blocks) {
         return;
     }
-    b.work.resize(static_cast<std::size_t>(blocks) * mkb::fsp_work_doubles(b.cap));
-    b.iwork.resize(static_cast<std::size_t>(blocks) * mkb::fsp_work_ints(b.cap));
+    b.work.resize(static_cast<std::size_t>(blocks) * mkb::fsp_work_doubles(b.cap, b.rmax));
+    b.iwork.resize(static_cast<std::size_t>(blocks) * mkb::fsp_work_ints(b.cap, b.rmax));
     b.workspace_blocks = blocks;
 }
 
+// blocks is the launch's total; the shared arena is what that many blocks per SM leave
 void launch(mk_fsp_batch_s &b, const mkb::FspInstance *d_inst, int n, int threads, int blocks,
             cudaStream_t stream) {
+    const int per_sm = std::max(1, (blocks + b.sms - 1) / b.sms);
+    const std::size_t arena = mkb::fsp_arena_bytes(threads, per_sm);
     blocks = std::max(1, std::min(blocks, n));
     ensure_workspace(b, blocks);
     mkb::check_cuda(cudaMemsetAsync(b.d_queue.get(), 0, sizeof(int), stream), "fsp queue reset");
@@ -125,6 +129,8 @@ void launch(mk_fsp_batch_s &b, const mkb::FspInstance *d_inst, int n, int thread
     v.work = b.work.get();
     v.iwork = b.iwork.get();
     v.cap = b.cap;
+    v.rmax = b.rmax;
+    v.arena_bytes = arena;
     mkb::check_cuda(mkb::launch_fsp_batch(v, threads, blocks, stream), "fsp kernel launch");
 }
 
@@ -222,6 +228,7 @@ int mk_fsp_batch_create(int n, const mk_fsp_problem *problems, mk_fsp_batch *out
             I.out_offset = b->total_box;
             b->total_box += box;
             b->cap = std::max(b->cap, box);
+            b->rmax = std::max(b->rmax, p.n_reactions);
         }
         std::vector<double> rates(static_cast<std::size_t>(std::max<std::int64_t>(rate_total, 1)),
                                   0.0);

@@ -13,16 +13,27 @@
 // dimension m, the augmented (m+2)-square Hessenberg, a Pade (6,6) exponential with scaling and
 // squaring, the two-term error estimate, safety factors 0.9 and 1.2, break-down below 1e-7.
 //
-// The support is a compact list of slots with a box-to-slot map, in the reference's order: an
-// expansion ring appends the new states in the order the reference discovers them (support
-// slot, then reaction; the first discoverer of a state wins, found with an atomic minimum over
-// candidate numbers), and dropped states are compacted out in order. Vectors and reductions
-// cost the support's size, not the box's.
-// One Arnoldi step is three block-wide phases: (1) the operator apply, which also writes the
-// basis vector V_j = p / ||p|| of the previous step and accumulates the first Gram-Schmidt
-// projections <V_i, Q V_j>; (2) the first subtraction fused with the second projections;
-// (3) the second subtraction fused with the norm. The small exponential's elimination runs on
-// two warps under a named barrier while the rest of the block waits once.
+// Data layout. The support is a compact list of slots with a box-to-slot map, in the
+// reference's order: an expansion ring appends new states in the order the reference discovers
+// them (support slot, then reaction; the first discoverer of a state wins, found with an atomic
+// minimum over candidate numbers), and dropped states are compacted out in order. After the
+// expansion, each attempt assembles Q on its support as R neighbour slots and coefficients per
+// state plus the exit rate (reaction-major arrays), as the reference assembles its generator,
+// so an apply is one gather per reaction. The assembled operator, the Krylov work vectors and
+// the basis go to the block's shared-memory arena in that order of priority, each wherever it
+// fits for the attempt's support size, else to the block's global workspace.
+//
+// One Arnoldi step is three block-wide phases with one barrier each: (1) the apply, which also
+// writes the basis vector V_j = p / ||p|| of the previous step and accumulates the first
+// Gram-Schmidt projections <V_i, Q V_j>; (2) the first subtraction fused with the second
+// projections; (3) the second subtraction fused with the norm. Reductions leave per-warp
+// partials in one of two alternating buffers, so each needs a single barrier.
+//
+// The Pade (6,6) approximant r(X) = q(X)^-1 p(X) of the scaled Hessenberg is formed from X^2,
+// X^4, X^6 and one product for the odd part; q(X)^-1 is computed by Newton-Schulz iteration
+// Y <- Y (2I - qY), which converges quadratically because ||I - q(X)|| <= 0.28 when
+// ||X|| <= 1/2; the iteration count follows from that norm. All of it is 32 x 32 products
+// spread over the whole block, not a serial elimination.
 // Every loop is bounded; no thread waits on another block.
 #include "fsp.cuh"
 #include "launch_count.hpp"
@@ -36,7 +47,6 @@ namespace {
 constexpr int kMaxWarps = 16;
 constexpr int kBasis = kFspMaxKrylov + 1;
 constexpr int kE = 32;               // side of the small dense matrices in shared memory
-constexpr int kDotChunk = 16;        // basis vectors per projection pass
 constexpr int kNoOwner = 0x7fffffff;
 constexpr int kSubstepLimit = 100000;
 constexpr std::int64_t kAttemptLimit = 1000000;
@@ -59,42 +69,116 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
-// barrier 1 over the first two warps only
-__device__ __forceinline__ void pair_barrier() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
-
 struct Shared {
     FspInstance in;
     double H[kE * kE];
-    double X[kE * kE], P[kE * kE], Q[kE * kE], PW[kE * kE], T[kE * kE], F[kE * kE];
-    double red[kMaxWarps * kE];
-    double h1[kE], h2[kE];
-    double fac[kE];
-    double s[8];
+    double M[7][kE * kE];            // the small exponential's matrices
+    double red[2][kMaxWarps * kE];   // alternating per-warp partials
+    double hw[kMaxWarps][kE];        // each warp's copy of the latest projections
+    double h1[kE];                   // first projections, kept for the Hessenberg column
     int i[8];
     int scan[kMaxWarps + 1];
 };
 
-// the block's sum (or max) of v, returned to all threads; fixed order, so reproducible
+struct Ctx {
+    const FspInstance *in; // the block's shared copy
+    const double *rate;
+    // the block's global workspace
+    double *gV, *prob, *gw, *gbuf0, *gbuf1, *gtmp, *gdiag, *gcoef;
+    int *b2s, *s2b, *itmp, *owner, *gnbr;
+    std::int64_t cap;
+    // this attempt's placement (shared arena or global workspace)
+    double *V, *w, *buf0, *buf1, *tmp, *diag, *coef;
+    int *nbr;
+    std::int64_t vs, es; // strides of basis vectors and of operator arrays
+    unsigned char *arena;
+    std::size_t arena_bytes;
+    int parity; // which partials buffer the next reduction uses
+};
+
+// the block's sum (or max) of v on every thread; one barrier
 template <int NT, bool MAX>
-__device__ double block_reduce(Shared &sh, double v) {
+__device__ double block_reduce(Shared &sh, Ctx &c, double v) {
     constexpr int W = NT / 32;
     v = MAX ? warp_max(v) : warp_sum(v);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *red = sh.red[c.parity];
+    c.parity ^= 1;
     if (lane == 0) {
-        sh.red[warp] = v;
+        red[warp] = v;
     }
     __syncthreads();
-    if (warp == 0) {
-        double t = lane < W ? sh.red[lane] : (MAX ? -INFINITY : 0.0);
-        t = MAX ? warp_max(t) : warp_sum(t);
-        if (lane == 0) {
-            sh.s[7] = t;
+    double t = red[0];
+#pragma unroll
+    for (int w = 1; w < W; ++w) {
+        t = MAX ? fmax(t, red[w]) : t + red[w];
+    }
+    return t;
+}
+
+// Reduces acc[q] over the warp (q < 16) with 16 shuffles: afterwards lane l holds the warp
+// total of one value, numbered by its lane bits 4..1. Writes the totals of values
+// k0 + q < K to red[warp * kE + k0 + q].
+__device__ __forceinline__ void stash_partials(double *red, double (&acc)[16], int k0, int K) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const bool hi = lane & 16;
+        const double send = hi ? acc[q] : acc[q + 8];
+        const double keep = hi ? acc[q + 8] : acc[q];
+        acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const bool hi = lane & 8;
+        const double send = hi ? acc[q] : acc[q + 4];
+        const double keep = hi ? acc[q + 4] : acc[q];
+        acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const bool hi = lane & 4;
+        const double send = hi ? acc[q] : acc[q + 2];
+        const double keep = hi ? acc[q + 2] : acc[q];
+        acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    {
+        const bool hi = lane & 2;
+        const double send = hi ? acc[0] : acc[1];
+        const double keep = hi ? acc[1] : acc[0];
+        acc[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
+    const int q = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 +
+                  ((lane >> 1) & 1);
+    if ((lane & 1) == 0 && k0 + q < K) {
+        red[warp * kE + k0 + q] = acc[0];
+    }
+}
+
+// after the partials of K values are stashed: one barrier, then every warp sums them into its
+// own row sh.hw[warp] (lane i holds value i), visible to the warp on return
+template <int NT>
+__device__ void finish_projections(Shared &sh, const double *red, int K) {
+    constexpr int W = NT / 32;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane < K) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            t += red[w * kE + lane];
         }
+        sh.hw[warp][lane] = t;
     }
-    __syncthreads();
-    const double r = sh.s[7];
-    __syncthreads();
-    return r;
+    __syncwarp();
+}
+
+__device__ __forceinline__ void zero16(double (&acc)[16]) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        acc[q] = 0.0;
+    }
 }
 
 // Order-preserving compaction of [0, L): emit(i, dest) for every i with pred(i), dest counting
@@ -136,15 +220,6 @@ __device__ int compact(Shared &sh, int L, Pred pred, Emit emit) {
     return base;
 }
 
-struct Ctx {
-    const FspInstance *in; // the block's shared copy
-    const double *rate;
-    double *V;             // kBasis vectors of stride cap
-    double *prob, *w, *buf0, *buf1, *tmp;
-    int *b2s, *s2b, *itmp, *owner;
-    std::int64_t cap;
-};
-
 __device__ __forceinline__ void coords(const FspInstance &in, int i, int (&x)[kFspMaxSpecies]) {
 #pragma unroll
     for (int s = 0; s < kFspMaxSpecies; ++s) {
@@ -152,318 +227,335 @@ __device__ __forceinline__ void coords(const FspInstance &in, int i, int (&x)[kF
     }
 }
 
-// Row k of Q applied to src: sum of in-jumps from supported states minus exit * src[k], or
-// with ABS the row's absolute sum (src unused). Every valid positive jump counts in the exit.
-template <bool ABS>
-__device__ __forceinline__ double row_apply(const Ctx &c, int k, const double *src) {
+// ---- placement and assembly -------------------------------------------------------------
+
+__device__ __forceinline__ void *take(Ctx &c, std::size_t &off, std::size_t bytes) {
+    bytes = (bytes + 15) & ~std::size_t(15);
+    if (off + bytes > c.arena_bytes) {
+        return nullptr;
+    }
+    void *p = c.arena + off;
+    off += bytes;
+    return p;
+}
+
+// where this attempt's operator, vectors and basis live (same answer on every thread)
+__device__ void place(Ctx &c, int n, int m) {
+    const int R = c.in->R;
+    std::size_t off = 0;
+    const std::size_t nd = static_cast<std::size_t>(n) * sizeof(double);
+    {
+        const std::size_t mark = off;
+        auto *coef = static_cast<double *>(take(c, off, nd * R));
+        auto *diag = static_cast<double *>(take(c, off, nd));
+        auto *nbr = static_cast<int *>(take(c, off, static_cast<std::size_t>(n) * R * sizeof(int)));
+        if (diag && (R == 0 || (coef && nbr))) {
+            c.coef = coef;
+            c.diag = diag;
+            c.nbr = nbr;
+            c.es = n;
+        } else {
+            off = mark;
+            c.coef = c.gcoef;
+            c.diag = c.gdiag;
+            c.nbr = c.gnbr;
+            c.es = c.cap;
+        }
+    }
+    {
+        const std::size_t mark = off;
+        auto *w = static_cast<double *>(take(c, off, nd));
+        auto *b0 = static_cast<double *>(take(c, off, nd));
+        auto *b1 = static_cast<double *>(take(c, off, nd));
+        auto *tmp = static_cast<double *>(take(c, off, nd));
+        if (w && b0 && b1 && tmp) {
+            c.w = w;
+            c.buf0 = b0;
+            c.buf1 = b1;
+            c.tmp = tmp;
+        } else {
+            off = mark;
+            c.w = c.gw;
+            c.buf0 = c.gbuf0;
+            c.buf1 = c.gbuf1;
+            c.tmp = c.gtmp;
+        }
+    }
+    auto *V = static_cast<double *>(take(c, off, nd * (m + 1)));
+    if (V) {
+        c.V = V;
+        c.vs = n;
+    } else {
+        c.V = c.gV;
+        c.vs = c.cap;
+    }
+}
+
+// Q on the support (generator.hpp:27-44, absorbing): for slot k and reaction r the source
+// slot and rate of the jump into k (coefficient 0 and the slot itself when there is none),
+// and the exit rate of k over every valid positive jump
+template <int NT>
+__device__ void assemble(const Ctx &c, int n) {
     const FspInstance &in = *c.in;
-    const int i = c.s2b[k];
-    int xi[kFspMaxSpecies];
-    coords(in, i, xi);
-    double acc = 0.0, ex = 0.0;
-    for (int r = 0; r < in.R; ++r) {
-        bool valid = true, inside = true;
-        int j = i;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        const int i = c.s2b[k];
+        int xi[kFspMaxSpecies];
+        coords(in, i, xi);
+        double ex = 0.0;
+        for (int r = 0; r < in.R; ++r) {
+            bool valid = true, inside = true;
+            int j = i;
 #pragma unroll
-        for (int s = 0; s < kFspMaxSpecies; ++s) {
-            if (s < in.S) {
-                const int ch = in.change[r][s];
-                valid = valid && xi[s] + ch >= 0;
-                const int xs = xi[s] - ch;
-                inside = inside && xs >= 0 && xs <= in.bound[s];
-                j -= ch * in.stride[s];
-            }
-        }
-        const double a = c.rate[static_cast<std::int64_t>(r) * in.box + i];
-        if (a > 0.0 && valid) {
-            ex += a;
-        }
-        if (inside) {
-            const int sl = c.b2s[j];
-            if (sl >= 0) {
-                const double aj = c.rate[static_cast<std::int64_t>(r) * in.box + j];
-                if (aj > 0.0) {
-                    if constexpr (ABS) {
-                        acc += aj;
-                    } else {
-                        acc += aj * src[sl];
-                    }
+            for (int s = 0; s < kFspMaxSpecies; ++s) {
+                if (s < in.S) {
+                    const int ch = in.change[r][s];
+                    valid = valid && xi[s] + ch >= 0;
+                    const int xs = xi[s] - ch;
+                    inside = inside && xs >= 0 && xs <= in.bound[s];
+                    j -= ch * in.stride[s];
                 }
             }
-        }
-    }
-    if constexpr (ABS) {
-        return acc + ex;
-    } else {
-        return acc - ex * src[k];
-    }
-}
-
-// out = Q src over the n slots
-template <int NT>
-__device__ void apply_plain(const Ctx &c, int n, const double *src, double *out) {
-    for (int k = threadIdx.x; k < n; k += NT) {
-        out[k] = row_apply<false>(c, k, src);
-    }
-    __syncthreads();
-}
-
-// warp partial sums of acc[q] (basis vector k0 + q, below K) into sh.red
-__device__ __forceinline__ void stash_partials(Shared &sh, const double (&acc)[kDotChunk], int k0,
-                                               int K) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-    for (int q = 0; q < kDotChunk; ++q) {
-        if (k0 + q < K) {
-            const double v = warp_sum(acc[q]);
-            if (lane == 0) {
-                sh.red[warp * kE + k0 + q] = v;
+            const double a = c.rate[static_cast<std::int64_t>(r) * in.box + i];
+            if (a > 0.0 && valid) {
+                ex += a;
             }
+            int sl = k;
+            double coef = 0.0;
+            if (inside) {
+                const int src = c.b2s[j];
+                const double aj = c.rate[static_cast<std::int64_t>(r) * in.box + j];
+                if (src >= 0 && aj > 0.0) {
+                    sl = src;
+                    coef = aj;
+                }
+            }
+            c.nbr[r * c.es + k] = sl;
+            c.coef[r * c.es + k] = coef;
         }
-    }
-}
-
-// h[i] = sum over warps of the stashed partials, i < K, visible to every thread on return
-template <int NT>
-__device__ void finish_dots(Shared &sh, int K, double *h) {
-    constexpr int W = NT / 32;
-    __syncthreads();
-    if (static_cast<int>(threadIdx.x) < K) {
-        double t = 0.0;
-        for (int w = 0; w < W; ++w) {
-            t += sh.red[w * kE + threadIdx.x];
-        }
-        h[threadIdx.x] = t;
+        c.diag[k] = ex;
     }
     __syncthreads();
 }
 
-__device__ __forceinline__ void zero(double (&acc)[kDotChunk]) {
-#pragma unroll
-    for (int q = 0; q < kDotChunk; ++q) {
-        acc[q] = 0.0;
+// (Q x)_k from the assembled operator
+__device__ __forceinline__ double row(const Ctx &c, int R, int k, const double *x) {
+    double acc = 0.0;
+    for (int r = 0; r < R; ++r) {
+        acc += c.coef[r * c.es + k] * x[c.nbr[r * c.es + k]];
     }
+    return acc - c.diag[k] * x[k];
 }
 
-// Arnoldi phase 1: V_j = src / div, out = Q V_j, sh.h1[i] = <V_i, out> for i <= j
+// ---- Arnoldi phases -------------------------------------------------------------------
+
+// phase 1: V_j = src / div, out = Q V_j, projections <V_i, out> for i <= j into sh.hw
 template <int NT>
-__device__ void arnoldi_apply(Shared &sh, const Ctx &c, int n, const double *src, double div,
-                              int j, double *out) {
-    const int K = j + 1;
-    double *Vj = c.V + static_cast<std::int64_t>(j) * c.cap;
-    double acc[kDotChunk];
-    zero(acc);
+__device__ void arnoldi_apply(Shared &sh, Ctx &c, int n, const double *src, double div, int j,
+                              double *out) {
+    const int K = j + 1, R = c.in->R;
+    double *Vj = c.V + j * c.vs;
+    double *red = sh.red[c.parity];
+    c.parity ^= 1;
+    double acc[16];
+    zero16(acc);
     for (int k = threadIdx.x; k < n; k += NT) {
-        const double y = row_apply<false>(c, k, src) / div;
+        const double y = row(c, R, k, src) / div;
         const double vk = src[k] / div;
         Vj[k] = vk;
         out[k] = y;
 #pragma unroll
-        for (int q = 0; q < kDotChunk; ++q) {
+        for (int q = 0; q < 16; ++q) {
             if (q < K) {
-                const double v = q == j ? vk : c.V[q * c.cap + k];
-                acc[q] += v * y;
+                acc[q] += (q == j ? vk : c.V[q * c.vs + k]) * y;
             }
         }
     }
-    stash_partials(sh, acc, 0, K);
-    for (int k0 = kDotChunk; k0 < K; k0 += kDotChunk) {
-        zero(acc);
+    stash_partials(red, acc, 0, K);
+    if (K > 16) {
+        zero16(acc);
         for (int k = threadIdx.x; k < n; k += NT) {
             const double y = out[k];
 #pragma unroll
-            for (int q = 0; q < kDotChunk; ++q) {
-                if (k0 + q < K) {
-                    acc[q] += c.V[(k0 + q) * c.cap + k] * y;
+            for (int q = 0; q < 16; ++q) {
+                if (16 + q < K) {
+                    acc[q] += (16 + q == j ? Vj[k] : c.V[(16 + q) * c.vs + k]) * y;
                 }
             }
         }
-        stash_partials(sh, acc, k0, K);
+        stash_partials(red, acc, 16, K);
     }
-    finish_dots<NT>(sh, K, sh.h1);
+    finish_projections<NT>(sh, red, K);
 }
 
-// Arnoldi phase 2: out -= sum_i h1[i] V_i, then sh.h2[i] = <V_i, out>
+// phase 2: out -= sum_i h1[i] V_i, then the second projections <V_i, out> into sh.hw
 template <int NT>
-__device__ void arnoldi_reorthogonalise(Shared &sh, const Ctx &c, int n, int K, double *out) {
-    double acc[kDotChunk];
-    zero(acc);
+__device__ void arnoldi_reorthogonalise(Shared &sh, Ctx &c, int n, int K, double *out) {
+    const int warp = threadIdx.x >> 5;
+    const double *h = sh.hw[warp];
+    double *red = sh.red[c.parity];
+    c.parity ^= 1;
+    double acc[16];
+    zero16(acc);
     for (int k = threadIdx.x; k < n; k += NT) {
         double v = out[k];
         for (int i = 0; i < K; ++i) {
-            v -= sh.h1[i] * c.V[i * c.cap + k];
+            v -= h[i] * c.V[i * c.vs + k];
         }
         out[k] = v;
 #pragma unroll
-        for (int q = 0; q < kDotChunk; ++q) {
+        for (int q = 0; q < 16; ++q) {
             if (q < K) {
-                acc[q] += c.V[q * c.cap + k] * v;
+                acc[q] += c.V[q * c.vs + k] * v;
             }
         }
     }
-    stash_partials(sh, acc, 0, K);
-    for (int k0 = kDotChunk; k0 < K; k0 += kDotChunk) {
-        zero(acc);
+    // keep the first projections for the Hessenberg column before sh.hw is overwritten
+    if (warp == 0 && static_cast<int>(threadIdx.x) < K) {
+        sh.h1[threadIdx.x] = h[threadIdx.x];
+    }
+    stash_partials(red, acc, 0, K);
+    if (K > 16) {
+        zero16(acc);
         for (int k = threadIdx.x; k < n; k += NT) {
             const double v = out[k];
 #pragma unroll
-            for (int q = 0; q < kDotChunk; ++q) {
-                if (k0 + q < K) {
-                    acc[q] += c.V[(k0 + q) * c.cap + k] * v;
+            for (int q = 0; q < 16; ++q) {
+                if (16 + q < K) {
+                    acc[q] += c.V[(16 + q) * c.vs + k] * v;
                 }
             }
         }
-        stash_partials(sh, acc, k0, K);
+        stash_partials(red, acc, 16, K);
     }
-    finish_dots<NT>(sh, K, sh.h2);
+    finish_projections<NT>(sh, red, K);
 }
 
-// Arnoldi phase 3: out -= sum_i h2[i] V_i; returns ||out||^2
+// phase 3: out -= sum_i h2[i] V_i; returns ||out||^2
 template <int NT>
-__device__ double arnoldi_finish(Shared &sh, const Ctx &c, int n, int K, double *out) {
+__device__ double arnoldi_finish(Shared &sh, Ctx &c, int n, int K, double *out) {
+    const double *h = sh.hw[threadIdx.x >> 5];
     double sq = 0.0;
     for (int k = threadIdx.x; k < n; k += NT) {
         double v = out[k];
         for (int i = 0; i < K; ++i) {
-            v -= sh.h2[i] * c.V[i * c.cap + k];
+            v -= h[i] * c.V[i * c.vs + k];
         }
         out[k] = v;
         sq += v * v;
     }
-    return block_reduce<NT, false>(sh, sq);
+    return block_reduce<NT, false>(sh, c, sq);
 }
 
-template <int NT>
-__device__ double dot(Shared &sh, const double *a, const double *b, int n) {
-    double v = 0.0;
-    for (int k = threadIdx.x; k < n; k += NT) {
-        v += a[k] * b[k];
-    }
-    return block_reduce<NT, false>(sh, v);
-}
+// ---- the small exponential ------------------------------------------------------------
 
-// C = A B for n x n matrices in shared memory (row-major, side kE)
-template <int NT>
+// C = A B (+ epilogue) for n x n matrices in shared memory (row-major, side kE):
+// MODE 0: C = A B; MODE 1: C = 2 A - A B
+template <int NT, int MODE>
 __device__ void matmul(const double *A, const double *B, double *C, int n) {
     for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e / n, j = e % n;
+        const int i = e / n, j = e - i * n;
         double s = 0.0;
         for (int k = 0; k < n; ++k) {
             s += A[i * kE + k] * B[k * kE + j];
         }
-        C[i * kE + j] = s;
+        C[i * kE + j] = MODE == 0 ? s : 2.0 * A[i * kE + j] - s;
     }
     __syncthreads();
 }
 
-// F = Q^{-1} F by Gauss-Jordan elimination with partial pivoting (first largest pivot), on the
-// first two warps: thread j < 32 owns column j of Q, thread 32 + j column j of F. The pivot
-// row is swapped in by each column's owner; the factors come from warp 0 before the swap.
+// exp(X) for the n x n matrix in sh.M[0] (overwritten); returns the matrix holding the result
 template <int NT>
-__device__ void solve_pade(Shared &sh, int n) {
-    if (threadIdx.x < 64) {
-        const int lane = threadIdx.x & 31;
-        double *M = threadIdx.x < 32 ? sh.Q : sh.F;
-        for (int k = 0; k < n; ++k) {
-            if (threadIdx.x < 32) {
-                double a = (lane >= k && lane < n) ? fabs(sh.Q[lane * kE + k]) : -1.0;
-                int idx = lane;
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const double oa = __shfl_xor_sync(0xffffffffu, a, off);
-                    const int oi = __shfl_xor_sync(0xffffffffu, idx, off);
-                    if (oa > a || (oa == a && oi < idx)) {
-                        a = oa;
-                        idx = oi;
-                    }
-                }
-                const int piv = idx;
-                const double pivot = sh.Q[piv * kE + k];
-                if (lane < n) {
-                    const int src = lane == k ? piv : (lane == piv ? k : lane);
-                    sh.fac[lane] = lane == k ? 0.0 : sh.Q[src * kE + k] / pivot;
-                }
-                if (lane == 0) {
-                    sh.i[0] = piv;
-                }
-            }
-            pair_barrier();
-            const int piv = sh.i[0];
-            if (lane < n) {
-                const double rk = M[piv * kE + lane];
-                M[piv * kE + lane] = M[k * kE + lane];
-                M[k * kE + lane] = rk;
-                for (int i = 0; i < n; ++i) {
-                    const double f = sh.fac[i];
-                    if (f != 0.0) {
-                        M[i * kE + lane] -= f * rk;
-                    }
-                }
-            }
-            pair_barrier();
-        }
-        if (threadIdx.x >= 32 && lane < n) {
-            for (int i = 0; i < n; ++i) {
-                sh.F[i * kE + lane] /= sh.Q[i * kE + i];
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// sh.F = exp(sh.X) for an n x n matrix: Pade (6,6) with scaling and squaring
-template <int NT>
-__device__ void small_expm(Shared &sh, int n) {
+__device__ const double *small_expm(Shared &sh, Ctx &c, int n) {
+    double *X = sh.M[0];
     double rowmax = 0.0;
     for (int i = threadIdx.x; i < n; i += NT) {
         double r = 0.0;
         for (int j = 0; j < n; ++j) {
-            r += fabs(sh.X[i * kE + j]);
+            r += fabs(X[i * kE + j]);
         }
         rowmax = fmax(rowmax, r);
     }
-    const double norm = block_reduce<NT, true>(sh, rowmax);
+    const double norm = block_reduce<NT, true>(sh, c, rowmax);
     int squarings = 0;
     if (norm > 0.5) {
         squarings = max(0, static_cast<int>(ceil(log2(norm / 0.5))));
     }
     const double scale = ldexp(1.0, -squarings);
     for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e / n, j = e % n;
-        sh.X[i * kE + j] *= scale;
-        const double id = i == j ? 1.0 : 0.0;
-        sh.PW[i * kE + j] = id;
-        sh.P[i * kE + j] = id;
-        sh.Q[i * kE + j] = id;
+        const int i = e / n, j = e - i * n;
+        X[i * kE + j] *= scale;
     }
     __syncthreads();
-    constexpr int p = 6;
-    double cf = 1.0;
-    for (int k = 1; k <= p; ++k) {
-        cf *= static_cast<double>(p - k + 1) / static_cast<double>(k * ((2 * p) - k + 1));
-        matmul<NT>(sh.PW, sh.X, sh.T, n);
-        const double sign = (k % 2 == 0) ? 1.0 : -1.0;
-        for (int e = threadIdx.x; e < n * n; e += NT) {
-            const int i = e / n, j = e % n;
-            const double v = sh.T[i * kE + j];
-            sh.PW[i * kE + j] = v;
-            sh.P[i * kE + j] += cf * v;
-            sh.Q[i * kE + j] += sign * cf * v;
-            if (k == p) {
-                sh.F[i * kE + j] = sh.P[i * kE + j];
-            }
-        }
-        __syncthreads();
+    // Pade (6,6) coefficients c_k = c_{k-1} (p - k + 1) / (k (2p - k + 1))
+    double cf[7];
+    cf[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= 6; ++k) {
+        cf[k] = cf[k - 1] * static_cast<double>(6 - k + 1) / static_cast<double>(k * (12 - k + 1));
     }
-    solve_pade<NT>(sh, n);
+    double *X2 = sh.M[1], *X4 = sh.M[2], *X6 = sh.M[3];
+    matmul<NT, 0>(X, X, X2, n);
+    matmul<NT, 0>(X2, X2, X4, n);
+    matmul<NT, 0>(X4, X2, X6, n);
+    // U = c0 + c2 X^2 + c4 X^4 + c6 X^6 (into M[4]); odd factor c1 + c3 X^2 + c5 X^4 (into M[3])
+    double *U = sh.M[4], *Vt = sh.M[3];
+    for (int e = threadIdx.x; e < n * n; e += NT) {
+        const int i = e / n, j = e - i * n;
+        const double id = i == j ? 1.0 : 0.0;
+        const double a = X2[i * kE + j], b = X4[i * kE + j], d = X6[i * kE + j];
+        U[i * kE + j] = cf[0] * id + cf[2] * a + cf[4] * b + cf[6] * d;
+        Vt[i * kE + j] = cf[1] * id + cf[3] * a + cf[5] * b;
+    }
+    __syncthreads();
+    double *Vo = sh.M[1];
+    matmul<NT, 0>(X, Vt, Vo, n); // odd part
+    // P = U + Vo (M[2]), Q = U - Vo (M[3]); ||I - Q||
+    double *P = sh.M[2], *Q = sh.M[3];
+    for (int e = threadIdx.x; e < n * n; e += NT) {
+        const int i = e / n, j = e - i * n;
+        const double u = U[i * kE + j], v = Vo[i * kE + j];
+        P[i * kE + j] = u + v;
+        Q[i * kE + j] = u - v;
+    }
+    __syncthreads();
+    double rowdev = 0.0;
+    for (int i = threadIdx.x; i < n; i += NT) {
+        double r = 0.0;
+        for (int j = 0; j < n; ++j) {
+            r += fabs((i == j ? 1.0 : 0.0) - Q[i * kE + j]);
+        }
+        rowdev = fmax(rowdev, r);
+    }
+    const double eps = block_reduce<NT, true>(sh, c, rowdev);
+    // Newton-Schulz: Y_0 = I, ||I - Q Y_k|| <= eps^(2^k); stop below 1e-18
+    int iters = 0;
+    if (eps > 0.0) {
+        iters = eps < 0.95 ? static_cast<int>(ceil(log2(log(1e-18) / log(eps)))) : 10;
+        iters = min(max(iters, 0), 10);
+    }
+    double *Y = sh.M[4], *Tm = sh.M[5], *Y2 = sh.M[6];
+    for (int e = threadIdx.x; e < n * n; e += NT) {
+        const int i = e / n, j = e - i * n;
+        Y[i * kE + j] = i == j ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int it = 0; it < iters; ++it) {
+        matmul<NT, 0>(Q, Y, Tm, n);
+        matmul<NT, 1>(Y, Tm, Y2, n);
+        double *t = Y;
+        Y = Y2;
+        Y2 = t;
+    }
+    double *F = Y2;
+    matmul<NT, 0>(Y, P, F, n);
+    double *spare = sh.M[0];
     for (int s = 0; s < squarings; ++s) {
-        matmul<NT>(sh.F, sh.F, sh.T, n);
-        for (int e = threadIdx.x; e < n * n; e += NT) {
-            const int i = e / n, j = e % n;
-            sh.F[i * kE + j] = sh.T[i * kE + j];
-        }
-        __syncthreads();
+        matmul<NT, 0>(F, F, spare, n);
+        double *t = F;
+        F = spare;
+        spare = t;
     }
+    return F;
 }
 
 // two significant digits, rounded up (Expokit's step rounding)
@@ -478,22 +570,29 @@ struct Counters {
 
 // c.w (n slots) <- exp(t Q) c.w; returns 0, or an FspOutcome status
 template <int NT>
-__device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double tol,
-                    Counters &cnt) {
+__device__ int expv(Shared &sh, Ctx &c, int n, int m, double t, double tol, Counters &cnt) {
     if (n == 0 || t == 0.0) {
         return 0;
     }
-    const int m = min(max(m_req, 1), n);
+    const int R = c.in->R;
     double rowmax = 0.0;
     for (int k = threadIdx.x; k < n; k += NT) {
-        rowmax = fmax(rowmax, row_apply<true>(c, k, nullptr));
+        double r = c.diag[k];
+        for (int q = 0; q < R; ++q) {
+            r += c.coef[q * c.es + k];
+        }
+        rowmax = fmax(rowmax, r);
     }
     ++cnt.applies;
-    const double anorm = fmax(block_reduce<NT, true>(sh, rowmax), 1e-300);
+    const double anorm = fmax(block_reduce<NT, true>(sh, c, rowmax), 1e-300);
     constexpr int max_reject = 10;
     constexpr double btol = 1e-7, gamma = 0.9, delta = 1.2;
     const double t_out = fabs(t), sgn = t < 0.0 ? -1.0 : 1.0;
-    double beta = sqrt(dot<NT>(sh, c.w, c.w, n));
+    double sq0 = 0.0;
+    for (int k = threadIdx.x; k < n; k += NT) {
+        sq0 += c.w[k] * c.w[k];
+    }
+    double beta = sqrt(block_reduce<NT, false>(sh, c, sq0));
     if (!(beta > 0.0)) {
         return 0;
     }
@@ -512,7 +611,6 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
         for (int e = threadIdx.x; e < hd * hd; e += NT) {
             sh.H[(e / hd) * kE + (e % hd)] = 0.0;
         }
-        __syncthreads();
         int k1 = 2, mb = m;
         const double *src = c.w;
         double div = beta;
@@ -520,8 +618,8 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
         for (int j = 0; j < m; ++j) {
             arnoldi_apply<NT>(sh, c, n, src, div, j, out);
             arnoldi_reorthogonalise<NT>(sh, c, n, j + 1, out);
-            for (int i = threadIdx.x; i <= j; i += NT) {
-                sh.H[i * kE + j] = sh.h1[i] + sh.h2[i];
+            if (threadIdx.x < 32 && static_cast<int>(threadIdx.x) <= j) {
+                sh.H[threadIdx.x * kE + j] = sh.h1[threadIdx.x] + sh.hw[0][threadIdx.x];
             }
             const double s = sqrt(arnoldi_finish<NT>(sh, c, n, j + 1, out));
             ++cnt.applies;
@@ -544,10 +642,10 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
         double avnorm = 0.0;
         if (k1 != 0) {
             // V_m = src / div, and ||Q V_m||
-            double *Vm = c.V + static_cast<std::int64_t>(m) * c.cap;
+            double *Vm = c.V + m * c.vs;
             double sq = 0.0;
             for (int k = threadIdx.x; k < n; k += NT) {
-                const double y = row_apply<false>(c, k, src) / div;
+                const double y = row(c, R, k, src) / div;
                 Vm[k] = src[k] / div;
                 sq += y * y;
             }
@@ -555,23 +653,26 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
             if (threadIdx.x == 0) {
                 sh.H[(m + 1) * kE + m] = 1.0;
             }
-            avnorm = sqrt(block_reduce<NT, false>(sh, sq));
+            avnorm = sqrt(block_reduce<NT, false>(sh, c, sq));
+        } else {
+            __syncthreads();
         }
         double err_loc = 0.0, xm = 1.0 / m;
+        const double *F = nullptr;
         for (int reject = 0;; ++reject) {
             const int mx = mb + k1;
             for (int e = threadIdx.x; e < mx * mx; e += NT) {
                 const int i = e / mx, j = e % mx;
-                sh.X[i * kE + j] = sgn * t_step * sh.H[i * kE + j];
+                sh.M[0][i * kE + j] = sgn * t_step * sh.H[i * kE + j];
             }
             __syncthreads();
-            small_expm<NT>(sh, mx);
+            F = small_expm<NT>(sh, c, mx);
             if (k1 == 0) {
                 err_loc = btol;
                 break;
             }
-            const double phi1 = fabs(beta * sh.F[m * kE]);
-            const double phi2 = fabs(beta * sh.F[(m + 1) * kE] * avnorm);
+            const double phi1 = fabs(beta * F[m * kE]);
+            const double phi2 = fabs(beta * F[(m + 1) * kE] * avnorm);
             if (phi1 > 10.0 * phi2) {
                 err_loc = phi2;
                 xm = 1.0 / m;
@@ -596,12 +697,12 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
         for (int k = threadIdx.x; k < n; k += NT) {
             double v = 0.0;
             for (int j = 0; j < used; ++j) {
-                v += (beta * sh.F[j * kE]) * c.V[static_cast<std::int64_t>(j) * c.cap + k];
+                v += (beta * F[j * kE]) * c.V[j * c.vs + k];
             }
             c.w[k] = v;
             sq += v * v;
         }
-        beta = sqrt(block_reduce<NT, false>(sh, sq));
+        beta = sqrt(block_reduce<NT, false>(sh, c, sq));
         t_now += t_step;
         t_new = gamma * t_step * pow(t_step * tol / fmax(err_loc, 1e-300), xm);
         t_new = round_step(t_new);
@@ -614,6 +715,8 @@ __device__ int expv(Shared &sh, const Ctx &c, int n, double t, int m_req, double
     }
     return 0;
 }
+
+// ---- support maintenance --------------------------------------------------------------
 
 // the state reached from slot k by reaction r, if the jump exists, stays in the box and leads
 // outside the support
@@ -684,23 +787,29 @@ __device__ int expand(Shared &sh, const Ctx &c, int n) {
 
 template <int NT>
 __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchView v) {
-    extern __shared__ double smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     Shared &sh = *reinterpret_cast<Shared *>(smem_raw);
     Ctx c;
     c.cap = v.cap;
     c.in = &sh.in;
-    double *wb = v.work + static_cast<std::int64_t>(blockIdx.x) * fsp_work_doubles(v.cap);
-    c.V = wb;
+    c.arena = smem_raw + ((sizeof(Shared) + 15) & ~std::size_t(15));
+    c.arena_bytes = v.arena_bytes;
+    c.parity = 0;
+    double *wb = v.work + static_cast<std::int64_t>(blockIdx.x) * fsp_work_doubles(v.cap, v.rmax);
+    c.gV = wb;
     c.prob = wb + kBasis * v.cap;
-    c.w = c.prob + v.cap;
-    c.buf0 = c.w + v.cap;
-    c.buf1 = c.buf0 + v.cap;
-    c.tmp = c.buf1 + v.cap;
-    int *ib = v.iwork + static_cast<std::int64_t>(blockIdx.x) * fsp_work_ints(v.cap);
+    c.gw = c.prob + v.cap;
+    c.gbuf0 = c.gw + v.cap;
+    c.gbuf1 = c.gbuf0 + v.cap;
+    c.gtmp = c.gbuf1 + v.cap;
+    c.gdiag = c.gtmp + v.cap;
+    c.gcoef = c.gdiag + v.cap;
+    int *ib = v.iwork + static_cast<std::int64_t>(blockIdx.x) * fsp_work_ints(v.cap, v.rmax);
     c.b2s = ib;
     c.s2b = ib + v.cap;
     c.itmp = ib + 2 * v.cap;
     c.owner = ib + 3 * v.cap;
+    c.gnbr = ib + 4 * v.cap;
 
     while (true) {
         if (threadIdx.x == 0) {
@@ -741,11 +850,13 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
         for (; t < in.final_time && attempt < limit; ++attempt) {
             tau = fmin(tau, in.final_time - t);
             n = expand<NT>(sh, c, n);
+            const int m = min(max(in.krylov_dim, 1), n);
+            place(c, n, m);
             for (int k = threadIdx.x; k < n; k += NT) {
                 c.w[k] = c.prob[k];
             }
-            __syncthreads();
-            status = expv<NT>(sh, c, n, tau, in.krylov_dim, in.krylov_tol, cnt);
+            assemble<NT>(c, n);
+            status = expv<NT>(sh, c, n, m, tau, in.krylov_tol, cnt);
             if (status != 0) {
                 break;
             }
@@ -753,17 +864,17 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
             for (int k = threadIdx.x; k < n; k += NT) {
                 pos += fmax(0.0, c.w[k]);
             }
-            const double mass = block_reduce<NT, false>(sh, pos);
+            const double mass = block_reduce<NT, false>(sh, c, pos);
             if (mass < 1.0 - (in.tolerance * (t + tau) / in.final_time) && tau > 1e-14) {
                 tau *= 0.5;
                 continue;
             }
             // dp = Q w; keep max(0, w); drop what is both unlikely and nearly constant
-            apply_plain<NT>(c, n, c.w, c.tmp);
-            ++cnt.applies;
             for (int k = threadIdx.x; k < n; k += NT) {
+                c.tmp[k] = row(c, in.R, k, c.w);
                 c.prob[k] = fmax(0.0, c.w[k]);
             }
+            ++cnt.applies;
             __syncthreads();
             const int kept = compact<NT>(
                 sh, n,
@@ -788,7 +899,7 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
                 tot += c.buf0[k];
             }
             n = kept;
-            const double total = block_reduce<NT, false>(sh, tot);
+            const double total = block_reduce<NT, false>(sh, c, tot);
             if (total > 0.0) {
                 for (int k = threadIdx.x; k < n; k += NT) {
                     c.prob[k] /= total;
@@ -825,9 +936,11 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
     }
 }
 
+constexpr std::size_t kFixedShared = (sizeof(Shared) + 15) & ~std::size_t(15);
+
 template <int NT>
 cudaError_t launch_shape(const FspBatchView &v, int blocks, cudaStream_t stream) {
-    const std::size_t smem = sizeof(Shared);
+    const std::size_t smem = kFixedShared + v.arena_bytes;
     cudaError_t e = cudaFuncSetAttribute(fsp_kernel<NT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
@@ -840,8 +953,8 @@ cudaError_t launch_shape(const FspBatchView &v, int blocks, cudaStream_t stream)
 }
 
 template <int NT>
-int blocks_per_sm_shape() {
-    const std::size_t smem = sizeof(Shared);
+int occupancy(std::size_t arena) {
+    const std::size_t smem = kFixedShared + arena;
     if (cudaFuncSetAttribute(fsp_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem)) != cudaSuccess) {
         return 0;
@@ -854,21 +967,48 @@ int blocks_per_sm_shape() {
     return blocks;
 }
 
-} // namespace
-
-std::size_t fsp_shared_bytes() { return sizeof(Shared); }
-
-int fsp_blocks_per_sm(int threads) {
+int occupancy_of(int threads, std::size_t arena) {
     switch (threads) {
     case 128:
-        return blocks_per_sm_shape<128>();
+        return occupancy<128>(arena);
     case 256:
-        return blocks_per_sm_shape<256>();
+        return occupancy<256>(arena);
     case 512:
-        return blocks_per_sm_shape<512>();
+        return occupancy<512>(arena);
     default:
         return 0;
     }
+}
+
+} // namespace
+
+std::size_t fsp_fixed_shared_bytes() { return kFixedShared; }
+
+int fsp_blocks_per_sm(int threads) { return occupancy_of(threads, 0); }
+
+std::size_t fsp_arena_bytes(int threads, int blocks_per_sm) {
+    if (blocks_per_sm < 1 || occupancy_of(threads, 0) < blocks_per_sm) {
+        return 0;
+    }
+    int dev = 0, per_sm = 0, per_block = 0, reserved = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) !=
+            cudaSuccess) {
+        return 0;
+    }
+    std::size_t share = static_cast<std::size_t>(per_sm) / blocks_per_sm;
+    share = share > static_cast<std::size_t>(reserved) ? share - reserved : 0;
+    share = share < static_cast<std::size_t>(per_block) ? share : per_block;
+    std::size_t arena = share > kFixedShared ? (share - kFixedShared) & ~std::size_t(1023) : 0;
+    // step down until the occupancy calculator agrees
+    while (arena > 0 && occupancy_of(threads, arena) < blocks_per_sm) {
+        arena = arena > 4096 ? arena - 4096 : 0;
+    }
+    return arena;
 }
 
 cudaError_t launch_fsp_batch(const FspBatchView &v, int threads, int blocks,

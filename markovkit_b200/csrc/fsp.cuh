@@ -2,6 +2,7 @@
 // (markovkit/fsp.hpp:190-254) in one persistent kernel, one block per instance.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -51,26 +52,38 @@ struct FspBatchView {
     double *out = nullptr;          // final distributions, box order
     FspOutcome *outcome = nullptr;
     int *queue = nullptr;           // next instance to take (atomic)
-    // per-block workspace of `cap` states: Krylov basis and vectors, slot maps
+    // per-block workspace of `cap` states (see fsp_work_doubles / fsp_work_ints)
     double *work = nullptr;
     int *iwork = nullptr;
     std::int64_t cap = 0;
+    int rmax = 0;                   // most reactions of any instance
+    // shared memory per block beyond the fixed part, for the vectors, the assembled operator
+    // and the Krylov basis of an instance small enough to keep there
+    std::size_t arena_bytes = 0;
 };
 
-// block shapes the kernel is built for (threads per block); the autotuner picks one of these
-// and the number of blocks
+// block sizes the kernel is built for; the autotuner picks one and the blocks per SM
 constexpr int kFspShapes[] = {128, 256, 512};
 
-// doubles and ints of per-block workspace for a capacity of `cap` states: the Krylov basis
-// (krylov_dim + 1 vectors) and five more vectors; the box-to-slot map, the slot list, a
-// compaction buffer and the first-discoverer map of the expansion
-__host__ __device__ inline std::int64_t fsp_work_doubles(std::int64_t cap) {
-    return (kFspMaxKrylov + 6) * cap;
+// Per-block global workspace for `cap` states and up to `rmax` reactions. Doubles: the Krylov
+// basis (krylov_dim + 1 vectors), five vectors and the assembled operator (rmax coefficients
+// and the exit rate per state). Ints: the box-to-slot map, the slot list, a compaction buffer,
+// the first-discoverer map of the expansion and rmax neighbour slots per state.
+__host__ __device__ inline std::int64_t fsp_work_doubles(std::int64_t cap, int rmax) {
+    return (kFspMaxKrylov + 7 + rmax) * cap;
 }
-__host__ __device__ inline std::int64_t fsp_work_ints(std::int64_t cap) { return 4 * cap; }
-std::size_t fsp_shared_bytes();
+__host__ __device__ inline std::int64_t fsp_work_ints(std::int64_t cap, int rmax) {
+    return (4 + rmax) * cap;
+}
 
-// resident blocks per SM of the kernel with `threads` threads per block
+// the fixed shared memory of a block
+std::size_t fsp_fixed_shared_bytes();
+
+// Largest arena with which `blocks_per_sm` blocks of `threads` threads fit on one SM (0 if
+// they do not fit even without one).
+std::size_t fsp_arena_bytes(int threads, int blocks_per_sm);
+
+// most resident blocks per SM of the kernel with `threads` threads and no arena
 int fsp_blocks_per_sm(int threads);
 
 // instances are taken in queue order: v.inst[0], v.inst[1], ...; *v.queue must be 0

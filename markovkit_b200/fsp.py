@@ -18,6 +18,7 @@ from typing import Callable, Optional, Sequence
 
 import numpy as np
 
+from . import _lib as _L
 from ._lib import MK_ENOTCONV, FspOptions, FspProblem, FspResult, check, load
 
 
@@ -191,11 +192,9 @@ class fsp_batch:
         self.offsets = np.array(offsets[:], dtype=np.int64)
 
     def __del__(self):
-        from . import _lib as L
-
         h = getattr(self, "_h", None)
-        if h and h.value and L._lib is not None:
-            L._lib.mk_fsp_batch_destroy(h)
+        if h and h.value and _L._lib is not None:
+            _L._lib.mk_fsp_batch_destroy(h)
             self._h = C.c_void_p()
 
     def __len__(self) -> int:
