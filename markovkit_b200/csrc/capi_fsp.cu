@@ -230,6 +230,8 @@ int mk_fsp_batch_create(int n, const mk_fsp_problem *problems, mk_fsp_batch *out
             b->cap = std::max(b->cap, box);
             b->rmax = std::max(b->rmax, p.n_reactions);
         }
+        // the kernel packs vectors at the support size rounded up to 4 states
+        b->cap = (b->cap + 3) & ~std::int64_t(3);
         std::vector<double> rates(static_cast<std::size_t>(std::max<std::int64_t>(rate_total, 1)),
                                   0.0);
         for (int k = 0; k < n; ++k) {

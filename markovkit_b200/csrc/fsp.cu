@@ -30,10 +30,9 @@
 // partials in one of two alternating buffers, so each needs a single barrier.
 //
 // The Pade (6,6) approximant r(X) = q(X)^-1 p(X) of the scaled Hessenberg is formed from X^2,
-// X^4, X^6 and one product for the odd part; q(X)^-1 is computed by Newton-Schulz iteration
-// Y <- Y (2I - qY), which converges quadratically because ||I - q(X)|| <= 0.28 when
-// ||X|| <= 1/2; the iteration count follows from that norm. All of it is 32 x 32 products
-// spread over the whole block, not a serial elimination.
+// X^4, X^6 and one product for the odd part, and q(X) F = p(X) is solved by Gauss-Jordan
+// elimination spread over the whole block, one barrier per pivot: ||I - q(X)|| <= 0.28 when
+// ||X|| <= 1/2, so q(X) is strictly diagonally dominant and needs no row exchanges.
 // Every loop is bounded; no thread waits on another block.
 #include "fsp.cuh"
 #include "launch_count.hpp"
@@ -255,11 +254,12 @@ __device__ void place(Ctx &c, int n, int m) {
             c.nbr = nbr;
             c.es = n;
         } else {
+            // the global copies are packed at the support's size too (few pages to touch)
             off = mark;
             c.coef = c.gcoef;
             c.diag = c.gdiag;
             c.nbr = c.gnbr;
-            c.es = c.cap;
+            c.es = (n + 3) & ~3;
         }
     }
     {
@@ -287,7 +287,7 @@ __device__ void place(Ctx &c, int n, int m) {
         c.vs = n;
     } else {
         c.V = c.gV;
-        c.vs = c.cap;
+        c.vs = (n + 3) & ~3;
     }
 }
 
@@ -397,15 +397,27 @@ __device__ void arnoldi_reorthogonalise(Shared &sh, Ctx &c, int n, int K, double
     double acc[16];
     zero16(acc);
     for (int k = threadIdx.x; k < n; k += NT) {
+        // the first 16 basis entries are loaded once for the subtraction and the projection
+        double vq[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            vq[q] = q < K ? c.V[q * c.vs + k] : 0.0;
+        }
         double v = out[k];
-        for (int i = 0; i < K; ++i) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if (q < K) {
+                v -= h[q] * vq[q];
+            }
+        }
+        for (int i = 8; i < K; ++i) {
             v -= h[i] * c.V[i * c.vs + k];
         }
         out[k] = v;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             if (q < K) {
-                acc[q] += c.V[q * c.vs + k] * v;
+                acc[q] += (q < 8 ? vq[q] : c.V[q * c.vs + k]) * v;
             }
         }
     }
@@ -448,17 +460,63 @@ __device__ double arnoldi_finish(Shared &sh, Ctx &c, int n, int K, double *out) 
 
 // ---- the small exponential ------------------------------------------------------------
 
-// C = A B (+ epilogue) for n x n matrices in shared memory (row-major, side kE):
-// MODE 0: C = A B; MODE 1: C = 2 A - A B
-template <int NT, int MODE>
+// C = A B for n x n matrices in shared memory (row-major, side kE): each thread computes the
+// outputs (i, j) and (i, j + 16) of one row, sharing the loads of A's row
+template <int NT>
 __device__ void matmul(const double *A, const double *B, double *C, int n) {
+    const int j0 = threadIdx.x & 15, j1 = j0 + 16;
+    for (int i = threadIdx.x >> 4; i < n; i += NT / 16) {
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < n; ++k) {
+            const double a = A[i * kE + k];
+            s0 += a * B[k * kE + j0];
+            s1 += a * B[k * kE + j1];
+        }
+        if (j0 < n) {
+            C[i * kE + j0] = s0;
+        }
+        if (j1 < n) {
+            C[i * kE + j1] = s1;
+        }
+    }
+    __syncthreads();
+}
+
+// F = Q^{-1} P by Gauss-Jordan elimination on [Q | P] (n rows, P in columns 32..), one
+// barrier per pivot: every element of step k is computed from step k-1's buffer into the
+// other. No row exchanges: Q = I - E with ||E|| <= 0.28 is strictly diagonally dominant by
+// rows, so the diagonal is the largest entry of its column at every step and partial pivoting
+// would choose it. Q and P are n x n with side kE; A and B hold 32 x 64 each; F gets the result.
+template <int NT>
+__device__ void gauss_jordan(const double *Q, const double *P, double *A, double *B, double *F,
+                             int n) {
+    constexpr int S = 2 * kE;
+    for (int e = threadIdx.x; e < n * kE; e += NT) {
+        const int i = e / kE, j = e - i * kE;
+        A[i * S + j] = j < n ? Q[i * kE + j] : 0.0;
+        A[i * S + kE + j] = j < n ? P[i * kE + j] : 0.0;
+    }
+    __syncthreads();
+    double *cur = A, *nxt = B;
+    for (int k = 0; k < n; ++k) {
+        const double rp = 1.0 / cur[k * S + k];
+        for (int e = threadIdx.x; e < n * S; e += NT) {
+            const int i = e / S, j = e - i * S;
+            double v = cur[i * S + j];
+            if (i != k) {
+                v -= (cur[i * S + k] * rp) * cur[k * S + j];
+            }
+            nxt[i * S + j] = v;
+        }
+        __syncthreads();
+        double *t = cur;
+        cur = nxt;
+        nxt = t;
+    }
     for (int e = threadIdx.x; e < n * n; e += NT) {
         const int i = e / n, j = e - i * n;
-        double s = 0.0;
-        for (int k = 0; k < n; ++k) {
-            s += A[i * kE + k] * B[k * kE + j];
-        }
-        C[i * kE + j] = MODE == 0 ? s : 2.0 * A[i * kE + j] - s;
+        F[i * kE + j] = cur[i * S + kE + j] / cur[i * S + i];
     }
     __syncthreads();
 }
@@ -494,9 +552,9 @@ __device__ const double *small_expm(Shared &sh, Ctx &c, int n) {
         cf[k] = cf[k - 1] * static_cast<double>(6 - k + 1) / static_cast<double>(k * (12 - k + 1));
     }
     double *X2 = sh.M[1], *X4 = sh.M[2], *X6 = sh.M[3];
-    matmul<NT, 0>(X, X, X2, n);
-    matmul<NT, 0>(X2, X2, X4, n);
-    matmul<NT, 0>(X4, X2, X6, n);
+    matmul<NT>(X, X, X2, n);
+    matmul<NT>(X2, X2, X4, n);
+    matmul<NT>(X4, X2, X6, n);
     // U = c0 + c2 X^2 + c4 X^4 + c6 X^6 (into M[4]); odd factor c1 + c3 X^2 + c5 X^4 (into M[3])
     double *U = sh.M[4], *Vt = sh.M[3];
     for (int e = threadIdx.x; e < n * n; e += NT) {
@@ -508,9 +566,9 @@ __device__ const double *small_expm(Shared &sh, Ctx &c, int n) {
     }
     __syncthreads();
     double *Vo = sh.M[1];
-    matmul<NT, 0>(X, Vt, Vo, n); // odd part
-    // P = U + Vo (M[2]), Q = U - Vo (M[3]); ||I - Q||
-    double *P = sh.M[2], *Q = sh.M[3];
+    matmul<NT>(X, Vt, Vo, n); // odd part
+    // P = U + Vo (M[5]), Q = U - Vo (M[6])
+    double *P = sh.M[5], *Q = sh.M[6];
     for (int e = threadIdx.x; e < n * n; e += NT) {
         const int i = e / n, j = e - i * n;
         const double u = U[i * kE + j], v = Vo[i * kE + j];
@@ -518,39 +576,12 @@ __device__ const double *small_expm(Shared &sh, Ctx &c, int n) {
         Q[i * kE + j] = u - v;
     }
     __syncthreads();
-    double rowdev = 0.0;
-    for (int i = threadIdx.x; i < n; i += NT) {
-        double r = 0.0;
-        for (int j = 0; j < n; ++j) {
-            r += fabs((i == j ? 1.0 : 0.0) - Q[i * kE + j]);
-        }
-        rowdev = fmax(rowdev, r);
-    }
-    const double eps = block_reduce<NT, true>(sh, c, rowdev);
-    // Newton-Schulz: Y_0 = I, ||I - Q Y_k|| <= eps^(2^k); stop below 1e-18
-    int iters = 0;
-    if (eps > 0.0) {
-        iters = eps < 0.95 ? static_cast<int>(ceil(log2(log(1e-18) / log(eps)))) : 10;
-        iters = min(max(iters, 0), 10);
-    }
-    double *Y = sh.M[4], *Tm = sh.M[5], *Y2 = sh.M[6];
-    for (int e = threadIdx.x; e < n * n; e += NT) {
-        const int i = e / n, j = e - i * n;
-        Y[i * kE + j] = i == j ? 1.0 : 0.0;
-    }
-    __syncthreads();
-    for (int it = 0; it < iters; ++it) {
-        matmul<NT, 0>(Q, Y, Tm, n);
-        matmul<NT, 1>(Y, Tm, Y2, n);
-        double *t = Y;
-        Y = Y2;
-        Y2 = t;
-    }
-    double *F = Y2;
-    matmul<NT, 0>(Y, P, F, n);
+    // [Q | P] ping-pongs between M[0..1] and M[2..3]; F lands in M[4]
+    double *F = sh.M[4];
+    gauss_jordan<NT>(Q, P, sh.M[0], sh.M[2], F, n);
     double *spare = sh.M[0];
     for (int s = 0; s < squarings; ++s) {
-        matmul<NT, 0>(F, F, spare, n);
+        matmul<NT>(F, F, spare, n);
         double *t = F;
         F = spare;
         spare = t;
