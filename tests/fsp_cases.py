@@ -8,27 +8,8 @@ from __future__ import annotations
 import numpy as np
 
 from markovkit_b200.fsp import box, krylov_fsp_options, reaction, reaction_network
+from markovkit_b200.fsp_models import birth_death, network_of, toggle  # noqa: F401
 from markovkit_b200.inputs import fsp_batch_instances
-
-
-def birth_death(b: float, d: float) -> reaction_network:
-    return reaction_network([reaction([1], lambda x: np.full(len(x), b)),
-                             reaction([-1], lambda x: d * x[:, 0])])
-
-
-def toggle(a1: float, a2: float, n1: float, n2: float) -> reaction_network:
-    return reaction_network([
-        reaction([1, 0], lambda x: a1 / (1.0 + np.power(x[:, 1].astype(np.float64), n1))),
-        reaction([0, 1], lambda x: a2 / (1.0 + np.power(x[:, 0].astype(np.float64), n2))),
-        reaction([-1, 0], lambda x: x[:, 0].astype(np.float64)),
-        reaction([0, -1], lambda x: x[:, 1].astype(np.float64)),
-    ])
-
-
-def network_of(inst: dict) -> reaction_network:
-    if inst["family"] == "birth_death":
-        return birth_death(float(inst["birth"]), float(inst["death"]))
-    return toggle(float(inst["a1"]), float(inst["a2"]), float(inst["n1"]), float(inst["n2"]))
 
 
 def _chain3() -> reaction_network:
