@@ -368,6 +368,18 @@ def _time_apply(Q, N, dev, flush=None, reps=20) -> float:
     return total / reps
 
 
+def ncu_traffic(name: str) -> float | None:
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch from a committed ncu summary
+    (profiles/<name>.md, the row 'traffic (read + write) | X MB per launch')."""
+    p = ROOT / "profiles" / f"{name}.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("| traffic (read + write)"):
+            return float(line.split("|")[2].split()[0]) * 1e6
+    return None
+
+
 def roofline(mk, Q, M, dev, N) -> dict:
     """The generator SpMV, the kernel the north star's roofline target names, on the 3-D
     16^3-voxel box of cap 2 (8,394,753 states): FP64 apply_shifted, one compulsory read of x and
@@ -396,7 +408,8 @@ def roofline(mk, Q, M, dev, N) -> dict:
         "peak_source": pk["source"],
         "unit": "GB/s",
         "frac": round(achieved / pk["hbm_gbs"], 4),
-        "traffic": None,
+        "traffic": ncu_traffic("row_kernel_spmv_birth_death_3d16"),
+        "traffic_source": "profiles/row_kernel_spmv_birth_death_3d16.md (ncu, bytes per launch)",
         "us_per_launch": round(ms * 1e3, 3),
         "algorithmic_bytes_per_launch": algo,
         "workload_spmv": {"kernel": "row_kernel<double,2,1>", "us_per_launch": round(ms_w * 1e3, 3),
