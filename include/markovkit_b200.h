@@ -256,6 +256,57 @@ int mk_fsp_batch_results(mk_fsp_batch batch, double *h_out, mk_fsp_result *resul
 int mk_fsp_krylov_batch(int n, const mk_fsp_problem *problems, double *h_out,
                         mk_fsp_result *results, void *stream);
 
+/* ---- Serving: a request loop of resolvent solves (no counterpart in the reference; each
+ * request is the reference's shifted_generator + sector_multigrid + num::gmres solve,
+ * tests/test_rdme.cpp:225-251, on a resident solver) ----
+ * Requests are served first come, first served by `slots` worker threads, each with its own
+ * CUDA stream, so up to `slots` solves overlap on the device. A resident solver (generator,
+ * multigrid, Krylov workspace) is kept per (problem, shift) for later requests. New solvers are
+ * admitted by their HBM footprint against the budget: idle solvers are evicted least recently
+ * used first, and a worker waits while the rest are busy. h_b and h_x are host arrays of the
+ * problem's size that must stay valid until the request completes. */
+typedef struct {
+    int slots;               /* concurrent solves (worker threads and streams), 1..64 */
+    size_t hbm_budget;       /* bytes for resident solvers; 0 = 80 % of the free memory */
+    int precision;           /* 1: FP32 multigrid inside FP64 flexible GMRES; 0: all FP64 */
+    int smoother;            /* multigrid smoother: 0 weighted Jacobi, 1 red-black Gauss-Seidel */
+    int restart;             /* GMRES restart, 1..64 */
+    int64_t max_iterations;
+    double rel_tolerance;    /* stop at ||b - A x|| <= rel_tolerance * ||b|| */
+} mk_server_options;
+typedef struct {
+    int64_t ticket;
+    int status;              /* MK_OK, MK_ENOTCONV, MK_ENOMEM (footprint above the budget), ... */
+    int64_t iterations;
+    double residual;         /* relative true residual */
+    double latency_ms;       /* submit to x on the host */
+    double queue_ms;         /* submit to having a slot and the memory */
+    double solve_ms;         /* the rest: set-up of a new resident solver, copies, solve */
+} mk_server_result;
+typedef struct {
+    int64_t completed;
+    double p50_ms, p99_ms;   /* latency percentiles over completed requests */
+    double solves_per_s;     /* completed / (first submit .. last completion) */
+    size_t resident_bytes, budget_bytes;
+    int64_t resident_solvers, evictions, memory_waits;
+} mk_server_stats;
+typedef struct mk_server_s *mk_server;
+void mk_server_options_default(mk_server_options *opt);
+int mk_server_create(const mk_server_options *opt, mk_server *out);
+/* finishes the queued requests, then stops the workers and frees every resident solver */
+void mk_server_destroy(mk_server server);
+/* copies what the server needs of a space and a model; returns the problem's number */
+int mk_server_register(mk_server server, mk_space space, mk_model model, int *problem);
+/* the footprint the admission control charges for a solver of this problem */
+int mk_server_footprint(mk_server server, int problem, size_t *bytes);
+int mk_server_submit(mk_server server, int problem, double shift, const double *h_b, double *h_x,
+                     int64_t *ticket);
+/* blocks until the request is done; returns its status */
+int mk_server_wait(mk_server server, int64_t ticket, mk_server_result *result);
+/* blocks until every submitted request is done */
+int mk_server_drain(mk_server server);
+int mk_server_stats_get(mk_server server, mk_server_stats *stats);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

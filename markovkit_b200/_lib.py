@@ -102,6 +102,44 @@ class FspResult(C.Structure):
     ]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("slots", C.c_int),
+        ("hbm_budget", C.c_size_t),
+        ("precision", C.c_int),
+        ("smoother", C.c_int),
+        ("restart", C.c_int),
+        ("max_iterations", C.c_int64),
+        ("rel_tolerance", C.c_double),
+    ]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_int64),
+        ("status", C.c_int),
+        ("iterations", C.c_int64),
+        ("residual", C.c_double),
+        ("latency_ms", C.c_double),
+        ("queue_ms", C.c_double),
+        ("solve_ms", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_int64),
+        ("p50_ms", C.c_double),
+        ("p99_ms", C.c_double),
+        ("solves_per_s", C.c_double),
+        ("resident_bytes", C.c_size_t),
+        ("budget_bytes", C.c_size_t),
+        ("resident_solvers", C.c_int64),
+        ("evictions", C.c_int64),
+        ("memory_waits", C.c_int64),
+    ]
+
+
 class SolverResult(C.Structure):
     _fields_ = [
         ("iterations", C.c_int64),
@@ -182,6 +220,15 @@ SIGNATURES = {
     "mk_fsp_batch_device_output": (C.c_int, [P, C.POINTER(P)]),
     "mk_fsp_batch_results": (C.c_int, [P, DP, C.POINTER(FspResult), P]),
     "mk_fsp_krylov_batch": (C.c_int, [C.c_int, C.POINTER(FspProblem), DP, C.POINTER(FspResult), P]),
+    "mk_server_options_default": (None, [C.POINTER(ServerOptions)]),
+    "mk_server_create": (C.c_int, [C.POINTER(ServerOptions), C.POINTER(P)]),
+    "mk_server_destroy": (None, [P]),
+    "mk_server_register": (C.c_int, [P, P, P, IP]),
+    "mk_server_footprint": (C.c_int, [P, C.c_int, C.POINTER(C.c_size_t)]),
+    "mk_server_submit": (C.c_int, [P, C.c_int, C.c_double, P, P, I64P]),
+    "mk_server_wait": (C.c_int, [P, I64, C.POINTER(ServerResult)]),
+    "mk_server_drain": (C.c_int, [P]),
+    "mk_server_stats_get": (C.c_int, [P, C.POINTER(ServerStats)]),
 }
 
 _lib: C.CDLL | None = None

@@ -61,3 +61,18 @@ def test_no_gpu_needed_for_errors(lib_built):
     rc = lib.mk_space_create_box(0, 1, (C.c_int * 1)(3), C.byref(out))
     assert rc == _lib.MK_EINVAL
     assert b"voxel" in lib.mk_last_error()
+
+
+def test_server_options_are_checked_before_device_work(lib_built):
+    import ctypes as C
+
+    from markovkit_b200 import _lib
+
+    lib = _lib.load()
+    o = _lib.ServerOptions()
+    lib.mk_server_options_default(C.byref(o))
+    assert o.slots >= 1 and o.precision == 1 and o.rel_tolerance == 1e-10
+    o.slots = 0
+    h = C.c_void_p()
+    assert lib.mk_server_create(C.byref(o), C.byref(h)) == _lib.MK_EINVAL
+    assert b"slots" in lib.mk_last_error()
