@@ -1,0 +1,724 @@
+// markovkit_b200 C++20 facade: MarkovKit's resolvent-path and Krylov-FSP API (names, argument
+// meaning, exceptions) over the C ABI of include/markovkit_b200.h. Header-only; link
+// libmarkovkit_b200.so. Vectors are host std::vectors, as in the reference; every call copies
+// them to the device, runs the sm_100a kernels and copies back, synchronously (the reference's
+// calls are synchronous too). Handles own device memory and free it on destruction.
+//
+// Reference interfaces mirrored (MarkovKit tree):
+//   population_box / population_sector        markovkit/rdme/population_space.hpp:105-196
+//   grid<D>, voxel_domain, local_reaction,
+//   reaction_diffusion                         markovkit/rdme/reaction_diffusion.hpp:15-118
+//   boundary, generator, shifted_generator     markovkit/generator.hpp:11-133
+//   multigrid_options, sector_multigrid        markovkit/rdme/multigrid.hpp:125-134,364-408
+//   num::gmres_options, num::solver_result,
+//   num::gmres(A, [M], b, x, options)          call sites tests/test_rdme.cpp:238-249
+//   reaction_network, box, krylov_fsp_options,
+//   fsp_solution, solve_krylov_fsp             markovkit/reaction_network.hpp, fsp.hpp:26-254
+// Differences: the voxel graph is a structured grid (grid<1..3>); a region for FSP is a box;
+// krylov_dim <= 30; fsp_solution keeps the initial and final snapshots only.
+#pragma once
+
+#include "../markovkit_b200.h"
+
+#include <array>
+#include <cmath>
+#include <concepts>
+#include <cstdint>
+#include <functional>
+#include <map>
+#include <memory>
+#include <optional>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace markovkit {
+
+using real = double;
+using idx = std::size_t;
+template <typename T>
+using vec = std::vector<T>;
+template <typename T>
+using array = std::vector<T>;
+template <typename T>
+using view = std::span<T>;
+using state = std::vector<int>;
+
+namespace detail {
+
+inline void check(int rc) {
+    if (rc == MK_OK) {
+        return;
+    }
+    const std::string msg = mk_last_error();
+    switch (rc) {
+    case MK_EINVAL:
+        throw std::invalid_argument(msg);
+    case MK_EOVERFLOW:
+        throw std::overflow_error(msg);
+    case MK_ENOMEM:
+        throw std::bad_alloc();
+    default:
+        throw std::runtime_error(msg);
+    }
+}
+
+// a device buffer of doubles for host-vector calls
+class device_vector {
+  public:
+    device_vector() = default;
+    explicit device_vector(std::size_t n) : n_(n) {
+        void *p = nullptr;
+        check(mk_device_alloc(n * sizeof(double), &p));
+        p_.reset(static_cast<double *>(p));
+    }
+    [[nodiscard]] double *get() const { return p_.get(); }
+    [[nodiscard]] std::size_t size() const { return n_; }
+    void upload(const double *h) { check(mk_memcpy_h2d(p_.get(), h, n_ * sizeof(double), nullptr)); }
+    void download(double *h) const {
+        check(mk_memcpy_d2h(h, p_.get(), n_ * sizeof(double), nullptr));
+        check(mk_stream_synchronize(nullptr));
+    }
+
+  private:
+    struct freer {
+        void operator()(double *p) const { mk_device_free(p); }
+    };
+    std::unique_ptr<double, freer> p_;
+    std::size_t n_ = 0;
+};
+
+template <typename H, void (*Destroy)(H)>
+struct handle_deleter {
+    void operator()(H h) const {
+        if (h) {
+            Destroy(h);
+        }
+    }
+};
+
+} // namespace detail
+
+// ---- spaces ------------------------------------------------------------------------------
+
+class population_space {
+  public:
+    [[nodiscard]] idx size() const {
+        int64_t n = 0;
+        detail::check(mk_space_size(h_.get(), &n));
+        return static_cast<idx>(n);
+    }
+    [[nodiscard]] idx n_voxels() const { return static_cast<idx>(voxels_); }
+    [[nodiscard]] idx n_species() const { return limits_.size(); }
+    [[nodiscard]] idx n_sectors() const {
+        int64_t k = 0;
+        detail::check(mk_space_n_sectors(h_.get(), &k));
+        return static_cast<idx>(k);
+    }
+    [[nodiscard]] idx sector_begin(idx k) const {
+        int64_t b = 0;
+        detail::check(mk_space_sector_begin(h_.get(), static_cast<int64_t>(k), &b));
+        return static_cast<idx>(b);
+    }
+    [[nodiscard]] idx sector_end(idx k) const {
+        return k + 1 < n_sectors() ? sector_begin(k + 1) : size();
+    }
+    [[nodiscard]] array<int> sector_totals(idx k) const {
+        array<int> t(n_species());
+        detail::check(mk_space_sector_totals(h_.get(), static_cast<int64_t>(k), t.data()));
+        return t;
+    }
+    [[nodiscard]] idx sector_of(idx i) const {
+        int64_t k = 0;
+        detail::check(mk_space_sector_of(h_.get(), static_cast<int64_t>(i), &k));
+        return static_cast<idx>(k);
+    }
+    [[nodiscard]] std::optional<idx> find_sector(const array<int> &totals) const {
+        int64_t k = -1;
+        detail::check(mk_space_find_sector(h_.get(), totals.data(), &k));
+        return k < 0 ? std::nullopt : std::optional<idx>(static_cast<idx>(k));
+    }
+    // find(x): the index of a voxel-major occupation vector, or nullopt
+    [[nodiscard]] std::optional<idx> find(const state &x) const {
+        if (x.size() != n_voxels() * n_species()) {
+            return std::nullopt;
+        }
+        int64_t i = -1;
+        detail::check(mk_space_find_host(h_.get(), x.data(), &i));
+        return i < 0 ? std::nullopt : std::optional<idx>(static_cast<idx>(i));
+    }
+    [[nodiscard]] state operator[](idx i) const {
+        state x(n_voxels() * n_species());
+        detail::check(mk_space_state_host(h_.get(), static_cast<int64_t>(i), x.data()));
+        return x;
+    }
+    [[nodiscard]] mk_space handle() const { return h_.get(); }
+    [[nodiscard]] const array<int> &limits() const { return limits_; }
+
+  protected:
+    population_space(idx voxels, array<int> limits, bool box)
+        : voxels_(static_cast<int64_t>(voxels)), limits_(std::move(limits)) {
+        mk_space h = nullptr;
+        detail::check(box ? mk_space_create_box(voxels_, static_cast<int>(limits_.size()),
+                                                limits_.data(), &h)
+                          : mk_space_create_sector(voxels_, static_cast<int>(limits_.size()),
+                                                   limits_.data(), &h));
+        h_ = std::shared_ptr<mk_space_s>(h, [](mk_space p) { mk_space_destroy(p); });
+    }
+
+  private:
+    int64_t voxels_ = 0;
+    array<int> limits_;
+    std::shared_ptr<mk_space_s> h_;
+};
+
+// every sector 0 <= t_s <= max_totals[s]
+class population_box : public population_space {
+  public:
+    population_box(idx voxels, array<int> max_totals)
+        : population_space(voxels, std::move(max_totals), true) {}
+};
+
+// the states with totals[s] molecules of each species
+class population_sector : public population_space {
+  public:
+    population_sector(idx voxels, array<int> totals)
+        : population_space(voxels, std::move(totals), false) {}
+};
+
+// ---- models -------------------------------------------------------------------------------
+
+// grid<D>(dims, spacing): a structured voxel grid (the reference's structured_grid_graph)
+template <int D>
+struct grid {
+    std::array<idx, D> dims;
+    std::array<real, D> spacing;
+    grid(std::array<idx, D> d, std::array<real, D> h) : dims(d), spacing(h) {}
+    [[nodiscard]] idx n_vertices() const {
+        idx n = 1;
+        for (idx d : dims) {
+            n *= d;
+        }
+        return n;
+    }
+    [[nodiscard]] real cell_volume() const {
+        real v = 1.0;
+        for (real h : spacing) {
+            v *= h;
+        }
+        return v;
+    }
+};
+
+template <int D>
+struct voxel_domain {
+    grid<D> graph;
+    vec<real> diffusivities;
+    vec<real> volumes;
+    voxel_domain(grid<D> g, vec<real> diff)
+        : graph(std::move(g)), diffusivities(std::move(diff)),
+          volumes(graph.n_vertices(), graph.cell_volume()) {}
+    [[nodiscard]] idx n_voxels() const { return graph.n_vertices(); }
+    [[nodiscard]] idx n_species() const { return diffusivities.size(); }
+};
+
+// a reaction inside one voxel: change vector and rate(counts, volume)
+struct local_reaction {
+    array<int> change;
+    std::function<real(view<const int>, real)> rate;
+};
+
+template <int D>
+struct reaction_diffusion {
+    voxel_domain<D> domain;
+    array<local_reaction> reactions;
+    [[nodiscard]] idx n_voxels() const { return domain.n_voxels(); }
+    [[nodiscard]] idx n_species() const { return domain.n_species(); }
+    [[nodiscard]] idx index(idx voxel, idx species) const { return voxel * n_species() + species; }
+};
+
+namespace detail {
+
+// the model handle of a reaction-diffusion model with its local rates tabulated over the
+// count tuples a space allows (n_s <= limits[s])
+template <int D>
+std::shared_ptr<mk_model_s> make_model(const reaction_diffusion<D> &m, const array<int> &limits) {
+    std::array<int64_t, 3> dims{1, 1, 1};
+    std::array<double, 3> spacing{1.0, 1.0, 1.0};
+    for (int a = 0; a < D; ++a) {
+        dims[a] = static_cast<int64_t>(m.domain.graph.dims[a]);
+        spacing[a] = m.domain.graph.spacing[a];
+    }
+    mk_model h = nullptr;
+    check(mk_model_create_grid(D, dims.data(), spacing.data(), static_cast<int>(m.n_species()),
+                               m.domain.diffusivities.data(), &h));
+    std::shared_ptr<mk_model_s> model(h, [](mk_model p) { mk_model_destroy(p); });
+    if (!m.reactions.empty()) {
+        const int S = static_cast<int>(m.n_species());
+        if (static_cast<int>(limits.size()) != S) {
+            throw std::invalid_argument("the space and the model have different species counts");
+        }
+        int ntuple = 1;
+        for (int t : limits) {
+            ntuple *= t + 1;
+        }
+        const int R = static_cast<int>(m.reactions.size());
+        std::vector<int> change;
+        std::vector<double> rates(static_cast<std::size_t>(R) * ntuple);
+        const real vol = m.domain.graph.cell_volume();
+        std::vector<int> counts(S);
+        for (int r = 0; r < R; ++r) {
+            if (static_cast<int>(m.reactions[r].change.size()) != S) {
+                throw std::invalid_argument("change vector length differs from the species count");
+            }
+            change.insert(change.end(), m.reactions[r].change.begin(), m.reactions[r].change.end());
+            for (int t = 0; t < ntuple; ++t) {
+                int rem = t;
+                for (int s = S - 1; s >= 0; --s) {
+                    counts[s] = rem % (limits[s] + 1);
+                    rem /= limits[s] + 1;
+                }
+                rates[static_cast<std::size_t>(r) * ntuple + t] =
+                    m.reactions[r].rate(view<const int>(counts.data(), counts.size()), vol);
+            }
+        }
+        check(mk_model_set_reactions(h, R, change.data(), limits.data(), 1, nullptr, rates.data()));
+    }
+    return model;
+}
+
+} // namespace detail
+
+// ---- generator ----------------------------------------------------------------------------
+
+enum class boundary : std::uint8_t { reflecting, absorbing };
+
+// Q with columns as sources, dp/dt = Q p; matrix-free on the device
+class generator {
+  public:
+    using domain_type = vec<real>;
+    using codomain_type = vec<real>;
+
+    template <int D>
+    generator(const population_space &space, const reaction_diffusion<D> &model,
+              boundary leaks = boundary::absorbing) {
+        model_ = detail::make_model(model, space.limits());
+        mk_generator h = nullptr;
+        detail::check(mk_generator_create(space.handle(), model_.get(),
+                                          leaks == boundary::absorbing ? 1 : 0, &h));
+        h_.reset(h, [](mk_generator p) { mk_generator_destroy(p); });
+        int64_t n = 0;
+        detail::check(mk_generator_rows(h, &n));
+        n_ = static_cast<idx>(n);
+        x_ = std::make_shared<detail::device_vector>(n_);
+        y_ = std::make_shared<detail::device_vector>(n_);
+    }
+    [[nodiscard]] idx rows() const { return n_; }
+    [[nodiscard]] idx cols() const { return n_; }
+    // y = Q x
+    void apply(const vec<real> &x, vec<real> &y) const {
+        x_->upload(x.data());
+        detail::check(mk_generator_apply(h_.get(), x_->get(), y_->get(), nullptr));
+        y.resize(n_);
+        y_->download(y.data());
+    }
+    // y = shift x - Q x
+    void apply_shifted(real shift, view<const real> x, view<real> y) const {
+        x_->upload(x.data());
+        detail::check(mk_generator_apply_shifted(h_.get(), shift, x_->get(), y_->get(), nullptr));
+        y_->download(y.data());
+    }
+    [[nodiscard]] array<real> exit_rates() const { return exit_leak().first; }
+    [[nodiscard]] array<real> leak_rates() const { return exit_leak().second; }
+    [[nodiscard]] mk_generator handle() const { return h_.get(); }
+    [[nodiscard]] mk_model model_handle() const { return model_.get(); }
+
+  private:
+    [[nodiscard]] std::pair<array<real>, array<real>> exit_leak() const {
+        detail::check(mk_generator_exit_leak(h_.get(), x_->get(), y_->get(), nullptr));
+        array<real> e(n_), l(n_);
+        x_->download(e.data());
+        y_->download(l.data());
+        return {e, l};
+    }
+    std::shared_ptr<mk_model_s> model_;
+    std::shared_ptr<mk_generator_s> h_;
+    std::shared_ptr<detail::device_vector> x_, y_;
+    idx n_ = 0;
+};
+
+// shift I - Q; reads Q by reference (the reference keeps a pointer too)
+class shifted_generator {
+  public:
+    using domain_type = vec<real>;
+    using codomain_type = vec<real>;
+    shifted_generator(const generator &Q, real shift) : Q_(&Q), shift_(shift) {}
+    [[nodiscard]] idx rows() const { return Q_->rows(); }
+    [[nodiscard]] idx cols() const { return Q_->cols(); }
+    [[nodiscard]] real shift() const { return shift_; }
+    [[nodiscard]] const generator &base() const { return *Q_; }
+    void apply(const vec<real> &x, vec<real> &y) const {
+        y.resize(rows());
+        Q_->apply_shifted(shift_, view<const real>(x.data(), x.size()), view<real>(y.data(), y.size()));
+    }
+
+  private:
+    const generator *Q_;
+    real shift_;
+};
+
+// ---- multigrid ----------------------------------------------------------------------------
+
+struct multigrid_options {
+    int pre_sweeps = 2;
+    int post_sweeps = 2;
+    real jacobi_weight = 2.0 / 3.0;
+    idx coarsest_size = 4;
+    int max_levels = 32;
+    int coarse_cycles = 1;
+    int sweep_growth = 0;
+    int smoother = 0;  // 0 weighted Jacobi (the reference's), 1 red-black Gauss-Seidel
+    int precision = 0; // 0 FP64, 1 FP32 (use with flexible GMRES)
+};
+
+class sector_multigrid {
+  public:
+    using domain_type = vec<real>;
+    using codomain_type = vec<real>;
+
+    template <int D>
+    sector_multigrid(const voxel_domain<D> &domain, const population_box &box, real shift,
+                     const multigrid_options &options = {}) {
+        init(reaction_diffusion<D>{domain, {}}, box, shift, options);
+    }
+    template <int D>
+    sector_multigrid(const voxel_domain<D> &domain, const population_sector &sector, real shift,
+                     const multigrid_options &options = {}) {
+        init(reaction_diffusion<D>{domain, {}}, sector, shift, options);
+    }
+    [[nodiscard]] idx rows() const { return n_; }
+    [[nodiscard]] idx cols() const { return n_; }
+    [[nodiscard]] int max_levels() const {
+        int l = 0;
+        detail::check(mk_multigrid_max_levels(h_.get(), &l));
+        return l;
+    }
+    // one cycle per sector from a zero initial guess: x = M b
+    void apply(const vec<real> &b, vec<real> &x) const {
+        b_->upload(b.data());
+        detail::check(mk_multigrid_apply(h_.get(), b_->get(), x_->get(), nullptr));
+        x.resize(n_);
+        x_->download(x.data());
+    }
+    [[nodiscard]] mk_multigrid handle() const { return h_.get(); }
+    [[nodiscard]] bool fp32() const { return fp32_; }
+
+  private:
+    template <int D>
+    void init(const reaction_diffusion<D> &m, const population_space &space, real shift,
+              const multigrid_options &o) {
+        auto model = detail::make_model(m, space.limits());
+        mk_multigrid_options c{};
+        mk_multigrid_options_default(&c);
+        c.pre_sweeps = o.pre_sweeps;
+        c.post_sweeps = o.post_sweeps;
+        c.jacobi_weight = o.jacobi_weight;
+        c.coarsest_size = static_cast<int64_t>(o.coarsest_size);
+        c.max_levels = o.max_levels;
+        c.coarse_cycles = o.coarse_cycles;
+        c.sweep_growth = o.sweep_growth;
+        c.smoother = o.smoother;
+        c.precision = o.precision;
+        mk_multigrid h = nullptr;
+        detail::check(mk_multigrid_create(space.handle(), model.get(), shift, &c, &h));
+        h_.reset(h, [](mk_multigrid p) { mk_multigrid_destroy(p); });
+        n_ = space.size();
+        fp32_ = o.precision == 1;
+        b_ = std::make_shared<detail::device_vector>(n_);
+        x_ = std::make_shared<detail::device_vector>(n_);
+    }
+    std::shared_ptr<mk_multigrid_s> h_;
+    std::shared_ptr<detail::device_vector> b_, x_;
+    idx n_ = 0;
+    bool fp32_ = false;
+};
+
+// ---- GMRES --------------------------------------------------------------------------------
+
+namespace num {
+
+using markovkit::idx;
+using markovkit::real;
+using markovkit::vec;
+
+template <typename Op, typename X, typename Y>
+concept linear_operator = requires(const Op &A, const X &x, Y &y) {
+    { A.rows() } -> std::convertible_to<idx>;
+    { A.cols() } -> std::convertible_to<idx>;
+    A.apply(x, y);
+};
+
+struct gmres_options {
+    real tolerance = 1e-8; // absolute, on ||b - A x||_2
+    idx max_iterations = 1000;
+    idx restart = 30;
+};
+
+struct solver_result {
+    idx iterations = 0;
+    real residual = 0.0;
+    bool converged = false;
+};
+
+namespace detail {
+
+inline solver_result run(const shifted_generator &A, const sector_multigrid *M, const vec<real> &b,
+                         vec<real> &x, const gmres_options &o) {
+    if (b.size() != A.rows() || x.size() != A.rows()) {
+        throw std::invalid_argument("gmres: vector sizes differ from the operator's");
+    }
+    mk_gmres_options c{};
+    mk_gmres_options_default(&c);
+    c.tolerance = o.tolerance;
+    c.max_iterations = static_cast<int64_t>(o.max_iterations);
+    c.restart = static_cast<int>(std::min<idx>(o.restart, 1u << 30));
+    c.flexible = (M && M->fp32()) ? 1 : 0;
+    mk_solver h = nullptr;
+    markovkit::detail::check(
+        mk_solver_create(A.base().handle(), A.shift(), M ? M->handle() : nullptr, &c, &h));
+    std::unique_ptr<mk_solver_s, void (*)(mk_solver)> solver(h, [](mk_solver p) { mk_solver_destroy(p); });
+    mk_solver_result r{};
+    const int rc = mk_solver_solve_host(h, b.data(), x.data(), &r, nullptr);
+    if (rc != MK_OK && rc != MK_ENOTCONV) {
+        markovkit::detail::check(rc);
+    }
+    return {static_cast<idx>(r.iterations), r.residual, r.converged != 0};
+}
+
+} // namespace detail
+
+// restarted GMRES on A = shift I - Q; x holds the initial guess and the solution
+inline solver_result gmres(const shifted_generator &A, const vec<real> &b, vec<real> &x,
+                           const gmres_options &options = {}) {
+    return detail::run(A, nullptr, b, x, options);
+}
+
+// right-preconditioned by a sector multigrid (flexible GMRES when it runs in FP32)
+inline solver_result gmres(const shifted_generator &A, const sector_multigrid &M,
+                           const vec<real> &b, vec<real> &x, const gmres_options &options = {}) {
+    return detail::run(A, &M, b, x, options);
+}
+
+} // namespace num
+
+// ---- Krylov FSP ---------------------------------------------------------------------------
+
+struct reaction {
+    state change;
+    std::function<real(const state &)> rate;
+};
+
+struct reaction_network {
+    array<reaction> reactions;
+};
+
+// box(bounds): 0 <= x[s] <= bounds[s]; the only region the device FSP supports
+struct region {
+    array<int> bounds;
+    [[nodiscard]] bool operator()(const state &x) const {
+        for (idx s = 0; s < x.size(); ++s) {
+            if (s >= bounds.size() || x[s] < 0 || x[s] > bounds[s]) {
+                return false;
+            }
+        }
+        return true;
+    }
+};
+
+inline region box(array<int> bounds) { return region{std::move(bounds)}; }
+
+struct krylov_fsp_options {
+    region inside;
+    real tolerance = 1e-6;
+    real initial_step = 1.0;
+    real step_growth = 2.0;
+    real drop_probability = 1e-10;
+    real drop_derivative = 1e-16;
+    int layers = 1;
+    int save_every = 1000; // accepted for source compatibility; only the final state is saved
+    int max_steps = 1 << 28;
+    int krylov_dim = 30;
+    real krylov_tol = 1e-8;
+};
+
+class distribution {
+  public:
+    distribution() = default;
+    distribution(array<state> states, array<real> p) : states_(std::move(states)), p_(std::move(p)) {}
+    [[nodiscard]] idx size() const { return states_.size(); }
+    [[nodiscard]] const state &operator[](idx i) const { return states_[i]; }
+    [[nodiscard]] const array<state> &states() const { return states_; }
+    [[nodiscard]] const array<real> &probabilities() const { return p_; }
+    [[nodiscard]] vec<real> means() const {
+        vec<real> m(states_.empty() ? 0 : states_.front().size(), 0.0);
+        for (idx i = 0; i < size(); ++i) {
+            for (idx s = 0; s < m.size(); ++s) {
+                m[s] += p_[i] * states_[i][s];
+            }
+        }
+        return m;
+    }
+    [[nodiscard]] std::map<int, real> marginal(idx s) const {
+        std::map<int, real> out;
+        for (idx i = 0; i < size(); ++i) {
+            out[states_[i][s]] += p_[i];
+        }
+        return out;
+    }
+
+  private:
+    array<state> states_;
+    array<real> p_;
+};
+
+struct fsp_solution {
+    array<real> times;
+    array<distribution> snapshots;
+    [[nodiscard]] std::vector<vec<real>> means() const {
+        std::vector<vec<real>> m;
+        for (const auto &d : snapshots) {
+            m.push_back(d.means());
+        }
+        return m;
+    }
+};
+
+namespace detail {
+
+struct fsp_tables {
+    array<int> bounds, change, initial;
+    array<real> rates;
+    idx box = 1;
+};
+
+inline fsp_tables tabulate(const reaction_network &model, const state &initial,
+                           const krylov_fsp_options &o) {
+    fsp_tables t;
+    t.bounds = o.inside.bounds;
+    const idx S = t.bounds.size();
+    if (S == 0 || S != initial.size()) {
+        throw std::invalid_argument("fsp: the device FSP needs box(bounds) over every species");
+    }
+    for (int b : t.bounds) {
+        t.box *= static_cast<idx>(b) + 1;
+    }
+    const idx R = model.reactions.size();
+    t.rates.assign(R * t.box, 0.0);
+    state x(S);
+    for (idx i = 0; i < t.box; ++i) {
+        idx rem = i;
+        for (idx s = S; s-- > 0;) {
+            x[s] = static_cast<int>(rem % (t.bounds[s] + 1));
+            rem /= t.bounds[s] + 1;
+        }
+        for (idx r = 0; r < R; ++r) {
+            t.rates[r * t.box + i] = model.reactions[r].rate(x);
+        }
+    }
+    for (const auto &rx : model.reactions) {
+        if (rx.change.size() != S) {
+            throw std::invalid_argument("fsp: change vector length differs from the species count");
+        }
+        t.change.insert(t.change.end(), rx.change.begin(), rx.change.end());
+    }
+    t.initial = initial;
+    return t;
+}
+
+inline mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model, real T,
+                              const krylov_fsp_options &o) {
+    mk_fsp_problem p{};
+    p.n_species = static_cast<int>(t.bounds.size());
+    p.n_reactions = static_cast<int>(model.reactions.size());
+    p.bounds = t.bounds.data();
+    p.change = t.change.data();
+    p.rates = t.rates.data();
+    p.initial = t.initial.data();
+    p.final_time = T;
+    mk_fsp_options_default(&p.options);
+    p.options.tolerance = o.tolerance;
+    p.options.initial_step = o.initial_step;
+    p.options.step_growth = o.step_growth;
+    p.options.drop_probability = o.drop_probability;
+    p.options.drop_derivative = o.drop_derivative;
+    p.options.layers = o.layers;
+    p.options.krylov_dim = o.krylov_dim;
+    p.options.max_steps = o.max_steps;
+    p.options.krylov_tol = o.krylov_tol;
+    return p;
+}
+
+} // namespace detail
+
+// solve_krylov_fsp for several instances in one launch
+inline array<fsp_solution> solve_krylov_fsp_batch(
+    const array<std::tuple<reaction_network, state, real, krylov_fsp_options>> &instances) {
+    array<detail::fsp_tables> tables;
+    array<mk_fsp_problem> problems;
+    tables.reserve(instances.size());
+    for (const auto &[model, initial, T, o] : instances) {
+        tables.push_back(detail::tabulate(model, initial, o));
+    }
+    for (idx k = 0; k < instances.size(); ++k) {
+        const auto &[model, initial, T, o] = instances[k];
+        problems.push_back(detail::problem(tables[k], model, T, o));
+    }
+    idx total = 0;
+    for (const auto &t : tables) {
+        total += t.box;
+    }
+    array<real> out(total);
+    array<mk_fsp_result> results(instances.size());
+    const int rc = mk_fsp_krylov_batch(static_cast<int>(problems.size()), problems.data(),
+                                       out.data(), results.data(), nullptr);
+    if (rc != MK_OK && rc != MK_ENOTCONV) {
+        markovkit::detail::check(rc);
+    }
+    array<fsp_solution> sols;
+    idx off = 0;
+    for (idx k = 0; k < instances.size(); ++k) {
+        const auto &t = tables[k];
+        const idx S = t.bounds.size();
+        array<state> states;
+        array<real> p;
+        for (idx i = 0; i < t.box; ++i) {
+            if (out[off + i] != 0.0) {
+                state x(S);
+                idx rem = i;
+                for (idx s = S; s-- > 0;) {
+                    x[s] = static_cast<int>(rem % (t.bounds[s] + 1));
+                    rem /= t.bounds[s] + 1;
+                }
+                states.push_back(std::move(x));
+                p.push_back(out[off + i]);
+            }
+        }
+        fsp_solution sol;
+        sol.times = {0.0, results[k].time};
+        sol.snapshots.emplace_back(array<state>{t.initial}, array<real>{1.0});
+        sol.snapshots.emplace_back(std::move(states), std::move(p));
+        sols.push_back(std::move(sol));
+        off += t.box;
+    }
+    return sols;
+}
+
+// the Krylov FSP of Vo and Sidje on the GPU (fsp.hpp:207-254)
+inline fsp_solution solve_krylov_fsp(const reaction_network &model, const state &initial,
+                                     real final_time, const krylov_fsp_options &options) {
+    return solve_krylov_fsp_batch({{model, initial, final_time, options}}).front();
+}
+
+} // namespace markovkit

@@ -1,0 +1,159 @@
+// A MarkovKit-style program against the C++20 facade (include/mk/markovkit.hpp): the calls a
+// reference caller makes (population_box, reaction_diffusion, generator, shifted_generator,
+// sector_multigrid, num::gmres, solve_krylov_fsp), with checks of the answers. Built by
+// tests/test_facade.py; run on a GPU it prints "facade: N checks passed" or exits 1.
+#include "mk/markovkit.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <numeric>
+
+using namespace markovkit;
+
+namespace {
+
+int checks = 0, failures = 0;
+
+void expect(bool ok, const char *what) {
+    ++checks;
+    if (!ok) {
+        ++failures;
+        std::printf("FAILED: %s\n", what);
+    }
+}
+
+array<local_reaction> birth_death(real birth, real death) {
+    return {{{1}, [=](view<const int>, real volume) { return birth * volume; }},
+            {{-1}, [=](view<const int> n, real) { return death * n[0]; }}};
+}
+
+real norm(const vec<real> &v) { return std::sqrt(std::inner_product(v.begin(), v.end(), v.begin(), 0.0)); }
+
+void spaces() {
+    population_box box(16, {3});
+    expect(box.size() == 969, "population_box(16, {3}) has 969 states");
+    expect(box.n_sectors() == 4 && box.sector_begin(3) == 153, "sector offsets 0/1/17/153");
+    for (idx i : {idx(0), idx(5), idx(200), idx(968)}) {
+        const auto found = box.find(box[i]);
+        expect(found && *found == i, "find(box[i]) == i");
+    }
+    state outside(16, 0);
+    outside[0] = 4;
+    expect(!box.find(outside), "a state outside the box is absent");
+    population_sector sector(8, {2});
+    expect(sector.size() == 36, "population_sector(8, {2}) has C(9, 2) = 36 states");
+}
+
+void resolvent() {
+    const reaction_diffusion<1> model{voxel_domain<1>(grid<1>({16}, {1.0 / 16}), {1.0}),
+                                      birth_death(0.05, 0.02)};
+    population_box box(16, {3});
+    const generator Q(box, model, boundary::absorbing);
+    constexpr real shift = 0.5;
+    const shifted_generator A(Q, shift);
+    static_assert(num::linear_operator<shifted_generator, vec<real>, vec<real>>);
+    vec<real> b(Q.rows());
+    for (idx i = 0; i < b.size(); ++i) {
+        b[i] = 1.0 + 0.25 * std::sin(0.37 * static_cast<real>(i));
+    }
+    // y = s x - Q x by both entry points
+    vec<real> qx, ax;
+    Q.apply(b, qx);
+    A.apply(b, ax);
+    real dev = 0.0;
+    for (idx i = 0; i < b.size(); ++i) {
+        dev = std::max(dev, std::abs(ax[i] - (shift * b[i] - qx[i])));
+    }
+    expect(dev < 1e-12, "apply_shifted = s x - apply");
+    const auto exits = Q.exit_rates();
+    expect(std::abs(exits[0] - 0.05 * 16 * (1.0 / 16)) < 1e-14, "exit rate of the empty state is the total birth rate");
+
+    const sector_multigrid M(model.domain, box, shift);
+    const num::gmres_options options{.tolerance = 1e-10 * norm(b), .max_iterations = 1000, .restart = 30};
+    vec<real> x_mg(Q.rows(), 0.0), x_plain(Q.rows(), 0.0), x32(Q.rows(), 0.0);
+    const auto mg = num::gmres(A, M, b, x_mg, options);
+    const auto plain = num::gmres(A, b, x_plain, options);
+    expect(mg.converged && plain.converged, "both solves converge");
+    expect(mg.iterations < plain.iterations, "the multigrid preconditioner cuts iterations");
+    vec<real> r;
+    A.apply(x_mg, r);
+    for (idx i = 0; i < r.size(); ++i) {
+        r[i] = b[i] - r[i];
+    }
+    expect(norm(r) <= 1e-10 * norm(b) * 1.0001, "true residual below 1e-10 relative");
+    real diff = 0.0;
+    for (idx i = 0; i < b.size(); ++i) {
+        diff = std::max(diff, std::abs(x_mg[i] - x_plain[i]));
+    }
+    expect(diff < 1e-8, "preconditioned and plain solutions agree");
+    multigrid_options o32;
+    o32.precision = 1;
+    const sector_multigrid M32(model.domain, box, shift, o32);
+    const auto s32 = num::gmres(A, M32, b, x32, options);
+    real d32 = 0.0;
+    for (idx i = 0; i < b.size(); ++i) {
+        d32 = std::max(d32, std::abs(x32[i] - x_mg[i]));
+    }
+    expect(s32.converged && d32 < 1e-8 * norm(x_mg), "FP32 multigrid in flexible GMRES agrees");
+}
+
+void annihilation_transform() {
+    // A + B -> nothing at rate 2 a b / V; E[exp(-sT)] + s S_hat(s) = 1 for the annihilation time
+    const reaction_diffusion<1> model{
+        voxel_domain<1>(grid<1>({4}, {0.25}), {1.0, 1.0}),
+        {{{-1, -1}, [](view<const int> n, real volume) { return 2.0 * n[0] * n[1] / volume; }}}};
+    population_box box(4, {1, 1});
+    const generator Q(box, model);
+    expect(Q.rows() == 25, "1 + V + V + V^2 states");
+    constexpr real shift = 0.5;
+    const shifted_generator A(Q, shift);
+    const sector_multigrid M(model.domain, box, shift);
+    const idx joint = *box.find_sector({1, 1});
+    const idx vacuum = *box.find(state(8, 0));
+    state initial(8, 0);
+    initial[model.index(0, 0)] = 1;
+    initial[model.index(2, 1)] = 1;
+    vec<real> b(Q.rows(), 0.0), x(Q.rows(), 0.0);
+    b[*box.find(initial)] = 1.0;
+    const auto res = num::gmres(A, M, b, x, {.tolerance = 1e-12, .max_iterations = 200, .restart = 25});
+    expect(res.converged, "transform solve converges");
+    real survival = 0.0;
+    for (idx i = box.sector_begin(joint); i < box.sector_end(joint); ++i) {
+        survival += x[i];
+    }
+    expect(std::abs(shift * x[vacuum] + shift * survival - 1.0) < 1e-10, "E[exp(-sT)] + s S(s) = 1");
+}
+
+void krylov_fsp() {
+    const reaction_network death{{{{-1}, [](const state &x) { return real(x[0]); }}}};
+    krylov_fsp_options o;
+    o.inside = box({5});
+    o.tolerance = 1e-10;
+    o.max_steps = 100;
+    o.krylov_tol = 1e-12;
+    const auto sol = solve_krylov_fsp(death, {5}, 1.0, o);
+    expect(sol.times.back() == 1.0, "Krylov FSP reaches the final time");
+    expect(std::abs(sol.means().back()[0] - 5.0 * std::exp(-1.0)) < 1e-8, "pure-death mean");
+    expect(std::abs(sol.snapshots.back().marginal(0).at(0) - std::pow(1.0 - std::exp(-1.0), 5)) < 1e-8,
+           "extinction probability");
+}
+
+} // namespace
+
+int main() {
+    try {
+        spaces();
+        resolvent();
+        annihilation_transform();
+        krylov_fsp();
+    } catch (const std::exception &e) {
+        std::printf("FAILED with exception: %s\n", e.what());
+        return 1;
+    }
+    if (failures) {
+        std::printf("facade: %d of %d checks failed\n", failures, checks);
+        return 1;
+    }
+    std::printf("facade: %d checks passed\n", checks);
+    return 0;
+}
