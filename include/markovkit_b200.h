@@ -124,7 +124,8 @@ typedef struct {
     int max_levels;
     int coarse_cycles;
     int sweep_growth;
-    int smoother;  /* 0 weighted Jacobi (reference default), 1 red-black Gauss-Seidel */
+    int smoother;  /* 0 weighted Jacobi (reference default), 1 red-black Gauss-Seidel,
+                      2 red-black ILU(0) (block ILU of rdme_full_multigrid.cpp:204-296 in colour order) */
     int precision; /* 0 FP64, 1 FP32 (use inside flexible GMRES) */
 } mk_multigrid_options;
 void mk_multigrid_options_default(mk_multigrid_options *opt);
@@ -160,6 +161,10 @@ int mk_multigrid_prolong(mk_multigrid mg, int depth, const double *d_coarse, dou
                          void *stream);
 int mk_multigrid_apply_system(mk_multigrid mg, int depth, const double *d_x, double *d_y,
                               void *stream);
+/* one sweep of the level's smoother on (b, x) at depth d, in place on x (FP64 hierarchies):
+ * the weighted Jacobi update of population_multigrid::smooth (multigrid.hpp:309-317), a
+ * red-then-black Gauss-Seidel pass pair, or one red-black ILU(0) sweep x += (LU)^-1 (b - A x) */
+int mk_multigrid_smooth(mk_multigrid mg, int depth, const double *d_b, double *d_x, void *stream);
 
 /* ---- GMRES: num::gmres(A, [M], b, x, options) (call sites tests/test_rdme.cpp:238-249) ---- */
 typedef struct {
@@ -269,7 +274,7 @@ typedef struct {
     int slots;               /* concurrent solves (worker threads and streams), 1..64 */
     size_t hbm_budget;       /* bytes for resident solvers; 0 = 80 % of the free memory */
     int precision;           /* 1: FP32 multigrid inside FP64 flexible GMRES; 0: all FP64 */
-    int smoother;            /* multigrid smoother: 0 weighted Jacobi, 1 red-black Gauss-Seidel */
+    int smoother;            /* multigrid smoother: 0 Jacobi, 1 red-black Gauss-Seidel, 2 ILU(0) */
     int restart;             /* GMRES restart, 1..64 */
     int64_t max_iterations;
     double rel_tolerance;    /* stop at ||b - A x|| <= rel_tolerance * ||b|| */

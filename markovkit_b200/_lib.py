@@ -202,6 +202,7 @@ SIGNATURES = {
     "mk_multigrid_restrict": (C.c_int, [P, C.c_int, P, P, P]),
     "mk_multigrid_prolong": (C.c_int, [P, C.c_int, P, P, P]),
     "mk_multigrid_apply_system": (C.c_int, [P, C.c_int, P, P, P]),
+    "mk_multigrid_smooth": (C.c_int, [P, C.c_int, P, P, P]),
     "mk_gmres_options_default": (None, [C.POINTER(GmresOptions)]),
     "mk_solver_create": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.POINTER(P)]),
     "mk_solver_destroy": (None, [P]),

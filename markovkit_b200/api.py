@@ -322,7 +322,7 @@ def multigrid_options(**kw) -> MultigridOptions:
     load().mk_multigrid_options_default(C.byref(o))
     for k, v in kw.items():
         if k == "smoother" and isinstance(v, str):
-            v = {"jacobi": 0, "gauss_seidel": 1}[v]
+            v = {"jacobi": 0, "gauss_seidel": 1, "ilu0": 2}[v]
         if k == "precision" and isinstance(v, str):
             v = {"fp64": 0, "fp32": 1}[v]
         setattr(o, k, v)
@@ -380,6 +380,11 @@ class sector_multigrid(_Handle):
     def apply_system(self, depth: int, x, y, stream=None):
         check(load().mk_multigrid_apply_system(self._h, int(depth), _ptr(x), _ptr(y), _stream(stream)))
         return y
+
+    def smooth(self, depth: int, b, x, stream=None):
+        """one sweep of the level's smoother on (b, x), in place on x (FP64 hierarchies)"""
+        check(load().mk_multigrid_smooth(self._h, int(depth), _ptr(b), _ptr(x), _stream(stream)))
+        return x
 
 
 def kernel_launches() -> int:

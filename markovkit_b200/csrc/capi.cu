@@ -420,6 +420,13 @@ int mk_multigrid_apply_system(mk_multigrid mg, int depth, const double *d_x, dou
     });
 }
 
+int mk_multigrid_smooth(mk_multigrid mg, int depth, const double *d_b, double *d_x, void *stream) {
+    return guarded([&] {
+        MK_REQUIRE(mg && d_b && d_x, "null argument");
+        mg->mg->smooth(depth, d_b, d_x, as_stream(stream));
+    });
+}
+
 // ---- GMRES
 
 void mk_gmres_options_default(mk_gmres_options *opt) {

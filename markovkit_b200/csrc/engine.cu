@@ -337,7 +337,7 @@ void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vec
         load_state<kMaxSpecies, 64>(B, sec, op.S, op.V, i, *st);
         double exit = 0.0, leak = 0.0;
         visit_row<double, kMaxSpecies, 64>(B, op.sectors.data(), sec, op.t64.host, i, *st, true, 0, 1, exit,
-                                leak, [&](std::int64_t j, double a) {
+                                leak, [&](std::int64_t j, double a, double) {
                                     A[static_cast<std::size_t>(i) * n + (j - sec.begin)] -= a;
                                 });
         A[static_cast<std::size_t>(i) * n + i] += shift + exit;
@@ -359,7 +359,7 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     if (model.V != space.V || model.S != space.S) {
         throw Error(kEInval, "model and space disagree on voxels or species");
     }
-    if (opt.smoother < 0 || opt.smoother > 1 || opt.precision < 0 || opt.precision > 1) {
+    if (opt.smoother < 0 || opt.smoother > 2 || opt.precision < 0 || opt.precision > 1) {
         throw Error(kEInval, "unknown smoother or precision");
     }
     const int S = space.S;
@@ -484,6 +484,62 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
             }
         }
     }
+    if (opt.smoother == 2) {
+        if (opt.precision == 0) {
+            ilu_pivots<double>();
+        } else {
+            ilu_pivots<float>();
+        }
+    }
+}
+
+// Red-black ILU(0) pivots of every level: the diagonal (shift + exit) into a work vector, then
+// P1 = D1 - diag(A10 D0^-1 A01) on the second colour. The diffusion-only level operator is
+// bipartite in the checkerboard colour of the state (each jump moves one molecule to a
+// neighbouring voxel, flipping the parity), so the elimination touches nothing but these pivots.
+template <typename T>
+void Multigrid::ilu_pivots() {
+    for (auto &Lp : levels) {
+        Level &L = *Lp;
+        const std::size_t nd = static_cast<std::size_t>(L.op.n);
+        DeviceArray<T> &piv = [&]() -> DeviceArray<T> & {
+            if constexpr (std::is_same_v<T, double>) {
+                return L.piv64;
+            } else {
+                return L.piv32;
+            }
+        }();
+        piv.resize(nd);
+        RowParams<T> p = L.op.params<T>();
+        p.shift = static_cast<T>(shift);
+        T *diag = buf<T>(L, 2);
+        p.y = diag;
+        L.op.run<T>(kDiagonal, p, nullptr);
+        // first-colour rows keep their diagonal; second-colour rows get the modified pivot
+        check_cuda(cudaMemcpyAsync(piv.get(), diag, nd * sizeof(T), cudaMemcpyDeviceToDevice, nullptr),
+                   "pivot copy");
+        p.aux = diag;
+        p.y = piv.get();
+        L.op.run<T>(kIluPivot, p, nullptr);
+    }
+    check_cuda(cudaStreamSynchronize(nullptr), "ILU(0) pivots");
+}
+
+template <typename T>
+void Multigrid::ilu_sweep(Level &L, RowParams<T> p, T *x, const T *rhs, T *work,
+                          cudaStream_t stream) {
+    p.x = x;
+    p.y = x;
+    p.b = rhs;
+    p.aux = work;
+    if constexpr (std::is_same_v<T, double>) {
+        p.piv = L.piv64.get();
+    } else {
+        p.piv = L.piv32.get();
+    }
+    L.op.run<T>(kIluFirst, p, stream);
+    L.op.run<T>(kIluSecond, p, stream);
+    L.op.run<T>(kIluThird, p, stream);
 }
 
 int Multigrid::levels_of_sector(int k) const {
@@ -563,7 +619,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
         } else {
             check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
         }
-    } else {
+    } else if (opt.smoother == 1) {
         check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
         for (int k = 0; k < L.pre; ++k) {
             for (int c = 0; c < 2; ++c) {
@@ -572,6 +628,11 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
                 p.colour = c;
                 L.op.run<T>(kGaussSeidel, p, stream);
             }
+        }
+    } else {
+        check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
+        for (int k = 0; k < L.pre; ++k) {
+            ilu_sweep<T>(L, p, x, rhs, tmp, stream);
         }
     }
 
@@ -636,7 +697,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
             L.op.run<T>(kJacobi, p, stream);
             std::swap(x, tmp);
         }
-    } else {
+    } else if (opt.smoother == 1) {
         for (int k = 0; k < L.post; ++k) {
             for (int c = 1; c >= 0; --c) {
                 p.b = rhs;
@@ -644,6 +705,10 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
                 p.colour = c;
                 L.op.run<T>(kGaussSeidel, p, stream);
             }
+        }
+    } else {
+        for (int k = 0; k < L.post; ++k) {
+            ilu_sweep<T>(L, p, x, rhs, tmp, stream);
         }
     }
     // keep the result in x's own buffer so the caller's view of the level stays fixed
@@ -690,6 +755,37 @@ void Multigrid::apply_system(int d, const double *x, double *y, cudaStream_t str
     p.x = x;
     p.y = y;
     L.op.run<double>(kApplyShifted, p, stream);
+}
+
+void Multigrid::smooth(int d, const double *b, double *x, cudaStream_t stream) {
+    if (d < 0 || d >= max_depth) {
+        throw Error(kEInval, "no such multigrid level");
+    }
+    if (opt.precision != 0) {
+        throw Error(kEInval, "smooth: FP64 preconditioners only");
+    }
+    Level &L = *levels[d];
+    RowParams<double> p = L.op.params<double>();
+    p.shift = shift;
+    p.omega = opt.jacobi_weight;
+    double *tmp = buf<double>(L, 2);
+    const std::size_t bytes = static_cast<std::size_t>(L.op.n) * sizeof(double);
+    if (opt.smoother == 0) {
+        p.x = x;
+        p.b = b;
+        p.y = tmp;
+        L.op.run<double>(kJacobi, p, stream);
+        check_cuda(cudaMemcpyAsync(x, tmp, bytes, cudaMemcpyDeviceToDevice, stream), "copy");
+    } else if (opt.smoother == 1) {
+        for (int c = 0; c < 2; ++c) {
+            p.b = b;
+            p.y = x;
+            p.colour = c;
+            L.op.run<double>(kGaussSeidel, p, stream);
+        }
+    } else {
+        ilu_sweep<double>(L, p, x, b, tmp, stream);
+    }
 }
 
 // The cycle works only on the hierarchy's own buffers, so it is captured once into a CUDA

@@ -155,7 +155,8 @@ struct MultigridOptions {
     int max_levels = 32;
     int coarse_cycles = 1;
     int sweep_growth = 0;
-    int smoother = 0;  // 0 weighted Jacobi (the reference's default), 1 red-black Gauss-Seidel
+    int smoother = 0;  // 0 weighted Jacobi (the reference's default), 1 red-black Gauss-Seidel,
+                       // 2 red-black ILU(0)
     int precision = 0; // 0 FP64, 1 FP32 preconditioner
 };
 
@@ -173,6 +174,9 @@ struct Multigrid {
         DeviceArray<TerminalBlock> d_term;
         DeviceArray<double> inv64;
         DeviceArray<float> inv32;
+        // red-black ILU(0) pivots (smoother 2): diagonal on colour 0, modified on colour 1
+        DeviceArray<double> piv64;
+        DeviceArray<float> piv32;
         // work vectors (precision of the preconditioner)
         DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
         DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
@@ -205,10 +209,17 @@ struct Multigrid {
     // between depth d and d + 1, and y = (shift I - Q_d) x on depth d
     void transfer(int d, int direction, const double *in, double *out, cudaStream_t stream);
     void apply_system(int d, const double *x, double *y, cudaStream_t stream);
+    // one sweep of the level's smoother on (b, x) at depth d, FP64 preconditioners only
+    // (the Jacobi update of multigrid.hpp:309-317, or one colour pass pair, or one ILU(0) sweep)
+    void smooth(int d, const double *b, double *x, cudaStream_t stream);
 
   private:
     template <typename T>
     T *cycle(int d, cudaStream_t stream);
+    template <typename T>
+    void ilu_pivots();
+    template <typename T>
+    void ilu_sweep(Level &L, RowParams<T> p, T *x, const T *rhs, T *work, cudaStream_t stream);
     template <typename T>
     T *buf(Level &L, int which);
     void ensure_graph();

@@ -191,7 +191,7 @@ MK_HD int reaction_source(const BinomTable &B, const ModelView<T> &md, const Sec
 // rank differs by C(u' + p, p + 1) - C(u + p, p + 1) for its position p; only a move past a
 // neighbouring molecule re-ranks the whole list (lists of up to two use a closed form).
 // On a structured grid the neighbours and edge coefficients are arithmetic, not loaded.
-template <typename T, int NS, int TMAX, bool WANT_IN, typename Acc>
+template <typename T, int NS, int TMAX, bool WANT_IN, bool WANT_REV, typename Acc>
 MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const SectorDesc &sec,
                            const RowState<NS, TMAX> &st, int s, int row, T &exit, Acc &acc) {
     const int t = sec.total[s];
@@ -211,7 +211,9 @@ MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const Se
         const int lo = p > 0 ? u[p > 0 ? p - 1 : 0] : -1;
         const int hi = p + 1 < t ? u[p + 1 < TMAX ? p + 1 : p] : 0x7fffffff;
         constexpr int J = p + 1 <= 4 ? p + 1 : 4;
-        // the in-jump from the neighbour whose reversed index is uw, with edge coefficient coef
+        // the in-jump from the neighbour whose reversed index is uw, with edge coefficient coef;
+        // the third argument of acc is the reverse jump's rate (one of this voxel's copies
+        // moving back), exact on grids of equal cell volumes where coef is symmetric
         auto in_jump = [&](int uw, T coef) {
             const bool up = uw > uu;
             if (up ? !last : !first) {
@@ -219,6 +221,10 @@ MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const Se
             }
             const int nw = count_of<TMAX>(u, t, uw);
             const T rate = T(nw + 1) * Ds * coef;
+            T rev = T(0);
+            if constexpr (WANT_REV) {
+                rev = T(count_of<TMAX>(u, t, uu)) * Ds * coef;
+            }
             int delta;
             if constexpr (TMAX <= 2) {
                 delta = static_cast<int>(rank_replace<TMAX>(B, u, t, uu, uw)) - st.rank[s];
@@ -227,7 +233,7 @@ MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const Se
             } else {
                 delta = static_cast<int>(rank_replace<TMAX>(B, u, t, uu, uw)) - st.rank[s];
             }
-            acc(row + delta * stride, rate);
+            acc(row + delta * stride, rate, rev);
         };
         if (md.grid_dim > 0) {
             int c[3];
@@ -285,7 +291,11 @@ MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const Se
                     const T rate = T(nw + 1) * Ds * load_ro(md.in_coef + e);
                     const int delta =
                         static_cast<int>(rank_replace<TMAX>(B, u, t, uu, uw)) - st.rank[s];
-                    acc(row + delta * stride, rate);
+                    T rev = T(0);
+                    if constexpr (WANT_REV) {
+                        rev = T(count_of<TMAX>(u, t, uu)) * Ds * load_ro(md.in_coef + e);
+                    }
+                    acc(row + delta * stride, rate, rev);
                 }
             }
         }
@@ -320,7 +330,7 @@ MK_HD std::int64_t rank_inserted(const int (&u)[TMAX], int t, const std::int64_t
 // Visit the row: acc(source_index, rate) for every in-jump; adds into exit and leak.
 // light: the exit/leak terms and the in-jumps that start in occupied voxels.
 // [lane, V) step nlanes: the all-voxel loop of heavy reactions.
-template <typename T, int NS, int TMAX, bool WANT_IN = true, typename Acc>
+template <typename T, int NS, int TMAX, bool WANT_IN = true, bool WANT_REV = false, typename Acc>
 MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const SectorDesc &sec,
                      const ModelView<T> &md, std::int64_t local, const RowState<NS, TMAX> &st,
                      bool light, int lane, int nlanes, T &exit, T &leak, Acc &&acc) {
@@ -345,7 +355,7 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
         const int row = static_cast<int>(sec.begin + local);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            diffusion_terms<T, NS, TMAX, WANT_IN>(B, md, sec, st, s, row, exit, acc);
+            diffusion_terms<T, NS, TMAX, WANT_IN, WANT_REV>(B, md, sec, st, s, row, exit, acc);
         }
         // reactions: each distinct occupied voxel once, at the first occurrence (s, p) of it
 #pragma unroll
@@ -410,7 +420,7 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                         if (ain > T(0)) {
                             acc(reaction_source<T, NS, TMAX>(B, md, sec, sectors[sec.src[r]], st,
                                                              r, uu),
-                                ain);
+                                ain, T(0));
                         }
                     }
                 }
@@ -476,7 +486,7 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                     }
                     src += static_cast<int>(rs) * static_cast<int>(ss.stride[s]);
                 }
-                acc(src, a);
+                acc(src, a, T(0));
             }
         }
     }

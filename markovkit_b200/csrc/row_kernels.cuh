@@ -32,6 +32,13 @@ enum RowMode : int {
     kDiagonal,            // y = shift + exit
     kRestrict,            // coarse[c(i)] += x_i                (population_transfer::restrict)
     kProlong,             // y_i = weight_i * coarse[c(i)]      (population_transfer::prolong)
+    // red-black ILU(0) of A = shift I - Q on a bipartite (diffusion-only) level, colour 0 first:
+    // with A = [D0 A01; A10 D1], L = [I 0; A10 D0^-1 I], U = [D0 A01; 0 P1], and the pivots
+    // P1 = D1 - diag(A10 D0^-1 A01). One sweep x += U^-1 L^-1 (b - A x) is three passes:
+    kIluPivot,            // colour 1: y = shift + exit - sum_j rate(j->i) rate(i->j) / aux_j (aux = diagonal)
+    kIluFirst,            // colour 0: aux = (b - A x) / (shift + exit)
+    kIluSecond,           // colour 1: z = (b - A x + sum_j rate(j->i) aux_j) / piv; aux = z; y = x + z
+    kIluThird,            // colour 0: y = x + aux + sum_j rate(j->i) aux_j / (shift + exit)
     kRowModeCount
 };
 
@@ -47,6 +54,7 @@ struct RowParams {
     T *y = nullptr;
     T *aux = nullptr;
     T *coarse = nullptr;
+    const T *piv = nullptr; // ILU(0) pivots of the second colour
     T shift = 0;
     T omega = 0;
     int colour = 0;

@@ -24,9 +24,27 @@ __device__ __forceinline__ T warp_sum(T v) {
 template <typename T, int NS, int TMAX>
 __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDesc &sec,
                                            std::int64_t local, const RowState<NS, TMAX> &st,
-                                           T exit, T leak, T in) {
+                                           T exit, T leak, T in, T in2) {
     const std::int64_t i = sec.begin + local;
     switch (p.mode) {
+    case kIluPivot:
+        p.y[i] = p.shift + exit - in;
+        break;
+    case kIluFirst: {
+        const T d = p.shift + exit;
+        p.aux[i] = (p.b[i] - (d * p.x[i] - in)) / d;
+        break;
+    }
+    case kIluSecond: {
+        const T xi = p.x[i];
+        const T z = (p.b[i] - ((p.shift + exit) * xi - in) + in2) / p.piv[i];
+        p.aux[i] = z;
+        p.y[i] = xi + z;
+        break;
+    }
+    case kIluThird:
+        p.y[i] = p.x[i] + p.aux[i] + in2 / (p.shift + exit);
+        break;
     case kApplyQ:
         p.y[i] = in - exit * p.x[i];
         break;
@@ -99,26 +117,62 @@ __device__ __forceinline__ bool needs_in(int mode) {
     return !(mode == kJacobiZero || mode == kExitLeak || mode == kDiagonal);
 }
 
+// the colour a pass visits (-1: every row)
+__device__ __forceinline__ int pass_colour(int mode, int colour) {
+    switch (mode) {
+    case kGaussSeidel:
+        return colour;
+    case kIluFirst:
+    case kIluThird:
+        return 0;
+    case kIluPivot:
+    case kIluSecond:
+        return 1;
+    default:
+        return -1;
+    }
+}
+
 // the terms of one row computed by `nlanes` cooperating threads; lane 0 takes the light terms
 template <typename T, int NS, int TMAX>
 __device__ __forceinline__ void row_terms(const RowParams<T> &p, const SectorDesc &sec,
                                           std::int64_t local, const RowState<NS, TMAX> &st,
-                                          int lane, int nlanes, T &exit, T &leak, T &in) {
+                                          int lane, int nlanes, T &exit, T &leak, T &in, T &in2) {
     if (!needs_in(p.mode)) {
         visit_row<T, NS, TMAX, false>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane,
-                                      nlanes, exit, leak, [&](int, T) {});
+                                      nlanes, exit, leak, [&](int, T, T) {});
         return;
     }
-    // Gauss-Seidel updates x (= y) in place: the reads are plain coherent loads throughout
-    const T *xs = p.mode == kGaussSeidel ? p.y : p.x;
+    if (p.mode == kIluPivot) {
+        // sum over in-jumps of rate(j -> i) rate(i -> j) / diagonal_j (aux holds the diagonal)
+        const T *dg = p.aux;
+        visit_row<T, NS, TMAX, true, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane,
+                                           nlanes, exit, leak,
+                                           [&](int j, T a, T rev) { in += a * rev / dg[j]; });
+        return;
+    }
+    // Gauss-Seidel and the ILU passes update x (= y) in place: rows of one colour read only
+    // the other colour's entries, through plain coherent loads
+    const int mode = p.mode;
+    const T *xs = mode == kGaussSeidel ? p.y : p.x;
+    const T *ax = p.aux;
     visit_row<T, NS, TMAX, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, nlanes,
-                                 exit, leak, [&](int j, T a) { in += a * xs[j]; });
+                                 exit, leak, [&](int j, T a, T) {
+                                     if (mode == kIluThird) {
+                                         in2 += a * ax[j];
+                                         return;
+                                     }
+                                     in += a * xs[j];
+                                     if (mode == kIluSecond) {
+                                         in2 += a * ax[j];
+                                     }
+                                 });
 }
 
 template <typename T, int NS, int TMAX>
 __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ RowParams<T> p) {
     __shared__ SectorDesc s_sec;
-    __shared__ T s_red[3][kRowBlock / 32];
+    __shared__ T s_red[4][kRowBlock / 32];
     const Tile tile = p.tiles[blockIdx.x];
     if (threadIdx.x == 0) {
         s_sec = p.sectors[tile.sector];
@@ -157,21 +211,23 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
         }
         return;
     }
-    if (p.mode == kGaussSeidel && state_colour<T, NS, TMAX>(p.md, sec, st) != p.colour) {
+    const int colour = pass_colour(p.mode, p.colour);
+    if (colour >= 0 && state_colour<T, NS, TMAX>(p.md, sec, st) != colour) {
         return; // uniform across the warp or block of a shared row
     }
-    T exit = T(0), leak = T(0), in = T(0);
-    row_terms<T, NS, TMAX>(p, sec, local, st, row_lane, row_lanes, exit, leak, in);
+    T exit = T(0), leak = T(0), in = T(0), in2 = T(0);
+    row_terms<T, NS, TMAX>(p, sec, local, st, row_lane, row_lanes, exit, leak, in, in2);
     if (tile.kind == 0) {
-        finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in);
+        finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in, in2);
         return;
     }
     exit = warp_sum(exit);
     leak = warp_sum(leak);
     in = warp_sum(in);
+    in2 = warp_sum(in2);
     if (tile.kind == 1) {
         if (lane == 0) {
-            finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in);
+            finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in, in2);
         }
         return;
     }
@@ -179,16 +235,18 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
         s_red[0][warp] = exit;
         s_red[1][warp] = leak;
         s_red[2][warp] = in;
+        s_red[3][warp] = in2;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        exit = leak = in = T(0);
+        exit = leak = in = in2 = T(0);
         for (int w = 0; w < kRowBlock / 32; ++w) {
             exit += s_red[0][w];
             leak += s_red[1][w];
             in += s_red[2][w];
+            in2 += s_red[3][w];
         }
-        finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in);
+        finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in, in2);
     }
 }
 

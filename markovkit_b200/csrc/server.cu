@@ -278,7 +278,7 @@ int mk_server_create(const mk_server_options *opt, mk_server *out) {
         MK_REQUIRE(opt->slots >= 1 && opt->slots <= 64, "server: slots must be in 1..64");
         MK_REQUIRE(opt->restart >= 1 && opt->restart <= 64, "server: restart must be in 1..64");
         MK_REQUIRE(opt->precision == 0 || opt->precision == 1, "server: precision is 0 or 1");
-        MK_REQUIRE(opt->smoother == 0 || opt->smoother == 1, "server: smoother is 0 or 1");
+        MK_REQUIRE(opt->smoother >= 0 && opt->smoother <= 2, "server: smoother is 0, 1 or 2");
         MK_REQUIRE(opt->max_iterations >= 1 && opt->rel_tolerance > 0.0,
                    "server: max_iterations >= 1 and rel_tolerance > 0");
         auto s = std::make_unique<mk_server_s>();

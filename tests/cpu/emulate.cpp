@@ -84,7 +84,7 @@ std::int64_t emu_generator(int dim, const std::int64_t *dims, const double *spac
                     double e = 0.0, l = 0.0, in = 0.0;
                     visit_row<double, NS, TMAX>(
                         p.B, p.sectors.data(), sec, p.t.view, local, st, true, 0, 1, e, l,
-                        [&](std::int64_t j, double a) {
+                        [&](std::int64_t j, double a, double) {
                             if (j < 0 || j >= p.n) {
                                 throw Error(kEInval, "in-jump source out of range");
                             }
