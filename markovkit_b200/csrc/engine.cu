@@ -657,8 +657,12 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
         } else {
             inv = L.inv32.get();
         }
-        check_cuda(launch_terminal<T>(L.d_term.get(), static_cast<int>(L.h_term.size()), inv, r,
-                                      x, stream),
+        int max_n = 0;
+        for (const TerminalBlock &tb : L.h_term) {
+            max_n = std::max(max_n, tb.n);
+        }
+        check_cuda(launch_terminal<T>(L.d_term.get(), static_cast<int>(L.h_term.size()), max_n,
+                                      inv, r, x, stream),
                    "terminal solve");
     }
     if (C) {

@@ -3,6 +3,8 @@
 #include "launch_count.hpp"
 #include "row_kernels.cuh"
 
+#include <algorithm>
+
 namespace mkb {
 
 int mol_cap_for(int n_species, int max_species_total) {
@@ -36,16 +38,31 @@ cudaError_t launch_rows<float>(RowMode mode, int S, int cap, const RowParams<flo
 
 namespace {
 
+constexpr int kTerminalThreads = 256;
+
+// x[begin + p] += inv[p] . r[begin ..]: one warp per row of a block's inverse, the lanes
+// striding its columns (coalesced); blockIdx.x picks the terminal block, blockIdx.y a group of
+// rows, so a large block's rows spread over many SMs
 template <typename T>
-__global__ void terminal_kernel(const TerminalBlock *blocks, const T *inv, const T *r, T *x) {
+__global__ void __launch_bounds__(kTerminalThreads)
+    terminal_kernel(const TerminalBlock *blocks, const T *inv, const T *r, T *x) {
     const TerminalBlock tb = blocks[blockIdx.x];
-    for (int p = static_cast<int>(threadIdx.x); p < tb.n; p += static_cast<int>(blockDim.x)) {
+    constexpr int warps = kTerminalThreads / 32;
+    const int warp = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
+    for (int p = static_cast<int>(blockIdx.y) * warps + warp; p < tb.n;
+         p += static_cast<int>(gridDim.y) * warps) {
         const T *row = inv + tb.inv_offset + static_cast<std::int64_t>(p) * tb.n;
         T e = T(0);
-        for (int q = 0; q < tb.n; ++q) {
+        for (int q = lane; q < tb.n; q += 32) {
             e += row[q] * r[tb.begin + q];
         }
-        x[tb.begin + p] += e;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, off);
+        }
+        if (lane == 0) {
+            x[tb.begin + p] += e;
+        }
     }
 }
 
@@ -157,19 +174,21 @@ __global__ void rank_kernel(const BinomTable B, const SectorDesc *sectors, int n
 } // namespace
 
 template <typename T>
-cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, const T *inv, const T *r,
-                            T *x, cudaStream_t stream) {
+cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, int max_n, const T *inv,
+                            const T *r, T *x, cudaStream_t stream) {
     if (n_blocks == 0) {
         return cudaSuccess;
     }
+    constexpr int warps = kTerminalThreads / 32;
+    const int groups = std::max(1, std::min((max_n + warps - 1) / warps, 256));
     count_launches(1);
-    terminal_kernel<T><<<n_blocks, 128, 0, stream>>>(blocks, inv, r, x);
+    terminal_kernel<T><<<dim3(n_blocks, groups), kTerminalThreads, 0, stream>>>(blocks, inv, r, x);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_terminal<double>(const TerminalBlock *, int, const double *,
+template cudaError_t launch_terminal<double>(const TerminalBlock *, int, int, const double *,
                                              const double *, double *, cudaStream_t);
-template cudaError_t launch_terminal<float>(const TerminalBlock *, int, const float *,
+template cudaError_t launch_terminal<float>(const TerminalBlock *, int, int, const float *,
                                             const float *, float *, cudaStream_t);
 
 cudaError_t launch_unrank(const BinomTable &B, const SectorDesc *sectors, int n_sectors, int S,

@@ -78,10 +78,10 @@ struct TerminalBlock {
     int pad = 0;
 };
 
-// x[begin + p] += sum_q inv[p][q] r[begin + q] for every terminal block
+// x[begin + p] += sum_q inv[p][q] r[begin + q] for every terminal block (max_n: the largest)
 template <typename T>
-cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, const T *inv, const T *r,
-                            T *x, cudaStream_t stream);
+cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, int max_n, const T *inv,
+                            const T *r, T *x, cudaStream_t stream);
 
 // bit-exact state indexing on the device
 cudaError_t launch_unrank(const BinomTable &B, const SectorDesc *sectors, int n_sectors, int S,
