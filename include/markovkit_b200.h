@@ -111,6 +111,10 @@ int mk_generator_apply(mk_generator gen, const double *d_x, double *d_y, void *s
 /* apply_shifted: y = shift x - Q x              generator.hpp:73-81 */
 int mk_generator_apply_shifted(mk_generator gen, double shift, const double *d_x, double *d_y,
                                void *stream);
+/* apply_shifted on nb <= 4 vectors at once (column c of x and y at c * ld): the row work is
+ * done once for every column */
+int mk_generator_apply_shifted_batch(mk_generator gen, double shift, const double *d_x,
+                                     double *d_y, int64_t ld, int nb, void *stream);
 int mk_generator_apply_f32(mk_generator gen, const float *d_x, float *d_y, void *stream);
 int mk_generator_apply_shifted_f32(mk_generator gen, float shift, const float *d_x, float *d_y,
                                    void *stream);
@@ -127,6 +131,7 @@ typedef struct {
     int smoother;  /* 0 weighted Jacobi (reference default), 1 red-black Gauss-Seidel,
                       2 red-black ILU(0) (block ILU of rdme_full_multigrid.cpp:204-296 in colour order) */
     int precision; /* 0 FP64, 1 FP32 (use inside flexible GMRES) */
+    int batch;     /* right-hand sides one cycle can serve at once (1..4), for batch solvers */
 } mk_multigrid_options;
 void mk_multigrid_options_default(mk_multigrid_options *opt);
 /* sector_multigrid(domain, box, shift, options) multigrid.hpp:377-384; a single-sector
@@ -136,6 +141,10 @@ int mk_multigrid_create(mk_space space, mk_model model, double shift,
 void mk_multigrid_destroy(mk_multigrid mg);
 /* apply(b, x): one cycle per sector             multigrid.hpp:397-403 */
 int mk_multigrid_apply(mk_multigrid mg, const double *d_b, double *d_x, void *stream);
+/* the same cycle for nb <= options.batch right-hand sides at once (column c of b at
+ * c * ldb, of x at c * ldx) */
+int mk_multigrid_apply_batch(mk_multigrid mg, const double *d_b, int64_t ldb, double *d_x,
+                             int64_t ldx, int nb, void *stream);
 /* The same cycle for callers that must not allocate device memory during the call: code that
  * runs while a stream is being captured into a CUDA graph (where cudaMalloc is not allowed),
  * or a host that fixes its device-memory budget at start-up and forbids allocation inside its
@@ -193,6 +202,21 @@ int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_
 /* the same with host vectors: copies in, solves, copies out */
 int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
                          mk_solver_result *result, void *stream);
+
+/* Several resolvent solves of one system at once (no counterpart in the reference; each column
+ * is num::gmres(A, M, b, x)): flexible GMRES advancing up to `width` right-hand sides in
+ * lockstep, one batched operator apply and one batched multigrid cycle per step for all of
+ * them. mg must have been created with options.batch >= width. */
+typedef struct mk_batch_solver_s *mk_batch_solver;
+int mk_batch_solver_create(mk_generator gen, double shift, mk_multigrid mg,
+                           const mk_gmres_options *opt, int width, mk_batch_solver *out);
+void mk_batch_solver_destroy(mk_batch_solver solver);
+/* nb <= width columns: column c of b and x at d_b + c * ld and d_x + c * ld (ld >= rows);
+ * x holds the initial guesses; column c stops at the absolute tolerance h_tolerances[c];
+ * results[c] per column. Returns the first column's failing status, if any. */
+int mk_batch_solver_solve(mk_batch_solver solver, const double *d_b, double *d_x, int64_t ld,
+                          int nb, const double *h_tolerances, mk_solver_result *results,
+                          void *stream);
 
 /* ---- Krylov FSP: solve_krylov_fsp(model, initial, final_time, options), markovkit/fsp.hpp ---- */
 /* krylov_fsp_options (fsp.hpp:190-202) with inside = box(bounds) (fsp.hpp:26-35); save_every

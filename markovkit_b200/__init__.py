@@ -17,6 +17,7 @@ from .api import (  # noqa: F401
     sector_multigrid,
     shifted_generator,
     solver,
+    batch_solver,
     voxel_domain,
 )
 from .inputs import dirichlet_rhs, uniform01, uniform_rhs  # noqa: F401

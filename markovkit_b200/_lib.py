@@ -51,6 +51,7 @@ class MultigridOptions(C.Structure):
         ("sweep_growth", C.c_int),
         ("smoother", C.c_int),
         ("precision", C.c_int),
+        ("batch", C.c_int),
     ]
 
 
@@ -189,12 +190,14 @@ SIGNATURES = {
     "mk_generator_exit_leak": (C.c_int, [P, P, P, P]),
     "mk_generator_apply": (C.c_int, [P, P, P, P]),
     "mk_generator_apply_shifted": (C.c_int, [P, C.c_double, P, P, P]),
+    "mk_generator_apply_shifted_batch": (C.c_int, [P, C.c_double, P, P, I64, C.c_int, P]),
     "mk_generator_apply_f32": (C.c_int, [P, P, P, P]),
     "mk_generator_apply_shifted_f32": (C.c_int, [P, C.c_float, P, P, P]),
     "mk_multigrid_options_default": (None, [C.POINTER(MultigridOptions)]),
     "mk_multigrid_create": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
     "mk_multigrid_destroy": (None, [P]),
     "mk_multigrid_apply": (C.c_int, [P, P, P, P]),
+    "mk_multigrid_apply_batch": (C.c_int, [P, P, I64, P, I64, C.c_int, P]),
     "mk_multigrid_apply_noalloc": (C.c_int, [P, P, P, P]),
     "mk_multigrid_max_levels": (C.c_int, [P, IP]),
     "mk_multigrid_depth": (C.c_int, [P, IP]),
@@ -209,6 +212,9 @@ SIGNATURES = {
     "mk_solver_set_tolerance": (C.c_int, [P, C.c_double]),
     "mk_solver_solve": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
     "mk_solver_solve_host": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
+    "mk_batch_solver_create": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.c_int, C.POINTER(P)]),
+    "mk_batch_solver_destroy": (None, [P]),
+    "mk_batch_solver_solve": (C.c_int, [P, P, P, I64, C.c_int, DP, C.POINTER(SolverResult), P]),
     "mk_fsp_options_default": (None, [C.POINTER(FspOptions)]),
     "mk_fsp_box_size": (C.c_int, [C.c_int, IP, I64P]),
     "mk_fsp_batch_create": (C.c_int, [C.c_int, C.POINTER(FspProblem), C.POINTER(P)]),

@@ -440,6 +440,30 @@ class solver(_Handle):
         return solver_result(r.iterations, r.residual, bool(r.converged), r.status)
 
 
+class batch_solver(_Handle):
+    """Flexible GMRES for up to `width` right-hand sides of one system at once: one batched
+    operator apply and one batched multigrid cycle per step (M built with batch >= width)."""
+
+    _destroy = "mk_batch_solver_destroy"
+
+    def __init__(self, A: shifted_generator, M: sector_multigrid, options: Optional[GmresOptions] = None,
+                 width: int = 4):
+        super().__init__()
+        self.A, self.M, self.width = A, M, int(width)
+        opts = options if options is not None else gmres_options()
+        check(load().mk_batch_solver_create(A.Q._h, A.shift(), M._h, C.byref(opts), self.width, C.byref(self._h)))
+
+    def solve(self, B, X, tolerances, stream=None) -> list:
+        """B, X: (nb, n) contiguous float64 CUDA tensors (X holds initial guesses); column c
+        stops at the absolute tolerance tolerances[c]"""
+        nb, n = B.shape
+        tol = (C.c_double * nb)(*[float(t) for t in tolerances])
+        res = (SolverResult * nb)()
+        check(load().mk_batch_solver_solve(self._h, _ptr(B), _ptr(X), int(B.stride(0)), nb, tol, res, _stream(stream)),
+              allow=(_lib.MK_ENOTCONV,))
+        return [solver_result(r.iterations, r.residual, bool(r.converged), r.status) for r in res]
+
+
 def gmres(A: shifted_generator, *args, **kw) -> solver_result:
     """num::gmres(A, [M], b, x, options): x holds the initial guess and gets the solution."""
     if len(args) >= 3 and isinstance(args[0], sector_multigrid):

@@ -300,6 +300,17 @@ int mk_generator_apply_shifted(mk_generator gen, double shift, const double *d_x
     });
 }
 
+int mk_generator_apply_shifted_batch(mk_generator gen, double shift, const double *d_x,
+                                     double *d_y, int64_t ld, int nb, void *stream) {
+    return guarded([&] {
+        MK_REQUIRE(gen && d_x && d_y, "null argument");
+        MK_REQUIRE(nb >= 1 && nb <= kRowBatch, "batch must be in 1..4");
+        MK_REQUIRE(ld >= gen->gen->op.n, "column stride shorter than the system");
+        gen->gen->apply<double>(kApplyShifted, shift, d_x, nullptr, d_y, nullptr,
+                                as_stream(stream), nb, ld);
+    });
+}
+
 int mk_generator_apply_f32(mk_generator gen, const float *d_x, float *d_y, void *stream) {
     return guarded([&] {
         MK_REQUIRE(gen && d_x && d_y, "null argument");
@@ -332,6 +343,7 @@ void mk_multigrid_options_default(mk_multigrid_options *opt) {
     opt->sweep_growth = d.sweep_growth;
     opt->smoother = d.smoother;
     opt->precision = d.precision;
+    opt->batch = d.batch;
 }
 
 int mk_multigrid_create(mk_space space, mk_model model, double shift,
@@ -353,6 +365,7 @@ int mk_multigrid_create(mk_space space, mk_model model, double shift,
             o.sweep_growth = opt->sweep_growth;
             o.smoother = opt->smoother;
             o.precision = opt->precision;
+            o.batch = opt->batch;
         }
         auto h = std::make_unique<mk_multigrid_s>();
         h->mg = std::make_unique<Multigrid>(*space->space, *model->model, shift, o);
@@ -366,6 +379,15 @@ int mk_multigrid_apply(mk_multigrid mg, const double *d_b, double *d_x, void *st
     return guarded([&] {
         MK_REQUIRE(mg && d_b && d_x, "null argument");
         mg->mg->apply(d_b, d_x, as_stream(stream));
+    });
+}
+
+int mk_multigrid_apply_batch(mk_multigrid mg, const double *d_b, int64_t ldb, double *d_x,
+                             int64_t ldx, int nb, void *stream) {
+    return guarded([&] {
+        MK_REQUIRE(mg && d_b && d_x, "null argument");
+        MK_REQUIRE(ldb >= mg->mg->n && ldx >= mg->mg->n, "column stride shorter than the system");
+        mg->mg->apply_batch(d_b, ldb, d_x, ldx, nb, as_stream(stream));
     });
 }
 
@@ -528,6 +550,78 @@ int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
         return rc;
     }
     return fill_result(r, result);
+}
+
+// ---- batched FGMRES
+
+int mk_batch_solver_create(mk_generator gen, double shift, mk_multigrid mg,
+                           const mk_gmres_options *opt, int width, mk_batch_solver *out) {
+    return guarded([&] {
+        MK_REQUIRE(gen && mg && out, "null argument");
+        MK_REQUIRE(shift > 0.0, "shift must be positive");
+        MK_REQUIRE(width >= 1 && width <= kRowBatch, "batch width must be in 1..4");
+        MK_REQUIRE(mg->mg->opt.batch >= width, "the multigrid was built for a narrower batch");
+        MK_REQUIRE(mg->mg->n == gen->gen->op.n, "multigrid and generator sizes differ");
+        auto h = std::make_unique<mk_batch_solver_s>();
+        h->gen = gen;
+        h->mg = mg;
+        h->shift = shift;
+        if (opt) {
+            MK_REQUIRE(opt->restart >= 1 && opt->max_iterations >= 0, "bad GMRES options");
+            h->opt.max_iterations = opt->max_iterations;
+            h->opt.restart = opt->restart;
+        }
+        h->opt.flexible = 1;
+        const int64_t n = gen->gen->op.n;
+        const int m = static_cast<int>(std::min<int64_t>(h->opt.restart, std::max<int64_t>(n, 1)));
+        h->ws = std::make_unique<KrylovBatch>(n, m, width);
+        h->b.resize(static_cast<std::size_t>(h->ws->ld) * width);
+        h->x.resize(static_cast<std::size_t>(h->ws->ld) * width);
+        *out = h.release();
+    });
+}
+
+void mk_batch_solver_destroy(mk_batch_solver solver) { delete solver; }
+
+int mk_batch_solver_solve(mk_batch_solver solver, const double *d_b, double *d_x, int64_t ld,
+                          int nb, const double *h_tolerances, mk_solver_result *results,
+                          void *stream) {
+    std::vector<SolverResult> r;
+    const int rc = guarded([&] {
+        MK_REQUIRE(solver && d_b && d_x && h_tolerances && results, "null argument");
+        KrylovBatch &ws = *solver->ws;
+        MK_REQUIRE(nb >= 1 && nb <= ws.nb, "more columns than the solver's width");
+        const int64_t n = ws.n;
+        MK_REQUIRE(ld >= n, "column stride shorter than the system");
+        cudaStream_t s = as_stream(stream);
+        // columns into the workspace's stride, solve, and back
+        for (int c = 0; c < nb; ++c) {
+            check_cuda(cudaMemcpyAsync(solver->b.get() + c * ws.ld, d_b + c * ld, n * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, s),
+                       "copy");
+            check_cuda(cudaMemcpyAsync(solver->x.get() + c * ws.ld, d_x + c * ld, n * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, s),
+                       "copy");
+        }
+        r = gmres_batch(*solver->gen->gen, solver->shift, *solver->mg->mg, solver->b.get(),
+                        solver->x.get(), nb, h_tolerances, solver->opt, ws, s);
+        for (int c = 0; c < nb; ++c) {
+            check_cuda(cudaMemcpyAsync(d_x + c * ld, solver->x.get() + c * ws.ld, n * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, s),
+                       "copy");
+        }
+    });
+    if (rc != MK_OK) {
+        return rc;
+    }
+    int first = MK_OK;
+    for (int c = 0; c < nb; ++c) {
+        const int st = fill_result(r[c], results + c);
+        if (st != MK_OK && first == MK_OK) {
+            first = st;
+        }
+    }
+    return first;
 }
 
 } // extern "C"

@@ -29,6 +29,14 @@ struct mk_solver_s {
     std::unique_ptr<mkb::Krylov> ws;
     mkb::DeviceArray<double> b, x; // staging for host-vector solves
 };
+struct mk_batch_solver_s {
+    mk_generator gen = nullptr;
+    mk_multigrid mg = nullptr;
+    double shift = 0.0;
+    mkb::GmresOptions opt;
+    std::unique_ptr<mkb::KrylovBatch> ws;
+    mkb::DeviceArray<double> b, x; // columns at the workspace's stride
+};
 
 namespace mkb::capi {
 

@@ -239,20 +239,22 @@ Generator::Generator(const Space &sp, const Model &model, bool absorbing_)
 
 template <typename T>
 void Generator::apply(RowMode mode, T shift, const T *x, const T *b, T *y, T *aux,
-                      cudaStream_t stream) const {
+                      cudaStream_t stream, int nb, std::int64_t ld) const {
     RowParams<T> p = op.params<T>();
     p.shift = shift;
     p.x = x;
     p.b = b;
     p.y = y;
     p.aux = aux;
+    p.nb = nb;
+    p.ldv = ld;
     op.run<T>(mode, p, stream);
 }
 
 template void Generator::apply<double>(RowMode, double, const double *, const double *, double *,
-                                       double *, cudaStream_t) const;
+                                       double *, cudaStream_t, int, std::int64_t) const;
 template void Generator::apply<float>(RowMode, float, const float *, const float *, float *,
-                                      float *, cudaStream_t) const;
+                                      float *, cudaStream_t, int, std::int64_t) const;
 
 // ---------------------------------------------------------------------------------------
 // multigrid
@@ -362,6 +364,9 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     if (opt.smoother < 0 || opt.smoother > 2 || opt.precision < 0 || opt.precision > 1) {
         throw Error(kEInval, "unknown smoother or precision");
     }
+    if (opt.batch < 1 || opt.batch > kRowBatch) {
+        throw Error(kEInval, "multigrid batch must be in 1.." + std::to_string(kRowBatch));
+    }
     const int S = space.S;
     std::vector<double> h_lgf(space.max_total + 2);
     for (std::size_t k = 0; k < h_lgf.size(); ++k) {
@@ -459,11 +464,15 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     }
     max_depth = static_cast<int>(levels.size());
 
-    // work vectors in the preconditioner's precision
+    // work vectors in the preconditioner's precision, one column per right-hand side
+    graph_exec_.assign(static_cast<std::size_t>(opt.batch) + 1, nullptr);
+    graph_kernels_.assign(static_cast<std::size_t>(opt.batch) + 1, 0);
     for (std::size_t d = 0; d < levels.size(); ++d) {
         Level &L = *levels[d];
-        const std::size_t nd = static_cast<std::size_t>(L.op.n);
-        const std::size_t nc = d + 1 < levels.size() ? static_cast<std::size_t>(levels[d + 1]->op.n) : 0;
+        const std::size_t nb = static_cast<std::size_t>(opt.batch);
+        const std::size_t nd = static_cast<std::size_t>(L.op.n) * nb;
+        const std::size_t nc =
+            d + 1 < levels.size() ? static_cast<std::size_t>(levels[d + 1]->op.n) * nb : 0;
         if (opt.precision == 0) {
             L.rhs64.resize(nd);
             L.x64.resize(nd);
@@ -599,10 +608,15 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
     T *x = buf<T>(L, 1);
     T *tmp = buf<T>(L, 2);
     T *r = buf<T>(L, 3);
+    // nb_ columns, column c of every level vector at c * nd
     const std::int64_t nd = L.op.n;
+    const int nb = nb_;
+    const std::int64_t ndb = nd * nb;
     RowParams<T> p = L.op.params<T>();
     p.shift = static_cast<T>(shift);
     p.omega = static_cast<T>(opt.jacobi_weight);
+    p.nb = nb;
+    p.ldv = nd;
 
     if (opt.smoother == 0) {
         if (L.pre > 0) {
@@ -617,10 +631,10 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
                 std::swap(x, tmp);
             }
         } else {
-            check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
+            check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
         }
     } else if (opt.smoother == 1) {
-        check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
+        check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
         for (int k = 0; k < L.pre; ++k) {
             for (int c = 0; c < 2; ++c) {
                 p.b = rhs;
@@ -630,7 +644,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
             }
         }
     } else {
-        check_cuda(cudaMemsetAsync(x, 0, nd * sizeof(T), stream), "memset");
+        check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
         for (int k = 0; k < L.pre; ++k) {
             ilu_sweep<T>(L, p, x, rhs, tmp, stream);
         }
@@ -638,7 +652,8 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
 
     Level *C = d + 1 < max_depth ? levels[d + 1].get() : nullptr;
     if (C) {
-        check_cuda(cudaMemsetAsync(buf<T>(*C, 0), 0, C->op.n * sizeof(T), stream), "memset");
+        check_cuda(cudaMemsetAsync(buf<T>(*C, 0), 0, C->op.n * nb * sizeof(T), stream), "memset");
+        p.ldc = C->op.n;
         p.tv.Vc = C->op.V;
         p.tv.parent = L.parent.get();
         p.tv.log_children = L.log_children.get();
@@ -661,9 +676,11 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
         for (const TerminalBlock &tb : L.h_term) {
             max_n = std::max(max_n, tb.n);
         }
-        check_cuda(launch_terminal<T>(L.d_term.get(), static_cast<int>(L.h_term.size()), max_n,
-                                      inv, r, x, stream),
-                   "terminal solve");
+        for (int c = 0; c < nb; ++c) {
+            check_cuda(launch_terminal<T>(L.d_term.get(), static_cast<int>(L.h_term.size()),
+                                          max_n, inv, r + c * nd, x + c * nd, stream),
+                       "terminal solve");
+        }
     }
     if (C) {
         T *cx = nullptr;
@@ -671,7 +688,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
             cx = cycle<T>(d + 1, stream);
         } else {
             T *acc = buf<T>(L, 4), *crhs = buf<T>(L, 5);
-            const std::size_t bytes = C->op.n * sizeof(T);
+            const std::size_t bytes = C->op.n * nb * sizeof(T);
             check_cuda(cudaMemcpyAsync(crhs, buf<T>(*C, 0), bytes, cudaMemcpyDeviceToDevice, stream),
                        "copy");
             T *e = cycle<T>(d + 1, stream);
@@ -682,9 +699,11 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
                 pc.x = acc;
                 pc.b = crhs;
                 pc.y = buf<T>(*C, 0);
+                pc.nb = nb;
+                pc.ldv = C->op.n;
                 C->op.run<T>(kResidual, pc, stream);
                 e = cycle<T>(d + 1, stream);
-                axpy_t<T>(T(1), e, acc, C->op.n, stream);
+                axpy_t<T>(T(1), e, acc, C->op.n * nb, stream);
             }
             cx = acc;
         }
@@ -717,7 +736,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
     }
     // keep the result in x's own buffer so the caller's view of the level stays fixed
     if (x != buf<T>(L, 1)) {
-        check_cuda(cudaMemcpyAsync(buf<T>(L, 1), x, nd * sizeof(T), cudaMemcpyDeviceToDevice,
+        check_cuda(cudaMemcpyAsync(buf<T>(L, 1), x, ndb * sizeof(T), cudaMemcpyDeviceToDevice,
                                    stream),
                    "copy");
     }
@@ -794,13 +813,14 @@ void Multigrid::smooth(int d, const double *b, double *x, cudaStream_t stream) {
 
 // The cycle works only on the hierarchy's own buffers, so it is captured once into a CUDA
 // graph (about six launches per level) and replayed on the caller's stream.
-void Multigrid::ensure_graph() {
-    if (graph_exec_) {
+void Multigrid::ensure_graph(int nb) {
+    if (graph_exec_[nb]) {
         return;
     }
     cudaStream_t cap = nullptr;
     check_cuda(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream");
     cudaGraph_t graph = nullptr;
+    nb_ = nb;
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
         try {
@@ -810,6 +830,7 @@ void Multigrid::ensure_graph() {
                 cycle<float>(0, cap);
             }
         } catch (...) {
+            nb_ = 1;
             cudaStreamEndCapture(cap, &graph);
             if (graph) {
                 cudaGraphDestroy(graph);
@@ -819,20 +840,22 @@ void Multigrid::ensure_graph() {
         }
         e = cudaStreamEndCapture(cap, &graph);
     }
+    nb_ = 1;
     cudaStreamDestroy(cap);
     check_cuda(e, "multigrid graph capture");
     std::size_t n_nodes = 0;
     cudaGraphGetNodes(graph, nullptr, &n_nodes);
     std::vector<cudaGraphNode_t> nodes(n_nodes);
     cudaGraphGetNodes(graph, nodes.data(), &n_nodes);
-    graph_kernels_ = 0;
+    std::uint64_t kernels = 0;
     for (cudaGraphNode_t node : nodes) {
         cudaGraphNodeType type;
         if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) {
-            ++graph_kernels_;
+            ++kernels;
         }
     }
-    e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+    graph_kernels_[nb] = kernels;
+    e = cudaGraphInstantiate(&graph_exec_[nb], graph, 0);
     cudaGraphDestroy(graph);
     check_cuda(e, "multigrid graph instantiate");
 }
@@ -901,31 +924,46 @@ void Multigrid::apply_in(const double *b, double *x, void *scratch, std::size_t 
 }
 
 Multigrid::~Multigrid() {
-    if (graph_exec_) {
-        cudaGraphExecDestroy(graph_exec_);
+    for (cudaGraphExec_t g : graph_exec_) {
+        if (g) {
+            cudaGraphExecDestroy(g);
+        }
     }
 }
 
 void Multigrid::apply(const double *b, double *x, cudaStream_t stream) {
+    apply_batch(b, n, x, n, 1, stream);
+}
+
+void Multigrid::apply_batch(const double *b, std::int64_t ldb, double *x, std::int64_t ldx, int nb,
+                            cudaStream_t stream) {
+    if (nb < 1 || nb > opt.batch) {
+        throw Error(kEInval, "multigrid: batch wider than the hierarchy was built for");
+    }
     Level &L0 = *levels[0];
-    const std::size_t n0 = static_cast<std::size_t>(L0.op.n);
-    ensure_graph();
-    if (opt.precision == 0) {
-        check_cuda(cudaMemcpyAsync(L0.rhs64.get(), b, n0 * sizeof(double), cudaMemcpyDeviceToDevice,
-                                   stream),
-                   "copy");
-        check_cuda(cudaGraphLaunch(graph_exec_, stream), "multigrid graph launch");
-        count_launches(graph_kernels_);
-        check_cuda(cudaMemcpyAsync(x, L0.x64.get(), n0 * sizeof(double), cudaMemcpyDeviceToDevice,
-                                   stream),
-                   "copy");
-    } else {
-        check_cuda(convert<double, float>(b, L0.rhs32.get(), static_cast<std::int64_t>(n0), stream),
-                   "convert");
-        check_cuda(cudaGraphLaunch(graph_exec_, stream), "multigrid graph launch");
-        count_launches(graph_kernels_);
-        check_cuda(convert<float, double>(L0.x32.get(), x, static_cast<std::int64_t>(n0), stream),
-                   "convert");
+    const std::int64_t n0 = L0.op.n;
+    ensure_graph(nb);
+    for (int c = 0; c < nb; ++c) {
+        if (opt.precision == 0) {
+            check_cuda(cudaMemcpyAsync(L0.rhs64.get() + c * n0, b + c * ldb, n0 * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, stream),
+                       "copy");
+        } else {
+            check_cuda(convert<double, float>(b + c * ldb, L0.rhs32.get() + c * n0, n0, stream),
+                       "convert");
+        }
+    }
+    check_cuda(cudaGraphLaunch(graph_exec_[nb], stream), "multigrid graph launch");
+    count_launches(graph_kernels_[nb]);
+    for (int c = 0; c < nb; ++c) {
+        if (opt.precision == 0) {
+            check_cuda(cudaMemcpyAsync(x + c * ldx, L0.x64.get() + c * n0, n0 * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, stream),
+                       "copy");
+        } else {
+            check_cuda(convert<float, double>(L0.x32.get() + c * n0, x + c * ldx, n0, stream),
+                       "convert");
+        }
     }
 }
 
@@ -1148,6 +1186,222 @@ SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double 
         }
     }
     res.status = kENotConv;
+    return res;
+}
+
+// ---------------------------------------------------------------------------------------
+// FGMRES for several right-hand sides in lockstep
+
+namespace {
+
+std::size_t arnoldi_small_size(int m) {
+    return static_cast<std::size_t>(m + 1) * m + 6 * static_cast<std::size_t>(m + 1) + 16;
+}
+
+ArnoldiState carve_arnoldi(double *p, int m) {
+    ArnoldiState st;
+    st.m = m;
+    st.H = p;
+    p += static_cast<std::size_t>(m + 1) * m;
+    st.cs = p;
+    p += m + 1;
+    st.sn = p;
+    p += m + 1;
+    st.g = p;
+    p += m + 1;
+    st.y = p;
+    p += m + 1;
+    st.h1 = p;
+    p += m + 1;
+    st.h2 = p;
+    p += m + 1;
+    st.hn = p++;
+    st.inv_hn = p++;
+    st.beta = p++;
+    st.report = p;
+    return st;
+}
+
+} // namespace
+
+KrylovBatch::KrylovBatch(std::int64_t n_, int m_, int nb_) : n(n_), m(m_), nb(nb_) {
+    if (m < 1 || nb < 1) {
+        throw Error(kEInval, "restart and batch must be positive");
+    }
+    ld = (n + 31) / 32 * 32;
+    V.resize(static_cast<std::size_t>(ld) * nb * (m + 1));
+    Z.resize(static_cast<std::size_t>(ld) * nb * m);
+    w.resize(static_cast<std::size_t>(ld) * nb);
+    r.resize(static_cast<std::size_t>(ld) * nb);
+    partials.resize(static_cast<std::size_t>(kDotBlocks) * kMaxFusedBasis);
+    const std::size_t per = arnoldi_small_size(m);
+    small.resize(per * nb);
+    for (int c = 0; c < nb; ++c) {
+        st.push_back(carve_arnoldi(small.get() + per * c, m));
+    }
+    check_cuda(cudaMallocHost(reinterpret_cast<void **>(&report_host), 4 * sizeof(double) * nb),
+               "cudaMallocHost");
+}
+
+KrylovBatch::~KrylovBatch() {
+    if (report_host) {
+        cudaFreeHost(report_host);
+    }
+}
+
+std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigrid &M,
+                                      const double *b, double *x, int nb, const double *tol,
+                                      const GmresOptions &opt, KrylovBatch &ws,
+                                      cudaStream_t stream) {
+    const std::int64_t n = A.op.n, ld = ws.ld;
+    if (ws.n != n || M.n != n) {
+        throw Error(kEInval, "workspace or preconditioner size does not match the system");
+    }
+    if (nb < 1 || nb > ws.nb || nb > M.opt.batch) {
+        throw Error(kEInval, "batch wider than the workspace or the multigrid");
+    }
+    const int m = std::min(ws.m, std::max(1, opt.restart));
+    std::vector<SolverResult> res(nb);
+    std::vector<char> active(nb, 1);
+    auto col = [&](const double *base, int c) { return base + c * ld; };
+    // basis vector j of column c and its stride inside the column
+    auto Vj = [&](int j, int c) { return ws.V.get() + (static_cast<std::int64_t>(j) * ws.nb + c) * ld; };
+    auto Zj = [&](int j, int c) { return ws.Z.get() + (static_cast<std::int64_t>(j) * ws.nb + c) * ld; };
+    const std::int64_t col_stride = static_cast<std::int64_t>(ws.nb) * ld;
+
+    auto read_reports = [&]() {
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+    };
+    // r = b - A x for every column, beta_c = ||r_c||; returns false on a non-finite residual
+    auto true_residuals = [&]() {
+        A.apply<double>(kResidual, shift, x, b, ws.r.get(), nullptr, stream, nb, ld);
+        for (int c = 0; c < nb; ++c) {
+            check_cuda(dot(col(ws.r.get(), c), col(ws.r.get(), c), n, ws.partials.get(),
+                           ws.st[c].beta, stream),
+                       "dot");
+            check_cuda(arnoldi_start(ws.st[c], stream), "arnoldi");
+            check_cuda(cudaMemcpyAsync(ws.report_host + 4 * c, ws.st[c].report, 4 * sizeof(double),
+                                       cudaMemcpyDeviceToHost, stream),
+                       "report");
+        }
+        read_reports();
+        for (int c = 0; c < nb; ++c) {
+            if (!active[c]) {
+                continue;
+            }
+            const double beta = ws.report_host[4 * c];
+            res[c].residual = beta;
+            if (!std::isfinite(beta)) {
+                res[c].status = kENan;
+                active[c] = 0;
+            } else if (beta <= tol[c]) {
+                res[c].converged = 1;
+                active[c] = 0;
+            } else if (res[c].iterations >= opt.max_iterations) {
+                res[c].status = kENotConv;
+                active[c] = 0;
+            }
+        }
+    };
+
+    true_residuals();
+    while (std::count(active.begin(), active.end(), 1) > 0) {
+        std::vector<int> k(nb, 0);
+        std::vector<char> running(active);
+        for (int c = 0; c < nb; ++c) {
+            if (running[c]) {
+                check_cuda(scale_copy(col(ws.r.get(), c), ws.st[c].beta, Vj(0, c), n, stream), "scale");
+            }
+        }
+        for (int j = 0; j < m; ++j) {
+            // one multigrid cycle and one operator apply serve every column of step j
+            M.apply_batch(Vj(j, 0), ld, Zj(j, 0), ld, nb, stream);
+            A.apply<double>(kApplyShifted, shift, Zj(j, 0), nullptr, ws.w.get(), nullptr, stream,
+                            nb, ld);
+            for (int c = 0; c < nb; ++c) {
+                if (!running[c]) {
+                    continue;
+                }
+                double *w = ws.w.get() + c * ld;
+                const int K = j + 1;
+                const double *Vc = Vj(0, c);
+                for (int c0 = 0; c0 < K; c0 += kMaxFusedBasis) {
+                    const int kc = std::min(kMaxFusedBasis, K - c0);
+                    check_cuda(cgs_pass(0, Vc + c0 * col_stride, col_stride, kc, w, n, nullptr,
+                                        ws.partials.get(), ws.st[c].h1 + c0, stream),
+                               "cgs");
+                }
+                for (int pass = 1; pass <= 2; ++pass) {
+                    const double *coef = pass == 1 ? ws.st[c].h1 : ws.st[c].h2;
+                    double *out = pass == 1 ? ws.st[c].h2 : ws.st[c].hn;
+                    if (K <= kMaxFusedBasis) {
+                        check_cuda(cgs_pass(pass, Vc, col_stride, K, w, n, coef, ws.partials.get(),
+                                            out, stream),
+                                   "cgs");
+                    } else {
+                        for (int c0 = 0; c0 < K; c0 += kMaxFusedBasis) {
+                            const int kc = std::min(kMaxFusedBasis, K - c0);
+                            check_cuda(cgs_pass(3, Vc + c0 * col_stride, col_stride, kc, w, n,
+                                                coef + c0, ws.partials.get(), nullptr, stream),
+                                       "cgs");
+                        }
+                        if (pass == 1) {
+                            for (int c0 = 0; c0 < K; c0 += kMaxFusedBasis) {
+                                const int kc = std::min(kMaxFusedBasis, K - c0);
+                                check_cuda(cgs_pass(0, Vc + c0 * col_stride, col_stride, kc, w, n,
+                                                    nullptr, ws.partials.get(), out + c0, stream),
+                                           "cgs");
+                            }
+                        } else {
+                            check_cuda(dot(w, w, n, ws.partials.get(), out, stream), "dot");
+                        }
+                    }
+                }
+                check_cuda(arnoldi_column(ws.st[c], j, stream), "arnoldi");
+                check_cuda(cudaMemcpyAsync(ws.report_host + 4 * c, ws.st[c].report,
+                                           4 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                           "report");
+            }
+            read_reports();
+            bool any = false;
+            for (int c = 0; c < nb; ++c) {
+                if (!running[c]) {
+                    continue;
+                }
+                const double *rep = ws.report_host + 4 * c;
+                ++res[c].iterations;
+                k[c] = j + 1;
+                if (!std::isfinite(rep[0]) || !std::isfinite(rep[1])) {
+                    res[c].status = kENan;
+                    active[c] = 0;
+                    running[c] = 0;
+                    continue;
+                }
+                if (rep[0] <= tol[c] || rep[2] != 0.0 || res[c].iterations >= opt.max_iterations) {
+                    running[c] = 0; // this cycle ends here for column c
+                    continue;
+                }
+                any = true;
+                if (j + 1 < m) {
+                    check_cuda(scale_copy(col(ws.w.get(), c), ws.st[c].inv_hn, Vj(j + 1, c), n,
+                                          stream),
+                               "scale");
+                }
+            }
+            if (!any) {
+                break;
+            }
+        }
+        for (int c = 0; c < nb; ++c) {
+            if (!active[c] || k[c] == 0) {
+                continue;
+            }
+            check_cuda(arnoldi_solve(ws.st[c], k[c], stream), "arnoldi");
+            check_cuda(multi_axpy(Zj(0, c), col_stride, k[c], ws.st[c].y, x + c * ld, n, stream),
+                       "update");
+        }
+        true_residuals();
+    }
     return res;
 }
 

@@ -142,9 +142,10 @@ struct Generator {
     bool absorbing = true;
     std::int64_t n_jumps_cache = -1;
     Generator(const Space &space, const Model &model, bool absorbing);
+    // one pass over every row; with nb > 1, nb right-hand sides whose columns sit ld apart
     template <typename T>
-    void apply(RowMode mode, T shift, const T *x, const T *b, T *y, T *aux,
-               cudaStream_t stream) const;
+    void apply(RowMode mode, T shift, const T *x, const T *b, T *y, T *aux, cudaStream_t stream,
+               int nb = 1, std::int64_t ld = 0) const;
 };
 
 struct MultigridOptions {
@@ -158,6 +159,7 @@ struct MultigridOptions {
     int smoother = 0;  // 0 weighted Jacobi (the reference's default), 1 red-black Gauss-Seidel,
                        // 2 red-black ILU(0)
     int precision = 0; // 0 FP64, 1 FP32 preconditioner
+    int batch = 1;     // right-hand sides one cycle can serve at once (work vectors per level)
 };
 
 // sector_multigrid (markovkit/rdme/multigrid.hpp:136-408): one geometric V-cycle per
@@ -197,6 +199,10 @@ struct Multigrid {
     Multigrid &operator=(const Multigrid &) = delete;
     // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
     void apply(const double *b, double *x, cudaStream_t stream);
+    // the same for nb <= opt.batch right-hand sides at once: column c of b at b + c * ldb,
+    // of x at x + c * ldx; one cycle serves all columns
+    void apply_batch(const double *b, std::int64_t ldb, double *x, std::int64_t ldx, int nb,
+                     cudaStream_t stream);
     // bytes of work vectors one cycle needs, each vector aligned to 256 bytes
     [[nodiscard]] std::size_t scratch_bytes() const;
     // the same cycle with every work vector carved from caller-given device memory of at
@@ -222,10 +228,12 @@ struct Multigrid {
     void ilu_sweep(Level &L, RowParams<T> p, T *x, const T *rhs, T *work, cudaStream_t stream);
     template <typename T>
     T *buf(Level &L, int which);
-    void ensure_graph();
-    cudaGraphExec_t graph_exec_ = nullptr;
-    std::uint64_t graph_kernels_ = 0; // kernel nodes of the captured cycle
+    void ensure_graph(int nb);
+    // the captured cycle for each batch width, and its kernel nodes
+    std::vector<cudaGraphExec_t> graph_exec_;
+    std::vector<std::uint64_t> graph_kernels_;
     bool use_carved_ = false;
+    int nb_ = 1; // columns the cycle being recorded or run serves
 };
 
 struct GmresOptions {
@@ -261,5 +269,30 @@ struct Krylov {
 // A = shift I - Q with classical Gram-Schmidt and one re-orthogonalisation
 SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double *b, double *x,
                    const GmresOptions &opt, Krylov &ws, cudaStream_t stream);
+
+// Workspace of FGMRES for nb right-hand sides advanced in lockstep. Basis vector j of column
+// c sits at V + (j * nb + c) * ld (and Z likewise), so step j of every column is one strided
+// block for the batched operator and multigrid, and column c's basis is strided by nb * ld
+// for its Gram-Schmidt passes.
+struct KrylovBatch {
+    std::int64_t n = 0, ld = 0;
+    int m = 0, nb = 0;
+    DeviceArray<double> V, Z, w, r, partials, small;
+    std::vector<ArnoldiState> st;
+    double *report_host = nullptr; // pinned, 4 per column
+    KrylovBatch(std::int64_t n, int m, int nb);
+    ~KrylovBatch();
+    KrylovBatch(const KrylovBatch &) = delete;
+    KrylovBatch &operator=(const KrylovBatch &) = delete;
+};
+
+// FGMRES on nb <= ws.nb right-hand sides at once (column c of b and x at c * ws.ld): one
+// batched operator apply and one batched multigrid cycle per step serve every column, the
+// Gram-Schmidt passes and Givens rotations run per column. Column c stops at its own absolute
+// tolerance tol[c] (opt.tolerance is unused); the batch stops when every column has.
+std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigrid &M,
+                                      const double *b, double *x, int nb, const double *tol,
+                                      const GmresOptions &opt, KrylovBatch &ws,
+                                      cudaStream_t stream);
 
 } // namespace mkb

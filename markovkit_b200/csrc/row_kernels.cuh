@@ -60,7 +60,14 @@ struct RowParams {
     int colour = 0;
     int n_tiles = 0;
     int mode = kApplyShifted;
+    // right-hand sides served at once (1..kRowBatch): column c of x, b, y and aux starts at
+    // c * ldv, column c of coarse at c * ldc
+    int nb = 1;
+    std::int64_t ldv = 0;
+    std::int64_t ldc = 0;
 };
+
+constexpr int kRowBatch = 4; // widest batch of the instantiated kernels
 
 // the largest species total the kernels handle: 64 with one species, 16 with more
 int mol_cap_for(int n_species, int max_species_total);
@@ -70,6 +77,9 @@ template <typename T>
 cudaError_t launch_rows(RowMode mode, int S, int cap, const RowParams<T> &p, cudaStream_t stream);
 cudaError_t launch_rows_f64(const RowParams<double> &p, int S, int cap, cudaStream_t stream);
 cudaError_t launch_rows_f32(const RowParams<float> &p, int S, int cap, cudaStream_t stream);
+// the batched instantiations (p.nb > 1)
+cudaError_t launch_rows_f64_batch(const RowParams<double> &p, int S, int cap, cudaStream_t stream);
+cudaError_t launch_rows_f32_batch(const RowParams<float> &p, int S, int cap, cudaStream_t stream);
 
 struct TerminalBlock {
     std::int64_t begin = 0;      // first row in the level space

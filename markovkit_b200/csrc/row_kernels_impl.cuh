@@ -1,9 +1,11 @@
 // sm_100a row kernels: the matrix-free generator gather and every multigrid pass built on it.
-// All of them are HBM-bound gathers (no dense contraction, so no tensor cores): each thread
-// unranks its state, visits its in-jumps and writes one value. Rows whose in-jumps fan in
-// from every voxel take a warp (tile kind 1) or a whole block (kind 2) each. The pass (SpMV,
-// residual, smoother sweep, transfer) is a launch parameter, uniform across the grid.
-// Instantiated per precision in row_kernels_f64.cu and row_kernels_f32.cu.
+// Each thread unranks its state, visits its in-jumps and writes one value per column. Rows
+// whose in-jumps fan in from every voxel take a warp (tile kind 1) or a whole block (kind 2)
+// each. The pass (SpMV, residual, smoother sweep, transfer) is a launch parameter, uniform
+// across the grid. NB > 1 instantiations serve up to NB right-hand sides at once (columns at
+// stride ldv, coarse columns at stride ldc): the ranking and rate work of a row, which bounds
+// these kernels, is done once for all columns.
+// Instantiated per precision and batch width in row_kernels_f64*.cu and row_kernels_f32*.cu.
 #pragma once
 
 #include "launch_count.hpp"
@@ -21,92 +23,112 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-template <typename T, int NS, int TMAX>
+template <typename T, int NS, int TMAX, int NB>
 __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDesc &sec,
                                            std::int64_t local, const RowState<NS, TMAX> &st,
-                                           T exit, T leak, T in, T in2) {
+                                           T exit, T leak, const T (&in)[NB], const T (&in2)[NB]) {
     const std::int64_t i = sec.begin + local;
-    switch (p.mode) {
-    case kIluPivot:
-        p.y[i] = p.shift + exit - in;
-        break;
-    case kIluFirst: {
-        const T d = p.shift + exit;
-        p.aux[i] = (p.b[i] - (d * p.x[i] - in)) / d;
-        break;
+    const T d = p.shift + exit;
+    std::int64_t ci = -1;
+    if (p.mode == kResidualRestrict && sec.coarse >= 0) {
+        ci = coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, nullptr);
     }
-    case kIluSecond: {
-        const T xi = p.x[i];
-        const T z = (p.b[i] - ((p.shift + exit) * xi - in) + in2) / p.piv[i];
-        p.aux[i] = z;
-        p.y[i] = xi + z;
-        break;
-    }
-    case kIluThird:
-        p.y[i] = p.x[i] + p.aux[i] + in2 / (p.shift + exit);
-        break;
-    case kApplyQ:
-        p.y[i] = in - exit * p.x[i];
-        break;
-    case kApplyShifted:
-        p.y[i] = (p.shift + exit) * p.x[i] - in;
-        break;
-    case kResidual:
-        p.y[i] = p.b[i] - ((p.shift + exit) * p.x[i] - in);
-        break;
-    case kJacobiZero:
-        p.y[i] = p.omega * p.b[i] / (p.shift + exit);
-        break;
-    case kJacobi: {
-        const T d = p.shift + exit;
-        const T xi = p.x[i];
-        p.y[i] = xi + p.omega * (p.b[i] - (d * xi - in)) / d;
-        break;
-    }
-    case kGaussSeidel:
-        p.y[i] = (p.b[i] + in) / (p.shift + exit);
-        break;
-    case kExitLeak:
-        p.y[i] = exit;
-        p.aux[i] = leak;
-        break;
-    case kResidualRestrict: {
-        const T r = p.b[i] - ((p.shift + exit) * p.x[i] - in);
-        if (sec.coarse >= 0) {
-            atomicAdd(p.coarse + coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, nullptr), r);
-        } else {
-            p.aux[i] = r;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        if (c >= p.nb) {
+            break;
         }
-        break;
-    }
-    case kDiagonal:
-        p.y[i] = p.shift + exit;
-        break;
-    default:
-        break;
+        const std::int64_t k = i + c * p.ldv;
+        switch (p.mode) {
+        case kIluPivot:
+            p.y[k] = d - in[c];
+            break;
+        case kIluFirst:
+            p.aux[k] = (p.b[k] - (d * p.x[k] - in[c])) / d;
+            break;
+        case kIluSecond: {
+            const T xi = p.x[k];
+            const T z = (p.b[k] - (d * xi - in[c]) + in2[c]) / p.piv[i];
+            p.aux[k] = z;
+            p.y[k] = xi + z;
+            break;
+        }
+        case kIluThird:
+            p.y[k] = p.x[k] + p.aux[k] + in2[c] / d;
+            break;
+        case kApplyQ:
+            p.y[k] = in[c] - exit * p.x[k];
+            break;
+        case kApplyShifted:
+            p.y[k] = d * p.x[k] - in[c];
+            break;
+        case kResidual:
+            p.y[k] = p.b[k] - (d * p.x[k] - in[c]);
+            break;
+        case kJacobiZero:
+            p.y[k] = p.omega * p.b[k] / d;
+            break;
+        case kJacobi: {
+            const T xi = p.x[k];
+            p.y[k] = xi + p.omega * (p.b[k] - (d * xi - in[c])) / d;
+            break;
+        }
+        case kGaussSeidel:
+            p.y[k] = (p.b[k] + in[c]) / d;
+            break;
+        case kExitLeak:
+            p.y[k] = exit;
+            p.aux[k] = leak;
+            break;
+        case kResidualRestrict: {
+            const T r = p.b[k] - (d * p.x[k] - in[c]);
+            if (ci >= 0) {
+                atomicAdd(p.coarse + ci + c * p.ldc, r);
+            } else {
+                p.aux[k] = r;
+            }
+            break;
+        }
+        case kDiagonal:
+            p.y[k] = d;
+            break;
+        default:
+            break;
+        }
     }
 }
 
-template <typename T, int NS, int TMAX>
+template <typename T, int NS, int TMAX, int NB>
 __device__ __forceinline__ void transfer_row(const RowParams<T> &p, const SectorDesc &sec,
                                              std::int64_t local, const RowState<NS, TMAX> &st) {
     const std::int64_t i = sec.begin + local;
     if (sec.coarse < 0) {
         if (p.mode == kProlong) {
-            p.y[i] = T(0);
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                if (c < p.nb) {
+                    p.y[i + c * p.ldv] = T(0);
+                }
+            }
         }
         return;
     }
-    if (p.mode == kRestrict) {
-        atomicAdd(p.coarse + coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, nullptr), p.x[i]);
-        return;
-    }
     double w = 0.0;
-    const std::int64_t c = coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, &w);
-    if (p.mode == kProlongAdd) {
-        p.y[i] += static_cast<T>(w) * p.coarse[c];
-    } else {
-        p.y[i] = static_cast<T>(w) * p.coarse[c];
+    const std::int64_t ci =
+        coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, p.mode == kRestrict ? nullptr : &w);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        if (c >= p.nb) {
+            break;
+        }
+        const std::int64_t k = i + c * p.ldv;
+        if (p.mode == kRestrict) {
+            atomicAdd(p.coarse + ci + c * p.ldc, p.x[k]);
+        } else if (p.mode == kProlongAdd) {
+            p.y[k] += static_cast<T>(w) * p.coarse[ci + c * p.ldc];
+        } else {
+            p.y[k] = static_cast<T>(w) * p.coarse[ci + c * p.ldc];
+        }
     }
 }
 
@@ -134,10 +156,11 @@ __device__ __forceinline__ int pass_colour(int mode, int colour) {
 }
 
 // the terms of one row computed by `nlanes` cooperating threads; lane 0 takes the light terms
-template <typename T, int NS, int TMAX>
+template <typename T, int NS, int TMAX, int NB>
 __device__ __forceinline__ void row_terms(const RowParams<T> &p, const SectorDesc &sec,
                                           std::int64_t local, const RowState<NS, TMAX> &st,
-                                          int lane, int nlanes, T &exit, T &leak, T &in, T &in2) {
+                                          int lane, int nlanes, T &exit, T &leak, T (&in)[NB],
+                                          T (&in2)[NB]) {
     if (!needs_in(p.mode)) {
         visit_row<T, NS, TMAX, false>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane,
                                       nlanes, exit, leak, [&](int, T, T) {});
@@ -148,31 +171,39 @@ __device__ __forceinline__ void row_terms(const RowParams<T> &p, const SectorDes
         const T *dg = p.aux;
         visit_row<T, NS, TMAX, true, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane,
                                            nlanes, exit, leak,
-                                           [&](int j, T a, T rev) { in += a * rev / dg[j]; });
+                                           [&](int j, T a, T rev) { in[0] += a * rev / dg[j]; });
         return;
     }
     // Gauss-Seidel and the ILU passes update x (= y) in place: rows of one colour read only
     // the other colour's entries, through plain coherent loads
-    const int mode = p.mode;
+    const int mode = p.mode, nb = p.nb;
+    const std::int64_t ldv = p.ldv;
     const T *xs = mode == kGaussSeidel ? p.y : p.x;
     const T *ax = p.aux;
     visit_row<T, NS, TMAX, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, nlanes,
                                  exit, leak, [&](int j, T a, T) {
-                                     if (mode == kIluThird) {
-                                         in2 += a * ax[j];
-                                         return;
-                                     }
-                                     in += a * xs[j];
-                                     if (mode == kIluSecond) {
-                                         in2 += a * ax[j];
+#pragma unroll
+                                     for (int c = 0; c < NB; ++c) {
+                                         if (c >= nb) {
+                                             break;
+                                         }
+                                         const std::int64_t k = j + c * ldv;
+                                         if (mode == kIluThird) {
+                                             in2[c] += a * ax[k];
+                                             continue;
+                                         }
+                                         in[c] += a * xs[k];
+                                         if (mode == kIluSecond) {
+                                             in2[c] += a * ax[k];
+                                         }
                                      }
                                  });
 }
 
-template <typename T, int NS, int TMAX>
+template <typename T, int NS, int TMAX, int NB>
 __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ RowParams<T> p) {
     __shared__ SectorDesc s_sec;
-    __shared__ T s_red[4][kRowBlock / 32];
+    __shared__ T s_red[2 + 2 * NB][kRowBlock / 32];
     const Tile tile = p.tiles[blockIdx.x];
     if (threadIdx.x == 0) {
         s_sec = p.sectors[tile.sector];
@@ -207,7 +238,7 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
     load_state<NS, TMAX>(p.B, sec, p.md.S, p.md.V, local, st);
     if (is_transfer(p.mode)) {
         if (row_lane == 0) {
-            transfer_row<T, NS, TMAX>(p, sec, local, st);
+            transfer_row<T, NS, TMAX, NB>(p, sec, local, st);
         }
         return;
     }
@@ -215,58 +246,77 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
     if (colour >= 0 && state_colour<T, NS, TMAX>(p.md, sec, st) != colour) {
         return; // uniform across the warp or block of a shared row
     }
-    T exit = T(0), leak = T(0), in = T(0), in2 = T(0);
-    row_terms<T, NS, TMAX>(p, sec, local, st, row_lane, row_lanes, exit, leak, in, in2);
+    T exit = T(0), leak = T(0);
+    T in[NB], in2[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] = T(0);
+        in2[c] = T(0);
+    }
+    row_terms<T, NS, TMAX, NB>(p, sec, local, st, row_lane, row_lanes, exit, leak, in, in2);
     if (tile.kind == 0) {
-        finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in, in2);
+        finish_row<T, NS, TMAX, NB>(p, sec, local, st, exit, leak, in, in2);
         return;
     }
     exit = warp_sum(exit);
     leak = warp_sum(leak);
-    in = warp_sum(in);
-    in2 = warp_sum(in2);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] = warp_sum(in[c]);
+        in2[c] = warp_sum(in2[c]);
+    }
     if (tile.kind == 1) {
         if (lane == 0) {
-            finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in, in2);
+            finish_row<T, NS, TMAX, NB>(p, sec, local, st, exit, leak, in, in2);
         }
         return;
     }
     if (lane == 0) {
         s_red[0][warp] = exit;
         s_red[1][warp] = leak;
-        s_red[2][warp] = in;
-        s_red[3][warp] = in2;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            s_red[2 + c][warp] = in[c];
+            s_red[2 + NB + c][warp] = in2[c];
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        exit = leak = in = in2 = T(0);
+        exit = leak = T(0);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            in[c] = in2[c] = T(0);
+        }
         for (int w = 0; w < kRowBlock / 32; ++w) {
             exit += s_red[0][w];
             leak += s_red[1][w];
-            in += s_red[2][w];
-            in2 += s_red[3][w];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                in[c] += s_red[2 + c][w];
+                in2[c] += s_red[2 + NB + c][w];
+            }
         }
-        finish_row<T, NS, TMAX>(p, sec, local, st, exit, leak, in, in2);
+        finish_row<T, NS, TMAX, NB>(p, sec, local, st, exit, leak, in, in2);
     }
 }
 
-template <typename T, int NS, int TMAX>
+template <typename T, int NS, int TMAX, int NB>
 cudaError_t launch_shape(const RowParams<T> &p, cudaStream_t stream) {
     if (p.n_tiles == 0) {
         return cudaSuccess;
     }
     count_launches(1);
-    row_kernel<T, NS, TMAX><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+    row_kernel<T, NS, TMAX, NB><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
     return cudaGetLastError();
 }
 
 } // namespace detail
 
 // (species, largest species total) -> the instantiated state shape
-template <typename T>
+template <typename T, int NB>
 cudaError_t launch_rows_impl(const RowParams<T> &p, int S, int cap, cudaStream_t stream) {
     return with_shape(S, cap, [&]<int NS, int TMAX>() {
-        return detail::launch_shape<T, NS, TMAX>(p, stream);
+        return detail::launch_shape<T, NS, TMAX, NB>(p, stream);
     });
 }
 
