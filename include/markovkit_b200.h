@@ -302,6 +302,9 @@ typedef struct {
     int restart;             /* GMRES restart, 1..64 */
     int64_t max_iterations;
     double rel_tolerance;    /* stop at ||b - A x|| <= rel_tolerance * ||b|| */
+    int batch;               /* queued requests with the same problem and shift solved together
+                              * by one batched FGMRES, 1..4 (the resident solver is that wide) */
+    int64_t coarsest_size;   /* multigrid sectors of at most this many states get a dense solve */
 } mk_server_options;
 typedef struct {
     int64_t ticket;
@@ -311,6 +314,7 @@ typedef struct {
     double latency_ms;       /* submit to x on the host */
     double queue_ms;         /* submit to having a slot and the memory */
     double solve_ms;         /* the rest: set-up of a new resident solver, copies, solve */
+    int batched;             /* requests solved together with this one (itself included) */
 } mk_server_result;
 typedef struct {
     int64_t completed;

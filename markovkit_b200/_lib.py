@@ -112,6 +112,8 @@ class ServerOptions(C.Structure):
         ("restart", C.c_int),
         ("max_iterations", C.c_int64),
         ("rel_tolerance", C.c_double),
+        ("batch", C.c_int),
+        ("coarsest_size", C.c_int64),
     ]
 
 
@@ -124,6 +126,7 @@ class ServerResult(C.Structure):
         ("latency_ms", C.c_double),
         ("queue_ms", C.c_double),
         ("solve_ms", C.c_double),
+        ("batched", C.c_int),
     ]
 
 

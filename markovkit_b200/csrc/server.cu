@@ -41,7 +41,9 @@ struct Resident {
     double shift = 0.0;
     std::unique_ptr<mkb::Generator> gen;
     std::unique_ptr<mkb::Multigrid> mg;
-    std::unique_ptr<mkb::Krylov> ws;
+    std::unique_ptr<mkb::Krylov> ws;        // batch width 1
+    std::unique_ptr<mkb::KrylovBatch> wsb;  // batch width > 1
+    std::int64_t ld = 0;                    // stride of the columns of b and x
     mkb::DeviceArray<double> b, x;
     std::size_t bytes = 0;   // admitted footprint
     bool busy = false;
@@ -84,10 +86,12 @@ struct mk_server_s {
 
     [[nodiscard]] std::size_t footprint(std::int64_t n) const {
         const std::int64_t m = opt.restart;
-        const std::int64_t krylov = (m + 1) + (opt.precision == 1 ? m : 0) + 7; // + w, r, t, b, x
-        const std::int64_t mg = opt.precision == 1 ? 48 : 96;                // level vectors
-        return static_cast<std::size_t>(n) * static_cast<std::size_t>(8 * krylov + mg) +
-               (std::size_t(16) << 20);
+        const bool flexible = opt.precision == 1 || opt.batch > 1;
+        const std::int64_t krylov = (m + 1) + (flexible ? m : 0) + 7; // + w, r, t, b, x
+        const std::int64_t mg = opt.precision == 1 ? 48 : 96;        // level vectors
+        const std::int64_t terminal = std::min<std::int64_t>(opt.coarsest_size, 8192);
+        return static_cast<std::size_t>(n) * static_cast<std::size_t>((8 * krylov + mg) * opt.batch) +
+               static_cast<std::size_t>(terminal * terminal * 12) + (std::size_t(16) << 20);
     }
 
     void finish(const Request &rq, mk_server_result r, Clock::time_point started) {
@@ -179,17 +183,30 @@ struct mk_server_s {
         cudaStream_t stream = nullptr;
         cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
         while (true) {
-            Request rq;
+            // the oldest request, and queued requests for the same (problem, shift) up to the
+            // batch width: they share one resident solver and one batched solve
+            std::vector<Request> batch;
             {
                 std::unique_lock<std::mutex> lock(mu);
                 cv_work.wait(lock, [&] { return stopping || !queue.empty(); });
                 if (stopping && queue.empty()) {
                     break;
                 }
-                rq = queue.front();
+                batch.push_back(queue.front());
                 queue.pop_front();
+                for (auto it = queue.begin(); it != queue.end() &&
+                                              static_cast<int>(batch.size()) < opt.batch;) {
+                    if (it->problem == batch[0].problem && it->shift == batch[0].shift) {
+                        batch.push_back(*it);
+                        it = queue.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
             }
-            mk_server_result res{};
+            const Request &rq = batch[0];
+            const int nb = static_cast<int>(batch.size());
+            std::vector<mk_server_result> res(nb);
             Resident *r = nullptr;
             {
                 std::unique_lock<std::mutex> lock(mu);
@@ -197,8 +214,10 @@ struct mk_server_s {
             }
             const auto started = Clock::now(); // a slot and the memory are ours from here
             if (!r) {
-                res.status = MK_ENOMEM;
-                finish(rq, res, started);
+                for (int c = 0; c < nb; ++c) {
+                    res[c].status = MK_ENOMEM;
+                    finish(batch[c], res[c], started);
+                }
                 continue;
             }
             bool keep = true;
@@ -209,49 +228,82 @@ struct mk_server_s {
                     mkb::MultigridOptions mo;
                     mo.precision = opt.precision == 1 ? 1 : 0;
                     mo.smoother = opt.smoother;
+                    mo.coarsest_size = opt.coarsest_size;
+                    mo.batch = opt.batch;
                     r->mg = std::make_unique<mkb::Multigrid>(*p.space, *p.model, rq.shift, mo);
-                    r->ws = std::make_unique<mkb::Krylov>(p.n, opt.restart, opt.precision == 1);
-                    r->b.resize(static_cast<std::size_t>(p.n));
-                    r->x.resize(static_cast<std::size_t>(p.n));
+                    if (opt.batch == 1) {
+                        r->ws = std::make_unique<mkb::Krylov>(p.n, opt.restart, opt.precision == 1);
+                        r->ld = p.n;
+                    } else {
+                        r->wsb = std::make_unique<mkb::KrylovBatch>(p.n, opt.restart, opt.batch);
+                        r->ld = r->wsb->ld;
+                    }
+                    r->b.resize(static_cast<std::size_t>(r->ld) * opt.batch);
+                    r->x.resize(static_cast<std::size_t>(r->ld) * opt.batch);
                     r->built = true;
                 }
-                double bnorm = 0.0;
-                for (std::int64_t i = 0; i < p.n; ++i) {
-                    bnorm += rq.h_b[i] * rq.h_b[i];
+                std::vector<double> tol(nb), bnorm(nb);
+                for (int c = 0; c < nb; ++c) {
+                    double s = 0.0;
+                    for (std::int64_t i = 0; i < p.n; ++i) {
+                        s += batch[c].h_b[i] * batch[c].h_b[i];
+                    }
+                    bnorm[c] = std::sqrt(s);
+                    tol[c] = opt.rel_tolerance * bnorm[c];
+                    mkb::check_cuda(cudaMemcpyAsync(r->b.get() + c * r->ld, batch[c].h_b,
+                                                    sizeof(double) * p.n, cudaMemcpyHostToDevice,
+                                                    stream),
+                                    "request b copy");
                 }
-                bnorm = std::sqrt(bnorm);
-                mkb::check_cuda(cudaMemcpyAsync(r->b.get(), rq.h_b, sizeof(double) * p.n,
-                                                cudaMemcpyHostToDevice, stream),
-                                "request b copy");
-                mkb::check_cuda(cudaMemsetAsync(r->x.get(), 0, sizeof(double) * p.n, stream),
+                mkb::check_cuda(cudaMemsetAsync(r->x.get(), 0, sizeof(double) * r->ld * nb, stream),
                                 "request x reset");
                 mkb::GmresOptions go;
-                go.tolerance = opt.rel_tolerance * bnorm;
                 go.max_iterations = opt.max_iterations;
                 go.restart = opt.restart;
                 go.flexible = opt.precision == 1 ? 1 : 0;
-                const mkb::SolverResult sr =
-                    mkb::gmres(*r->gen, rq.shift, r->mg.get(), r->b.get(), r->x.get(), go, *r->ws,
-                               stream);
-                mkb::check_cuda(cudaMemcpyAsync(rq.h_x, r->x.get(), sizeof(double) * p.n,
-                                                cudaMemcpyDeviceToHost, stream),
-                                "request x copy");
+                std::vector<mkb::SolverResult> sr;
+                if (r->ws) {
+                    go.tolerance = tol[0];
+                    sr.push_back(mkb::gmres(*r->gen, rq.shift, r->mg.get(), r->b.get(), r->x.get(),
+                                            go, *r->ws, stream));
+                } else {
+                    sr = mkb::gmres_batch(*r->gen, rq.shift, *r->mg, r->b.get(), r->x.get(), nb,
+                                          tol.data(), go, *r->wsb, stream);
+                }
+                for (int c = 0; c < nb; ++c) {
+                    mkb::check_cuda(cudaMemcpyAsync(batch[c].h_x, r->x.get() + c * r->ld,
+                                                    sizeof(double) * p.n, cudaMemcpyDeviceToHost,
+                                                    stream),
+                                    "request x copy");
+                }
                 mkb::check_cuda(cudaStreamSynchronize(stream), "request sync");
-                res.iterations = sr.iterations;
-                res.residual = sr.residual / (bnorm > 0.0 ? bnorm : 1.0);
-                res.status = sr.converged ? MK_OK : (sr.status != 0 ? sr.status : MK_ENOTCONV);
+                for (int c = 0; c < nb; ++c) {
+                    res[c].iterations = sr[c].iterations;
+                    res[c].residual = sr[c].residual / (bnorm[c] > 0.0 ? bnorm[c] : 1.0);
+                    res[c].status = sr[c].converged ? MK_OK
+                                                    : (sr[c].status != 0 ? sr[c].status : MK_ENOTCONV);
+                    res[c].batched = nb;
+                }
             } catch (const mkb::Error &e) {
-                res.status = e.code;
+                for (auto &x : res) {
+                    x.status = e.code;
+                }
                 keep = false;
             } catch (const std::bad_alloc &) {
-                res.status = MK_ENOMEM;
+                for (auto &x : res) {
+                    x.status = MK_ENOMEM;
+                }
                 keep = false;
             } catch (const std::exception &) {
-                res.status = MK_ECUDA;
+                for (auto &x : res) {
+                    x.status = MK_ECUDA;
+                }
                 keep = false;
             }
             release(r, keep && r->built);
-            finish(rq, res, started);
+            for (int c = 0; c < nb; ++c) {
+                finish(batch[c], res[c], started);
+            }
         }
         cudaStreamDestroy(stream);
     }
@@ -270,6 +322,8 @@ void mk_server_options_default(mk_server_options *opt) {
     opt->restart = 30;
     opt->max_iterations = 5000;
     opt->rel_tolerance = 1e-10;
+    opt->batch = 4;
+    opt->coarsest_size = 256;
 }
 
 int mk_server_create(const mk_server_options *opt, mk_server *out) {
@@ -281,6 +335,9 @@ int mk_server_create(const mk_server_options *opt, mk_server *out) {
         MK_REQUIRE(opt->smoother >= 0 && opt->smoother <= 2, "server: smoother is 0, 1 or 2");
         MK_REQUIRE(opt->max_iterations >= 1 && opt->rel_tolerance > 0.0,
                    "server: max_iterations >= 1 and rel_tolerance > 0");
+        MK_REQUIRE(opt->batch >= 1 && opt->batch <= mkb::kRowBatch, "server: batch must be in 1..4");
+        MK_REQUIRE(opt->coarsest_size >= 1 && opt->coarsest_size <= 8192,
+                   "server: coarsest_size must be in 1..8192");
         auto s = std::make_unique<mk_server_s>();
         s->opt = *opt;
         mkb::check_cuda(cudaGetDevice(&s->device), "cudaGetDevice");

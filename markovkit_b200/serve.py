@@ -31,11 +31,13 @@ class request_result:
     latency_ms: float
     queue_ms: float
     solve_ms: float
+    batched: int = 1
 
 
 class server:
     def __init__(self, slots: int = 4, precision: str = "fp32", hbm_budget: int = 0, smoother: str = "jacobi",
-                 restart: int = 30, max_iterations: int = 5000, rel_tolerance: float = 1e-10):
+                 restart: int = 30, max_iterations: int = 5000, rel_tolerance: float = 1e-10,
+                 batch: int = 4, coarsest_size: int = 256):
         lib = load()
         o = ServerOptions()
         lib.mk_server_options_default(C.byref(o))
@@ -46,6 +48,8 @@ class server:
         o.restart = int(restart)
         o.max_iterations = int(max_iterations)
         o.rel_tolerance = float(rel_tolerance)
+        o.batch = int(batch)
+        o.coarsest_size = int(coarsest_size)
         self._h = C.c_void_p()
         check(lib.mk_server_create(C.byref(o), C.byref(self._h)))
         self._sizes = {}
@@ -99,7 +103,8 @@ class server:
         rc = load().mk_server_wait(self._h, int(ticket), C.byref(r))
         check(rc, allow=(MK_ENOTCONV,))
         b, x = self._pending.pop(ticket, (None, None))
-        return x, request_result(r.ticket, r.status, r.iterations, r.residual, r.latency_ms, r.queue_ms, r.solve_ms)
+        return x, request_result(r.ticket, r.status, r.iterations, r.residual, r.latency_ms, r.queue_ms, r.solve_ms,
+                                 r.batched)
 
     def drain(self) -> None:
         check(load().mk_server_drain(self._h))

@@ -97,6 +97,8 @@ def test_same_alone_and_in_the_mix(spaces, alone):
         st = srv.stats()
     assert st["completed"] == len(mixed)
     assert st["p99_ms"] >= st["p50_ms"] > 0
+    # queued requests with one key were solved together
+    assert max(r.batched for _, r in mixed) >= 2
     for (xa, ra), (xm, rm) in zip(alone, mixed):
         assert rm.status == _lib.MK_OK and rm.residual <= 1e-10
         assert _rel(xm, xa) <= 1e-8
@@ -109,7 +111,8 @@ def test_configuration_0_matches_the_reference(alone):
 
 
 def test_fp64_path_agrees(spaces, alone):
-    with server(slots=2, precision="fp64") as srv:
+    # the all-FP64 path, one request per solve (no batching), reference multigrid defaults
+    with server(slots=2, precision="fp64", batch=1, coarsest_size=4) as srv:
         res = _serve(srv, _requests()[:5], spaces, at_once=True)
     for (x64, r64), (x32, r32) in zip(res, alone[:5]):
         assert r64.status == _lib.MK_OK and r64.residual <= 1e-10
