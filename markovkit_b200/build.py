@@ -19,7 +19,7 @@ CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libmarkovkit_b200.so"
 
-SOURCES = ["row_kernels_f64.cu", "row_kernels_f32.cu", "row_kernels_f64_batch.cu", "row_kernels_f32_batch.cu", "row_kernels.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu", "capi_fsp.cu", "server.cu"]
+SOURCES = ["row_kernels_f64.cu", "row_kernels_f32.cu", "row_kernels_f64_batch.cu", "row_kernels_f32_batch.cu", "row_kernels.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu", "capi_fsp.cu", "server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [
     "-std=c++20",
