@@ -1239,11 +1239,19 @@ KrylovBatch::KrylovBatch(std::int64_t n_, int m_, int nb_) : n(n_), m(m_), nb(nb
     for (int c = 0; c < nb; ++c) {
         st.push_back(carve_arnoldi(small.get() + per * c, m));
     }
-    check_cuda(cudaMallocHost(reinterpret_cast<void **>(&report_host), 4 * sizeof(double) * nb),
+    check_cuda(cudaMallocHost(reinterpret_cast<void **>(&report_host), 8 * sizeof(double) * nb),
                "cudaMallocHost");
+    for (auto &e : step_done) {
+        check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    }
 }
 
 KrylovBatch::~KrylovBatch() {
+    for (auto &e : step_done) {
+        if (e) {
+            cudaEventDestroy(e);
+        }
+    }
     if (report_host) {
         cudaFreeHost(report_host);
     }
@@ -1313,13 +1321,17 @@ std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigri
                 check_cuda(scale_copy(col(ws.r.get(), c), ws.st[c].beta, Vj(0, c), n, stream), "scale");
             }
         }
-        for (int j = 0; j < m; ++j) {
+        // Step j of every column still running when it is enqueued; its estimates land in
+        // pinned slot j % 2. Step j + 1 is enqueued before the host waits for step j, as in
+        // the single-column solver: a column that converges at step j ignores step j + 1,
+        // which touched only its H column j + 1, g[j + 1..] and basis vector j + 2.
+        auto enqueue = [&](int j, const std::vector<char> &cols) {
             // one multigrid cycle and one operator apply serve every column of step j
             M.apply_batch(Vj(j, 0), ld, Zj(j, 0), ld, nb, stream);
             A.apply<double>(kApplyShifted, shift, Zj(j, 0), nullptr, ws.w.get(), nullptr, stream,
                             nb, ld);
             for (int c = 0; c < nb; ++c) {
-                if (!running[c]) {
+                if (!cols[c]) {
                     continue;
                 }
                 double *w = ws.w.get() + c * ld;
@@ -1358,17 +1370,37 @@ std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigri
                     }
                 }
                 check_cuda(arnoldi_column(ws.st[c], j, stream), "arnoldi");
-                check_cuda(cudaMemcpyAsync(ws.report_host + 4 * c, ws.st[c].report,
-                                           4 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                double *slot = ws.report_host + 4 * (nb * (j & 1) + c);
+                check_cuda(cudaMemcpyAsync(slot, ws.st[c].report, 4 * sizeof(double),
+                                           cudaMemcpyDeviceToHost, stream),
                            "report");
+                if (j + 1 < m) {
+                    check_cuda(scale_copy(w, ws.st[c].inv_hn, Vj(j + 1, c), n, stream), "scale");
+                }
             }
-            read_reports();
+            check_cuda(cudaEventRecord(ws.step_done[j & 1], stream), "event");
+        };
+        std::vector<int> steps_left(nb);
+        for (int c = 0; c < nb; ++c) {
+            steps_left[c] = static_cast<int>(
+                std::min<std::int64_t>(m, std::max<std::int64_t>(0, opt.max_iterations - res[c].iterations)));
+        }
+        enqueue(0, running);
+        for (int j = 0; j < m; ++j) {
+            bool next = false;
+            for (int c = 0; c < nb; ++c) {
+                next = next || (running[c] && j + 1 < steps_left[c]);
+            }
+            if (next && j + 1 < m) {
+                enqueue(j + 1, running);
+            }
+            check_cuda(cudaEventSynchronize(ws.step_done[j & 1]), "sync");
             bool any = false;
             for (int c = 0; c < nb; ++c) {
                 if (!running[c]) {
                     continue;
                 }
-                const double *rep = ws.report_host + 4 * c;
+                const double *rep = ws.report_host + 4 * (nb * (j & 1) + c);
                 ++res[c].iterations;
                 k[c] = j + 1;
                 if (!std::isfinite(rep[0]) || !std::isfinite(rep[1])) {
@@ -1377,21 +1409,17 @@ std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigri
                     running[c] = 0;
                     continue;
                 }
-                if (rep[0] <= tol[c] || rep[2] != 0.0 || res[c].iterations >= opt.max_iterations) {
+                if (rep[0] <= tol[c] || rep[2] != 0.0 || j + 1 >= steps_left[c]) {
                     running[c] = 0; // this cycle ends here for column c
                     continue;
                 }
                 any = true;
-                if (j + 1 < m) {
-                    check_cuda(scale_copy(col(ws.w.get(), c), ws.st[c].inv_hn, Vj(j + 1, c), n,
-                                          stream),
-                               "scale");
-                }
             }
-            if (!any) {
+            if (!any || !next) {
                 break;
             }
         }
+        check_cuda(cudaStreamSynchronize(stream), "sync");
         for (int c = 0; c < nb; ++c) {
             if (!active[c] || k[c] == 0) {
                 continue;

@@ -279,7 +279,8 @@ struct KrylovBatch {
     int m = 0, nb = 0;
     DeviceArray<double> V, Z, w, r, partials, small;
     std::vector<ArnoldiState> st;
-    double *report_host = nullptr; // pinned, 4 per column
+    double *report_host = nullptr; // pinned: two slots (steps j and j + 1) of 4 per column
+    cudaEvent_t step_done[2] = {nullptr, nullptr};
     KrylovBatch(std::int64_t n, int m, int nb);
     ~KrylovBatch();
     KrylovBatch(const KrylovBatch &) = delete;

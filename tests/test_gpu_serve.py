@@ -97,11 +97,32 @@ def test_same_alone_and_in_the_mix(spaces, alone):
         st = srv.stats()
     assert st["completed"] == len(mixed)
     assert st["p99_ms"] >= st["p50_ms"] > 0
-    # queued requests with one key were solved together
-    assert max(r.batched for _, r in mixed) >= 2
     for (xa, ra), (xm, rm) in zip(alone, mixed):
         assert rm.status == _lib.MK_OK and rm.residual <= 1e-10
         assert _rel(xm, xa) <= 1e-8
+
+
+def test_queued_requests_with_one_key_are_solved_together(spaces, alone):
+    """One worker: while it solves a first request, four requests for one (problem, shift)
+    queue up behind it and are then solved by one batched FGMRES; each matches its solve alone."""
+    reqs = _requests()
+    same = [r for r in reqs if r[0] == "cfg0"]  # cfg0 requests: (name, shift, seed, kind)
+    key_shift = same[0][1]
+    with server(slots=1, precision="fp32", batch=4) as srv:
+        pids = {name: srv.register(*spaces[name]) for name in PROBLEMS}
+        n = spaces["cfg0"][0].size()
+        blocker = srv.submit(pids["bd1d64"], 1.0, dirichlet_rhs(77, spaces["bd1d64"][0].size()))
+        tickets = [srv.submit(pids["cfg0"], key_shift, _rhs("dirichlet" if k else "uniform", 0 if k == 0 else 900 + k, n))
+                   for k in range(4)]
+        srv.wait(blocker)
+        out = [srv.wait(t) for t in tickets]
+    assert max(r.batched for _, r in out) >= 2
+    # the first of them is the configuration-0 golden request: same solution as alone
+    x0, r0 = out[0]
+    assert r0.status == _lib.MK_OK and r0.residual <= 1e-10
+    assert _rel(x0, alone[0][0]) <= 1e-8
+    for x, r in out[1:]:
+        assert r.status == _lib.MK_OK and r.residual <= 1e-10
 
 
 def test_configuration_0_matches_the_reference(alone):
