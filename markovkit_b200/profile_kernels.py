@@ -9,6 +9,8 @@ Cases:
                              annihilation box {1, 1} (1,050,625 states) after one warm-up solve
   solve_birth_death_3d16     the same on the 3-D box above
   mg_birth_death_3d16        one FP32 sector-multigrid V-cycle on the 3-D box (after one warm-up)
+  mg_annihilation_2d32       the same on the 2-D annihilation box (sectors of <= 256 states
+                             solved densely)
   fsp_toggle                 one batched Krylov-FSP launch of 8 toggle-switch instances of the
                              batching workload (after one warm-up launch)
 
@@ -53,16 +55,17 @@ def main(case: str) -> None:
             Q.apply_shifted(1.0, x, y)
         torch.cuda.synchronize()
         print(json.dumps({"case": case, "states": box.size(), "launches": 5}))
-    elif case in ("solve_annihilation_2d32", "solve_birth_death_3d16", "mg_birth_death_3d16"):
-        if case == "solve_annihilation_2d32":
+    elif case in ("solve_annihilation_2d32", "solve_birth_death_3d16", "mg_birth_death_3d16",
+                  "mg_annihilation_2d32"):
+        if case in ("solve_annihilation_2d32", "mg_annihilation_2d32"):
             dom, box, Q, A = _rdme(mk, 2, 32, [1, 1], "annihilation", 1.0)
             rhs = dirichlet_rhs
         else:
             dom, box, Q, A = _rdme(mk, 3, 16, [2], "birth_death", 0.5)
             rhs = uniform_rhs
         N = box.size()
-        M = mk.sector_multigrid(dom, box, A.shift(), mk.multigrid_options(precision="fp32"))
-        if case == "mg_birth_death_3d16":
+        M = mk.sector_multigrid(dom, box, A.shift(), mk.multigrid_options(precision="fp32", coarsest_size=256))
+        if case.startswith("mg_"):
             b = torch.from_numpy(rhs(2, N)).to(dev)
             x = torch.zeros_like(b)
             M.apply(b, x)
