@@ -180,6 +180,15 @@ __device__ __forceinline__ void row_terms(const RowParams<T> &p, const SectorDes
     const std::int64_t ldv = p.ldv;
     const T *xs = mode == kGaussSeidel ? p.y : p.x;
     const T *ax = p.aux;
+    if constexpr (NB == 1) {
+        // one column: the common passes gather x alone, with 32-bit indices
+        if (mode != kIluSecond && mode != kIluThird) {
+            visit_row<T, NS, TMAX, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane,
+                                         nlanes, exit, leak,
+                                         [&](int j, T a, T) { in[0] += a * xs[j]; });
+            return;
+        }
+    }
     visit_row<T, NS, TMAX, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, nlanes,
                                  exit, leak, [&](int j, T a, T) {
 #pragma unroll
