@@ -303,7 +303,9 @@ typedef struct {
     int64_t max_iterations;
     double rel_tolerance;    /* stop at ||b - A x|| <= rel_tolerance * ||b|| */
     int batch;               /* queued requests with the same problem and shift solved together
-                              * by one batched FGMRES, 1..4 (the resident solver is that wide) */
+                              * by one batched FGMRES, 1..4: a problem's resident solvers are the
+                              * widest up to this whose footprint is at most hbm_budget / slots,
+                              * else one request wide */
     int64_t coarsest_size;   /* multigrid sectors of at most this many states get a dense solve */
 } mk_server_options;
 typedef struct {

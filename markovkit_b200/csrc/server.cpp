@@ -39,6 +39,7 @@ struct Problem {
 struct Resident {
     int problem = -1;
     double shift = 0.0;
+    int width = 1;                          // requests one solve serves
     std::unique_ptr<mkb::Generator> gen;
     std::unique_ptr<mkb::Multigrid> mg;
     std::unique_ptr<mkb::Krylov> ws;        // batch width 1
@@ -84,14 +85,31 @@ struct mk_server_s {
     std::condition_variable cv_work, cv_mem, cv_done;
     std::vector<std::thread> workers;
 
-    [[nodiscard]] std::size_t footprint(std::int64_t n) const {
+    // bytes charged for a resident solver of n states that solves `width` requests together
+    [[nodiscard]] std::size_t footprint(std::int64_t n, int width) const {
         const std::int64_t m = opt.restart;
-        const bool flexible = opt.precision == 1 || opt.batch > 1;
+        const bool flexible = opt.precision == 1 || width > 1;
         const std::int64_t krylov = (m + 1) + (flexible ? m : 0) + 7; // + w, r, t, b, x
         const std::int64_t mg = opt.precision == 1 ? 48 : 96;        // level vectors
         const std::int64_t terminal = std::min<std::int64_t>(opt.coarsest_size, 8192);
-        return static_cast<std::size_t>(n) * static_cast<std::size_t>((8 * krylov + mg) * opt.batch) +
+        return static_cast<std::size_t>(n) * static_cast<std::size_t>((8 * krylov + mg) * width) +
                static_cast<std::size_t>(terminal * terminal * 12) + (std::size_t(16) << 20);
+    }
+
+    // the batch width of a problem's resident solvers: the widest up to opt.batch whose
+    // footprint leaves every slot an equal share of the budget, else 1 (large spaces, such as a
+    // 186M-state box, are served one request at a time instead of being refused)
+    [[nodiscard]] int width_for(std::int64_t n) const {
+        for (int w = opt.batch; w > 1; --w) {
+            if (footprint(n, w) <= budget / static_cast<std::size_t>(opt.slots)) {
+                return w;
+            }
+        }
+        return 1;
+    }
+
+    [[nodiscard]] std::size_t footprint(std::int64_t n) const {
+        return footprint(n, width_for(n));
     }
 
     void finish(const Request &rq, mk_server_result r, Clock::time_point started) {
@@ -155,6 +173,7 @@ struct mk_server_s {
         auto r = std::make_unique<Resident>();
         r->problem = rq.problem;
         r->shift = rq.shift;
+        r->width = width_for(problems[rq.problem]->n);
         r->bytes = need;
         r->busy = true;
         resident_bytes += need;
@@ -194,8 +213,9 @@ struct mk_server_s {
                 }
                 batch.push_back(queue.front());
                 queue.pop_front();
+                const int width = width_for(problems[batch[0].problem]->n);
                 for (auto it = queue.begin(); it != queue.end() &&
-                                              static_cast<int>(batch.size()) < opt.batch;) {
+                                              static_cast<int>(batch.size()) < width;) {
                     if (it->problem == batch[0].problem && it->shift == batch[0].shift) {
                         batch.push_back(*it);
                         it = queue.erase(it);
@@ -229,17 +249,17 @@ struct mk_server_s {
                     mo.precision = opt.precision == 1 ? 1 : 0;
                     mo.smoother = opt.smoother;
                     mo.coarsest_size = opt.coarsest_size;
-                    mo.batch = opt.batch;
+                    mo.batch = r->width;
                     r->mg = std::make_unique<mkb::Multigrid>(*p.space, *p.model, rq.shift, mo);
-                    if (opt.batch == 1) {
+                    if (r->width == 1) {
                         r->ws = std::make_unique<mkb::Krylov>(p.n, opt.restart, opt.precision == 1);
                         r->ld = p.n;
                     } else {
-                        r->wsb = std::make_unique<mkb::KrylovBatch>(p.n, opt.restart, opt.batch);
+                        r->wsb = std::make_unique<mkb::KrylovBatch>(p.n, opt.restart, r->width);
                         r->ld = r->wsb->ld;
                     }
-                    r->b.resize(static_cast<std::size_t>(r->ld) * opt.batch);
-                    r->x.resize(static_cast<std::size_t>(r->ld) * opt.batch);
+                    r->b.resize(static_cast<std::size_t>(r->ld) * r->width);
+                    r->x.resize(static_cast<std::size_t>(r->ld) * r->width);
                     r->built = true;
                 }
                 std::vector<double> tol(nb), bnorm(nb);

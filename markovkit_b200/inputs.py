@@ -86,3 +86,35 @@ def fsp_instance_line(inst: dict, krylov_tol: float = 1e-8, krylov_dim: int = 30
                      str(inst["bounds"][0]), str(inst["bounds"][1]), g(inst["final_time"]),
                      g(inst["tolerance"]), g(krylov_tol), str(krylov_dim), str(inst["initial"][0]),
                      str(inst["initial"][1])])
+
+
+SERVING_MODELS = ("cfg0", "cfg1", "cfg2", "bd1d")
+
+
+def serving_requests(seed: int = 4, count: int = 24, rate: float = 20.0) -> list:
+    """Seeded resolvent requests of the serving workload, in arrival order: Poisson arrivals at
+    `rate` per second; the model uniform over the 1-D 16-voxel birth-death box of cap 3 (cfg0),
+    the 2-D 32 x 32 annihilation box {1, 1} (cfg1), the 3-D 16^3 birth-death box of cap 2 (cfg2)
+    and a 1-D birth-death box of V voxels, V uniform over the multiples of 16 in [64, 256], and
+    cap ~ U{2..4} (bd1d, 2,145 to 186,043,585 states); shift log-uniform in [0.1, 10];
+    right-hand side Dirichlet(1) of seed rhs_seed. Request k draws u(seed, 8k + j), j < 5.
+    V is a multiple of 16 because sector_multigrid halves the grid only while its length is
+    even (markovkit/rdme/multigrid.hpp:24-42) and factors what is left densely: a 1-D grid that
+    stops above 16 voxels leaves sectors of hundreds of thousands of states at cap 4."""
+    u = uniform01(seed, 8 * count)
+    fixed = {"cfg0": (16, 3), "cfg1": (1024, 1), "cfg2": (4096, 2)}
+    out, t = [], 0.0
+    for k in range(count):
+        v = u[8 * k : 8 * k + 8]
+        t += -float(np.log1p(-v[0])) / rate
+        model = SERVING_MODELS[min(3, int(4 * v[1]))]
+        voxels, cap = fixed.get(model, (64 + 16 * int(13 * v[2]), 2 + int(3 * v[3])))
+        out.append({
+            "arrival_s": t,
+            "model": model,
+            "voxels": voxels,
+            "cap": cap,
+            "shift": float(10.0 ** (-1.0 + 2.0 * v[4])),
+            "rhs_seed": 1000 * seed + k,
+        })
+    return out

@@ -113,3 +113,27 @@ class server:
         s = ServerStats()
         check(load().mk_server_stats_get(self._h, C.byref(s)))
         return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+
+def serving_problem(model: str, voxels: int, cap: int):
+    """The population box and RDME model of a serving-workload request
+    (markovkit_b200.inputs.serving_requests): unit diffusion; birth 0.05 vol and death 0.02 n
+    for the birth-death boxes, annihilation A + B -> 0 at 10 nA nB / vol on the 2-D box {1, 1}.
+    cfg0-2 use the unit domain (spacing 1 / cells). The 1-D boxes of 64-256 voxels keep
+    configuration 0's voxel size 1/16 (a longer line): on the unit domain their jump rates reach
+    8 D V^2 per state, and at small shifts the FP64 residual floor eps ||A|| / s lies above the
+    1e-10 target (V = 208, cap 3, s = 0.113 stalls at 2.6e-10 relative in FP64 GMRES)."""
+    from . import api as mk
+
+    dim = {"cfg0": 1, "cfg1": 2, "cfg2": 3, "bd1d": 1}[model]
+    cells = round(voxels ** (1.0 / dim))
+    h = 1.0 / 16 if model == "bd1d" else 1.0 / cells
+    if model == "cfg1":
+        D, caps = [1.0, 1.0], [cap, cap]
+        rx = [mk.local_reaction([-1, -1], lambda n, vol: 10.0 * n[0] * n[1] / vol)]
+    else:
+        D, caps = [1.0], [cap]
+        rx = [mk.local_reaction([1], lambda n, vol: 0.05 * vol), mk.local_reaction([-1], lambda n, vol: 0.02 * n[0])]
+    dom = mk.voxel_domain(mk.grid([cells] * dim, [h] * dim), D)
+    assert cells ** dim == voxels
+    return mk.population_box(voxels, caps), mk.reaction_diffusion(dom, rx)

@@ -155,9 +155,11 @@ def test_admission_by_footprint(spaces, alone):
     for (xa, ra), (xm, rm) in zip(alone, res):
         assert rm.status == _lib.MK_OK
         assert _rel(xm, xa) <= 1e-8
-    # a request larger than the whole budget is refused, not run
-    with server(slots=1, precision="fp32", hbm_budget=min(foot.values()) - 1) as small:
+    # a request larger than the whole budget is refused, not run (every footprint holds a fixed
+    # 16 MiB besides the vectors, so 1 MiB is too small for any problem at any batch width)
+    with server(slots=1, precision="fp32", hbm_budget=1 << 20) as small:
         pid = small.register(*spaces["bd1d64"])
+        assert small.footprint(pid) > 1 << 20
         n = spaces["bd1d64"][0].size()
         t = small.submit(pid, 1.0, dirichlet_rhs(9, n))
         with pytest.raises(_lib.MkError):
