@@ -279,6 +279,8 @@ def run_ours(args) -> dict | None:
     roof = roofline(mk, Q, M=results["fp32"]["M"], dev=dev, N=N)
     launches = r32["launches"]
     served = serve_measure(mk, box, model, w, host_b, W, K)
+    # the mixed serving workload runs on one GPU only (it is a per-device measurement)
+    served_mix = serve_mix_measure() if world == 1 and not args.no_serve_mix else None
 
     if rank != 0:
         return None
@@ -326,6 +328,7 @@ def run_ours(args) -> dict | None:
             "d2h_bytes_per_step": N * 8,
         },
         "served": served,
+        "served_mix": served_mix,
         "roofline": roof,
         "gpu_launches": launches,
         "clocks": r32["clocks"],
@@ -376,6 +379,65 @@ def serve_measure(mk, box, model, w, host_b, W, K) -> dict:
     out["note"] = ("K requests submitted at once; host b and x; resident solver per slot; fp32: "
                    "batch 4, FGMRES(15), dense solve of sectors <= 256 states; fp64: batch 1, "
                    "GMRES(30), the reference's multigrid options")
+    return out
+
+
+MIX_COUNT = 24
+MIX_RATE = 20.0    # requests per second
+MIX_RESTART = 30   # the 1-D boxes of 10^7-10^8 states need ~75 FGMRES(15) steps, ~45 at 30
+
+
+def serve_mix_measure() -> dict:
+    """The serving workload: MIX_COUNT seeded requests (markovkit_b200.inputs.serving_requests)
+    with Poisson arrivals at MIX_RATE per second, models uniform over configurations 0-2 and 1-D
+    birth-death boxes of 64-256 voxels and cap 2-4 (969 to 186,043,585 states), shifts
+    log-uniform in [0.1, 10], Dirichlet(1) right-hand sides. Each request is submitted at its
+    arrival time (host b and x); latency runs from submit to x on the host; solves/s is the count
+    over the wall time from the first arrival to the last completion. Shifts differ, so requests
+    never share a resident solver and no batching happens; the served FP32 path gains only by
+    overlapping SERVE_SLOTS solves and by its cheaper V-cycle."""
+    from markovkit_b200.inputs import serving_requests
+    from markovkit_b200.serve import server, serving_problem
+
+    reqs = serving_requests(count=MIX_COUNT, rate=MIX_RATE)
+    keys = sorted({(r["model"], r["voxels"], r["cap"]) for r in reqs})
+    problems = {k: serving_problem(*k) for k in keys}
+    sizes = {k: problems[k][0].size() for k in keys}
+    bs = [rhs_of({"rhs": "dirichlet"}, r["rhs_seed"], sizes[(r["model"], r["voxels"], r["cap"])]) for r in reqs]
+    out = {}
+    variants = {"fp32": dict(precision="fp32", slots=SERVE_SLOTS, batch=4, coarsest_size=FP32_COARSEST,
+                             restart=MIX_RESTART),
+                "fp64": dict(precision="fp64", slots=1, batch=1, coarsest_size=4, restart=RESTART)}
+    for precision, kw in variants.items():
+        with server(rel_tolerance=REL_TOL, **kw) as srv:
+            pids = {k: srv.register(*problems[k]) for k in keys}
+            t0 = time.perf_counter()
+            tickets = []
+            for r, b in zip(reqs, bs):
+                wait = r["arrival_s"] - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                tickets.append(srv.submit(pids[(r["model"], r["voxels"], r["cap"])], r["shift"], b))
+            res = [srv.wait(t)[1] for t in tickets]
+            wall = time.perf_counter() - t0 - reqs[0]["arrival_s"]
+            st = srv.stats()
+        lat = sorted(r.latency_ms for r in res)
+        out[precision] = {
+            "value": round(len(res) / wall, 3),
+            "unit": "solves/s",
+            "p50_ms": round(lat[len(lat) // 2], 3),
+            "p99_ms": round(lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))], 3),
+            "worst_rel_residual": max(r.residual for r in res),
+            "all_converged": all(r.status == 0 for r in res),
+            "evictions": st["evictions"],
+            "memory_waits": st["memory_waits"],
+        }
+    out["fp32_over_fp64"] = round(out["fp32"]["value"] / out["fp64"]["value"], 3)
+    out["requests"] = len(reqs)
+    out["largest_states"] = max(sizes.values())
+    out["note"] = (f"Poisson arrivals at {MIX_RATE}/s, seed 4; fp32: {SERVE_SLOTS} slots, FGMRES({MIX_RESTART}), "
+                   "dense solve of sectors <= 256 states; fp64: 1 slot, GMRES(30), the reference's "
+                   "multigrid options; 1-D boxes use configuration 0's voxel size 1/16")
     return out
 
 
@@ -553,6 +615,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve-mix", action="store_true", help="skip the mixed serving workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -45,15 +45,19 @@ __device__ __forceinline__ void block_partials(double (&acc)[KMAX], int K, doubl
 // once; left unbounded, KMAX 16 takes 145 registers and one block per SM.
 template <int KMAX, int MODE>
 constexpr int cgs_min_blocks() {
-    if (MODE == 1) {
+    if constexpr (MODE == 1) {
         return KMAX >= 32 ? 1 : (KMAX >= 16 ? 2 : (KMAX >= 8 ? 3 : 4));
+    } else if constexpr (MODE == 2) {
+        return KMAX >= 16 ? 2 : 4;
+    } else {
+        return KMAX >= 32 ? 1 : (KMAX >= 16 ? (MODE == 0 ? 3 : 2) : 4);
     }
-    return KMAX >= 32 ? 2 : (KMAX >= 16 ? 3 : 4);
 }
 
 // mode 0: dots; mode 1: update then dots; mode 2: update then norm^2; mode 3: update only.
-// The update coefficients sit in shared memory (a broadcast read per use), which leaves the
-// registers to the loaded basis values and the accumulators. Columns k >= K are skipped.
+// Each element's K basis values are loaded first (all in flight at once), then used. The update
+// coefficients sit in shared memory (a broadcast read per use), which leaves the registers to
+// the loaded values and the accumulators.
 template <int KMAX, int MODE>
 __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
     cgs_kernel(const double *__restrict__ V, std::int64_t ld, int K, double *__restrict__ w,
@@ -73,43 +77,25 @@ __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
     const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
     for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += stride) {
+        double v[KMAX];
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            v[k] = k < K ? __ldcs(V + k * ld + i) : 0.0;
+        }
         double wi = w[i];
-        if constexpr (MODE == 0) {
+        if constexpr (MODE != 0) {
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {
-                if (k < K) {
-                    acc[k] += __ldcs(V + k * ld + i) * wi;
-                }
-            }
-        } else if constexpr (MODE == 1) {
-            double v[KMAX];
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k) {
-                v[k] = k < K ? __ldcs(V + k * ld + i) : 0.0;
-            }
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k) {
-                if (k < K) {
-                    wi -= c[k] * v[k];
-                }
+                wi -= c[k] * v[k];
             }
             w[i] = wi;
+        }
+        if constexpr (MODE == 2) {
+            acc[0] += wi * wi;
+        } else if constexpr (MODE == 0 || MODE == 1) {
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {
-                if (k < K) {
-                    acc[k] += v[k] * wi;
-                }
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < KMAX; ++k) {
-                if (k < K) {
-                    wi -= c[k] * __ldcs(V + k * ld + i);
-                }
-            }
-            w[i] = wi;
-            if constexpr (MODE == 2) {
-                acc[0] += wi * wi;
+                acc[k] += v[k] * wi;
             }
         }
     }
