@@ -118,6 +118,27 @@ int mk_generator_apply_shifted_batch(mk_generator gen, double shift, const doubl
 int mk_generator_apply_f32(mk_generator gen, const float *d_x, float *d_y, void *stream);
 int mk_generator_apply_shifted_f32(mk_generator gen, float shift, const float *d_x, float *d_y,
                                    void *stream);
+/* n_jumps(): the jumps between states of the space     generator.hpp:48 */
+int mk_generator_n_jumps(mk_generator gen, int64_t *n_jumps, void *stream);
+
+/* ---- the assembled generator: generator.hpp:84-107 ----
+ * A CSR matrix in device memory owned by the handle: row_ptr[rows + 1], col[nonzeros] and
+ * val[nonzeros], 64-bit indices, each row's columns ascending, the rates of distinct jumps
+ * between one pair of states summed into one entry (num::spmat::from_triplets). Assembly
+ * allocates device memory of about 40 bytes per entry while it runs; more than 2^31 - 1
+ * entries before merging fails with MK_EOVERFLOW. */
+typedef struct mk_csr_s *mk_csr;
+/* matrix(): Q                                   generator.hpp:84 */
+int mk_generator_matrix(mk_generator gen, mk_csr *out, void *stream);
+/* characteristic_matrix(shift): shift I - Q     generator.hpp:87-90; shifted_generator::matrix()
+ * generator.hpp:128 */
+int mk_generator_characteristic_matrix(mk_generator gen, double shift, mk_csr *out, void *stream);
+int mk_csr_size(mk_csr m, int64_t *rows, int64_t *nonzeros);
+/* the device arrays (valid until mk_csr_destroy) */
+int mk_csr_device(mk_csr m, const int64_t **row_ptr, const int64_t **col, const double **val);
+/* copies into host arrays of rows + 1, nonzeros and nonzeros elements */
+int mk_csr_copy_host(mk_csr m, int64_t *row_ptr, int64_t *col, double *val);
+void mk_csr_destroy(mk_csr m);
 
 /* ---- sector multigrid: markovkit/rdme/multigrid.hpp ---- */
 typedef struct {

@@ -296,6 +296,60 @@ std::shared_ptr<mk_model_s> make_model(const reaction_diffusion<D> &m, const arr
 enum class boundary : std::uint8_t { reflecting, absorbing };
 
 // Q with columns as sources, dp/dt = Q p; matrix-free on the device
+namespace num {
+
+// an assembled sparse matrix on the host in CSR (what generator::matrix() returns): each row's
+// columns ascending, equal positions summed
+class spmat {
+  public:
+    using domain_type = vec<real>;
+    using codomain_type = vec<real>;
+    spmat() = default;
+    spmat(idx rows, idx cols, array<real> values, array<idx> columns, array<idx> row_ptr)
+        : rows_(rows), cols_(cols), value_(std::move(values)), column_(std::move(columns)),
+          ptr_(std::move(row_ptr)) {}
+    [[nodiscard]] idx rows() const { return rows_; }
+    [[nodiscard]] idx cols() const { return cols_; }
+    [[nodiscard]] idx nonzeros() const { return value_.size(); }
+    [[nodiscard]] const array<idx> &row_ptr() const { return ptr_; }
+    [[nodiscard]] const array<idx> &columns() const { return column_; }
+    [[nodiscard]] const array<real> &values() const { return value_; }
+    void apply(const vec<real> &x, vec<real> &y) const {
+        y.assign(rows_, 0.0);
+        for (idx i = 0; i < rows_; ++i) {
+            real sum = 0.0;
+            for (idx k = ptr_[i]; k < ptr_[i + 1]; ++k) {
+                sum += value_[k] * x[column_[k]];
+            }
+            y[i] = sum;
+        }
+    }
+
+  private:
+    idx rows_ = 0, cols_ = 0;
+    array<real> value_;
+    array<idx> column_;
+    array<idx> ptr_;
+};
+
+} // namespace num
+
+namespace detail {
+
+// copies an assembled generator (mk_csr) to a host spmat and frees it
+inline num::spmat take_csr(mk_csr m) {
+    std::unique_ptr<mk_csr_s, void (*)(mk_csr)> hold(m, mk_csr_destroy);
+    int64_t rows = 0, nnz = 0;
+    check(mk_csr_size(m, &rows, &nnz));
+    std::vector<int64_t> ptr(static_cast<std::size_t>(rows) + 1), col(static_cast<std::size_t>(nnz));
+    array<real> val(static_cast<std::size_t>(nnz));
+    check(mk_csr_copy_host(m, ptr.data(), col.data(), val.data()));
+    return num::spmat(static_cast<idx>(rows), static_cast<idx>(rows), std::move(val),
+                      array<idx>(col.begin(), col.end()), array<idx>(ptr.begin(), ptr.end()));
+}
+
+} // namespace detail
+
 class generator {
   public:
     using domain_type = vec<real>;
@@ -332,6 +386,23 @@ class generator {
     }
     [[nodiscard]] array<real> exit_rates() const { return exit_leak().first; }
     [[nodiscard]] array<real> leak_rates() const { return exit_leak().second; }
+    [[nodiscard]] idx n_jumps() const {
+        int64_t n = 0;
+        detail::check(mk_generator_n_jumps(h_.get(), &n, nullptr));
+        return static_cast<idx>(n);
+    }
+    // Q, assembled
+    [[nodiscard]] num::spmat matrix() const {
+        mk_csr m = nullptr;
+        detail::check(mk_generator_matrix(h_.get(), &m, nullptr));
+        return detail::take_csr(m);
+    }
+    // shift I - Q, assembled
+    [[nodiscard]] num::spmat characteristic_matrix(real shift) const {
+        mk_csr m = nullptr;
+        detail::check(mk_generator_characteristic_matrix(h_.get(), shift, &m, nullptr));
+        return detail::take_csr(m);
+    }
     [[nodiscard]] mk_generator handle() const { return h_.get(); }
     [[nodiscard]] mk_model model_handle() const { return model_.get(); }
 
@@ -363,6 +434,7 @@ class shifted_generator {
         y.resize(rows());
         Q_->apply_shifted(shift_, view<const real>(x.data(), x.size()), view<real>(y.data(), y.size()));
     }
+    [[nodiscard]] num::spmat matrix() const { return Q_->characteristic_matrix(shift_); }
 
   private:
     const generator *Q_;

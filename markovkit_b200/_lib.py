@@ -196,6 +196,13 @@ SIGNATURES = {
     "mk_generator_apply_shifted_batch": (C.c_int, [P, C.c_double, P, P, I64, C.c_int, P]),
     "mk_generator_apply_f32": (C.c_int, [P, P, P, P]),
     "mk_generator_apply_shifted_f32": (C.c_int, [P, C.c_float, P, P, P]),
+    "mk_generator_n_jumps": (C.c_int, [P, I64P, P]),
+    "mk_generator_matrix": (C.c_int, [P, C.POINTER(P), P]),
+    "mk_generator_characteristic_matrix": (C.c_int, [P, C.c_double, C.POINTER(P), P]),
+    "mk_csr_size": (C.c_int, [P, I64P, I64P]),
+    "mk_csr_device": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "mk_csr_copy_host": (C.c_int, [P, I64P, I64P, C.POINTER(C.c_double)]),
+    "mk_csr_destroy": (None, [P]),
     "mk_multigrid_options_default": (None, [C.POINTER(MultigridOptions)]),
     "mk_multigrid_create": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
     "mk_multigrid_destroy": (None, [P]),

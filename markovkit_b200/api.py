@@ -296,6 +296,76 @@ class generator(_Handle):
             check(load().mk_generator_apply_shifted(self._h, float(shift), _ptr(x), _ptr(y), _stream(stream)))
         return y
 
+    def n_jumps(self) -> int:
+        """The jumps between states of the space (generator.hpp:48)."""
+        n = C.c_int64()
+        check(load().mk_generator_n_jumps(self._h, C.byref(n), None))
+        return n.value
+
+    def matrix(self, device: bool = False):
+        """Q assembled (generator.hpp:84): a scipy.sparse CSR matrix on the host, or with
+        device=True a csr_matrix of device tensors."""
+        return csr_matrix._assemble(self, None, device)
+
+    def characteristic_matrix(self, shift: float, device: bool = False):
+        """shift I - Q assembled (generator.hpp:87-90)."""
+        return csr_matrix._assemble(self, float(shift), device)
+
+
+class csr_matrix(_Handle):
+    """An assembled generator in device memory (mk_csr): row_ptr, col (int64) and val (float64)
+    as CUDA tensors viewing the library's arrays; kept alive by this object."""
+
+    _destroy = "mk_csr_destroy"
+
+    @classmethod
+    def _assemble(cls, Q: "generator", shift, device: bool):
+        m = cls()
+        if shift is None:
+            check(load().mk_generator_matrix(Q._h, C.byref(m._h), None))
+        else:
+            check(load().mk_generator_characteristic_matrix(Q._h, shift, C.byref(m._h), None))
+        return m if device else m.to_scipy()
+
+    def size(self) -> tuple[int, int]:
+        rows, nnz = C.c_int64(), C.c_int64()
+        check(load().mk_csr_size(self._h, C.byref(rows), C.byref(nnz)))
+        return rows.value, nnz.value
+
+    def to_scipy(self):
+        import numpy as np
+        import scipy.sparse as sp
+
+        rows, nnz = self.size()
+        ptr = np.empty(rows + 1, dtype=np.int64)
+        col = np.empty(max(nnz, 1), dtype=np.int64)
+        val = np.empty(max(nnz, 1), dtype=np.float64)
+        check(load().mk_csr_copy_host(self._h, ptr.ctypes.data_as(C.POINTER(C.c_int64)),
+                                      col.ctypes.data_as(C.POINTER(C.c_int64)),
+                                      val.ctypes.data_as(C.POINTER(C.c_double))))
+        return sp.csr_matrix((val[:nnz], col[:nnz], ptr), shape=(rows, rows))
+
+    def tensors(self):
+        """(row_ptr, col, val) as CUDA tensors over the library's arrays (no copy); each
+        tensor keeps this matrix alive."""
+        import torch
+
+        rows, nnz = self.size()
+        p, c, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(load().mk_csr_device(self._h, C.byref(p), C.byref(c), C.byref(v)))
+        return (torch.as_tensor(_DeviceArray(self, p.value, rows + 1, "<i8"), device="cuda"),
+                torch.as_tensor(_DeviceArray(self, c.value, nnz, "<i8"), device="cuda"),
+                torch.as_tensor(_DeviceArray(self, v.value, nnz, "<f8"), device="cuda"))
+
+
+class _DeviceArray:
+    """A library-owned device array seen through __cuda_array_interface__; holds its owner."""
+
+    def __init__(self, owner, ptr, n, typestr):
+        self.owner = owner
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr,
+                                         "data": (int(ptr or 0), False), "version": 3}
+
 
 class shifted_generator:
     """shift I - Q; reads Q by reference (generator.hpp:116-133)."""
@@ -315,6 +385,10 @@ class shifted_generator:
 
     def apply(self, x, y, stream=None):
         return self.Q.apply_shifted(self._shift, x, y, stream)
+
+    def matrix(self, device: bool = False):
+        """shift I - Q assembled (generator.hpp:128)."""
+        return self.Q.characteristic_matrix(self._shift, device)
 
 
 def multigrid_options(**kw) -> MultigridOptions:

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -19,7 +20,7 @@ CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libmarkovkit_b200.so"
 
-SOURCES = ["row_kernels_f64.cu", "row_kernels_f32.cu", "row_kernels_f64_batch.cu", "row_kernels_f32_batch.cu", "row_kernels.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu", "capi_fsp.cu", "server.cpp"]
+SOURCES = ["row_kernels_f64.cu", "row_kernels_f32.cu", "row_kernels_f64_batch.cu", "row_kernels_f32_batch.cu", "row_kernels.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu", "capi_fsp.cu", "server.cpp", "assemble.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [
     "-std=c++20",
@@ -55,15 +56,32 @@ def _stale(obj: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _local_includes(src: Path, seen: set[Path] | None = None) -> set[Path]:
+    """The project headers a source includes, transitively (quoted includes found next to the
+    including file or under include/)."""
+    seen = set() if seen is None else seen
+    for name in _INCLUDE.findall(src.read_text()):
+        for base in (src.parent, ROOT / "include"):
+            h = (base / name).resolve()
+            if h.exists():
+                if h not in seen:
+                    seen.add(h)
+                    _local_includes(h, seen)
+                break
+    return seen
+
+
 def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     extra = extra or []
     BUILD.mkdir(exist_ok=True)
-    headers = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + [ROOT / "include" / "markovkit_b200.h"]
     jobs = []
     for name in SOURCES:
         src = CSRC / name
         obj = BUILD / (src.stem + ".o")
-        if _stale(obj, [src, *headers, Path(__file__)]):
+        if _stale(obj, [src, *sorted(_local_includes(src)), Path(__file__)]):
             jobs.append((src, obj))
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:

@@ -2,6 +2,7 @@
 // and the mapping of C++ errors to MK_* status codes.
 #include "capi_internal.hpp"
 
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -283,6 +284,67 @@ int mk_generator_exit_leak(mk_generator gen, double *d_exit, double *d_leak, voi
                                 as_stream(stream));
     });
 }
+
+int mk_generator_n_jumps(mk_generator gen, int64_t *n_jumps, void *stream) {
+    return guarded([&] {
+        MK_REQUIRE(gen && n_jumps, "null argument");
+        *n_jumps = mkb::count_jumps(*gen->gen, as_stream(stream));
+    });
+}
+
+int mk_generator_matrix(mk_generator gen, mk_csr *out, void *stream) {
+    return guarded([&] {
+        MK_REQUIRE(gen && out, "null argument");
+        auto m = std::make_unique<mk_csr_s>();
+        mkb::assemble(*gen->gen, 0.0, 1.0, m->csr, as_stream(stream));
+        *out = m.release();
+    });
+}
+
+int mk_generator_characteristic_matrix(mk_generator gen, double shift, mk_csr *out, void *stream) {
+    return guarded([&] {
+        MK_REQUIRE(gen && out, "null argument");
+        MK_REQUIRE(std::isfinite(shift), "shift must be finite");
+        auto m = std::make_unique<mk_csr_s>();
+        mkb::assemble(*gen->gen, shift, -1.0, m->csr, as_stream(stream));
+        *out = m.release();
+    });
+}
+
+int mk_csr_size(mk_csr m, int64_t *rows, int64_t *nonzeros) {
+    return guarded([&] {
+        MK_REQUIRE(m && rows && nonzeros, "null argument");
+        *rows = m->csr.rows;
+        *nonzeros = m->csr.nnz;
+    });
+}
+
+int mk_csr_device(mk_csr m, const int64_t **row_ptr, const int64_t **col, const double **val) {
+    return guarded([&] {
+        MK_REQUIRE(m && row_ptr && col && val, "null argument");
+        *row_ptr = m->csr.row_ptr.get();
+        *col = m->csr.col.get();
+        *val = m->csr.val.get();
+    });
+}
+
+int mk_csr_copy_host(mk_csr m, int64_t *row_ptr, int64_t *col, double *val) {
+    return guarded([&] {
+        MK_REQUIRE(m && row_ptr && (m->csr.nnz == 0 || (col && val)), "null argument");
+        const auto &c = m->csr;
+        check_cuda(cudaMemcpy(row_ptr, c.row_ptr.get(), sizeof(int64_t) * (c.rows + 1),
+                              cudaMemcpyDeviceToHost),
+                   "csr row_ptr copy");
+        if (c.nnz > 0) {
+            check_cuda(cudaMemcpy(col, c.col.get(), sizeof(int64_t) * c.nnz, cudaMemcpyDeviceToHost),
+                       "csr col copy");
+            check_cuda(cudaMemcpy(val, c.val.get(), sizeof(double) * c.nnz, cudaMemcpyDeviceToHost),
+                       "csr val copy");
+        }
+    });
+}
+
+void mk_csr_destroy(mk_csr m) { delete m; }
 
 int mk_generator_apply(mk_generator gen, const double *d_x, double *d_y, void *stream) {
     return guarded([&] {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "../../include/markovkit_b200.h"
+#include "assemble.hpp"
 #include "engine.hpp"
 
 #include <new>
@@ -17,6 +18,9 @@ struct mk_model_s {
 struct mk_generator_s {
     std::unique_ptr<mkb::Space> space; // private copy of the geometry the generator indexes
     std::unique_ptr<mkb::Generator> gen;
+};
+struct mk_csr_s {
+    mkb::Csr csr;
 };
 struct mk_multigrid_s {
     std::unique_ptr<mkb::Multigrid> mg;

@@ -171,6 +171,20 @@ int run(const args &a) {
         write_f64(out + "/Ax.f64", z);
     }
 
+    // the assembled Q and shift I - Q (generator.hpp:84-107) as CSR: <name>_ptr, _col, _val
+    if (a.integer("dump_matrix", 0)) {
+        const auto dump = [&](const std::string &name, const num::spmat &m) {
+            write_f64(out + "/" + name + "_ptr.f64",
+                      std::vector<double>(m.row_ptr().begin(), m.row_ptr().end()));
+            write_f64(out + "/" + name + "_col.f64",
+                      std::vector<double>(m.columns().begin(), m.columns().end()));
+            write_f64(out + "/" + name + "_val.f64",
+                      std::vector<double>(m.values().begin(), m.values().end()));
+        };
+        dump("Qm", Q.matrix());
+        dump("Am", A.matrix());
+    }
+
     const std::string rhs_kind = a.get("rhs", "uniform");
     const std::uint64_t seed = static_cast<std::uint64_t>(a.integer("seed", 0));
     vec<real> b;

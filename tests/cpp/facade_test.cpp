@@ -65,6 +65,19 @@ void resolvent() {
         dev = std::max(dev, std::abs(ax[i] - (shift * b[i] - qx[i])));
     }
     expect(dev < 1e-12, "apply_shifted = s x - apply");
+    // the assembled operators reproduce the matrix-free ones (tests/test_rdme.cpp:100-158)
+    vec<real> mq, ma;
+    Q.matrix().apply(b, mq);
+    A.matrix().apply(b, ma);
+    real dq = 0.0, da = 0.0, sq = 0.0, sa = 0.0;
+    for (idx i = 0; i < b.size(); ++i) {
+        dq = std::max(dq, std::abs(mq[i] - qx[i]));
+        da = std::max(da, std::abs(ma[i] - ax[i]));
+        sq = std::max(sq, std::abs(qx[i]));
+        sa = std::max(sa, std::abs(ax[i]));
+    }
+    expect(dq <= 1e-13 * sq && da <= 1e-13 * sa, "matrix().apply = apply (1e-13 relative)");
+    expect(Q.matrix().nonzeros() == Q.rows() + Q.n_jumps(), "one entry per jump plus the diagonal");
     const auto exits = Q.exit_rates();
     expect(std::abs(exits[0] - 0.05 * 16 * (1.0 / 16)) < 1e-14, "exit rate of the empty state is the total birth rate");
 

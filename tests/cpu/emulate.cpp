@@ -106,6 +106,57 @@ std::int64_t emu_generator(int dim, const std::int64_t *dims, const double *spac
     }
 }
 
+// the triplets of sign * (Q - shift I) row by row, as the device assembly makes them: each
+// row's diagonal -sign (exit + shift), then sign * rate for each in-jump in visit order.
+// Returns the triplet count; writes them when it is at most `capacity`.
+std::int64_t emu_matrix(int dim, const std::int64_t *dims, const double *spacing, int S,
+                        const double *D, int R, const int *change, const int *tmax,
+                        const double *rates, int is_box, const int *limits, int absorbing,
+                        double shift, double sign, std::int64_t *row, std::int64_t *col,
+                        double *val, std::int64_t capacity, char *err, int csr) {
+    try {
+        Problem p =
+            make(dim, dims, spacing, S, D, R, change, tmax, rates, is_box, limits, absorbing, csr);
+        std::int64_t k = 0;
+        const auto put = [&](std::int64_t i, std::int64_t j, double v) {
+            if (k < capacity) {
+                row[k] = i;
+                col[k] = j;
+                val[k] = v;
+            }
+            ++k;
+        };
+        with_shape(S, max_species_total(p.sectors), [&]<int NS, int TMAX>() {
+            for (const SectorDesc &sec : p.sectors) {
+                for (std::int64_t local = 0; local < sec.size; ++local) {
+                    RowState<NS, TMAX> st;
+                    load_state<NS, TMAX>(p.B, sec, S, p.model->V, local, st);
+                    const std::int64_t i = sec.begin + local;
+                    std::vector<std::pair<std::int64_t, double>> in;
+                    double e = 0.0, l = 0.0;
+                    visit_row<double, NS, TMAX>(p.B, p.sectors.data(), sec, p.t.view, local, st,
+                                                true, 0, 1, e, l,
+                                                [&](std::int64_t j, double a, double) {
+                                                    if (j < 0 || j >= p.n) {
+                                                        throw Error(kEInval, "in-jump source out of range");
+                                                    }
+                                                    in.emplace_back(j, a);
+                                                });
+                    put(i, i, -sign * (e + shift));
+                    for (const auto &[j, a] : in) {
+                        put(i, j, sign * a);
+                    }
+                }
+            }
+            return 0;
+        });
+        return k;
+    } catch (const std::exception &e) {
+        write_err(err, e.what());
+        return -1;
+    }
+}
+
 // states (n x V*S, voxel-major) of every index by the product's unrank, and the product's
 // rank of each of them
 std::int64_t emu_states(int V, int S, const int *limits, int is_box, int *states,

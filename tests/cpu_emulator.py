@@ -70,6 +70,46 @@ def generator(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=T
     return out
 
 
+def matrix(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=True, shift=0.0, sign=1.0, csr=False):
+    """sign * (Q - shift I) assembled from the row visits (scipy CSR, equal positions summed)."""
+    import scipy.sparse as sp
+
+    L = lib()
+    S = len(D)
+    dims_a = np.array(list(dims) + [1] * (3 - dim), dtype=np.int64)
+    sp_a = np.array(list(spacing) + [1.0] * (3 - dim), dtype=np.float64)
+    D_a = np.array(D, dtype=np.float64)
+    lim = np.array(limits, dtype=np.int32)
+    R = len(reactions)
+    change = np.array([c for ch, _ in reactions for c in ch] or [0], dtype=np.int32)
+    tmax = np.array(limits, dtype=np.int32)
+    vol = float(np.prod(spacing))
+    rates = rate_table(reactions, list(limits), vol).ravel() if R else np.zeros(1)
+    err = C.create_string_buffer(256)
+    fn = L.emu_matrix
+    fn.restype = C.c_int64
+    args = [C.c_int(dim), _d(dims_a), _d(sp_a), C.c_int(S), _d(D_a), C.c_int(R), _d(change), _d(tmax),
+            _d(rates), C.c_int(int(is_box)), _d(lim), C.c_int(int(absorbing)), C.c_double(shift), C.c_double(sign)]
+    n = fn(*args, None, None, None, C.c_int64(0), err, C.c_int(int(csr)))
+    if n < 0:
+        raise ValueError(err.value.decode())
+    row = np.zeros(n, dtype=np.int64)
+    col = np.zeros(n, dtype=np.int64)
+    val = np.zeros(n)
+    N = int(emu_size(dim, dims, spacing, D, reactions, limits, is_box, absorbing, csr))
+    m = fn(*args, _d(row), _d(col), _d(val), C.c_int64(n), err, C.c_int(int(csr)))
+    if m != n:
+        raise ValueError(err.value.decode() or "triplet count changed")
+    out = sp.coo_matrix((val, (row, col)), shape=(N, N)).tocsr()
+    out.sum_duplicates()
+    out.sort_indices()
+    return out
+
+
+def emu_size(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=True, csr=False):
+    return len(generator(dim, dims, spacing, D, reactions, limits, is_box, absorbing, csr=csr)["exit"])
+
+
 def states(V, limits, is_box=True):
     L = lib()
     S = len(limits)

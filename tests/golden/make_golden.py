@@ -68,6 +68,7 @@ def run_case(name: str, spec: dict, work: Path) -> dict:
         args.append("do_transfer=1")
     if spec.get("states"):
         args.append("dump_states=1")
+    args.append("dump_matrix=1")  # the reference's Q.matrix() and A.matrix() (Qm_*, Am_*)
     proc = subprocess.run(args, capture_output=True, text=True, check=True)
     meta = json.loads(proc.stdout.strip().splitlines()[-1])
     out = {"meta": np.array(json.dumps({"spec": spec, "ref": meta, "voxels": dims_n}))}

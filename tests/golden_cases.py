@@ -67,6 +67,15 @@ class Case:
     def n(self) -> int:
         return int(self.ref["N"])
 
+    def csr(self, which: str):
+        """the reference's assembled matrix ("Qm": Q.matrix(), "Am": A.matrix() = shift I - Q)
+        as scipy CSR"""
+        import scipy.sparse as sp
+
+        ptr = self.data[f"{which}_ptr"].astype(np.int64)
+        col = self.data[f"{which}_col"].astype(np.int64)
+        return sp.csr_matrix((self.data[f"{which}_val"], col, ptr), shape=(self.n, self.n))
+
 
 def load(name: str) -> Case:
     raw = np.load(GOLDEN / f"{name}.npz")

@@ -55,3 +55,52 @@ def test_transfer_matches_reference(name):
         Pc, Rg = emu.transfer(c.dim, c.dims, c.spacing, totals, c.data[f"sector{k}_c"], c.data[f"sector{k}_g"])
         np.testing.assert_allclose(Pc, c.data[f"sector{k}_Pc"], rtol=1e-13, atol=1e-16)
         np.testing.assert_allclose(Rg, c.data[f"sector{k}_Rg"], rtol=1e-13, atol=1e-15)
+
+
+def _same_csr(a, b, rtol):
+    """identical sparsity (row pointers and sorted columns), values within rtol of the largest
+    magnitude of their row"""
+    a = a.tocsr()
+    b = b.tocsr()
+    a.sort_indices()
+    b.sort_indices()
+    np.testing.assert_array_equal(a.indptr, b.indptr)
+    np.testing.assert_array_equal(a.indices, b.indices)
+    scale = np.repeat(np.maximum.reduceat(np.abs(b.data), b.indptr[:-1]) if b.nnz else np.zeros(0),
+                      np.diff(b.indptr))
+    assert np.all(np.abs(a.data - b.data) <= rtol * scale), np.max(np.abs(a.data - b.data) / scale)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_matrix_is_its_apply(name):
+    """the oracle's own pin: the reference's assembled Q and shift I - Q reproduce its matrix-free
+    apply (tests/test_rdme.cpp:100-158 checks the same), and A = shift I - Q entrywise"""
+    c = gc.load(name)
+    Qm, Am = c.csr("Qm"), c.csr("Am")
+    x = c.data["x"]
+    for m, key in ((Qm, "Qx"), (Am, "Ax")):
+        ref = c.data[key]
+        assert np.max(np.abs(m @ x - ref)) <= 1e-14 * np.max(np.abs(ref))
+    diff = (Am - (c.shift * _eye(c.n) - Qm)).tocsr()
+    assert (abs(diff).max() if diff.nnz else 0.0) <= 1e-15 * abs(Am).max()
+    # one entry per jump before equal positions merge: nnz <= N + n_jumps
+    assert Qm.nnz <= c.n + int(c.ref["n_jumps"])
+
+
+def _eye(n):
+    import scipy.sparse as sp
+
+    return sp.identity(n, format="csr")
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("csr", [False, True], ids=["grid", "csr"])
+def test_assembled_rows_match_reference_matrix(name, csr):
+    """the rows the device assembly writes (diagonal, then one entry per in-jump), merged like
+    num::spmat::from_triplets, equal the reference's matrix() and characteristic_matrix()"""
+    c = gc.load(name)
+    args = (c.dim, c.dims, c.spacing, c.diffusivities, c.reactions, c.caps, True, c.absorbing)
+    Q = emu.matrix(*args, shift=0.0, sign=1.0, csr=csr)
+    A = emu.matrix(*args, shift=c.shift, sign=-1.0, csr=csr)
+    _same_csr(Q, c.csr("Qm"), 1e-14)
+    _same_csr(A, c.csr("Am"), 1e-14)
