@@ -52,6 +52,7 @@ struct ModelView {
     int gstride[3] = {1, 1, 1};
     float ginv[3] = {1, 1, 1}; // 1 / gdims for coordinate division
     T axis_coef[3] = {};       // weight / volume of an edge along each axis
+    int stencil = 0;           // grid model without reactions: one-molecule rows are a stencil
 };
 
 // q = v / d for 0 <= v < 2^24 from a float reciprocal and one correction
@@ -327,6 +328,48 @@ MK_HD std::int64_t rank_inserted(const int (&u)[TMAX], int t, const std::int64_t
     return r + mine;
 }
 
+// A row of a diffusion-only model on a structured grid whose species hold at most one molecule
+// each (TMAX 1): the state is one voxel per present species, and each in-jump moves one of them
+// in from a grid neighbour, so its source index is row + (uw - uu) * stride_s with
+// uw = uu +/- gstride. The terms, their values and their order are those of diffusion_terms
+// (rate = 1 * D_s * coef, the lower neighbour first), so the results are bit-identical; what
+// goes is the general machinery (run detection, counts, re-ranking) around them.
+template <typename T, int NS, bool WANT_IN, bool WANT_REV, typename Acc>
+MK_HD void stencil_row(const ModelView<T> &md, const SectorDesc &sec, const RowState<NS, 1> &st,
+                       int row, T &exit, Acc &acc) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        if (sec.total[s] < 1) {
+            continue;
+        }
+        const T Ds = md.diff[s];
+        const int stride = static_cast<int>(sec.stride[s]);
+        int c[3];
+        grid_coords(md, md.V - 1 - st.u[s][0], c);
+        T deg = T(0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a >= md.grid_dim) {
+                continue;
+            }
+            const bool has_lo = c[a] > 0, has_hi = c[a] + 1 < md.gdims[a];
+            deg += T((has_lo ? 1 : 0) + (has_hi ? 1 : 0)) * md.axis_coef[a];
+            if constexpr (WANT_IN) {
+                const T rate = T(1) * Ds * md.axis_coef[a];
+                const T rev = WANT_REV ? rate : T(0);
+                const int step = md.gstride[a] * stride;
+                if (has_lo) {
+                    acc(row + step, rate, rev);
+                }
+                if (has_hi) {
+                    acc(row - step, rate, rev);
+                }
+            }
+        }
+        exit += Ds * deg;
+    }
+}
+
 // Visit the row: acc(source_index, rate) for every in-jump; adds into exit and leak.
 // light: the exit/leak terms and the in-jumps that start in occupied voxels.
 // [lane, V) step nlanes: the all-voxel loop of heavy reactions.
@@ -335,6 +378,13 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                      const ModelView<T> &md, std::int64_t local, const RowState<NS, TMAX> &st,
                      bool light, int lane, int nlanes, T &exit, T &leak, Acc &&acc) {
     const int V = md.V, R = md.R;
+    if constexpr (TMAX == 1) {
+        if (md.stencil && light && nlanes == 1) {
+            stencil_row<T, NS, WANT_IN, WANT_REV>(md, sec, st, static_cast<int>(sec.begin + local),
+                                                  exit, acc);
+            return;
+        }
+    }
     if (light) {
         // reactions firing from empty voxels: the all-empty total, corrected per occupied voxel
         for (int r = 0; r < R; ++r) {

@@ -367,6 +367,9 @@ struct HostTables {
                 mv.axis_coef[a] =
                     a < m.dim ? static_cast<T>((face / m.spacing[a]) / m.volumes[0]) : T(0);
             }
+            // diffusion only (the multigrid level operators): rows of one molecule per species
+            // take the stencil path of visit_row
+            mv.stencil = mv.R == 0 ? 1 : 0;
         }
         view = mv;
         bind_host();

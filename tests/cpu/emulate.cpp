@@ -47,11 +47,15 @@ Problem make(int dim, const std::int64_t *dims, const double *spacing, int S, co
     p.B = {p.binom.data(), max_total + 1, p.model->V + max_total + 1};
     const auto totals = is_box ? box_totals(lim) : std::vector<std::vector<int>>{lim};
     p.sectors = layout_sectors(p.model->V, S, totals, p.B, &p.n);
-    if (csr) {
+    if (csr == 1) {
         // the same voxel graph given as explicit neighbour lists (the general-graph path)
         p.model->has_grid = false;
     }
     p.t.build(*p.model, 1.0, true, absorbing != 0);
+    if (csr == 2) {
+        // the structured grid through the general row visit (no stencil path)
+        p.t.view.stencil = 0;
+    }
     couple_sectors<double>(p.sectors, S, *p.model, p.t.view, true);
     return p;
 }

@@ -104,3 +104,21 @@ def test_assembled_rows_match_reference_matrix(name, csr):
     A = emu.matrix(*args, shift=c.shift, sign=-1.0, csr=csr)
     _same_csr(Q, c.csr("Qm"), 1e-14)
     _same_csr(A, c.csr("Am"), 1e-14)
+
+
+@pytest.mark.parametrize("dim,cells", [(1, 7), (2, 6), (3, 3)])
+def test_stencil_rows_bit_identical(dim, cells):
+    """diffusion-only rows of one molecule per species (the multigrid level operators of
+    two-species boxes of cap 1) take visit_row's stencil path on grids; it must give exactly
+    the general visit's exit rates and applies, and agree with the neighbour-list path"""
+    dims, h = [cells] * dim, [1.0 / cells] * dim
+    D, caps, x = [0.7, 1.9], [1, 1], None
+    outs = {}
+    for mode in (0, 2, 1):  # stencil, general grid visit, neighbour lists
+        n = len(emu.generator(dim, dims, h, D, [], caps, True, True, 0.5, None, csr=mode)["exit"])
+        if x is None:
+            x = np.sin(0.37 * np.arange(n)) + 1.5
+        outs[mode] = emu.generator(dim, dims, h, D, [], caps, True, True, 0.5, x, csr=mode)
+    for key in ("exit", "leak", "Qx", "Ax"):
+        np.testing.assert_array_equal(outs[0][key], outs[2][key])
+        np.testing.assert_allclose(outs[0][key], outs[1][key], rtol=1e-14, atol=1e-12)
