@@ -1233,8 +1233,10 @@ KrylovBatch::KrylovBatch(std::int64_t n_, int m_, int nb_) : n(n_), m(m_), nb(nb
     Z.resize(static_cast<std::size_t>(ld) * nb * m);
     w.resize(static_cast<std::size_t>(ld) * nb);
     r.resize(static_cast<std::size_t>(ld) * nb);
-    partials.resize(static_cast<std::size_t>(kDotBlocks) * kMaxFusedBasis);
+    partials.resize(static_cast<std::size_t>(kDotBlocks) * kMaxFusedBasis * nb);
+    reports.resize(static_cast<std::size_t>(4) * nb);
     const std::size_t per = arnoldi_small_size(m);
+    small_stride = static_cast<std::int64_t>(per);
     small.resize(per * nb);
     for (int c = 0; c < nb; ++c) {
         st.push_back(carve_arnoldi(small.get() + per * c, m));
@@ -1330,6 +1332,30 @@ std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigri
             M.apply_batch(Vj(j, 0), ld, Zj(j, 0), ld, nb, stream);
             A.apply<double>(kApplyShifted, shift, Zj(j, 0), nullptr, ws.w.get(), nullptr, stream,
                             nb, ld);
+            if (j + 1 <= kMaxFusedBasis && nb <= 32) {
+                // every running column's Gram-Schmidt, Givens column and next basis vector in
+                // one launch per pass, and one copy of their reports
+                ColumnBatch cb;
+                cb.V = ws.V.get();
+                cb.vstride = col_stride;
+                cb.w = ws.w.get();
+                cb.col = ld;
+                cb.st = ws.st[0];
+                cb.small = ws.small_stride;
+                cb.partials = ws.partials.get();
+                cb.reports = ws.reports.get();
+                cb.nb = nb;
+                cb.n = n;
+                for (int c = 0; c < nb; ++c) {
+                    cb.mask |= cols[c] ? (1U << c) : 0U;
+                }
+                check_cuda(cgs_step_batch(cb, j, j + 1 < m, stream), "batched Gram-Schmidt");
+                check_cuda(cudaMemcpyAsync(ws.report_host + 4 * nb * (j & 1), ws.reports.get(),
+                                           4 * nb * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                           "report");
+                check_cuda(cudaEventRecord(ws.step_done[j & 1], stream), "event");
+                return;
+            }
             for (int c = 0; c < nb; ++c) {
                 if (!cols[c]) {
                     continue;

@@ -278,6 +278,8 @@ struct KrylovBatch {
     std::int64_t n = 0, ld = 0;
     int m = 0, nb = 0;
     DeviceArray<double> V, Z, w, r, partials, small;
+    DeviceArray<double> reports;      // 4 per column: the last batched step's Givens reports
+    std::int64_t small_stride = 0;    // doubles between consecutive columns' Arnoldi states
     std::vector<ArnoldiState> st;
     double *report_host = nullptr; // pinned: two slots (steps j and j + 1) of 4 per column
     cudaEvent_t step_done[2] = {nullptr, nullptr};
@@ -288,8 +290,8 @@ struct KrylovBatch {
 };
 
 // FGMRES on nb <= ws.nb right-hand sides at once (column c of b and x at c * ws.ld): one
-// batched operator apply and one batched multigrid cycle per step serve every column, the
-// Gram-Schmidt passes and Givens rotations run per column. Column c stops at its own absolute
+// batched operator apply and one batched multigrid cycle per step serve every column, and one
+// launch per Gram-Schmidt pass serves every running column (per-column arithmetic unchanged). Column c stops at its own absolute
 // tolerance tol[c] (opt.tolerance is unused); the batch stops when every column has.
 std::vector<SolverResult> gmres_batch(const Generator &A, double shift, Multigrid &M,
                                       const double *b, double *x, int nb, const double *tol,

@@ -58,10 +58,23 @@ constexpr int cgs_min_blocks() {
 // Each element's K basis values are loaded first (all in flight at once), then used. The update
 // coefficients sit in shared memory (a broadcast read per use), which leaves the registers to
 // the loaded values and the accumulators.
+// Column blockIdx.y of a batch (ColumnBatch) sits at V + col * y, w + col * y,
+// coef + coef_stride * y and partials + part_stride * y; columns whose mask bit is clear skip.
 template <int KMAX, int MODE>
 __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
     cgs_kernel(const double *__restrict__ V, std::int64_t ld, int K, double *__restrict__ w,
-               std::int64_t n, const double *__restrict__ coef, double *__restrict__ partials) {
+               std::int64_t n, const double *__restrict__ coef, double *__restrict__ partials,
+               std::int64_t col, std::int64_t coef_stride, std::int64_t part_stride,
+               unsigned mask) {
+    if (!((mask >> blockIdx.y) & 1U)) {
+        return;
+    }
+    V += col * blockIdx.y;
+    w += col * blockIdx.y;
+    if (coef) {
+        coef += coef_stride * blockIdx.y;
+    }
+    partials += part_stride * blockIdx.y;
     __shared__ double c[KMAX];
     if constexpr (MODE != 0) {
         if (static_cast<int>(threadIdx.x) < KMAX) {
@@ -104,8 +117,15 @@ __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
     }
 }
 
-// out[k] = sum_b partials[k * nb + b], one warp per k, fixed order
-__global__ void finalize_kernel(const double *partials, int nb, int K, double *out) {
+// out[k] = sum_b partials[k * nb + b], one warp per k, fixed order; block y serves column y of
+// a batch (partials + part_stride * y, out + out_stride * y)
+__global__ void finalize_kernel(const double *partials, int nb, int K, double *out,
+                                std::int64_t part_stride, std::int64_t out_stride, unsigned mask) {
+    if (!((mask >> blockIdx.x) & 1U)) {
+        return;
+    }
+    partials += part_stride * blockIdx.x;
+    out += out_stride * blockIdx.x;
     const int warp = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
     for (int k = warp; k < K; k += blockDim.x >> 5) {
         double s = 0.0;
@@ -123,9 +143,11 @@ template <int KMAX, int MODE>
 cudaError_t launch_cgs(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
                        const double *coef, double *partials, double *out, cudaStream_t stream) {
     count_launches(MODE != 3 ? 2 : 1);
-    cgs_kernel<KMAX, MODE><<<kDotBlocks, kDotThreads, 0, stream>>>(V, ld, K, w, n, coef, partials);
+    cgs_kernel<KMAX, MODE>
+        <<<kDotBlocks, kDotThreads, 0, stream>>>(V, ld, K, w, n, coef, partials, 0, 0, 0, 1U);
     if (MODE != 3) {
-        finalize_kernel<<<1, 1024, 0, stream>>>(partials, kDotBlocks, MODE == 2 ? 1 : K, out);
+        finalize_kernel<<<1, 1024, 0, stream>>>(partials, kDotBlocks, MODE == 2 ? 1 : K, out, 0, 0,
+                                                1U);
     }
     return cudaGetLastError();
 }
@@ -143,6 +165,49 @@ cudaError_t launch_cgs_k(const double *V, std::int64_t ld, int K, double *w, std
         return launch_cgs<16, MODE>(V, ld, K, w, n, coef, partials, out, stream);
     }
     return launch_cgs<32, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+}
+
+// one CGS pass for every selected column of a batch: grid (kDotBlocks, nb), then nb finalizes
+template <int KMAX, int MODE>
+void launch_cgs_batch(const ColumnBatch &b, int K, const double *coef, double *out,
+                      cudaStream_t stream) {
+    const std::int64_t part = static_cast<std::int64_t>(kDotBlocks) * kMaxFusedBasis;
+    count_launches(2);
+    cgs_kernel<KMAX, MODE><<<dim3(kDotBlocks, b.nb), kDotThreads, 0, stream>>>(
+        b.V, b.vstride, K, b.w, b.n, coef, b.partials, b.col, b.small, part, b.mask);
+    finalize_kernel<<<b.nb, 1024, 0, stream>>>(b.partials, kDotBlocks, MODE == 2 ? 1 : K, out,
+                                               part, b.small, b.mask);
+}
+
+template <int MODE>
+void launch_cgs_batch_k(const ColumnBatch &b, int K, const double *coef, double *out,
+                        cudaStream_t stream) {
+    if (K <= 4) {
+        launch_cgs_batch<4, MODE>(b, K, coef, out, stream);
+    } else if (K <= 8) {
+        launch_cgs_batch<8, MODE>(b, K, coef, out, stream);
+    } else if (K <= 16) {
+        launch_cgs_batch<16, MODE>(b, K, coef, out, stream);
+    } else {
+        launch_cgs_batch<32, MODE>(b, K, coef, out, stream);
+    }
+}
+
+// y = x * (*scale); block row y of the grid serves column y of a batch
+__global__ void scale_copy_batch_kernel(const double *x, const double *scale, double *y,
+                                        std::int64_t n, std::int64_t col, std::int64_t small,
+                                        unsigned mask) {
+    if (!((mask >> blockIdx.y) & 1U)) {
+        return;
+    }
+    x += col * blockIdx.y;
+    y += col * blockIdx.y;
+    const double a = scale[small * blockIdx.y];
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        y[i] = x[i] * a;
+    }
 }
 
 __global__ void scale_copy_kernel(const double *x, const double *scale, double *y, std::int64_t n) {
@@ -202,7 +267,7 @@ __global__ void arnoldi_start_kernel(ArnoldiState s) {
     s.report[2] = 0.0;
 }
 
-__global__ void arnoldi_column_kernel(ArnoldiState s, int j) {
+__device__ void arnoldi_column_step(const ArnoldiState &s, int j) {
     const int ld = s.m + 1;
     double *col = s.H + static_cast<std::int64_t>(j) * ld;
     for (int i = 0; i <= j; ++i) {
@@ -227,6 +292,34 @@ __global__ void arnoldi_column_kernel(ArnoldiState s, int j) {
     s.report[0] = fabs(s.g[j + 1]);
     s.report[1] = hn;
     s.report[2] = (hn > 0.0 && isfinite(hn)) ? 0.0 : 1.0;
+}
+
+__global__ void arnoldi_column_kernel(ArnoldiState s, int j) { arnoldi_column_step(s, j); }
+
+// block c: the Givens column of batch column c, its report also copied to reports + 4 c
+__global__ void arnoldi_column_batch_kernel(ArnoldiState s0, std::int64_t small, unsigned mask,
+                                            int j, double *reports) {
+    const int c = static_cast<int>(blockIdx.x);
+    if (!((mask >> c) & 1U)) {
+        return;
+    }
+    ArnoldiState s = s0;
+    const std::int64_t off = small * c;
+    s.H += off;
+    s.cs += off;
+    s.sn += off;
+    s.g += off;
+    s.y += off;
+    s.h1 += off;
+    s.h2 += off;
+    s.hn += off;
+    s.inv_hn += off;
+    s.beta += off;
+    s.report += off;
+    arnoldi_column_step(s, j);
+    for (int k = 0; k < 4; ++k) {
+        reports[4 * c + k] = s.report[k];
+    }
 }
 
 __global__ void arnoldi_solve_kernel(ArnoldiState s, int k) {
@@ -259,6 +352,26 @@ cudaError_t cgs_pass(int mode, const double *V, std::int64_t ld, int K, double *
     default:
         return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t cgs_step_batch(const ColumnBatch &b, int j, bool next, cudaStream_t stream) {
+    const int K = j + 1;
+    if (K < 1 || K > kMaxFusedBasis || b.nb < 1 || b.nb > 32) {
+        return cudaErrorInvalidValue;
+    }
+    const ArnoldiState &s = b.st;
+    launch_cgs_batch_k<0>(b, K, nullptr, s.h1, stream);
+    launch_cgs_batch_k<1>(b, K, s.h1, s.h2, stream);
+    launch_cgs_batch_k<2>(b, K, s.h2, s.hn, stream);
+    count_launches(1);
+    arnoldi_column_batch_kernel<<<b.nb, 1, 0, stream>>>(s, b.small, b.mask, j, b.reports);
+    if (next) {
+        count_launches(1);
+        scale_copy_batch_kernel<<<dim3(stream_blocks(b.n), b.nb), 256, 0, stream>>>(
+            b.w, s.inv_hn, b.V + static_cast<std::int64_t>(j + 1) * b.vstride, b.n, b.col,
+            b.small, b.mask);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t dot(const double *a, const double *b, std::int64_t n, double *partials, double *out,

@@ -55,6 +55,32 @@ struct ArnoldiState {
     int m = 0;
 };
 
+// The running columns of a lockstep batch (batched FGMRES): column c's basis vector k sits at
+// V + c * col + k * vstride, its w at w + c * col, its Arnoldi state at st's pointers + c * small
+// (offsets in doubles); partials hold nb * kDotBlocks * kMaxFusedBasis doubles; bit c of mask
+// selects column c.
+struct ColumnBatch {
+    double *V = nullptr;
+    std::int64_t vstride = 0;
+    double *w = nullptr;
+    std::int64_t col = 0;
+    ArnoldiState st;
+    std::int64_t small = 0;
+    double *partials = nullptr;
+    double *reports = nullptr; // 4 per column, contiguous: the step's Givens report
+    int nb = 0;
+    unsigned mask = 0;
+    std::int64_t n = 0;
+};
+
+// Step j's classical Gram-Schmidt with one re-orthogonalisation for every selected column at
+// once (K = j + 1 <= kMaxFusedBasis): h1 = V^T w; w -= V h1, h2 = V^T w; w -= V h2,
+// hn = <w, w>; the Givens column j (as arnoldi_column, its report also copied to reports);
+// and, when next, V_{j+1} = w / sqrt(hn). One launch per pass serves every column; per column
+// the arithmetic is that of cgs_pass, arnoldi_column and scale_copy, so the results are the
+// same bit for bit.
+cudaError_t cgs_step_batch(const ColumnBatch &b, int j, bool next, cudaStream_t stream);
+
 // g = (||r||, 0, ...), beta <- 1/||r|| (reads beta = <r, r>)
 cudaError_t arnoldi_start(const ArnoldiState &s, cudaStream_t stream);
 // fold column j (h1 + h2, sqrt(hn)) into H, rotate, update g; report |g_{j+1}|
