@@ -469,7 +469,9 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     graph_kernels_.assign(static_cast<std::size_t>(opt.batch) + 1, 0);
     for (std::size_t d = 0; d < levels.size(); ++d) {
         Level &L = *levels[d];
-        const std::size_t nb = static_cast<std::size_t>(opt.batch);
+        // the FP32 batched cycle interleaves kRowBatch lanes whatever the batch width
+        const std::size_t nb = static_cast<std::size_t>(
+            opt.precision == 1 && opt.batch > 1 ? kRowBatch : opt.batch);
         const std::size_t nd = static_cast<std::size_t>(L.op.n) * nb;
         const std::size_t nc =
             d + 1 < levels.size() ? static_cast<std::size_t>(levels[d + 1]->op.n) * nb : 0;
@@ -608,10 +610,13 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
     T *x = buf<T>(L, 1);
     T *tmp = buf<T>(L, 2);
     T *r = buf<T>(L, 3);
-    // nb_ columns, column c of every level vector at c * nd
+    // nb_ columns: column c of every level vector at c * nd, except in the FP32 batched cycle,
+    // whose kernels interleave kRowBatch lanes (entry (i, c) at i * kRowBatch + c)
     const std::int64_t nd = L.op.n;
     const int nb = nb_;
-    const std::int64_t ndb = nd * nb;
+    const bool inter = std::is_same_v<T, float> && nb > 1;
+    const int lanes = inter ? kRowBatch : nb;
+    const std::int64_t ndb = nd * lanes;
     RowParams<T> p = L.op.params<T>();
     p.shift = static_cast<T>(shift);
     p.omega = static_cast<T>(opt.jacobi_weight);
@@ -652,7 +657,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
 
     Level *C = d + 1 < max_depth ? levels[d + 1].get() : nullptr;
     if (C) {
-        check_cuda(cudaMemsetAsync(buf<T>(*C, 0), 0, C->op.n * nb * sizeof(T), stream), "memset");
+        check_cuda(cudaMemsetAsync(buf<T>(*C, 0), 0, C->op.n * lanes * sizeof(T), stream), "memset");
         p.ldc = C->op.n;
         p.tv.Vc = C->op.V;
         p.tv.parent = L.parent.get();
@@ -677,8 +682,9 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
             max_n = std::max(max_n, tb.n);
         }
         for (int c = 0; c < nb; ++c) {
+            const std::int64_t off = inter ? c : c * nd;
             check_cuda(launch_terminal<T>(L.d_term.get(), static_cast<int>(L.h_term.size()),
-                                          max_n, inv, r + c * nd, x + c * nd, stream),
+                                          max_n, inv, r + off, x + off, inter ? lanes : 1, stream),
                        "terminal solve");
         }
     }
@@ -688,7 +694,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
             cx = cycle<T>(d + 1, stream);
         } else {
             T *acc = buf<T>(L, 4), *crhs = buf<T>(L, 5);
-            const std::size_t bytes = C->op.n * nb * sizeof(T);
+            const std::size_t bytes = C->op.n * lanes * sizeof(T);
             check_cuda(cudaMemcpyAsync(crhs, buf<T>(*C, 0), bytes, cudaMemcpyDeviceToDevice, stream),
                        "copy");
             T *e = cycle<T>(d + 1, stream);
@@ -703,7 +709,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
                 pc.ldv = C->op.n;
                 C->op.run<T>(kResidual, pc, stream);
                 e = cycle<T>(d + 1, stream);
-                axpy_t<T>(T(1), e, acc, C->op.n * nb, stream);
+                axpy_t<T>(T(1), e, acc, C->op.n * lanes, stream);
             }
             cx = acc;
         }
@@ -931,6 +937,62 @@ Multigrid::~Multigrid() {
     }
 }
 
+namespace {
+
+// y[i * kRowBatch + c] = float(x[c * ldx + i]) for c < nb, 0 for the other lanes
+__global__ void pack_lanes_kernel(const double *x, std::int64_t ldx, int nb, float *y,
+                                  std::int64_t n) {
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        float v[kRowBatch];
+#pragma unroll
+        for (int c = 0; c < kRowBatch; ++c) {
+            v[c] = c < nb ? static_cast<float>(x[c * ldx + i]) : 0.0f;
+        }
+        *reinterpret_cast<float4 *>(y + i * kRowBatch) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+// y[c * ldy + i] = double(x[i * kRowBatch + c]) for c < nb
+__global__ void unpack_lanes_kernel(const float *x, std::int64_t n, int nb, double *y,
+                                    std::int64_t ldy) {
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        const float4 v = *reinterpret_cast<const float4 *>(x + i * kRowBatch);
+        const float u[kRowBatch] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int c = 0; c < kRowBatch; ++c) {
+            if (c < nb) {
+                y[c * ldy + i] = static_cast<double>(u[c]);
+            }
+        }
+    }
+}
+
+unsigned lane_blocks(std::int64_t n) {
+    return static_cast<unsigned>(std::max<std::int64_t>(1, std::min<std::int64_t>((n + 255) / 256, 148 * 8)));
+}
+
+} // namespace
+
+static_assert(kRowBatch == 4, "the interleaved FP32 batch moves four lanes as one float4");
+
+cudaError_t Multigrid::pack_lanes(const double *x, std::int64_t ldx, int nb, float *y,
+                                  std::int64_t n, cudaStream_t stream) {
+    count_launches(1);
+    pack_lanes_kernel<<<lane_blocks(n), 256, 0, stream>>>(x, ldx, nb, y, n);
+    return cudaGetLastError();
+}
+
+cudaError_t Multigrid::unpack_lanes(const float *x, std::int64_t n, int nb, double *y,
+                                    std::int64_t ldy, cudaStream_t stream) {
+    count_launches(1);
+    unpack_lanes_kernel<<<lane_blocks(n), 256, 0, stream>>>(x, n, nb, y, ldy);
+    return cudaGetLastError();
+}
+
 void Multigrid::apply(const double *b, double *x, cudaStream_t stream) {
     apply_batch(b, n, x, n, 1, stream);
 }
@@ -943,7 +1005,11 @@ void Multigrid::apply_batch(const double *b, std::int64_t ldb, double *x, std::i
     Level &L0 = *levels[0];
     const std::int64_t n0 = L0.op.n;
     ensure_graph(nb);
-    for (int c = 0; c < nb; ++c) {
+    const bool inter = opt.precision == 1 && nb > 1;
+    if (inter) {
+        check_cuda(pack_lanes(b, ldb, nb, L0.rhs32.get(), n0, stream), "pack");
+    }
+    for (int c = 0; c < nb && !inter; ++c) {
         if (opt.precision == 0) {
             check_cuda(cudaMemcpyAsync(L0.rhs64.get() + c * n0, b + c * ldb, n0 * sizeof(double),
                                        cudaMemcpyDeviceToDevice, stream),
@@ -955,7 +1021,10 @@ void Multigrid::apply_batch(const double *b, std::int64_t ldb, double *x, std::i
     }
     check_cuda(cudaGraphLaunch(graph_exec_[nb], stream), "multigrid graph launch");
     count_launches(graph_kernels_[nb]);
-    for (int c = 0; c < nb; ++c) {
+    if (inter) {
+        check_cuda(unpack_lanes(L0.x32.get(), n0, nb, x, ldx, stream), "unpack");
+    }
+    for (int c = 0; c < nb && !inter; ++c) {
         if (opt.precision == 0) {
             check_cuda(cudaMemcpyAsync(x + c * ldx, L0.x64.get() + c * n0, n0 * sizeof(double),
                                        cudaMemcpyDeviceToDevice, stream),

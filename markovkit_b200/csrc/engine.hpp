@@ -203,6 +203,12 @@ struct Multigrid {
     // of x at x + c * ldx; one cycle serves all columns
     void apply_batch(const double *b, std::int64_t ldb, double *x, std::int64_t ldx, int nb,
                      cudaStream_t stream);
+    // the FP32 batched cycle's interleaved lanes: pack nb FP64 columns (c at c * ldx) into y,
+    // lanes >= nb zero; unpack lanes < nb into FP64 columns at c * ldy
+    static cudaError_t pack_lanes(const double *x, std::int64_t ldx, int nb, float *y,
+                                  std::int64_t n, cudaStream_t stream);
+    static cudaError_t unpack_lanes(const float *x, std::int64_t n, int nb, double *y,
+                                    std::int64_t ldy, cudaStream_t stream);
     // bytes of work vectors one cycle needs, each vector aligned to 256 bytes
     [[nodiscard]] std::size_t scratch_bytes() const;
     // the same cycle with every work vector carved from caller-given device memory of at

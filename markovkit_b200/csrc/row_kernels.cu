@@ -42,10 +42,11 @@ constexpr int kTerminalThreads = 256;
 
 // x[begin + p] += inv[p] . r[begin ..]: one warp per row of a block's inverse, the lanes
 // striding its columns (coalesced); blockIdx.x picks the terminal block, blockIdx.y a group of
-// rows, so a large block's rows spread over many SMs
+// rows, so a large block's rows spread over many SMs. Entry q of r and x sits at q * stride
+// (stride > 1: one column of interleaved right-hand sides).
 template <typename T>
 __global__ void __launch_bounds__(kTerminalThreads)
-    terminal_kernel(const TerminalBlock *blocks, const T *inv, const T *r, T *x) {
+    terminal_kernel(const TerminalBlock *blocks, const T *inv, const T *r, T *x, int stride) {
     const TerminalBlock tb = blocks[blockIdx.x];
     constexpr int warps = kTerminalThreads / 32;
     const int warp = static_cast<int>(threadIdx.x) >> 5, lane = static_cast<int>(threadIdx.x) & 31;
@@ -54,14 +55,14 @@ __global__ void __launch_bounds__(kTerminalThreads)
         const T *row = inv + tb.inv_offset + static_cast<std::int64_t>(p) * tb.n;
         T e = T(0);
         for (int q = lane; q < tb.n; q += 32) {
-            e += row[q] * r[tb.begin + q];
+            e += row[q] * r[(tb.begin + q) * stride];
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             e += __shfl_xor_sync(0xffffffffu, e, off);
         }
         if (lane == 0) {
-            x[tb.begin + p] += e;
+            x[(tb.begin + p) * stride] += e;
         }
     }
 }
@@ -175,21 +176,22 @@ __global__ void rank_kernel(const BinomTable B, const SectorDesc *sectors, int n
 
 template <typename T>
 cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, int max_n, const T *inv,
-                            const T *r, T *x, cudaStream_t stream) {
+                            const T *r, T *x, int stride, cudaStream_t stream) {
     if (n_blocks == 0) {
         return cudaSuccess;
     }
     constexpr int warps = kTerminalThreads / 32;
     const int groups = std::max(1, std::min((max_n + warps - 1) / warps, 256));
     count_launches(1);
-    terminal_kernel<T><<<dim3(n_blocks, groups), kTerminalThreads, 0, stream>>>(blocks, inv, r, x);
+    terminal_kernel<T>
+        <<<dim3(n_blocks, groups), kTerminalThreads, 0, stream>>>(blocks, inv, r, x, stride);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_terminal<double>(const TerminalBlock *, int, int, const double *,
-                                             const double *, double *, cudaStream_t);
+                                             const double *, double *, int, cudaStream_t);
 template cudaError_t launch_terminal<float>(const TerminalBlock *, int, int, const float *,
-                                            const float *, float *, cudaStream_t);
+                                            const float *, float *, int, cudaStream_t);
 
 cudaError_t launch_unrank(const BinomTable &B, const SectorDesc *sectors, int n_sectors, int S,
                           int V, const std::int64_t *index, std::int64_t count, int *states,

@@ -88,10 +88,11 @@ struct TerminalBlock {
     int pad = 0;
 };
 
-// x[begin + p] += sum_q inv[p][q] r[begin + q] for every terminal block (max_n: the largest)
+// x[begin + p] += sum_q inv[p][q] r[begin + q] for every terminal block (max_n: the largest);
+// entry q of r and x at q * stride
 template <typename T>
 cudaError_t launch_terminal(const TerminalBlock *blocks, int n_blocks, int max_n, const T *inv,
-                            const T *r, T *x, cudaStream_t stream);
+                            const T *r, T *x, int stride, cudaStream_t stream);
 
 // bit-exact state indexing on the device
 cudaError_t launch_unrank(const BinomTable &B, const SectorDesc *sectors, int n_sectors, int S,

@@ -11,8 +11,26 @@
 #include "launch_count.hpp"
 #include "row_kernels.cuh"
 
+#include <type_traits>
+
 namespace mkb {
 namespace detail {
+
+// The FP32 kernels that serve kRowBatch right-hand sides (the batched multigrid cycle) keep
+// them interleaved: element (i, c) at i * kRowBatch + c, so an in-jump's kRowBatch source
+// values are one 16-byte load. They compute every lane; lanes at or above p.nb hold zeros.
+// The other batched kernels keep column c at c * ldv (ldc on the coarse level).
+template <typename T, int NB>
+constexpr bool kInterleaved = std::is_same_v<T, float> && NB == kRowBatch && kRowBatch == 4;
+
+template <typename T, int NB>
+__device__ __forceinline__ std::int64_t at(std::int64_t i, int c, std::int64_t ld) {
+    if constexpr (kInterleaved<T, NB>) {
+        return i * NB + c;
+    } else {
+        return i + c * ld;
+    }
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -35,10 +53,10 @@ __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDe
     }
 #pragma unroll
     for (int c = 0; c < NB; ++c) {
-        if (c >= p.nb) {
+        if (!kInterleaved<T, NB> && c >= p.nb) {
             break;
         }
-        const std::int64_t k = i + c * p.ldv;
+        const std::int64_t k = at<T, NB>(i, c, p.ldv);
         switch (p.mode) {
         case kIluPivot:
             p.y[k] = d - in[c];
@@ -83,7 +101,7 @@ __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDe
         case kResidualRestrict: {
             const T r = p.b[k] - (d * p.x[k] - in[c]);
             if (ci >= 0) {
-                atomicAdd(p.coarse + ci + c * p.ldc, r);
+                atomicAdd(p.coarse + at<T, NB>(ci, c, p.ldc), r);
             } else {
                 p.aux[k] = r;
             }
@@ -106,8 +124,8 @@ __device__ __forceinline__ void transfer_row(const RowParams<T> &p, const Sector
         if (p.mode == kProlong) {
 #pragma unroll
             for (int c = 0; c < NB; ++c) {
-                if (c < p.nb) {
-                    p.y[i + c * p.ldv] = T(0);
+                if (kInterleaved<T, NB> || c < p.nb) {
+                    p.y[at<T, NB>(i, c, p.ldv)] = T(0);
                 }
             }
         }
@@ -118,16 +136,17 @@ __device__ __forceinline__ void transfer_row(const RowParams<T> &p, const Sector
         coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, p.mode == kRestrict ? nullptr : &w);
 #pragma unroll
     for (int c = 0; c < NB; ++c) {
-        if (c >= p.nb) {
+        if (!kInterleaved<T, NB> && c >= p.nb) {
             break;
         }
-        const std::int64_t k = i + c * p.ldv;
+        const std::int64_t k = at<T, NB>(i, c, p.ldv);
+        const std::int64_t kc = at<T, NB>(ci, c, p.ldc);
         if (p.mode == kRestrict) {
-            atomicAdd(p.coarse + ci + c * p.ldc, p.x[k]);
+            atomicAdd(p.coarse + kc, p.x[k]);
         } else if (p.mode == kProlongAdd) {
-            p.y[k] += static_cast<T>(w) * p.coarse[ci + c * p.ldc];
+            p.y[k] += static_cast<T>(w) * p.coarse[kc];
         } else {
-            p.y[k] = static_cast<T>(w) * p.coarse[ci + c * p.ldc];
+            p.y[k] = static_cast<T>(w) * p.coarse[kc];
         }
     }
 }
@@ -188,6 +207,29 @@ __device__ __forceinline__ void row_terms(const RowParams<T> &p, const SectorDes
                                          [&](int j, T a, T) { in[0] += a * xs[j]; });
             return;
         }
+    }
+    if constexpr (kInterleaved<T, NB>) {
+        // the kRowBatch source values of an in-jump in one 16-byte load
+        visit_row<T, NS, TMAX, true>(
+            p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, nlanes, exit, leak,
+            [&](int j, T a, T) {
+                const std::int64_t k = static_cast<std::int64_t>(j) * NB;
+                if (mode != kIluThird) {
+                    const float4 v = *reinterpret_cast<const float4 *>(xs + k);
+                    in[0] += a * v.x;
+                    in[1] += a * v.y;
+                    in[2] += a * v.z;
+                    in[3] += a * v.w;
+                }
+                if (mode == kIluSecond || mode == kIluThird) {
+                    const float4 u = *reinterpret_cast<const float4 *>(ax + k);
+                    in2[0] += a * u.x;
+                    in2[1] += a * u.y;
+                    in2[2] += a * u.z;
+                    in2[3] += a * u.w;
+                }
+            });
+        return;
     }
     visit_row<T, NS, TMAX, true>(p.B, p.sectors, sec, p.md, local, st, lane == 0, lane, nlanes,
                                  exit, leak, [&](int j, T a, T) {
