@@ -223,6 +223,18 @@ int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_
 /* the same with host vectors: copies in, solves, copies out */
 int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
                          mk_solver_result *result, void *stream);
+/* Time stepping by repeated resolvents (no counterpart in the library; the paper driver's
+ * integrators, rdme/cpp/rdme_full_multigrid.cpp:1173-1238), on the device vector d_p of the
+ * solver's size, in place. With the solver's shift s:
+ *   integrator 0, backward Euler: p <- (s I - Q)^{-1} (s p), one step of length 1/s;
+ *   integrator 1, Crank-Nicolson with a Rannacher start (s = 2/dt): two backward-Euler steps of
+ *     length dt/2, then p <- (s I - Q)^{-1} (2 s p - (s I - Q) p) per step of length dt;
+ *     `steps` counts the steps of length dt, so steps + 1 solves run.
+ * Each solve starts from the current p and stops at ||rhs - A p|| <= rel_tolerance * ||rhs||;
+ * results[k] (optional, steps + integrator entries) reports solve k. Stops at the first solve
+ * that does not converge and returns its status. */
+int mk_solver_time_steps(mk_solver solver, int integrator, int steps, double rel_tolerance,
+                         double *d_p, mk_solver_result *results, void *stream);
 
 /* Several resolvent solves of one system at once (no counterpart in the reference; each column
  * is num::gmres(A, M, b, x)): flexible GMRES advancing up to `width` right-hand sides in

@@ -222,6 +222,7 @@ SIGNATURES = {
     "mk_solver_set_tolerance": (C.c_int, [P, C.c_double]),
     "mk_solver_solve": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
     "mk_solver_solve_host": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
+    "mk_solver_time_steps": (C.c_int, [P, C.c_int, C.c_int, C.c_double, P, C.POINTER(SolverResult), P]),
     "mk_batch_solver_create": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.c_int, C.POINTER(P)]),
     "mk_batch_solver_destroy": (None, [P]),
     "mk_batch_solver_solve": (C.c_int, [P, P, P, I64, C.c_int, DP, C.POINTER(SolverResult), P]),

@@ -513,6 +513,19 @@ class solver(_Handle):
         )
         return solver_result(r.iterations, r.residual, bool(r.converged), r.status)
 
+    def time_steps(self, p, steps: int, integrator: str = "be", rel_tolerance: float = 1e-10,
+                   stream=None) -> list:
+        """Advance the device vector p in place by `steps` steps of backward Euler ("be", step
+        1/shift) or Crank-Nicolson with a Rannacher start ("cn", shift = 2/dt, step dt), each
+        solve to rel_tolerance; returns one solver_result per solve."""
+        kind = {"be": 0, "cn": 1}[integrator]
+        n = max(1, steps + (kind if steps > 0 else 0))
+        rs = (SolverResult * n)()
+        check(load().mk_solver_time_steps(self._h, kind, int(steps), float(rel_tolerance), _ptr(p), rs,
+                                          _stream(stream)), allow=(_lib.MK_ENOTCONV,))
+        return [solver_result(r.iterations, r.residual, bool(r.converged), r.status)
+                for r in rs[: steps + (kind if steps > 0 else 0)]]
+
 
 class batch_solver(_Handle):
     """Flexible GMRES for up to `width` right-hand sides of one system at once: one batched

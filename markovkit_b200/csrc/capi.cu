@@ -589,6 +589,56 @@ int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_
     return fill_result(r, result);
 }
 
+int mk_solver_time_steps(mk_solver solver, int integrator, int steps, double rel_tolerance,
+                         double *d_p, mk_solver_result *results, void *stream) {
+    int status = MK_OK;
+    const int rc = guarded([&] {
+        MK_REQUIRE(solver && d_p, "null argument");
+        MK_REQUIRE(integrator == 0 || integrator == 1, "integrator must be 0 (backward Euler) or 1 (Crank-Nicolson)");
+        MK_REQUIRE(steps >= 0, "steps must be non-negative");
+        MK_REQUIRE(rel_tolerance > 0.0 && std::isfinite(rel_tolerance), "rel_tolerance must be positive");
+        const Generator &A = *solver->gen->gen;
+        const int64_t n = A.op.n;
+        const double s = solver->shift;
+        cudaStream_t st = as_stream(stream);
+        if (solver->b.size() != static_cast<std::size_t>(n)) {
+            solver->b.resize(n);
+            solver->x.resize(n);
+        }
+        DeviceArray<double> tmp(static_cast<std::size_t>(n)), partials(kDotBlocks), norm2(1);
+        double *rhs = solver->b.get(), *x = solver->x.get();
+        const std::size_t bytes = static_cast<std::size_t>(n) * sizeof(double);
+        const int solves = steps + (integrator == 1 && steps > 0 ? 1 : 0);
+        for (int k = 0; k < solves; ++k) {
+            check_cuda(cudaMemsetAsync(rhs, 0, bytes, st), "rhs");
+            if (integrator == 1 && k >= 2) {
+                // rhs = 2 s p - (s I - Q) p
+                check_cuda(cudaMemsetAsync(tmp.get(), 0, bytes, st), "rhs");
+                check_cuda(axpy(2.0 * s, d_p, tmp.get(), n, st), "rhs");
+                A.apply<double>(kResidual, s, d_p, tmp.get(), rhs, nullptr, st);
+            } else {
+                check_cuda(axpy(s, d_p, rhs, n, st), "rhs");
+            }
+            check_cuda(dot(rhs, rhs, n, partials.get(), norm2.get(), st), "norm");
+            double nr2 = 0.0;
+            check_cuda(cudaMemcpyAsync(&nr2, norm2.get(), sizeof nr2, cudaMemcpyDeviceToHost, st), "norm");
+            check_cuda(cudaMemcpyAsync(x, d_p, bytes, cudaMemcpyDeviceToDevice, st), "guess");
+            check_cuda(cudaStreamSynchronize(st), "sync");
+            GmresOptions o = solver->opt;
+            o.tolerance = rel_tolerance * std::sqrt(nr2);
+            const SolverResult r = gmres(A, s, solver->mg ? solver->mg->mg.get() : nullptr, rhs, x,
+                                         o, *solver->ws, st);
+            check_cuda(cudaMemcpyAsync(d_p, x, bytes, cudaMemcpyDeviceToDevice, st), "step");
+            check_cuda(cudaStreamSynchronize(st), "sync");
+            status = fill_result(r, results ? results + k : nullptr);
+            if (status != MK_OK) {
+                return;
+            }
+        }
+    });
+    return rc != MK_OK ? rc : status;
+}
+
 int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
                          mk_solver_result *result, void *stream) {
     SolverResult r;
