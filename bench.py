@@ -142,7 +142,9 @@ class ClockSampler:
         }
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE / MASTER_*); a short
+    process-group timeout so that ranks waiting on a lost peer end with an error."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -151,8 +153,40 @@ def dist_setup():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def dist_teardown(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        if dist.is_initialized():
+            dist.destroy_process_group()
+
+
+def replica_seeds(base: int, rank: int, count: int) -> list[int]:
+    """The right-hand-side seeds of one replica: each rank solves its own, disjoint stream."""
+    return [base + 1_000_003 * rank + s for s in range(count)]
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The slowest rank's time: whole-job throughput is all ranks' work over this."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_ours(args) -> dict | None:
@@ -176,7 +210,7 @@ def run_ours(args) -> dict | None:
 
     # right-hand sides resident in HBM (each rank its own stream of seeds)
     K, W = args.steps, args.warmup
-    seeds = [w["seed"] + 1_000_003 * rank + s for s in range(W + K)]
+    seeds = replica_seeds(w["seed"], rank, W + K)
     host_b = [rhs_of(w, s, N) for s in seeds]
     dev_b = [torch.from_numpy(b).to(dev) for b in host_b]
     bnorm = [float(np.linalg.norm(b)) for b in host_b]
@@ -234,8 +268,7 @@ def run_ours(args) -> dict | None:
     for precision in ("fp32", "fp64"):
         M, solver = make_solver(precision)
         solve_all(solver, range(W))
-        if world > 1:
-            torch.distributed.barrier()
+        barrier(world)
         torch.cuda.synchronize()
         sampler = ClockSampler(_uuid(dev)) if precision == "fp32" else None
         if sampler:
@@ -247,11 +280,7 @@ def run_ours(args) -> dict | None:
         if sampler:
             sampler.__exit__(None, None, None)
         worst = max(true_rel(x, W + i) for i, x in enumerate(xs))
-        total_ms = sum(lat)
-        if world > 1:
-            t = torch.tensor([total_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = max_over_ranks(sum(lat), world, dev)
         results[precision] = dict(
             lat=lat, its=its, converged=all(conv), worst_true_rel=worst, total_ms=total_ms,
             clocks=sampler.summary() if sampler else None, M=M, solver=solver, xs=xs,
@@ -260,11 +289,7 @@ def run_ours(args) -> dict | None:
         if precision == "fp32":
             # e2e through the C ABI with host buffers
             lat_h, its_h, conv_h, xs_h = solve_all(solver, range(W, W + K), host_side=True)
-            total_h = sum(lat_h)
-            if world > 1:
-                t = torch.tensor([total_h], device=dev)
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                total_h = float(t.item())
+            total_h = max_over_ranks(sum(lat_h), world, dev)
             results["e2e"] = dict(lat=lat_h, total_ms=total_h, converged=all(conv_h),
                                   worst_true_rel=max(true_rel(x, W + i) for i, x in enumerate(xs_h)))
             # the same solution as the FP64 oracle path is checked below
@@ -282,6 +307,7 @@ def run_ours(args) -> dict | None:
     # the mixed serving workload runs on one GPU only (it is a per-device measurement)
     served_mix = serve_mix_measure() if world == 1 and not args.no_serve_mix else None
 
+    dist_teardown(world)
     if rank != 0:
         return None
     solves = world * K
