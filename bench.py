@@ -12,6 +12,13 @@ with the right-hand sides already resident in HBM (device-timed with CUDA events
 between steps, max over ranks); `e2e` is the same through the C ABI with host buffers, the
 host->device copy of b and device->host copy of x inside the timed region.
 
+Beside it: `fp64_path` (the plain FP64 drop-in path, one request at a time), `served` (64
+requests of the same workload through the request loop, FP32 path batched four wide against
+the FP64 path; `fp32_over_plain_fp64_path` is the serving speed-up), `served_mix` (one GPU only:
+the seeded serving workload of markovkit_b200.inputs.serving_requests, Poisson arrivals over
+mixed models of up to 186,043,585 states), `roofline` (the generator SpMV on the 3-D 16^3 box of
+cap 2) and `cpu_baseline`.
+
 Multi-GPU: independent replicas (one resident solver per rank, each solving its own
 right-hand sides; no collective on the data path), weak scaling.
 
