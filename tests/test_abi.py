@@ -76,3 +76,23 @@ def test_server_options_are_checked_before_device_work(lib_built):
     h = C.c_void_p()
     assert lib.mk_server_create(C.byref(o), C.byref(h)) == _lib.MK_EINVAL
     assert b"slots" in lib.mk_last_error()
+
+
+def test_matrix_and_time_step_arguments_checked_before_device_work(lib_built):
+    """The assembled-generator and time-stepping entry points reject missing handles and bad
+    arguments with MK_EINVAL and a message, before touching a device."""
+    import ctypes as C
+
+    from markovkit_b200 import _lib
+
+    lib = _lib.load()
+    m = C.c_void_p()
+    assert lib.mk_generator_matrix(None, C.byref(m), None) == _lib.MK_EINVAL
+    assert lib.mk_generator_characteristic_matrix(None, 0.5, C.byref(m), None) == _lib.MK_EINVAL
+    n = C.c_int64()
+    assert lib.mk_generator_n_jumps(None, C.byref(n), None) == _lib.MK_EINVAL
+    rows, nnz = C.c_int64(), C.c_int64()
+    assert lib.mk_csr_size(None, C.byref(rows), C.byref(nnz)) == _lib.MK_EINVAL
+    lib.mk_csr_destroy(None)  # a null handle is ignored
+    assert lib.mk_solver_time_steps(None, 0, 1, 1e-10, None, None, None) == _lib.MK_EINVAL
+    assert b"null" in lib.mk_last_error()
