@@ -1,40 +1,48 @@
 #!/usr/bin/env python
 """Resolvent solves/sec at 1e-10 relative true residual on B200: FP32-multigrid-preconditioned
-FP64 flexible GMRES (the served path) beside the plain FP64 GMRES + FP64 multigrid path.
+FP64 flexible GMRES beside the plain FP64 GMRES + FP64 multigrid path.
 
-Workload (default): two-particle annihilation A + B -> 0 on a 2-D 32 x 32 grid, h = 1/32,
-D_A = D_B = 1, reaction 10 / voxel volume on a shared voxel, population_box(1024, {1, 1})
-(N = 1,050,625 states), shift s = 1, Dirichlet(1) right-hand sides from a seeded counter
-generator, GMRES(30) with sector_multigrid, tolerance 1e-10 * ||b||.
+Workload (default; the largest single-GPU configuration): single-species birth-death on the
+3-D 16 x 16 x 16 grid, h = 1/16, D = 1, birth 0.05 * voxel volume, death 0.02 * n,
+population_box(4096, {2}) (N = 8,394,753 states), shift s = 0.5, right-hand sides Uniform(0, 1)
+normalised to sum 1 from a seeded counter generator, GMRES(30), tolerance 1e-10 * ||b||. The
+FP32 path is flexible GMRES(30) around a sector multigrid whose smoothers, transfers and coarse
+solves all run in FP32 (smoother FP32_SMOOTHER); the plain FP64 path is GMRES(30) around the
+reference's default multigrid (weighted Jacobi 2/2, coarsest 4) in FP64.
 
-One step = one resolvent solve of a fresh right-hand side. `value` is whole-job solves/sec
-with the right-hand sides already resident in HBM (device-timed with CUDA events, L2 flushed
-between steps, max over ranks); `e2e` is the same through the C ABI with host buffers, the
-host->device copy of b and device->host copy of x inside the timed region.
+One step = one resolvent solve of a fresh right-hand side. `value` is whole-job solves/sec with
+the right-hand sides already resident in HBM (device-timed with CUDA events, inputs larger than
+L2 and L2 flushed between steps, max over ranks); `e2e` is the same through the C ABI with host
+buffers, the host->device copy of b and device->host copy of x inside the timed region.
 
-Beside it: `fp64_path` (the plain FP64 drop-in path, one request at a time), `served` (64
-requests of the same workload through the request loop, FP32 path batched four wide against
-the FP64 path; `fp32_over_plain_fp64_path` is the serving speed-up), `served_mix` (one GPU only:
-the seeded serving workload of markovkit_b200.inputs.serving_requests, Poisson arrivals over
-mixed models of up to 186,043,585 states), `roofline` (the generator SpMV on the 3-D 16^3 box of
-cap 2) and `cpu_baseline`.
+Beside it: `fp64_path`; `rel_error_vs_oracle` (each path's solution against the FP64 solution of
+the matrix-free CPU port of the reference's path, oracle/_ref/mf_port, for the first timed
+right-hand side); `fp32_smoothers` (the FP32 path with each smoother); `secondary` (the 2-D 32 x 32
+two-particle annihilation box of 1,050,625 states); `served` (requests of the workload through the
+request loop, batched four wide); `served_mix` (the seeded serving workload of
+markovkit_b200.inputs.serving_requests against the plain FP64 path on the same arrivals);
+`fsp_batch` (512 Krylov-FSP propagations in one persistent launch, with its CPU baseline);
+`roofline` (the generator SpMV of the workload) and `cpu_baseline`.
 
 Multi-GPU: independent replicas (one resident solver per rank, each solving its own
-right-hand sides; no collective on the data path), weak scaling.
+right-hand sides; no collective on the data path), weak scaling. `--gpus N` outside torchrun
+re-launches itself under torchrun with N ranks.
 
---impl reference times the reference's own CPU implementation (MarkovKit's headers compiled
-against the numerics shim, oracle/_ref/ref_driver) on this host's cores, rank 0 only.
+--impl reference times the reference's CPU path on this host's cores, rank 0 only: for the
+default workload the matrix-free port (the reference's own containers need ~275 GB and days of
+single-threaded set-up at 8.4M states), for the 2-D workload the reference's own headers compiled
+against the numerics shim (oracle/_ref/ref_driver).
 """
 
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from pathlib import Path
 
@@ -60,11 +68,14 @@ WORKLOADS = {
         rhs="uniform", seed=2,
     ),
 }
-DEFAULT_WORKLOAD = "annihilation_2d32"
+DEFAULT_WORKLOAD = "birth_death_3d16"
+SECONDARY_WORKLOAD = "annihilation_2d32"
 REL_TOL = 1e-10
 RESTART = 30
+FP32_SMOOTHER = "gauss_seidel"
 FP32_COARSEST = 256
 L2_FLUSH_BYTES = 256 << 20
+METRIC = "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)"
 
 
 def peaks() -> dict:
@@ -89,6 +100,20 @@ def rhs_of(w: dict, seed: int, n: int) -> np.ndarray:
     from markovkit_b200.inputs import dirichlet_rhs, uniform_rhs
 
     return dirichlet_rhs(seed, n) if w["rhs"] == "dirichlet" else uniform_rhs(seed, n)
+
+
+def problem_of(mk, w: dict):
+    dims = [w["cells"]] * w["dim"]
+    h = 1.0 / w["cells"]
+    dom = mk.voxel_domain(mk.grid(dims, [h] * w["dim"]), w["D"])
+    model = mk.reaction_diffusion(dom, [mk.local_reaction(c, f) for c, f in reactions_of(w)])
+    box = mk.population_box(int(np.prod(dims)), w["caps"])
+    return dom, model, box
+
+
+def pct(values, p):
+    v = sorted(values)
+    return v[min(len(v) - 1, int(round(p / 100 * (len(v) - 1))))]
 
 
 class ClockSampler:
@@ -205,12 +230,7 @@ def run_ours(args) -> dict | None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     w = WORKLOADS[args.workload]
-    dims = [w["cells"]] * w["dim"]
-    h = 1.0 / w["cells"]
-    dom = mk.voxel_domain(mk.grid(dims, [h] * w["dim"]), w["D"])
-    model = mk.reaction_diffusion(dom, [mk.local_reaction(c, f) for c, f in reactions_of(w)])
-    V = int(np.prod(dims))
-    box = mk.population_box(V, w["caps"])
+    dom, model, box = problem_of(mk, w)
     Q = mk.generator(box, model, "absorbing")
     A = mk.shifted_generator(Q, w["shift"])
     N = box.size()
@@ -221,113 +241,81 @@ def run_ours(args) -> dict | None:
     host_b = [rhs_of(w, s, N) for s in seeds]
     dev_b = [torch.from_numpy(b).to(dev) for b in host_b]
     bnorm = [float(np.linalg.norm(b)) for b in host_b]
+    pinned_b = [torch.from_numpy(b).pin_memory() for b in host_b]
+    pinned_x = torch.zeros(N, dtype=torch.float64).pin_memory()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-
-    def make_solver(precision: str):
-        # the FP32 path uses a dense solve for sectors of at most 256 states; the FP64 path
-        # keeps the reference's multigrid_options (coarsest 4)
-        mo = (mk.multigrid_options(precision="fp32", coarsest_size=FP32_COARSEST) if precision == "fp32"
-              else mk.multigrid_options(precision="fp64"))
-        M = mk.sector_multigrid(dom, box, w["shift"], mo)
-        opts = mk.gmres_options(tolerance=REL_TOL * bnorm[0], max_iterations=2000, restart=RESTART,
-                                flexible=(precision == "fp32"))
-        return M, mk.solver(A, M, opts)
-
-    def solve_all(solver, steps, host_side=False):
-        lat, its, res = [], [], []
-        xs = []
-        stream = torch.cuda.current_stream()
-        for s in steps:
-            opts_tol = REL_TOL * bnorm[s]
-            _set_tolerance(solver, opts_tol)
-            flush.zero_()
-            x = torch.zeros(N, dtype=torch.float64, device=dev)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            if host_side:
-                hb = pinned_b[s]
-                hx = pinned_x
-                hx.zero_()
-                e0.record(stream)
-                r = solver.solve_host(hb.numpy(), hx.numpy())
-                e1.record(stream)
-                x = hx.to(dev)
-            else:
-                e0.record(stream)
-                r = solver.solve(dev_b[s], x)
-                e1.record(stream)
-            e1.synchronize()
-            lat.append(e0.elapsed_time(e1))
-            its.append(r.iterations)
-            res.append(r.converged)
-            xs.append(x)
-        return lat, its, res, xs
 
     def true_rel(x, s):
         r = torch.empty_like(x)
         A.apply(x, r)
         return float(torch.linalg.norm(dev_b[s] - r)) / bnorm[s]
 
-    pinned_b = [torch.from_numpy(b).pin_memory() for b in host_b]
-    pinned_x = torch.zeros(N, dtype=torch.float64).pin_memory()
-
     results = {}
-    for precision in ("fp32", "fp64"):
-        M, solver = make_solver(precision)
-        solve_all(solver, range(W))
+    for key, (precision, smoother, coarsest) in PATHS.items():
+        solver = make_solver(mk, A, dom, box, w["shift"], precision, smoother, coarsest, bnorm[0])
+        solve_steps(solver, dev_b, bnorm, flush, range(W), dev)
         barrier(world)
         torch.cuda.synchronize()
-        sampler = ClockSampler(_uuid(dev)) if precision == "fp32" else None
+        sampler = ClockSampler(_uuid(dev)) if key == "fp32" else None
         if sampler:
             sampler.__enter__()
         launches0 = mk.api.kernel_launches()
-        lat, its, conv, xs = solve_all(solver, range(W, W + K))
+        lat, its, conv, xs = solve_steps(solver, dev_b, bnorm, flush, range(W, W + K), dev)
         torch.cuda.synchronize()
         launches = mk.api.kernel_launches() - launches0
         if sampler:
             sampler.__exit__(None, None, None)
-        worst = max(true_rel(x, W + i) for i, x in enumerate(xs))
-        total_ms = max_over_ranks(sum(lat), world, dev)
-        results[precision] = dict(
-            lat=lat, its=its, converged=all(conv), worst_true_rel=worst, total_ms=total_ms,
-            clocks=sampler.summary() if sampler else None, M=M, solver=solver, xs=xs,
-            launches=launches,
-        )
-        if precision == "fp32":
-            # e2e through the C ABI with host buffers
-            lat_h, its_h, conv_h, xs_h = solve_all(solver, range(W, W + K), host_side=True)
-            total_h = max_over_ranks(sum(lat_h), world, dev)
-            results["e2e"] = dict(lat=lat_h, total_ms=total_h, converged=all(conv_h),
-                                  worst_true_rel=max(true_rel(x, W + i) for i, x in enumerate(xs_h)))
-            # the same solution as the FP64 oracle path is checked below
+        res = dict(lat=lat, its=its, converged=all(conv), total_ms=max_over_ranks(sum(lat), world, dev),
+                   worst_true_rel=max(true_rel(x, W + i) for i, x in enumerate(xs)),
+                   clocks=sampler.summary() if sampler else None, launches=launches,
+                   x_first=xs[0].cpu().numpy())
+        if key == "fp32":
+            # e2e through the C ABI with host buffers: b in and x out every step
+            lat_h = []
+            for s in range(W, W + K):
+                solver.set_tolerance(REL_TOL * bnorm[s])
+                flush.zero_()
+                pinned_x.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                stream = torch.cuda.current_stream()
+                e0.record(stream)
+                solver.solve_host(pinned_b[s].numpy(), pinned_x.numpy())
+                e1.record(stream)
+                e1.synchronize()
+                lat_h.append(e0.elapsed_time(e1))
+            res["e2e_ms"] = max_over_ranks(sum(lat_h), world, dev)
+            res["e2e_true_rel"] = true_rel(pinned_x.to(dev), W + K - 1)
+        results[key] = res
+        del solver, xs
+        torch.cuda.empty_cache()
 
-    # error of each FP32-MG solution against the FP64 path's solution of the same right-hand side
-    r32 = results["fp32"]
-    r64 = results["fp64"]
-    err_vs_fp64 = max(
-        float(torch.linalg.norm(a - b64) / torch.linalg.norm(b64)) for a, b64 in zip(r32["xs"], r64["xs"])
-    )
-
-    roof = roofline(mk, Q, M=results["fp32"]["M"], dev=dev, N=N)
-    launches = r32["launches"]
-    served = serve_measure(mk, box, model, w, host_b, W, K)
-    # the mixed serving workload runs on one GPU only (it is a per-device measurement)
-    served_mix = serve_mix_measure() if world == 1 and not args.no_serve_mix else None
-
+    # the FP32 path with each smoother, a few solves each
+    smoothers = {}
+    for sm in ("jacobi", "gauss_seidel", "ilu0"):
+        solver = make_solver(mk, A, dom, box, w["shift"], "fp32", sm, FP32_COARSEST, bnorm[0])
+        solve_steps(solver, dev_b, bnorm, flush, range(1), dev)
+        n_s = min(K, 5)
+        lat, its, conv, xs = solve_steps(solver, dev_b, bnorm, flush, range(W, W + n_s), dev)
+        smoothers[sm] = {"value": round(world * n_s / (max_over_ranks(sum(lat), world, dev) / 1e3), 3),
+                         "unit": "solves/s", "iterations_median": int(np.median(its)),
+                         "worst_true_rel_residual": max(true_rel(x, W + i) for i, x in enumerate(xs)),
+                         "all_converged": all(conv)}
+        del solver, xs
+    roof = roofline(mk, Q, dev, N, w)
+    secondary = None if args.no_secondary else secondary_line(mk, args, world, rank, dev)
+    served = None if args.no_serve else serve_measure(mk, box, model, w, host_b, W, K)
+    served_mix = serve_mix_measure(mk) if world == 1 and not args.no_serve_mix else None
+    fsp = fsp_batch_measure(rank == 0 and world == 1 and not args.no_cpu_baseline) if not args.no_fsp else None
     dist_teardown(world)
     if rank != 0:
         return None
+
+    r32, r64 = results["fp32"], results["fp64"]
     solves = world * K
-    value = solves / (r32["total_ms"] / 1e3)
-    e2e_value = solves / (results["e2e"]["total_ms"] / 1e3)
-    lat_sorted = sorted(r32["lat"])
-
-    def pct(p):
-        return lat_sorted[min(len(lat_sorted) - 1, int(round(p / 100 * (len(lat_sorted) - 1))))]
-
     line = {
-        "metric": "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)",
-        "value": round(value, 3),
+        "metric": METRIC,
+        "value": round(solves / (r32["total_ms"] / 1e3), 3),
         "unit": "solves/s",
         "n_gpus": world,
         "steps": K,
@@ -337,46 +325,129 @@ def run_ours(args) -> dict | None:
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64 (Krylov) + f32 (multigrid)",
-        "data": "synthetic: seeded Dirichlet(1) right-hand sides; model built from its definition",
+        "data": "synthetic: seeded right-hand sides; model built from its definition",
         "config": {
-            "workload": w["workload"], "states": N, "voxels": V, "shift": w["shift"],
+            "workload": w["workload"], "states": N, "voxels": box.n_voxels(), "shift": w["shift"],
             "gmres_restart": RESTART, "tolerance": "1e-10 relative true residual",
-            "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
+            "fp32_multigrid": f"smoother {FP32_SMOOTHER}, dense solve of sectors <= {FP32_COARSEST} states",
+            "parallelism": f"replicas x{world}",
+            "l2": f"inputs of {N * 8 / 1e6:.0f} MB per vector and L2 flushed between steps (256 MiB write)",
         },
-        "latency_ms": {"p50": round(pct(50), 4), "p99": round(pct(99), 4)},
+        "latency_ms": {"p50": round(pct(r32["lat"], 50), 4), "p99": round(pct(r32["lat"], 99), 4)},
         "iterations": {"median": int(np.median(r32["its"])), "max": int(max(r32["its"]))},
         "worst_true_rel_residual": r32["worst_true_rel"],
-        "rel_error_vs_fp64_path": err_vs_fp64,
+        "all_converged": r32["converged"],
+        "rel_error_fp32_vs_fp64_path": float(np.linalg.norm(r32["x_first"] - r64["x_first"]) /
+                                             np.linalg.norm(r64["x_first"])),
         "fp64_path": {
-            "value": round(world * K / (r64["total_ms"] / 1e3), 3),
+            "value": round(solves / (r64["total_ms"] / 1e3), 3),
             "unit": "solves/s",
             "ms_per_step": round(r64["total_ms"] / K, 4),
+            "latency_ms": {"p50": round(pct(r64["lat"], 50), 4), "p99": round(pct(r64["lat"], 99), 4)},
             "iterations_median": int(np.median(r64["its"])),
             "worst_true_rel_residual": r64["worst_true_rel"],
+            "multigrid": "the reference's multigrid_options (weighted Jacobi 2/2, coarsest 4), FP64 GMRES(30)",
         },
+        "fp32_over_fp64_path": round(r64["total_ms"] / r32["total_ms"], 3),
         "e2e": {
-            "value": round(e2e_value, 3),
+            "value": round(solves / (r32["e2e_ms"] / 1e3), 3),
             "unit": "solves/s",
-            "h2d_bytes_per_step": N * 8 * 2,
+            "h2d_bytes_per_step": N * 8,
             "d2h_bytes_per_step": N * 8,
+            "worst_true_rel_residual": r32["e2e_true_rel"],
         },
+        "fp32_smoothers": smoothers,
+        "secondary": secondary,
         "served": served,
         "served_mix": served_mix,
+        "fsp_batch": fsp,
         "roofline": roof,
-        "gpu_launches": launches,
+        "gpu_launches": r32["launches"],
         "clocks": r32["clocks"],
     }
-    # the served path against the plain FP64 drop-in path (one stream, one request at a time)
-    served["fp32_over_plain_fp64_path"] = round(served["fp32"]["value"] / line["fp64_path"]["value"], 3)
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w)
+    if served:
+        served["fp32_over_plain_fp64_path"] = round(served["fp32"]["value"] / line["fp64_path"]["value"], 3)
+    if not args.no_cpu_baseline and world == 1:
+        cb, x_port = cpu_baseline(w, seeds[W])
+        line["cpu_baseline"] = cb
+        if x_port is not None:
+            nrm = float(np.linalg.norm(x_port))
+            line["rel_error_vs_oracle"] = {
+                "fp32_path": float(np.linalg.norm(r32["x_first"] - x_port)) / nrm,
+                "fp64_path": float(np.linalg.norm(r64["x_first"] - x_port)) / nrm,
+                "oracle": "oracle/_ref/mf_port FP64 solution of the first timed right-hand side "
+                          "(the reference's path restated matrix-free, GMRES(30) to 1e-10)",
+            }
     print(json.dumps(line), flush=True)
     return line
 
 
+# headline FP32 path and the plain FP64 drop-in path: (precision, smoother, coarsest sector size)
+PATHS = {"fp32": ("fp32", FP32_SMOOTHER, FP32_COARSEST), "fp64": ("fp64", "jacobi", 4)}
+
+
+def make_solver(mk, A, dom, box, shift, precision, smoother, coarsest, bnorm0):
+    mo = mk.multigrid_options(precision=precision, smoother=smoother, coarsest_size=coarsest)
+    M = mk.sector_multigrid(dom, box, shift, mo)
+    opts = mk.gmres_options(tolerance=REL_TOL * bnorm0, max_iterations=2000, restart=RESTART,
+                            flexible=(precision == "fp32"))
+    s = mk.solver(A, M, opts)
+    return s
+
+
+def solve_steps(solver, dev_b, bnorm, flush, steps, dev):
+    """One device-timed solve per step from x = 0 (CUDA events on the launching stream, L2
+    flushed before each); returns latencies (ms), iterations, convergence flags, solutions."""
+    import torch
+
+    lat, its, conv, xs = [], [], [], []
+    stream = torch.cuda.current_stream()
+    for s in steps:
+        solver.set_tolerance(REL_TOL * bnorm[s])
+        flush.zero_()
+        x = torch.zeros_like(dev_b[s])
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = solver.solve(dev_b[s], x)
+        e1.record(stream)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+        its.append(r.iterations)
+        conv.append(r.converged)
+        xs.append(x)
+    return lat, its, conv, xs
+
+
+def secondary_line(mk, args, world, rank, dev) -> dict:
+    """The 2-D two-particle annihilation box (1,050,625 states): both paths, a few solves."""
+    import torch
+
+    w = WORKLOADS[SECONDARY_WORKLOAD]
+    dom, model, box = problem_of(mk, w)
+    Q = mk.generator(box, model, "absorbing")
+    A = mk.shifted_generator(Q, w["shift"])
+    N = box.size()
+    n_s = 10
+    seeds = replica_seeds(w["seed"], rank, 3 + n_s)
+    host_b = [rhs_of(w, s, N) for s in seeds]
+    dev_b = [torch.from_numpy(b).to(dev) for b in host_b]
+    bnorm = [float(np.linalg.norm(b)) for b in host_b]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    out = {"workload": w["workload"], "states": N, "shift": w["shift"]}
+    for key, (precision, smoother, coarsest) in PATHS.items():
+        solver = make_solver(mk, A, dom, box, w["shift"], precision, smoother, coarsest, bnorm[0])
+        solve_steps(solver, dev_b, bnorm, flush, range(3), dev)
+        lat, its, conv, xs = solve_steps(solver, dev_b, bnorm, flush, range(3, 3 + n_s), dev)
+        out[key] = {"value": round(world * n_s / (max_over_ranks(sum(lat), world, dev) / 1e3), 3),
+                    "unit": "solves/s", "p50_ms": round(pct(lat, 50), 4),
+                    "iterations_median": int(np.median(its)), "all_converged": all(conv)}
+    out["fp32_over_fp64_path"] = round(out["fp32"]["value"] / out["fp64"]["value"], 3)
+    return out
+
+
 SERVE_SLOTS = 4
-SERVE_REQUESTS = 64
-SERVE_RESTART = 15  # a batched step's Gram-Schmidt cost grows with the basis; 15 served best
+SERVE_REQUESTS = 32
 
 
 def serve_measure(mk, box, model, w, host_b, W, K) -> dict:
@@ -384,18 +455,18 @@ def serve_measure(mk, box, model, w, host_b, W, K) -> dict:
     through the request loop (markovkit_b200.serve): all submitted at once to SERVE_SLOTS workers
     that overlap their solves on the device, host buffers in and out, after warm-up requests
     that make the resident solvers. Host wall clock from the first submit to the last
-    completion. The count keeps every slot busy for several rounds, so the number is the
-    loop's steady throughput rather than one round and its tail."""
+    completion."""
     from markovkit_b200.serve import server
 
     n = box.size()
     extra = [rhs_of(w, w["seed"] + 7_000_001 + k, n) for k in range(max(0, SERVE_REQUESTS - K))]
     reqs = (host_b[W:W + K] + extra)[:SERVE_REQUESTS]
     out = {}
-    # served path: FP32 multigrid, same-key requests batched four wide; the FP64 line is the
+    # served path: FP32 multigrid, same-problem requests batched four wide; the FP64 line is the
     # plain path through the same loop (no batching, the reference's multigrid options)
-    variants = {"fp32": dict(precision="fp32", batch=4, coarsest_size=FP32_COARSEST, restart=SERVE_RESTART),
-                "fp64": dict(precision="fp64", batch=1, coarsest_size=4, restart=RESTART)}
+    variants = {"fp32": dict(precision="fp32", batch=4, coarsest_size=FP32_COARSEST, restart=RESTART,
+                             smoother=FP32_SMOOTHER),
+                "fp64": dict(precision="fp64", batch=1, coarsest_size=4, restart=RESTART, smoother="jacobi")}
     for precision, kw in variants.items():
         with server(slots=SERVE_SLOTS, rel_tolerance=REL_TOL, **kw) as srv:
             pid = srv.register(box, model)
@@ -406,38 +477,40 @@ def serve_measure(mk, box, model, w, host_b, W, K) -> dict:
             tickets = [srv.submit(pid, w["shift"], b) for b in reqs]
             res = [srv.wait(t)[1] for t in tickets]
             wall = time.perf_counter() - t0
-            lat = sorted(r.latency_ms for r in res)
+            lat = [r.latency_ms for r in res]
             out[precision] = {
                 "value": round(len(reqs) / wall, 3),
                 "unit": "solves/s",
-                "p50_ms": round(lat[len(lat) // 2], 3),
-                "p99_ms": round(lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))], 3),
+                "p50_ms": round(pct(lat, 50), 3),
+                "p99_ms": round(pct(lat, 99), 3),
                 "worst_rel_residual": max(r.residual for r in res),
                 "all_converged": all(r.status == 0 for r in res),
             }
     out["slots"] = SERVE_SLOTS
     out["fp32_over_fp64"] = round(out["fp32"]["value"] / out["fp64"]["value"], 3)
     out["requests"] = len(reqs)
-    out["note"] = ("requests submitted at once; host b and x; resident solver per slot; fp32: "
-                   "batch 4, FGMRES(15), dense solve of sectors <= 256 states; fp64: batch 1, "
-                   "GMRES(30), the reference's multigrid options")
+    out["note"] = (f"requests submitted at once; host b and x; resident solver per slot; fp32: batch 4, "
+                   f"FGMRES({RESTART}), smoother {FP32_SMOOTHER}, dense solve of sectors <= {FP32_COARSEST} "
+                   f"states; fp64: batch 1, GMRES({RESTART}), the reference's multigrid options")
     return out
 
 
 MIX_COUNT = 24
-MIX_RATE = 20.0    # requests per second
-MIX_RESTART = 30   # the 1-D boxes of 10^7-10^8 states need ~75 FGMRES(15) steps, ~45 at 30
+MIX_RATE = 20.0  # requests per second
 
 
-def serve_mix_measure() -> dict:
+def serve_mix_measure(mk) -> dict:
     """The serving workload: MIX_COUNT seeded requests (markovkit_b200.inputs.serving_requests)
     with Poisson arrivals at MIX_RATE per second, models uniform over configurations 0-2 and 1-D
     birth-death boxes of 64-256 voxels and cap 2-4 (969 to 186,043,585 states), shifts
     log-uniform in [0.1, 10], Dirichlet(1) right-hand sides. Each request is submitted at its
     arrival time (host b and x); latency runs from submit to x on the host; solves/s is the count
-    over the wall time from the first arrival to the last completion. Shifts differ, so requests
-    never share a resident solver and no batching happens; the served FP32 path gains only by
-    overlapping SERVE_SLOTS solves and by its cheaper V-cycle."""
+    over the wall time from the first arrival to the last completion. The served FP32 path runs
+    SERVE_SLOTS slots with requests of one problem batched together whatever their shifts; the
+    plain FP64 path solves the requests one at a time in arrival order through the drop-in
+    solver (GMRES(30) + the reference's FP64 multigrid, set-up included in each latency)."""
+    import torch
+
     from markovkit_b200.inputs import serving_requests
     from markovkit_b200.serve import server, serving_problem
 
@@ -447,44 +520,160 @@ def serve_mix_measure() -> dict:
     sizes = {k: problems[k][0].size() for k in keys}
     bs = [rhs_of({"rhs": "dirichlet"}, r["rhs_seed"], sizes[(r["model"], r["voxels"], r["cap"])]) for r in reqs]
     out = {}
-    variants = {"fp32": dict(precision="fp32", slots=SERVE_SLOTS, batch=4, coarsest_size=FP32_COARSEST,
-                             restart=MIX_RESTART),
-                "fp64": dict(precision="fp64", slots=1, batch=1, coarsest_size=4, restart=RESTART)}
-    for precision, kw in variants.items():
-        with server(rel_tolerance=REL_TOL, **kw) as srv:
-            pids = {k: srv.register(*problems[k]) for k in keys}
-            t0 = time.perf_counter()
-            tickets = []
-            for r, b in zip(reqs, bs):
-                wait = r["arrival_s"] - (time.perf_counter() - t0)
-                if wait > 0:
-                    time.sleep(wait)
-                tickets.append(srv.submit(pids[(r["model"], r["voxels"], r["cap"])], r["shift"], b))
-            res = [srv.wait(t)[1] for t in tickets]
-            wall = time.perf_counter() - t0 - reqs[0]["arrival_s"]
-            st = srv.stats()
-        lat = sorted(r.latency_ms for r in res)
-        out[precision] = {
-            "value": round(len(res) / wall, 3),
-            "unit": "solves/s",
-            "p50_ms": round(lat[len(lat) // 2], 3),
-            "p99_ms": round(lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))], 3),
-            "worst_rel_residual": max(r.residual for r in res),
-            "all_converged": all(r.status == 0 for r in res),
-            "evictions": st["evictions"],
-            "memory_waits": st["memory_waits"],
-        }
-    out["fp32_over_fp64"] = round(out["fp32"]["value"] / out["fp64"]["value"], 3)
+    kw = dict(precision="fp32", slots=SERVE_SLOTS, batch=4, coarsest_size=FP32_COARSEST, restart=RESTART,
+              smoother=FP32_SMOOTHER)
+    with server(rel_tolerance=REL_TOL, **kw) as srv:
+        pids = {k: srv.register(*problems[k]) for k in keys}
+        t0 = time.perf_counter()
+        tickets = []
+        for r, b in zip(reqs, bs):
+            wait = r["arrival_s"] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            tickets.append(srv.submit(pids[(r["model"], r["voxels"], r["cap"])], r["shift"], b))
+        res = [srv.wait(t)[1] for t in tickets]
+        wall = time.perf_counter() - t0 - reqs[0]["arrival_s"]
+        st = srv.stats()
+    lat = [r.latency_ms for r in res]
+    out["fp32"] = {
+        "value": round(len(res) / wall, 3),
+        "unit": "solves/s",
+        "p50_ms": round(pct(lat, 50), 3),
+        "p99_ms": round(pct(lat, 99), 3),
+        "worst_rel_residual": max(r.residual for r in res),
+        "all_converged": all(r.status == 0 for r in res),
+        "batched_requests": int(sum(1 for r in res if r.batched > 1)),
+        "evictions": st["evictions"],
+        "memory_waits": st["memory_waits"],
+    }
+    # the plain FP64 drop-in path on the same arrivals, one request at a time
+    dev = torch.device("cuda", torch.cuda.current_device())
+    clock = reqs[0]["arrival_s"]
+    lat64, rel64, conv64 = [], [], []
+    for r, b in zip(reqs, bs):
+        box, model = problems[(r["model"], r["voxels"], r["cap"])]
+        start = max(clock, r["arrival_s"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Q = mk.generator(box, model, "absorbing")
+        A = mk.shifted_generator(Q, r["shift"])
+        M = mk.sector_multigrid(model.domain, box, r["shift"], mk.multigrid_options(precision="fp64"))
+        bn = float(np.linalg.norm(b))
+        s = mk.solver(A, M, mk.gmres_options(tolerance=REL_TOL * bn, max_iterations=2000, restart=RESTART))
+        x = np.zeros_like(b)
+        res64 = s.solve_host(b, x)
+        torch.cuda.synchronize()
+        took = time.perf_counter() - t0
+        clock = start + took
+        lat64.append((clock - r["arrival_s"]) * 1e3)
+        rel64.append(res64.residual / bn if bn > 0 else 0.0)
+        conv64.append(res64.converged)
+        del s, M, A, Q
+        torch.cuda.empty_cache()
+    out["plain_fp64_path"] = {
+        "value": round(len(reqs) / (clock - reqs[0]["arrival_s"]), 3),
+        "unit": "solves/s",
+        "p50_ms": round(pct(lat64, 50), 3),
+        "p99_ms": round(pct(lat64, 99), 3),
+        "worst_rel_residual": max(rel64),
+        "all_converged": all(conv64),
+    }
+    out["fp32_over_plain_fp64_path"] = round(out["fp32"]["value"] / out["plain_fp64_path"]["value"], 3)
     out["requests"] = len(reqs)
     out["largest_states"] = max(sizes.values())
-    out["note"] = (f"Poisson arrivals at {MIX_RATE}/s, seed 4; fp32: {SERVE_SLOTS} slots, FGMRES({MIX_RESTART}), "
-                   "dense solve of sectors <= 256 states; fp64: 1 slot, GMRES(30), the reference's "
-                   "multigrid options; 1-D boxes use configuration 0's voxel size 1/16")
+    out["note"] = (f"Poisson arrivals at {MIX_RATE}/s, seed 4; fp32: {SERVE_SLOTS} slots, batch 4 across shifts, "
+                   f"FGMRES({RESTART}), smoother {FP32_SMOOTHER}, dense solve of sectors <= {FP32_COARSEST} "
+                   "states; plain fp64: one request at a time, GMRES(30), the reference's multigrid options, "
+                   "generator and multigrid set-up inside each latency; 1-D boxes use configuration 0's "
+                   "voxel size 1/16")
     return out
 
 
-def _set_tolerance(solver, tol):
-    solver.set_tolerance(tol)
+FSP_MAX_STEPS = 2000
+FSP_CPU_SAMPLE = 16  # instances of each family the CPU baseline runs
+
+
+def fsp_batch_measure(with_cpu: bool) -> dict:
+    """The batching workload: the 512 seeded Krylov-FSP propagations to t = 2 of
+    markovkit_b200.inputs.fsp_batch_instances (256 birth-death boxes of 100-2000 states, 256
+    toggle switches of 2,601-90,601 states), tolerance 1e-8, at most FSP_MAX_STEPS attempts each,
+    in one persistent launch with autotuned shapes (the autotune runs untimed first). Timed with
+    CUDA events around the launch. The CPU baseline runs the reference's solve_krylov_fsp
+    (oracle/_ref/ref_fsp) on the first FSP_CPU_SAMPLE instances of each family, one process per
+    host core, and scales the family-weighted mean time per instance to the batch."""
+    import torch
+
+    from markovkit_b200.fsp import _Problem, box as fbox, fsp_batch, krylov_fsp_options
+    from markovkit_b200.fsp_models import network_of
+    from markovkit_b200.inputs import fsp_batch_instances
+
+    inst = fsp_batch_instances()
+    probs = [_Problem(network_of(x), x["initial"], x["final_time"],
+                      krylov_fsp_options(inside=fbox(x["bounds"]), tolerance=x["tolerance"], max_steps=FSP_MAX_STEPS))
+             for x in inst]
+    b = fsp_batch(probs)
+    threads, blocks = b.autotune(sample=0)
+    b.run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.run()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    _, res = b.results()
+    finished = sum(1 for r in res if r.status == 0)
+    out = {
+        "metric": "Krylov-FSP propagations/sec to t = 2 (FSP tolerance 1e-8), one persistent launch",
+        "value": round(len(probs) / (ms / 1e3), 2),
+        "unit": "instances/s",
+        "ms": round(ms, 3),
+        "instances": len(probs),
+        "finished": finished,
+        "capped": len(probs) - finished,
+        "max_steps": FSP_MAX_STEPS,
+        "shape": {"threads": threads, "blocks": blocks},
+    }
+    if with_cpu:
+        out["cpu_baseline"] = fsp_cpu_baseline(inst)
+    return out
+
+
+def fsp_cpu_baseline(inst) -> dict:
+    from concurrent.futures import ThreadPoolExecutor
+
+    from markovkit_b200.inputs import fsp_instance_line
+
+    driver = ROOT / "oracle" / "_ref" / "ref_fsp"
+    if not driver.exists():
+        return {"value": None, "unit": "instances/s", "cores": None, "kind": "reference",
+                "sample": "oracle/_ref/ref_fsp not built"}
+    half = len(inst) // 2
+    sample = list(range(FSP_CPU_SAMPLE)) + list(range(half, half + FSP_CPU_SAMPLE))
+    cores = os.cpu_count() or 1
+
+    def one(k):
+        line = fsp_instance_line(inst[k], max_steps=FSP_MAX_STEPS) + "\n"
+        t0 = time.perf_counter()
+        p = subprocess.run([str(driver)], input=line, capture_output=True, text=True, timeout=600)
+        return k, time.perf_counter() - t0, p.returncode
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        done = list(ex.map(one, sample))
+    wall = time.perf_counter() - t0
+    per = {"birth_death": [], "toggle": []}
+    for k, sec, rc in done:
+        if rc == 0:
+            per[inst[k]["family"]].append(sec)
+    # the batch's instances are half of each family: expected single-core seconds per instance
+    mean = 0.5 * float(np.mean(per["birth_death"])) + 0.5 * float(np.mean(per["toggle"]))
+    value = cores / mean
+    return {"value": round(value, 3), "unit": "instances/s", "cores": cores, "kind": "reference",
+            "sample": f"{len(sample)} instances (the first {FSP_CPU_SAMPLE} of each family), one ref_fsp "
+                      f"process per core, {wall:.1f} s wall; instances/s = cores / family-weighted mean "
+                      f"seconds per instance ({mean:.3f} s)"}
 
 
 def _uuid(dev) -> str | None:
@@ -497,9 +686,9 @@ def _uuid(dev) -> str | None:
         return None
 
 
-def _time_apply(Q, N, dev, flush=None, reps=20) -> float:
-    """Average ms of one FP64 apply_shifted, CUDA events on its launch stream, each launch timed
-    on its own (L2 flushed before each when `flush` is given)."""
+def _time_apply(Q, N, dev, flush, reps=20) -> float:
+    """Average ms of one FP64 apply_shifted (every kernel of the pass), CUDA events on its launch
+    stream, each launch timed on its own with L2 flushed before it."""
     import torch
 
     x = torch.rand(N, dtype=torch.float64, device=dev)
@@ -510,8 +699,7 @@ def _time_apply(Q, N, dev, flush=None, reps=20) -> float:
     stream = torch.cuda.current_stream()
     total = 0.0
     for _ in range(reps):
-        if flush is not None:
-            flush.zero_()
+        flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -523,8 +711,8 @@ def _time_apply(Q, N, dev, flush=None, reps=20) -> float:
 
 
 def ncu_traffic(name: str) -> float | None:
-    """dram__bytes_read.sum + dram__bytes_write.sum per launch from a committed ncu summary
-    (profiles/<name>.md, the row 'traffic (read + write) | X MB per launch')."""
+    """dram__bytes_read.sum + dram__bytes_write.sum per apply from the committed ncu summary of
+    the kernel (the row 'traffic (read + write) | X MB per apply' of profiles/<name>.md)."""
     p = ROOT / "profiles" / f"{name}.md"
     if not p.exists():
         return None
@@ -534,40 +722,35 @@ def ncu_traffic(name: str) -> float | None:
     return None
 
 
-def roofline(mk, Q, M, dev, N) -> dict:
-    """The generator SpMV, the kernel the north star's roofline target names, on the 3-D
-    16^3-voxel box of cap 2 (8,394,753 states): FP64 apply_shifted, one compulsory read of x and
-    write of y, 16 bytes per state (134 MB per launch, larger than L2), L2 flushed before each
-    timed launch. The bench workload's own SpMV (16.8 MB, L2-resident) is reported beside it."""
+SPMV_PROFILE = "spmv_pair_rows_birth_death_3d16"
+
+
+def roofline(mk, Q, dev, N, w) -> dict:
+    """The generator SpMV of the workload, the kernel the roofline target names: FP64
+    apply_shifted, one compulsory read of x and write of y, 16 bytes per state (134 MB per apply
+    on the 16^3 box, larger than L2), L2 flushed before each timed apply; every kernel of the
+    pass is inside the timed region (the pair-row kernel for the light rows and the general one
+    for the rows whose in-jumps come from every voxel)."""
     import torch
 
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     pk = peaks()
-    w = WORKLOADS["birth_death_3d16"]
-    dom = mk.voxel_domain(mk.grid([16] * 3, [1 / 16] * 3), w["D"])
-    model = mk.reaction_diffusion(dom, [mk.local_reaction(c, f) for c, f in reactions_of(w)])
-    box = mk.population_box(4096, w["caps"])
-    Q3 = mk.generator(box, model, "absorbing")
-    N3 = box.size()
-    ms = _time_apply(Q3, N3, dev, flush)
-    algo = N3 * 16
+    ms = _time_apply(Q, N, dev, flush)
+    algo = N * 16
     achieved = algo / (ms * 1e-3) / 1e9
-    ms_w = _time_apply(Q, N, dev, None)
-    achieved_w = N * 16 / (ms_w * 1e-3) / 1e9
     return {
-        "kernel": "generator apply_shifted, FP64 gather SpMV (row_kernel<double,1,2>), 3-D 16^3 box cap 2",
+        "kernel": "generator apply_shifted, FP64 gather SpMV (pair_kernel<double,1> light rows + "
+                  "row_kernel<double,1,2> all-voxel rows)",
         "bound": "hbm",
         "achieved": round(achieved, 1),
         "peak": pk["hbm_gbs"],
         "peak_source": pk["source"],
         "unit": "GB/s",
         "frac": round(achieved / pk["hbm_gbs"], 4),
-        "traffic": ncu_traffic("row_kernel_spmv_birth_death_3d16"),
-        "traffic_source": "profiles/row_kernel_spmv_birth_death_3d16.md (ncu, bytes per launch)",
-        "us_per_launch": round(ms * 1e3, 3),
-        "algorithmic_bytes_per_launch": algo,
-        "workload_spmv": {"kernel": "row_kernel<double,2,1>", "us_per_launch": round(ms_w * 1e3, 3),
-                          "achieved_gbs": round(achieved_w, 1), "note": "16.8 MB per launch, L2-resident"},
+        "traffic": ncu_traffic(SPMV_PROFILE) if w["workload"].startswith("rdme_birth_death_3d_16") else None,
+        "traffic_source": f"profiles/{SPMV_PROFILE}.md (ncu dram bytes, both kernels of one apply)",
+        "us_per_apply": round(ms * 1e3, 3),
+        "algorithmic_bytes_per_apply": algo,
     }
 
 
@@ -582,71 +765,110 @@ def _problem_args(w: dict) -> list[str]:
     return [f"{k}={v}" for k, v in keys.items()]
 
 
-def cpu_baseline(w) -> dict:
-    """The matrix-free CPU port (oracle/_ref/mf_port, a restatement of the reference's path
-    validated against it) on this host's cores: full solves of the same workload, setup excluded."""
+def cpu_baseline(w, seed: int):
+    """The matrix-free CPU port of the reference's path (oracle/_ref/mf_port) on this host's
+    cores: one full solve of the first timed right-hand side, set-up excluded. Returns the
+    baseline and the port's FP64 solution (the oracle the GPU paths are compared with)."""
     port = ROOT / "oracle" / "_ref" / "mf_port"
     if not port.exists():
-        return {"value": None, "unit": "solves/s", "cores": None, "kind": "port", "sample": "oracle/_ref/mf_port not built"}
+        return {"value": None, "unit": "solves/s", "cores": None, "kind": "port",
+                "sample": "oracle/_ref/mf_port not built"}, None
     threads = os.cpu_count() or 1
-    solves = 2
-    args = [str(port), *_problem_args(w), f"rhs={w['rhs']}", f"seed={w['seed']}", "tol=1e-10",
-            f"restart={RESTART}", f"threads={threads}", f"solves={solves}"]
-    proc = subprocess.run(args, capture_output=True, text=True, timeout=1800)
-    if proc.returncode != 0:
-        return {"value": None, "unit": "solves/s", "cores": threads, "kind": "port", "sample": proc.stderr[-200:]}
-    m = json.loads(proc.stdout.strip().splitlines()[-1])
+    with tempfile.TemporaryDirectory() as tmp:
+        args = [str(port), *_problem_args(w), f"rhs={w['rhs']}", f"seed={seed}", "tol=1e-10",
+                f"restart={RESTART}", f"threads={threads}", "solves=1", f"out={tmp}"]
+        proc = subprocess.run(args, capture_output=True, text=True, timeout=3600)
+        if proc.returncode != 0:
+            return {"value": None, "unit": "solves/s", "cores": threads, "kind": "port",
+                    "sample": proc.stderr[-200:]}, None
+        m = json.loads(proc.stdout.strip().splitlines()[-1])
+        x = np.fromfile(Path(tmp) / "x_port.f64", dtype=np.float64)
     secs = sum(m["solve_ms"]) / 1e3
     return {
-        "value": round(solves / secs, 5), "unit": "solves/s", "cores": m["threads"], "kind": "port",
-        "sample": f"{solves} full solves ({m['iterations']} MG-GMRES iterations each, true rel. residual "
+        "value": round(1.0 / secs, 5), "unit": "solves/s", "cores": m["threads"], "kind": "port",
+        "sample": f"1 full solve ({m['iterations']} MG-GMRES iterations, true rel. residual "
                   f"{m['true_rel_residual']:.2e}) after an untimed {m['setup_ms'] / 1e3:.1f} s set-up",
-    }
+    }, x
+
+
+REF_SAMPLE_ITERS = 3
 
 
 def run_reference(args) -> None:
-    """The reference's own CPU path (MarkovKit headers + numerics shim, oracle/_ref/ref_driver),
-    single-threaded as the reference is. Its set-up (population_box, generator, sector_multigrid)
-    runs untimed once; one full solve gives the iteration count; each step is a bounded sample of
-    SAMPLE_ITERS Arnoldi iterations, and solves/sec = SAMPLE_ITERS / (iterations * step time)."""
+    """The reference's CPU path on this host's cores. For the 2-D workload the reference's own
+    headers against the numerics shim (oracle/_ref/ref_driver), single-threaded as the reference
+    is; for the other workloads the matrix-free port (oracle/_ref/mf_port) on all cores, because
+    the reference's containers need ~275 GB and its generator set-up copies a 4096-entry state
+    for each of ~3.4e10 jumps at 8.4M states. Set-up runs untimed once; one full solve gives the
+    iteration count; each step is a bounded sample of REF_SAMPLE_ITERS Arnoldi iterations and
+    solves/sec = REF_SAMPLE_ITERS / (iterations * step time)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = WORKLOADS[args.workload]
-    driver = ROOT / "oracle" / "_ref" / "ref_driver"
-    if not driver.exists():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver is not built"}))
-        return
-    sample_iters = 6
     K, W = args.steps, args.warmup
+    use_ref = args.workload == "annihilation_2d32"
+    exe = ROOT / "oracle" / "_ref" / ("ref_driver" if use_ref else "mf_port")
+    if not exe.exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"{exe.relative_to(ROOT)} is not built"}))
+        return
+    threads = 1 if use_ref else (os.cpu_count() or 1)
     with tempfile.TemporaryDirectory() as tmp:
-        cmd = [str(driver), *_problem_args(w), f"rhs={w['rhs']}", f"seed={w['seed']}", "tol=1e-10",
-               f"restart={RESTART}", "do_apply=0", "do_plain=0", "warmup=1", f"solves={W + K}",
-               f"sample_iters={sample_iters}", f"out={tmp}"]
+        if use_ref:
+            cmd = [str(exe), *_problem_args(w), f"rhs={w['rhs']}", f"seed={w['seed']}", "tol=1e-10",
+                   f"restart={RESTART}", "do_apply=0", "do_plain=0", "warmup=1", f"solves={W + K}",
+                   f"sample_iters={REF_SAMPLE_ITERS}", f"out={tmp}"]
+        else:
+            cmd = [str(exe), *_problem_args(w), f"rhs={w['rhs']}", f"seed={w['seed']}", "tol=1e-10",
+                   f"restart={RESTART}", f"threads={threads}", "warmup=1", f"solves={W + K}",
+                   f"sample_iters={REF_SAMPLE_ITERS}"]
         t0 = time.time()
         proc = subprocess.run(cmd, capture_output=True, text=True)
         wall = time.time() - t0
     if proc.returncode != 0:
-        print(json.dumps({"impl": "reference", "unavailable": "ref_driver failed: " + proc.stderr[-200:].replace("\n", " ")}))
+        print(json.dumps({"impl": "reference", "unavailable": f"{exe.name} failed: " +
+                          proc.stderr[-200:].replace("\n", " ")}))
         return
     m = json.loads(proc.stdout.strip().splitlines()[-1])
-    its = m["full_solve_iterations"]
-    steps_ms = m["gmres_mg"]["solve_ms"][W:]
-    per_solve_s = (sum(steps_ms) / len(steps_ms)) / 1e3 * its / sample_iters
+    if use_ref:
+        its = m["full_solve_iterations"]
+        steps_ms = m["gmres_mg"]["solve_ms"][W:]
+        setup_s = (m["box_ms"] + m["generator_ms"] + m["mg_setup_ms"]) / 1e3
+        kind = "reference"
+    else:
+        # the warm-up solve ran to convergence: its iteration count is the full solve's
+        its = m["full_iterations"]
+        steps_ms = m["solve_ms"][W:]
+        setup_s = m["setup_ms"] / 1e3
+        kind = "port"
+    per_solve_s = (sum(steps_ms) / len(steps_ms)) / 1e3 * its / REF_SAMPLE_ITERS
     value = 1.0 / per_solve_s
-    sample = (f"each step: {sample_iters} of the {its} MG-GMRES iterations of a full solve, scaled; "
-              f"untimed set-up {(m['box_ms'] + m['generator_ms'] + m['mg_setup_ms']) / 1e3:.0f} s")
+    sample = (f"each step: {REF_SAMPLE_ITERS} of the {its} MG-GMRES iterations of a full solve, scaled; "
+              f"untimed set-up {setup_s:.0f} s; {threads} host thread(s)")
     line = {
-        "metric": "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)",
-        "impl": "reference", "value": round(value, 5), "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": K, "warmup": W, "ms_per_step": round(per_solve_s * 1e3, 2), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded right-hand side",
-        "config": {"workload": w["workload"], "states": m["N"], "parallelism": "1 host thread"},
-        "cpu_baseline": {"value": round(value, 5), "unit": "solves/s", "cores": 1, "kind": "reference", "sample": sample},
+        "metric": METRIC, "impl": "reference", "value": round(value, 5), "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": K, "warmup": W, "ms_per_step": round(per_solve_s * 1e3, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded right-hand side",
+        "config": {"workload": w["workload"], "states": m["N"], "parallelism": f"{threads} host thread(s)"},
+        "cpu_baseline": {"value": round(value, 5), "unit": "solves/s", "cores": threads, "kind": kind,
+                         "sample": sample},
         "e2e": {"value": round(value, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(wall, 1),
     }
     print(json.dumps(line), flush=True)
+
+
+def relaunch_under_torchrun(args) -> None:
+    """--gpus N outside torchrun: run this script as N ranks of one node."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    raise SystemExit(subprocess.call(cmd))
 
 
 def main() -> None:
@@ -657,10 +879,15 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served line")
     ap.add_argument("--no-serve-mix", action="store_true", help="skip the mixed serving workload")
+    ap.add_argument("--no-fsp", action="store_true", help="skip the Krylov-FSP batch line")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the 2-D secondary workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch_under_torchrun(args)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -46,6 +46,13 @@ int mk_version(void);
 /* kernels this library has launched in this process (a graph launch counts its kernel nodes) */
 int mk_kernel_launches(uint64_t *count);
 
+/* Which kernel runs the rows of the solve passes (no reference counterpart; the reference has one
+ * CPU code path): 0 (default) the stencil row kernel on the light rows of structured-grid levels
+ * whose states hold one species of at most four molecules or two species of at most one, the
+ * general row kernel elsewhere; 1 the general kernel everywhere. Both give bit-identical results;
+ * the switch exists so that they can be compared. Process-wide; MK_EINVAL for other values. */
+int mk_set_row_path(int path);
+
 /* ---- device memory helpers (for callers without their own CUDA runtime) ---- */
 int mk_device_alloc(size_t bytes, void **d_ptr);
 int mk_device_free(void *d_ptr);

@@ -18,6 +18,7 @@ from .api import (  # noqa: F401
     shifted_generator,
     solver,
     batch_solver,
+    set_row_path,
     voxel_domain,
 )
 from .inputs import dirichlet_rhs, uniform01, uniform_rhs  # noqa: F401

@@ -164,6 +164,7 @@ SIGNATURES = {
     "mk_last_error": (C.c_char_p, []),
     "mk_version": (C.c_int, []),
     "mk_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
+    "mk_set_row_path": (C.c_int, [C.c_int]),
     "mk_device_alloc": (C.c_int, [C.c_size_t, C.POINTER(P)]),
     "mk_device_free": (C.c_int, [P]),
     "mk_memcpy_h2d": (C.c_int, [P, P, C.c_size_t, P]),

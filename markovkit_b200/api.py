@@ -468,6 +468,13 @@ def kernel_launches() -> int:
     return v.value
 
 
+def set_row_path(path: str = "stencil") -> None:
+    """Which kernel runs the rows of the solve passes: "stencil" (default: the stencil row kernel
+    wherever a level allows it) or "general" (the general row kernel everywhere). Both give
+    bit-identical results; process-wide."""
+    check(load().mk_set_row_path({"stencil": 0, "general": 1}[path]))
+
+
 def gmres_options(tolerance: float = 1e-8, max_iterations: int = 1000, restart: int = 30, flexible: bool = False) -> GmresOptions:
     o = GmresOptions()
     o.tolerance = float(tolerance)

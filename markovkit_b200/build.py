@@ -20,7 +20,24 @@ CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "libmarkovkit_b200.so"
 
-SOURCES = ["row_kernels_f64.cu", "row_kernels_f32.cu", "row_kernels_f64_batch.cu", "row_kernels_f32_batch.cu", "row_kernels.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu", "capi_fsp.cu", "server.cpp", "assemble.cu"]
+PLAIN = ["row_kernels.cu", "transfer.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu",
+         "capi_fsp.cu", "server.cpp", "assemble.cu"]
+PRECISIONS = {"f64": "double", "f32": "float"}
+N_SHAPES = 10  # the state shapes of with_shape (generator_row.cuh)
+
+
+def units() -> list[tuple[str, list[str], str]]:
+    """(source, defines, object stem): the plain sources once each; the general row kernel once
+    per (precision, batch width, state shape) and the stencil row kernel once per (precision,
+    batch width), so the heavy template instantiations compile in parallel."""
+    out = [(name, [], Path(name).stem) for name in PLAIN]
+    for tag, t in PRECISIONS.items():
+        for nb in (1, 4):
+            out.append(("stencil_rows.cu", [f"-DMK_T={t}", f"-DMK_NB={nb}"], f"stencil_rows_{tag}_nb{nb}"))
+            for shape in range(N_SHAPES):
+                out.append(("row_kernels_inst.cu", [f"-DMK_T={t}", f"-DMK_NB={nb}", f"-DMK_SHAPE={shape}"],
+                            f"row_kernels_{tag}_nb{nb}_s{shape}"))
+    return out
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [
     "-std=c++20",
@@ -78,17 +95,20 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     extra = extra or []
     BUILD.mkdir(exist_ok=True)
     jobs = []
-    for name in SOURCES:
+    objs = []
+    for name, defines, stem in units():
         src = CSRC / name
-        obj = BUILD / (src.stem + ".o")
+        obj = BUILD / (stem + ".o")
+        objs.append(str(obj))
         if _stale(obj, [src, *sorted(_local_includes(src)), Path(__file__)]):
-            jobs.append((src, obj))
+            jobs.append((src, obj, defines))
+    # the slowest units first, so the pool's tail is short
+    jobs.sort(key=lambda j: 0 if "row_kernels_inst" in j[0].name else 1)
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
-            for obj, log in ex.map(lambda j: _compile(j[0], j[1], extra), jobs):
+            for obj, log in ex.map(lambda j: _compile(j[0], j[1], [*j[2], *extra]), jobs):
                 if verbose and log.strip():
                     print(log, file=sys.stderr)
-    objs = [str(BUILD / (Path(s).stem + ".o")) for s in SOURCES]
     if jobs or not LIB.exists():
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]

@@ -25,6 +25,13 @@ int mk_kernel_launches(uint64_t *count) {
     });
 }
 
+int mk_set_row_path(int path) {
+    return guarded([&] {
+        MK_REQUIRE(path == 0 || path == 1, "row path must be 0 (stencil where possible) or 1 (general)");
+        set_row_path(path);
+    });
+}
+
 int mk_device_alloc(size_t bytes, void **d_ptr) {
     return guarded([&] {
         MK_REQUIRE(d_ptr, "null output pointer");

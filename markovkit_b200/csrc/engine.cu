@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <map>
@@ -139,6 +140,7 @@ void ModelTables<T>::build(const Model &m, double diff_scale, bool with_reaction
     in_coef.upload(h.in_coef);
     deg_coef.upload(h.deg_coef);
     vparity.upload(h.vparity);
+    vmask.upload(h.vmask);
     vclass.upload(h.vclass);
     rate.upload(h.rate);
     host = h.view;
@@ -148,6 +150,7 @@ void ModelTables<T>::build(const Model &m, double diff_scale, bool with_reaction
     dev.in_coef = in_coef.get();
     dev.deg_coef = deg_coef.get();
     dev.vparity = vparity.get();
+    dev.vmask = h.vmask.empty() ? nullptr : vmask.get();
     dev.vclass = h.vclass.empty() ? nullptr : vclass.get();
     dev.rate = h.rate.empty() ? nullptr : rate.get();
 }
@@ -157,6 +160,13 @@ template struct ModelTables<float>;
 
 // ---------------------------------------------------------------------------------------
 // operator levels and the generator
+
+namespace {
+std::atomic<int> g_row_path{0};
+} // namespace
+
+void set_row_path(int path) { g_row_path.store(path == 1 ? 1 : 0); }
+int row_path() { return g_row_path.load(); }
 
 void OperatorLevel::finalize(const Model &m, bool with_reactions) {
     if (n >= (std::int64_t(1) << 31)) {
@@ -170,8 +180,10 @@ void OperatorLevel::finalize(const Model &m, bool with_reactions) {
     tiles.clear();
     for (std::size_t k = 0; k < sectors.size(); ++k) {
         const SectorDesc &sec = sectors[k];
-        // heavy rows: a warp each, or a whole block each when the sector has few of them
-        const int kind = sec.heavy ? (sec.size <= 4 * 148 ? 2 : 1) : 0;
+        // heavy rows: a warp each, or a whole block each when warps alone would fill less than
+        // about two waves of the GPU while each lane loops over many voxels
+        const bool few = sec.size <= 4 * 148 || (sec.size * 32 <= 2 * 148 * 2048 && V >= 1024);
+        const int kind = sec.heavy ? (few ? 2 : 1) : 0;
         const int rows = kind == 0 ? kRowBlock : (kind == 1 ? kWarpRows : 1);
         for (std::int64_t l = 0; l < sec.size; l += rows) {
             Tile t;
@@ -185,8 +197,49 @@ void OperatorLevel::finalize(const Model &m, bool with_reactions) {
     if (tiles.size() > 0x7fffffffULL) {
         throw Error(kEInval, "space too large for one launch");
     }
+    // rows the stencil kernels serve: light rows of a structured grid with per-voxel masks; in
+    // the pair and single-molecule shapes, only sectors whose reactions their tables cover
+    stencil_tiles.clear();
+    general_tiles.clear();
+    std::vector<StencilSector<float>> h_ss32;
+    std::vector<double> h_ddeg64;
+    std::vector<float> h_ddeg32;
+    const bool pair = build_stencil_tables<double>(sectors, S, mol_cap, t64.h.view, t64.h.rate,
+                                                   t64.h.deg_coef, h_ss64, h_ddeg64, sv64);
+    build_stencil_tables<float>(sectors, S, mol_cap, t64.h.view, t64.h.rate, t64.h.deg_coef, h_ss32,
+                                h_ddeg32, sv32);
+    heavy_tiles.clear();
+    general_rest.clear();
+    if (t64.host.grid_dim > 0 && !t64.h.vmask.empty() && stencil_shape(S, mol_cap)) {
+        for (const Tile &t : tiles) {
+            const bool light = t.kind == 0 && !sectors[t.sector].heavy;
+            const bool served = light && (!pair || h_ss64[t.sector].fast);
+            (served ? stencil_tiles : general_tiles).push_back(t);
+            if (!served) {
+                const bool heavy = pair && !light && h_ss64[t.sector].fast && h_ss64[t.sector].heavy_ok;
+                (heavy ? heavy_tiles : general_rest).push_back(t);
+            }
+        }
+        if (stencil_tiles.empty()) {
+            general_tiles.clear();
+            heavy_tiles.clear();
+            general_rest.clear();
+        }
+    }
+    d_heavy_tiles.upload(heavy_tiles);
+    d_general_rest.upload(general_rest);
+    ss64.upload(h_ss64);
+    ss32.upload(h_ss32);
+    ddeg64.upload(h_ddeg64);
+    ddeg32.upload(h_ddeg32);
+    sv64.sectors = pair ? ss64.get() : nullptr;
+    sv64.ddeg = pair ? ddeg64.get() : nullptr;
+    sv32.sectors = pair ? ss32.get() : nullptr;
+    sv32.ddeg = pair ? ddeg32.get() : nullptr;
     d_sectors.upload(sectors);
     d_tiles.upload(tiles);
+    d_stencil_tiles.upload(stencil_tiles);
+    d_general_tiles.upload(general_tiles);
 }
 
 template <typename T>
@@ -197,8 +250,10 @@ RowParams<T> OperatorLevel::params() const {
     p.tiles = d_tiles.get();
     if constexpr (std::is_same_v<T, double>) {
         p.md = t64.dev;
+        p.sv = sv64;
     } else {
         p.md = t32.dev;
+        p.sv = sv32;
     }
     p.n_tiles = static_cast<int>(tiles.size());
     return p;
@@ -206,7 +261,42 @@ RowParams<T> OperatorLevel::params() const {
 
 template <typename T>
 void OperatorLevel::run(RowMode mode, const RowParams<T> &p, cudaStream_t stream) const {
-    check_cuda(launch_rows<T>(mode, S, mol_cap, p, stream), "row kernel launch");
+    if (stencil_tiles.empty() || !stencil_mode(mode) || row_path() == 1) {
+        check_cuda(launch_rows<T>(mode, S, mol_cap, p, stream), "row kernel launch");
+        return;
+    }
+    RowParams<T> q = p;
+    q.mode = mode;
+    if (!heavy_tiles.empty() && pair_heavy_mode(mode)) {
+        // rows with in-jumps from every voxel first (they read the whole next sector), then the rest
+        q.tiles = d_heavy_tiles.get();
+        q.n_tiles = static_cast<int>(heavy_tiles.size());
+        cudaError_t e;
+        if constexpr (std::is_same_v<T, double>) {
+            e = launch_pair_heavy_rows_f64(q, stream);
+        } else {
+            e = launch_pair_heavy_rows_f32(q, stream);
+        }
+        check_cuda(e, "pair heavy row kernel launch");
+        if (!general_rest.empty()) {
+            q.tiles = d_general_rest.get();
+            q.n_tiles = static_cast<int>(general_rest.size());
+            check_cuda(launch_rows<T>(mode, S, mol_cap, q, stream), "row kernel launch");
+        }
+    } else if (!general_tiles.empty()) {
+        q.tiles = d_general_tiles.get();
+        q.n_tiles = static_cast<int>(general_tiles.size());
+        check_cuda(launch_rows<T>(mode, S, mol_cap, q, stream), "row kernel launch");
+    }
+    q.tiles = d_stencil_tiles.get();
+    q.n_tiles = static_cast<int>(stencil_tiles.size());
+    cudaError_t e;
+    if constexpr (std::is_same_v<T, double>) {
+        e = launch_stencil_rows_f64(q, S, mol_cap, stream);
+    } else {
+        e = launch_stencil_rows_f32(q, S, mol_cap, stream);
+    }
+    check_cuda(e, "stencil row kernel launch");
 }
 
 template RowParams<double> OperatorLevel::params<double>() const;
@@ -495,6 +585,7 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
             }
         }
     }
+    build_transfers();
     if (opt.smoother == 2) {
         if (opt.precision == 0) {
             ilu_pivots<double>();
@@ -655,21 +746,18 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
         }
     }
 
+    // r = b - A x on every row; the coarse right-hand side is its restriction, summed in a
+    // fixed order (terminal sectors keep r for their dense solve)
     Level *C = d + 1 < max_depth ? levels[d + 1].get() : nullptr;
-    if (C) {
-        check_cuda(cudaMemsetAsync(buf<T>(*C, 0), 0, C->op.n * lanes * sizeof(T), stream), "memset");
-        p.ldc = C->op.n;
-        p.tv.Vc = C->op.V;
-        p.tv.parent = L.parent.get();
-        p.tv.log_children = L.log_children.get();
-        p.tv.lgf = lgf.get();
-        p.tv.coarse_sectors = C->op.d_sectors.get();
-        p.coarse = buf<T>(*C, 0);
-    }
     p.x = x;
     p.b = rhs;
-    p.aux = r;
-    L.op.run<T>(kResidualRestrict, p, stream);
+    p.y = r;
+    L.op.run<T>(kResidual, p, stream);
+    if (C) {
+        check_cuda(launch_restrict<T>(L.child_begin.get(), L.children.get(), C->op.n, r, nd,
+                                      buf<T>(*C, 0), C->op.n, nb, inter, stream),
+                   "restrict");
+    }
     if (!L.h_term.empty()) {
         const T *inv;
         if constexpr (std::is_same_v<T, double>) {
@@ -713,9 +801,9 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
             }
             cx = acc;
         }
-        p.coarse = cx;
-        p.y = x;
-        L.op.run<T>(kProlongAdd, p, stream);
+        check_cuda(launch_prolong<T>(L.coarse_of.get(), weights<T>(L), nd, cx, C->op.n, x, nd, nb,
+                                     inter, true, stream),
+                   "prolong");
     }
 
     if (opt.smoother == 0) {
@@ -756,21 +844,55 @@ void Multigrid::transfer(int d, int direction, const double *in, double *out,
     }
     Level &L = *levels[d];
     Level &C = *levels[d + 1];
-    RowParams<double> p = L.op.params<double>();
-    p.tv.Vc = C.op.V;
-    p.tv.parent = L.parent.get();
-    p.tv.log_children = L.log_children.get();
-    p.tv.lgf = lgf.get();
-    p.tv.coarse_sectors = C.op.d_sectors.get();
     if (direction == 0) {
-        check_cuda(cudaMemsetAsync(out, 0, C.op.n * sizeof(double), stream), "memset");
-        p.x = in;
-        p.coarse = out;
-        L.op.run<double>(kRestrict, p, stream);
+        check_cuda(launch_restrict<double>(L.child_begin.get(), L.children.get(), C.op.n, in, L.op.n,
+                                           out, C.op.n, 1, false, stream),
+                   "restrict");
     } else {
-        p.coarse = const_cast<double *>(in);
-        p.y = out;
-        L.op.run<double>(kProlong, p, stream);
+        check_cuda(launch_prolong<double>(L.coarse_of.get(), L.w64.get(), L.op.n, in, C.op.n, out,
+                                          L.op.n, 1, false, false, stream),
+                   "prolong");
+    }
+}
+
+// Per fine state of each non-terminal level: its coarse state and prolongation weight (one
+// kCoarseIndex pass), then the children lists of the coarse states (one stable sort).
+void Multigrid::build_transfers() {
+    for (int d = 0; d + 1 < max_depth; ++d) {
+        Level &L = *levels[d];
+        Level &C = *levels[d + 1];
+        const auto nf = static_cast<std::size_t>(L.op.n);
+        L.coarse_of.resize(nf);
+        L.w64.resize(nf);
+        L.children.resize(nf);
+        L.child_begin.resize(static_cast<std::size_t>(C.op.n) + 1);
+        RowParams<double> p = L.op.params<double>();
+        p.tv.Vc = C.op.V;
+        p.tv.parent = L.parent.get();
+        p.tv.log_children = L.log_children.get();
+        p.tv.lgf = lgf.get();
+        p.tv.coarse_sectors = C.op.d_sectors.get();
+        p.idx = L.coarse_of.get();
+        p.wout = L.w64.get();
+        L.op.run<double>(kCoarseIndex, p, nullptr);
+        DeviceArray<unsigned char> scratch(children_scratch_bytes(L.op.n));
+        check_cuda(build_children(L.coarse_of.get(), L.op.n, C.op.n, L.children.get(),
+                                  L.child_begin.get(), scratch.get(), scratch.size(), nullptr),
+                   "multigrid children lists");
+        if (opt.precision == 1) {
+            L.w32.resize(nf);
+            check_cuda(convert<double, float>(L.w64.get(), L.w32.get(), L.op.n, nullptr), "convert");
+        }
+        check_cuda(cudaStreamSynchronize(nullptr), "multigrid transfers");
+    }
+}
+
+template <typename T>
+const T *Multigrid::weights(const Level &L) const {
+    if constexpr (std::is_same_v<T, double>) {
+        return L.w64.get();
+    } else {
+        return L.w32.get();
     }
 }
 

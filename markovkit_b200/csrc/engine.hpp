@@ -7,6 +7,7 @@
 #include "krylov.cuh"
 #include "launch_count.hpp"
 #include "row_kernels.cuh"
+#include "transfer.cuh"
 
 #include <cstdint>
 #include <memory>
@@ -111,9 +112,15 @@ struct ModelTables {
     DeviceArray<int> nbr_ptr, nbr_idx, vclass;
     DeviceArray<T> in_coef, deg_coef, rate;
     DeviceArray<unsigned char> vparity;
+    DeviceArray<unsigned> vmask;
     ModelView<T> host, dev;
     void build(const Model &m, double diff_scale, bool with_reactions, bool absorbing);
 };
+
+// Which kernel runs the rows of the solve passes: 0 (default) the stencil kernel wherever a level
+// allows it, 1 the general kernel everywhere (both give bit-identical results).
+void set_row_path(int path);
+int row_path();
 
 // A level space with one model: the unit the row kernels run over.
 struct OperatorLevel {
@@ -122,8 +129,24 @@ struct OperatorLevel {
     int mol_cap = 4;
     std::vector<SectorDesc> sectors;
     DeviceArray<SectorDesc> d_sectors;
-    std::vector<Tile> tiles;
+    std::vector<Tile> tiles; // every row
     DeviceArray<Tile> d_tiles;
+    // the same rows split between the stencil kernel (light rows of a structured grid in a
+    // stencil shape) and the general kernel (the rest); empty when the level has no stencil rows
+    std::vector<Tile> stencil_tiles, general_tiles;
+    DeviceArray<Tile> d_stencil_tiles, d_general_tiles;
+    // rows with in-jumps from every voxel that the pair-form heavy kernel serves in the operator
+    // passes (then general_rest holds the general kernel's other rows)
+    std::vector<Tile> heavy_tiles, general_rest;
+    DeviceArray<Tile> d_heavy_tiles, d_general_rest;
+    // tables of the pair and single-molecule row forms (stencil_tables.hpp), per precision
+    std::vector<StencilSector<double>> h_ss64;
+    DeviceArray<StencilSector<double>> ss64;
+    DeviceArray<StencilSector<float>> ss32;
+    DeviceArray<double> ddeg64;
+    DeviceArray<float> ddeg32;
+    StencilView<double> sv64;
+    StencilView<float> sv32;
     ModelTables<double> t64;
     ModelTables<float> t32;
     std::shared_ptr<Binomials> binom;
@@ -168,9 +191,13 @@ struct Multigrid {
     struct Level {
         OperatorLevel op;
         int pre = 2, post = 2;
-        // transfer to the next level
+        // transfer to the next level: parent voxels (set-up), and per fine state its coarse state
+        // and prolongation weight; the fine states of each coarse state in ascending order
         DeviceArray<int> parent;
         DeviceArray<double> log_children;
+        DeviceArray<int> coarse_of, children, child_begin;
+        DeviceArray<double> w64;
+        DeviceArray<float> w32;
         // dense terminal blocks of sectors that stop here
         std::vector<TerminalBlock> h_term;
         DeviceArray<TerminalBlock> d_term;
@@ -234,6 +261,9 @@ struct Multigrid {
     void ilu_sweep(Level &L, RowParams<T> p, T *x, const T *rhs, T *work, cudaStream_t stream);
     template <typename T>
     T *buf(Level &L, int which);
+    template <typename T>
+    const T *weights(const Level &L) const;
+    void build_transfers();
     void ensure_graph(int nb);
     // the captured cycle for each batch width, and its kernel nodes
     std::vector<cudaGraphExec_t> graph_exec_;

@@ -53,7 +53,12 @@ struct ModelView {
     float ginv[3] = {1, 1, 1}; // 1 / gdims for coordinate division
     T axis_coef[3] = {};       // weight / volume of an edge along each axis
     int stencil = 0;           // grid model without reactions: one-molecule rows are a stencil
+    // structured grid: per voxel, bit 2a (2a + 1) set when it has a lower (upper) neighbour
+    // along axis a, bit 6 its checkerboard colour (null for general graphs)
+    const unsigned *vmask = nullptr;
 };
+
+constexpr unsigned kVoxelColourBit = 6;
 
 // q = v / d for 0 <= v < 2^24 from a float reciprocal and one correction
 MK_HD int div_small(int v, int d, float inv) {
@@ -209,9 +214,9 @@ MK_HD void diffusion_terms(const BinomTable &B, const ModelView<T> &md, const Se
         const int v = V - 1 - uu;
         const bool first = p == 0 || u[p > 0 ? p - 1 : 0] != uu;
         const bool last = p + 1 >= t || u[p + 1 < TMAX ? p + 1 : p] != uu;
-        const int lo = p > 0 ? u[p > 0 ? p - 1 : 0] : -1;
-        const int hi = p + 1 < t ? u[p + 1 < TMAX ? p + 1 : p] : 0x7fffffff;
-        constexpr int J = p + 1 <= 4 ? p + 1 : 4;
+        [[maybe_unused]] const int lo = p > 0 ? u[p > 0 ? p - 1 : 0] : -1;
+        [[maybe_unused]] const int hi = p + 1 < t ? u[p + 1 < TMAX ? p + 1 : p] : 0x7fffffff;
+        [[maybe_unused]] constexpr int J = p + 1 <= 4 ? p + 1 : 4;
         // the in-jump from the neighbour whose reversed index is uw, with edge coefficient coef;
         // the third argument of acc is the reverse jump's rate (one of this voxel's copies
         // moving back), exact on grids of equal cell volumes where coef is symmetric
@@ -370,6 +375,103 @@ MK_HD void stencil_row(const ModelView<T> &md, const SectorDesc &sec, const RowS
     }
 }
 
+// Reactions that fire from empty voxels: their all-empty total goes to exit (or leak when the
+// product leaves the space); light rows only.
+template <typename T>
+MK_HD void empty_reaction_terms(const SectorDesc &sec, const ModelView<T> &md, T &exit, T &leak) {
+    for (int r = 0; r < md.R; ++r) {
+        if (!((md.nonneg_mask >> r) & 1U)) {
+            continue;
+        }
+        const T E = md.empty_total[r];
+        if (sec.dst[r] >= 0) {
+            exit += E;
+        } else {
+            leak += E;
+            if (md.absorbing) {
+                exit += E;
+            }
+        }
+    }
+}
+
+// Local reactions of the occupied voxels, each distinct voxel once at the first occurrence
+// (s, p) of it: the rate out of the voxel (corrected for the all-empty total counted above),
+// and the in-jumps of reactions whose source is a state with the voxel's counts changed
+// (heavy reactions, whose sources can sit in any empty voxel, are visited separately).
+template <typename T, int NS, int TMAX, bool WANT_IN, typename Acc>
+MK_HD void occupied_reaction_terms(const BinomTable &B, const SectorDesc *sectors,
+                                   const SectorDesc &sec, const ModelView<T> &md,
+                                   const RowState<NS, TMAX> &st, T &exit, T &leak, Acc &acc) {
+    const int V = md.V, R = md.R;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        MK_UNROLL_MOL
+        for (int p = 0; p < TMAX; ++p) {
+            if (R == 0 || p >= sec.total[s]) {
+                continue;
+            }
+            const int uu = st.u[s][p];
+            if (p > 0 && st.u[s][p - 1] == uu) {
+                continue;
+            }
+            bool seen = false;
+#pragma unroll
+            for (int s2 = 0; s2 < s; ++s2) {
+                seen = seen || count_of<TMAX>(st.u[s2], sec.total[s2], uu) > 0;
+            }
+            if (seen) {
+                continue;
+            }
+            const int v = V - 1 - uu;
+            int n[NS];
+            int ti = 0;
+#pragma unroll
+            for (int s2 = 0; s2 < NS; ++s2) {
+                n[s2] = count_of<TMAX>(st.u[s2], sec.total[s2], uu);
+                ti += n[s2] * md.tstride[s2];
+            }
+            const int vc = md.vclass ? load_ro(md.vclass + v) : 0;
+            for (int r = 0; r < R; ++r) {
+                const T *rrow = md.rate + (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple;
+                bool valid = true;
+                int tm = 0;
+                bool ok = true;
+#pragma unroll
+                for (int s4 = 0; s4 < NS; ++s4) {
+                    valid = valid && n[s4] + md.change[r][s4] >= 0;
+                    const int m = n[s4] - md.change[r][s4];
+                    ok = ok && m >= 0 && m <= md.tmax[s4];
+                    tm += m * md.tstride[s4];
+                }
+                // out of this voxel; and it is not one of the empty voxels counted above
+                T a = valid ? load_ro(rrow + ti) : T(0);
+                if ((md.nonneg_mask >> r) & 1U) {
+                    a -= load_ro(rrow);
+                }
+                if (sec.dst[r] >= 0) {
+                    exit += a;
+                } else {
+                    leak += a;
+                    if (md.absorbing) {
+                        exit += a;
+                    }
+                }
+                if constexpr (WANT_IN) {
+                    if (((md.heavy_mask >> r) & 1U) || sec.src[r] < 0 || !ok) {
+                        continue;
+                    }
+                    const T ain = load_ro(rrow + tm);
+                    if (ain > T(0)) {
+                        acc(reaction_source<T, NS, TMAX>(B, md, sec, sectors[sec.src[r]], st, r, uu),
+                            ain, T(0));
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Visit the row: acc(source_index, rate) for every in-jump; adds into exit and leak.
 // light: the exit/leak terms and the in-jumps that start in occupied voxels.
 // [lane, V) step nlanes: the all-voxel loop of heavy reactions.
@@ -386,96 +488,14 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
         }
     }
     if (light) {
-        // reactions firing from empty voxels: the all-empty total, corrected per occupied voxel
-        for (int r = 0; r < R; ++r) {
-            if (!((md.nonneg_mask >> r) & 1U)) {
-                continue;
-            }
-            const T E = md.empty_total[r];
-            if (sec.dst[r] >= 0) {
-                exit += E;
-            } else {
-                leak += E;
-                if (md.absorbing) {
-                    exit += E;
-                }
-            }
-        }
+        empty_reaction_terms<T>(sec, md, exit, leak);
         // diffusion, molecule by molecule: out of its voxel, and into it from each neighbour
         const int row = static_cast<int>(sec.begin + local);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             diffusion_terms<T, NS, TMAX, WANT_IN, WANT_REV>(B, md, sec, st, s, row, exit, acc);
         }
-        // reactions: each distinct occupied voxel once, at the first occurrence (s, p) of it
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            MK_UNROLL_MOL
-            for (int p = 0; p < TMAX; ++p) {
-                if (R == 0 || p >= sec.total[s]) {
-                    continue;
-                }
-                const int uu = st.u[s][p];
-                if (p > 0 && st.u[s][p - 1] == uu) {
-                    continue;
-                }
-                bool seen = false;
-#pragma unroll
-                for (int s2 = 0; s2 < s; ++s2) {
-                    seen = seen || count_of<TMAX>(st.u[s2], sec.total[s2], uu) > 0;
-                }
-                if (seen) {
-                    continue;
-                }
-                const int v = V - 1 - uu;
-                int n[NS];
-                int ti = 0;
-#pragma unroll
-                for (int s2 = 0; s2 < NS; ++s2) {
-                    n[s2] = count_of<TMAX>(st.u[s2], sec.total[s2], uu);
-                    ti += n[s2] * md.tstride[s2];
-                }
-                const int vc = md.vclass ? load_ro(md.vclass + v) : 0;
-                for (int r = 0; r < R; ++r) {
-                    const T *rrow =
-                        md.rate + (static_cast<std::int64_t>(r) * md.nvc + vc) * md.ntuple;
-                    bool valid = true;
-                    int tm = 0;
-                    bool ok = true;
-#pragma unroll
-                    for (int s4 = 0; s4 < NS; ++s4) {
-                        valid = valid && n[s4] + md.change[r][s4] >= 0;
-                        const int m = n[s4] - md.change[r][s4];
-                        ok = ok && m >= 0 && m <= md.tmax[s4];
-                        tm += m * md.tstride[s4];
-                    }
-                    // out of this voxel; and it is not one of the empty voxels counted above
-                    T a = valid ? load_ro(rrow + ti) : T(0);
-                    if ((md.nonneg_mask >> r) & 1U) {
-                        a -= load_ro(rrow);
-                    }
-                    if (sec.dst[r] >= 0) {
-                        exit += a;
-                    } else {
-                        leak += a;
-                        if (md.absorbing) {
-                            exit += a;
-                        }
-                    }
-                    if constexpr (WANT_IN) {
-                        if (((md.heavy_mask >> r) & 1U) || sec.src[r] < 0 || !ok) {
-                            continue;
-                        }
-                        const T ain = load_ro(rrow + tm);
-                        if (ain > T(0)) {
-                            acc(reaction_source<T, NS, TMAX>(B, md, sec, sectors[sec.src[r]], st,
-                                                             r, uu),
-                                ain, T(0));
-                        }
-                    }
-                }
-            }
-        }
+        occupied_reaction_terms<T, NS, TMAX, WANT_IN>(B, sectors, sec, md, st, exit, leak, acc);
     }
     // heavy reactions: a source in every voxel
     if constexpr (WANT_IN) {
@@ -501,6 +521,8 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                     });
                 }
             }
+            // unrolled so that several lanes' gathers are in flight at once
+#pragma unroll 4
             for (int v = lane; v < V; v += nlanes) {
                 const int uu = V - 1 - v;
                 int tm = 0;

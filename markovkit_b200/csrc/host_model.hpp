@@ -242,6 +242,7 @@ struct HostTables {
     std::vector<int> nbr_ptr, nbr_idx, vclass;
     std::vector<T> in_coef, deg_coef, rate;
     std::vector<unsigned char> vparity;
+    std::vector<unsigned> vmask; // structured grids only
     ModelView<T> view; // scalars and masks; pointers set by bind()
 
     void build(const Model &m, double diff_scale, bool with_reactions, bool absorbing) {
@@ -370,6 +371,20 @@ struct HostTables {
             // diffusion only (the multigrid level operators): rows of one molecule per species
             // take the stencil path of visit_row
             mv.stencil = mv.R == 0 ? 1 : 0;
+            vmask.assign(V, 0U);
+            for (int v = 0; v < V; ++v) {
+                std::int64_t rem = v;
+                unsigned mask = static_cast<unsigned>(vparity[v]) << kVoxelColourBit;
+                for (int a = 0; a < m.dim; ++a) {
+                    const std::int64_t c = rem % m.dims[a];
+                    rem /= m.dims[a];
+                    mask |= (c > 0 ? 1U : 0U) << (2 * a);
+                    mask |= (c + 1 < m.dims[a] ? 1U : 0U) << (2 * a + 1);
+                }
+                vmask[v] = mask;
+            }
+        } else {
+            vmask.clear();
         }
         view = mv;
         bind_host();
@@ -382,6 +397,7 @@ struct HostTables {
         view.in_coef = in_coef.data();
         view.deg_coef = deg_coef.data();
         view.vparity = vparity.data();
+        view.vmask = vmask.empty() ? nullptr : vmask.data();
         view.vclass = vclass.empty() ? nullptr : vclass.data();
         view.rate = rate.empty() ? nullptr : rate.data();
     }

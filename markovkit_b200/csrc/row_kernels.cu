@@ -1,5 +1,6 @@
-// Dispatch of the row kernels (instantiated in row_kernels_f64.cu / row_kernels_f32.cu), the
-// dense terminal solve of the multigrid, and bit-exact state indexing on the device.
+// Dispatch of the row kernels (the general kernel instantiated per shape by
+// row_kernels_inst.cu, the stencil kernel by stencil_rows.cu), the dense terminal solve of the
+// multigrid, and bit-exact state indexing on the device.
 #include "launch_count.hpp"
 #include "row_kernels.cuh"
 
@@ -20,6 +21,34 @@ int mol_cap_for(int n_species, int max_species_total) {
     return -1;
 }
 
+namespace {
+
+// (species, largest species total) -> the general kernel of that state shape
+template <typename T, int NB>
+cudaError_t launch_general(const RowParams<T> &p, int S, int cap, cudaStream_t stream) {
+    return with_shape(S, cap, [&]<int NS, int TMAX>() {
+        return detail::launch_shape<T, NS, TMAX, NB>(p, stream);
+    });
+}
+
+} // namespace
+
+cudaError_t launch_rows_f64(const RowParams<double> &p, int S, int cap, cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? launch_general<double, kRowBatch>(p, S, cap, stream)
+                    : launch_general<double, 1>(p, S, cap, stream);
+}
+
+cudaError_t launch_rows_f32(const RowParams<float> &p, int S, int cap, cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? launch_general<float, kRowBatch>(p, S, cap, stream)
+                    : launch_general<float, 1>(p, S, cap, stream);
+}
+
 template <>
 cudaError_t launch_rows<double>(RowMode mode, int S, int cap, const RowParams<double> &p,
                                 cudaStream_t stream) {
@@ -34,6 +63,61 @@ cudaError_t launch_rows<float>(RowMode mode, int S, int cap, const RowParams<flo
     RowParams<float> q = p;
     q.mode = mode;
     return launch_rows_f32(q, S, cap, stream);
+}
+
+bool stencil_shape(int S, int cap) { return (S == 1 && cap <= 4) || (S == 2 && cap <= 1); }
+
+bool stencil_mode(int mode) {
+    switch (mode) {
+    case kApplyQ:
+    case kApplyShifted:
+    case kResidual:
+    case kJacobiZero:
+    case kJacobi:
+    case kGaussSeidel:
+    case kIluFirst:
+    case kIluSecond:
+    case kIluThird:
+        return true;
+    default:
+        return false;
+    }
+}
+
+cudaError_t launch_stencil_rows_f64(const RowParams<double> &p, int S, int cap,
+                                    cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch || !stencil_shape(S, cap) || !stencil_mode(p.mode)) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? detail::launch_stencil<double, kRowBatch>(p, S, cap, stream)
+                    : detail::launch_stencil<double, 1>(p, S, cap, stream);
+}
+
+cudaError_t launch_stencil_rows_f32(const RowParams<float> &p, int S, int cap,
+                                    cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch || !stencil_shape(S, cap) || !stencil_mode(p.mode)) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? detail::launch_stencil<float, kRowBatch>(p, S, cap, stream)
+                    : detail::launch_stencil<float, 1>(p, S, cap, stream);
+}
+
+bool pair_heavy_mode(int mode) { return mode == kApplyQ || mode == kApplyShifted || mode == kResidual; }
+
+cudaError_t launch_pair_heavy_rows_f64(const RowParams<double> &p, cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch || !pair_heavy_mode(p.mode)) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? detail::launch_pair_heavy<double, kRowBatch>(p, stream)
+                    : detail::launch_pair_heavy<double, 1>(p, stream);
+}
+
+cudaError_t launch_pair_heavy_rows_f32(const RowParams<float> &p, cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch || !pair_heavy_mode(p.mode)) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? detail::launch_pair_heavy<float, kRowBatch>(p, stream)
+                    : detail::launch_pair_heavy<float, 1>(p, stream);
 }
 
 namespace {

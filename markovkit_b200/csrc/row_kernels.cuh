@@ -3,6 +3,7 @@
 #pragma once
 
 #include "generator_row.cuh"
+#include "stencil_tables.hpp"
 #include <cuda_runtime.h>
 
 namespace mkb {
@@ -19,6 +20,8 @@ struct Tile {
 constexpr int kRowBlock = 256;
 constexpr int kWarpRows = kRowBlock / 32;
 
+constexpr int kRowBatch = 4; // widest batch of the instantiated kernels
+
 enum RowMode : int {
     kApplyQ = 0,          // y = Q x
     kApplyShifted,        // y = shift x - Q x
@@ -27,11 +30,9 @@ enum RowMode : int {
     kJacobi,              // y = x + omega (b - A x) / (shift + exit)
     kGaussSeidel,         // x_i = (b_i + in_i) / (shift + exit_i) for states of one colour
     kExitLeak,            // y = exit, aux = leak
-    kResidualRestrict,    // r = b - A x; coarse[c(i)] += r (or aux = r on terminal sectors)
-    kProlongAdd,          // y += weight * coarse[c(i)]
     kDiagonal,            // y = shift + exit
-    kRestrict,            // coarse[c(i)] += x_i                (population_transfer::restrict)
-    kProlong,             // y_i = weight_i * coarse[c(i)]      (population_transfer::prolong)
+    kCoarseIndex,         // idx_i = coarse state of fine state i (-1 on terminal sectors) and
+                          // wout_i = its prolongation weight (multigrid set-up)
     // red-black ILU(0) of A = shift I - Q on a bipartite (diffusion-only) level, colour 0 first:
     // with A = [D0 A01; A10 D1], L = [I 0; A10 D0^-1 I], U = [D0 A01; 0 P1], and the pivots
     // P1 = D1 - diag(A10 D0^-1 A01). One sweep x += U^-1 L^-1 (b - A x) is three passes:
@@ -49,25 +50,29 @@ struct RowParams {
     const Tile *tiles = nullptr;
     ModelView<T> md;
     TransferView tv;
+    StencilView<T> sv;
     const T *x = nullptr;
     const T *b = nullptr;
     T *y = nullptr;
     T *aux = nullptr;
-    T *coarse = nullptr;
     const T *piv = nullptr; // ILU(0) pivots of the second colour
+    int *idx = nullptr;     // kCoarseIndex output
+    double *wout = nullptr; // kCoarseIndex output
     T shift = 0;
     T omega = 0;
     int colour = 0;
     int n_tiles = 0;
     int mode = kApplyShifted;
     // right-hand sides served at once (1..kRowBatch): column c of x, b, y and aux starts at
-    // c * ldv, column c of coarse at c * ldc
+    // c * ldv (the interleaved FP32 batch keeps entry (i, c) at i * kRowBatch + c)
     int nb = 1;
     std::int64_t ldv = 0;
-    std::int64_t ldc = 0;
+    // batched requests of one problem with different shifts: column c uses col_shift[c], and
+    // with piv_per_col its ILU(0) pivots sit at column c of piv (laid out like x)
+    int per_col_shift = 0;
+    int piv_per_col = 0;
+    T col_shift[kRowBatch] = {};
 };
-
-constexpr int kRowBatch = 4; // widest batch of the instantiated kernels
 
 // the largest species total the kernels handle: 64 with one species, 16 with more
 int mol_cap_for(int n_species, int max_species_total);
@@ -75,11 +80,35 @@ int mol_cap_for(int n_species, int max_species_total);
 // one pass over every tile; (S, cap) select the kernel's state shape
 template <typename T>
 cudaError_t launch_rows(RowMode mode, int S, int cap, const RowParams<T> &p, cudaStream_t stream);
+// the general row kernel for every shape (p.nb > 1 selects the batched instantiations)
 cudaError_t launch_rows_f64(const RowParams<double> &p, int S, int cap, cudaStream_t stream);
 cudaError_t launch_rows_f32(const RowParams<float> &p, int S, int cap, cudaStream_t stream);
-// the batched instantiations (p.nb > 1)
-cudaError_t launch_rows_f64_batch(const RowParams<double> &p, int S, int cap, cudaStream_t stream);
-cudaError_t launch_rows_f32_batch(const RowParams<float> &p, int S, int cap, cudaStream_t stream);
+
+// The stencil row kernel (stencil_row.cuh): light rows of structured-grid levels whose state
+// shape is one species of at most four molecules or two species of at most one, for the passes
+// of the solve (kApplyQ .. kGaussSeidel and the ILU sweeps). p.tiles lists only such rows.
+bool stencil_shape(int S, int cap);
+bool stencil_mode(int mode);
+cudaError_t launch_stencil_rows_f64(const RowParams<double> &p, int S, int cap, cudaStream_t stream);
+cudaError_t launch_stencil_rows_f32(const RowParams<float> &p, int S, int cap, cudaStream_t stream);
+// Rows of one species of cap <= 2 whose in-jumps come from every voxel, in the operator passes
+// (kApplyQ, kApplyShifted, kResidual): a warp or a block per row with closed-form source ranks.
+bool pair_heavy_mode(int mode);
+cudaError_t launch_pair_heavy_rows_f64(const RowParams<double> &p, cudaStream_t stream);
+cudaError_t launch_pair_heavy_rows_f32(const RowParams<float> &p, cudaStream_t stream);
+
+namespace detail {
+// the general row kernel of one state shape (row_kernels_impl.cuh, instantiated per shape by
+// row_kernels_inst.cu)
+template <typename T, int NS, int TMAX, int NB>
+cudaError_t launch_shape(const RowParams<T> &p, cudaStream_t stream);
+// the stencil row kernel of the shape (S, cap) (stencil_rows.cu, one unit per T and NB)
+template <typename T, int NB>
+cudaError_t launch_stencil(const RowParams<T> &p, int S, int cap, cudaStream_t stream);
+// the pair-form kernel for rows with in-jumps from every voxel (one species of cap <= 2)
+template <typename T, int NB>
+cudaError_t launch_pair_heavy(const RowParams<T> &p, cudaStream_t stream);
+} // namespace detail
 
 struct TerminalBlock {
     std::int64_t begin = 0;      // first row in the level space

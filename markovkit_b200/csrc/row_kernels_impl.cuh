@@ -1,11 +1,12 @@
 // sm_100a row kernels: the matrix-free generator gather and every multigrid pass built on it.
 // Each thread unranks its state, visits its in-jumps and writes one value per column. Rows
 // whose in-jumps fan in from every voxel take a warp (tile kind 1) or a whole block (kind 2)
-// each. The pass (SpMV, residual, smoother sweep, transfer) is a launch parameter, uniform
-// across the grid. NB > 1 instantiations serve up to NB right-hand sides at once (columns at
-// stride ldv, coarse columns at stride ldc): the ranking and rate work of a row, which bounds
-// these kernels, is done once for all columns.
-// Instantiated per precision and batch width in row_kernels_f64*.cu and row_kernels_f32*.cu.
+// each. The pass (SpMV, residual, smoother sweep, multigrid set-up) is a launch parameter,
+// uniform across the grid. NB > 1 instantiations serve up to NB right-hand sides at once
+// (columns at stride ldv): the ranking and rate work of a row, which bounds these kernels, is
+// done once for all columns.
+// Instantiated once per (precision, batch width, state shape) by row_kernels_inst.cu, so the
+// shapes compile in parallel; row_kernels.cu dispatches to them.
 #pragma once
 
 #include "launch_count.hpp"
@@ -19,7 +20,7 @@ namespace detail {
 // The FP32 kernels that serve kRowBatch right-hand sides (the batched multigrid cycle) keep
 // them interleaved: element (i, c) at i * kRowBatch + c, so an in-jump's kRowBatch source
 // values are one 16-byte load. They compute every lane; lanes at or above p.nb hold zeros.
-// The other batched kernels keep column c at c * ldv (ldc on the coarse level).
+// The other batched kernels keep column c at c * ldv.
 template <typename T, int NB>
 constexpr bool kInterleaved = std::is_same_v<T, float> && NB == kRowBatch && kRowBatch == 4;
 
@@ -41,23 +42,27 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-template <typename T, int NS, int TMAX, int NB>
-__device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDesc &sec,
-                                           std::int64_t local, const RowState<NS, TMAX> &st,
-                                           T exit, T leak, const T (&in)[NB], const T (&in2)[NB]) {
-    const std::int64_t i = sec.begin + local;
-    const T d = p.shift + exit;
-    std::int64_t ci = -1;
-    if (p.mode == kResidualRestrict && sec.coarse >= 0) {
-        ci = coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, nullptr);
-    }
+// the diagonal of column c: its shift plus the row's exit rate
+template <typename T>
+__device__ __forceinline__ T column_shift(const RowParams<T> &p, int c) {
+    return p.per_col_shift ? p.col_shift[c] : p.shift;
+}
+
+// write one row's result for each column from its accumulated terms; every pass writes rows
+// of its own tile only, so results do not depend on how rows are spread over blocks. MODE >= 0
+// fixes the pass at compile time (else p.mode selects it).
+template <typename T, int NB, int MODE = -1>
+__device__ __forceinline__ void finish_row(const RowParams<T> &p, std::int64_t i, T exit, T leak,
+                                           const T (&in)[NB], const T (&in2)[NB]) {
+    const int mode = MODE >= 0 ? MODE : p.mode;
 #pragma unroll
     for (int c = 0; c < NB; ++c) {
         if (!kInterleaved<T, NB> && c >= p.nb) {
             break;
         }
+        const T d = column_shift(p, c) + exit;
         const std::int64_t k = at<T, NB>(i, c, p.ldv);
-        switch (p.mode) {
+        switch (mode) {
         case kIluPivot:
             p.y[k] = d - in[c];
             break;
@@ -66,7 +71,7 @@ __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDe
             break;
         case kIluSecond: {
             const T xi = p.x[k];
-            const T z = (p.b[k] - (d * xi - in[c]) + in2[c]) / p.piv[i];
+            const T z = (p.b[k] - (d * xi - in[c]) + in2[c]) / p.piv[p.piv_per_col ? k : i];
             p.aux[k] = z;
             p.y[k] = xi + z;
             break;
@@ -98,15 +103,6 @@ __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDe
             p.y[k] = exit;
             p.aux[k] = leak;
             break;
-        case kResidualRestrict: {
-            const T r = p.b[k] - (d * p.x[k] - in[c]);
-            if (ci >= 0) {
-                atomicAdd(p.coarse + at<T, NB>(ci, c, p.ldc), r);
-            } else {
-                p.aux[k] = r;
-            }
-            break;
-        }
         case kDiagonal:
             p.y[k] = d;
             break;
@@ -116,44 +112,21 @@ __device__ __forceinline__ void finish_row(const RowParams<T> &p, const SectorDe
     }
 }
 
-template <typename T, int NS, int TMAX, int NB>
-__device__ __forceinline__ void transfer_row(const RowParams<T> &p, const SectorDesc &sec,
-                                             std::int64_t local, const RowState<NS, TMAX> &st) {
+// multigrid set-up: the coarse state of a fine state and its prolongation weight
+template <typename T, int NS, int TMAX>
+__device__ __forceinline__ void coarse_index_row(const RowParams<T> &p, const SectorDesc &sec,
+                                                 std::int64_t local, const RowState<NS, TMAX> &st) {
     const std::int64_t i = sec.begin + local;
     if (sec.coarse < 0) {
-        if (p.mode == kProlong) {
-#pragma unroll
-            for (int c = 0; c < NB; ++c) {
-                if (kInterleaved<T, NB> || c < p.nb) {
-                    p.y[at<T, NB>(i, c, p.ldv)] = T(0);
-                }
-            }
-        }
+        p.idx[i] = -1;
+        p.wout[i] = 0.0;
         return;
     }
     double w = 0.0;
-    const std::int64_t ci =
-        coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, p.mode == kRestrict ? nullptr : &w);
-#pragma unroll
-    for (int c = 0; c < NB; ++c) {
-        if (!kInterleaved<T, NB> && c >= p.nb) {
-            break;
-        }
-        const std::int64_t k = at<T, NB>(i, c, p.ldv);
-        const std::int64_t kc = at<T, NB>(ci, c, p.ldc);
-        if (p.mode == kRestrict) {
-            atomicAdd(p.coarse + kc, p.x[k]);
-        } else if (p.mode == kProlongAdd) {
-            p.y[k] += static_cast<T>(w) * p.coarse[kc];
-        } else {
-            p.y[k] = static_cast<T>(w) * p.coarse[kc];
-        }
-    }
+    p.idx[i] = static_cast<int>(coarse_index<NS, TMAX>(p.B, p.tv, sec, p.md.V, st, &w));
+    p.wout[i] = w;
 }
 
-__device__ __forceinline__ bool is_transfer(int mode) {
-    return mode == kProlongAdd || mode == kProlong || mode == kRestrict;
-}
 __device__ __forceinline__ bool needs_in(int mode) {
     return !(mode == kJacobiZero || mode == kExitLeak || mode == kDiagonal);
 }
@@ -287,9 +260,9 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
     }
     RowState<NS, TMAX> st;
     load_state<NS, TMAX>(p.B, sec, p.md.S, p.md.V, local, st);
-    if (is_transfer(p.mode)) {
+    if (p.mode == kCoarseIndex) {
         if (row_lane == 0) {
-            transfer_row<T, NS, TMAX, NB>(p, sec, local, st);
+            coarse_index_row<T, NS, TMAX>(p, sec, local, st);
         }
         return;
     }
@@ -306,7 +279,7 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
     }
     row_terms<T, NS, TMAX, NB>(p, sec, local, st, row_lane, row_lanes, exit, leak, in, in2);
     if (tile.kind == 0) {
-        finish_row<T, NS, TMAX, NB>(p, sec, local, st, exit, leak, in, in2);
+        finish_row<T, NB>(p, sec.begin + local, exit, leak, in, in2);
         return;
     }
     exit = warp_sum(exit);
@@ -318,7 +291,7 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
     }
     if (tile.kind == 1) {
         if (lane == 0) {
-            finish_row<T, NS, TMAX, NB>(p, sec, local, st, exit, leak, in, in2);
+            finish_row<T, NB>(p, sec.begin + local, exit, leak, in, in2);
         }
         return;
     }
@@ -347,7 +320,7 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
                 in2[c] += s_red[2 + NB + c][w];
             }
         }
-        finish_row<T, NS, TMAX, NB>(p, sec, local, st, exit, leak, in, in2);
+        finish_row<T, NB>(p, sec.begin + local, exit, leak, in, in2);
     }
 }
 
@@ -362,13 +335,4 @@ cudaError_t launch_shape(const RowParams<T> &p, cudaStream_t stream) {
 }
 
 } // namespace detail
-
-// (species, largest species total) -> the instantiated state shape
-template <typename T, int NB>
-cudaError_t launch_rows_impl(const RowParams<T> &p, int S, int cap, cudaStream_t stream) {
-    return with_shape(S, cap, [&]<int NS, int TMAX>() {
-        return detail::launch_shape<T, NS, TMAX, NB>(p, stream);
-    });
-}
-
 } // namespace mkb

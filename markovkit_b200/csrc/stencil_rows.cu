@@ -1,0 +1,399 @@
+// The stencil row kernels: one thread per light row of a structured-grid level (two consecutive
+// rows per thread in the colour passes of Gauss-Seidel and ILU(0), so that the rows of the other
+// colour cost a warp no lanes), for the passes of the solve, each pass a separate instantiation.
+// Rows of one species of at most two molecules or two species of at most one take the pair and
+// single-molecule forms (pair_rows.cuh); rows of up to four molecules of one species the stencil
+// forms (stencil_row.cuh). Rows whose in-jumps come from every voxel take pair_heavy_kernel in the
+// operator passes (a warp or a block per row). The build compiles this file once per (precision
+// MK_T, batch width MK_NB); the tiles each kernel gets list only rows its forms serve.
+#include "pair_rows.cuh"
+#include "row_kernels_impl.cuh"
+#include "stencil_row.cuh"
+
+#include <type_traits>
+
+#if !defined(MK_T) || !defined(MK_NB)
+#error "compile with -DMK_T=<double|float> -DMK_NB=<1|4>"
+#endif
+
+namespace mkb::detail {
+namespace {
+
+static_assert(sizeof(SectorDesc) % sizeof(int) == 0, "sector descriptors copy as words");
+static_assert(sizeof(StencilSector<MK_T>) % sizeof(int) == 0, "stencil sectors copy as words");
+
+template <int MODE>
+constexpr bool kColourPass = MODE == kGaussSeidel || MODE == kIluFirst || MODE == kIluSecond ||
+                             MODE == kIluThird;
+template <int MODE>
+constexpr int kRowsPerThread = kColourPass<MODE> ? 2 : 1;
+
+template <typename S>
+__device__ __forceinline__ void copy_to_shared(const S *src, S &dst) {
+    constexpr int kWords = static_cast<int>(sizeof(S) / sizeof(int));
+    const int *from = reinterpret_cast<const int *>(src);
+    int *to = reinterpret_cast<int *>(&dst);
+    for (int k = static_cast<int>(threadIdx.x); k < kWords; k += static_cast<int>(blockDim.x)) {
+        to[k] = from[k];
+    }
+}
+
+// The in-jump sums of one row for pass MODE (row_terms for any row visitor):
+// visit(std::bool_constant<WANT_IN>, acc) runs the row with acc(source, rate, reverse_rate).
+template <typename T, int NB, int MODE, typename Visit>
+__device__ __forceinline__ void accumulate_terms(const RowParams<T> &p, Visit &&visit, T (&in)[NB],
+                                                 T (&in2)[NB]) {
+    if constexpr (MODE == kJacobiZero) {
+        visit(std::false_type{}, [](int, T, T) {});
+        return;
+    } else {
+        // Gauss-Seidel and the ILU passes update x (= y) in place: rows of one colour read only
+        // the other colour's entries, through plain coherent loads
+        const T *xs = MODE == kGaussSeidel ? p.y : p.x;
+        const T *ax = p.aux;
+        if constexpr (NB == 1) {
+            if constexpr (MODE == kIluThird) {
+                visit(std::true_type{}, [&](int j, T a, T) { in2[0] += a * ax[j]; });
+            } else if constexpr (MODE == kIluSecond) {
+                visit(std::true_type{}, [&](int j, T a, T) {
+                    in[0] += a * xs[j];
+                    in2[0] += a * ax[j];
+                });
+            } else {
+                visit(std::true_type{}, [&](int j, T a, T) { in[0] += a * xs[j]; });
+            }
+        } else if constexpr (kInterleaved<T, NB>) {
+            // the kRowBatch source values of an in-jump in one 16-byte load
+            visit(std::true_type{}, [&](int j, T a, T) {
+                const std::int64_t k = static_cast<std::int64_t>(j) * NB;
+                if constexpr (MODE != kIluThird) {
+                    const float4 v = *reinterpret_cast<const float4 *>(xs + k);
+                    in[0] += a * v.x;
+                    in[1] += a * v.y;
+                    in[2] += a * v.z;
+                    in[3] += a * v.w;
+                }
+                if constexpr (MODE == kIluSecond || MODE == kIluThird) {
+                    const float4 u = *reinterpret_cast<const float4 *>(ax + k);
+                    in2[0] += a * u.x;
+                    in2[1] += a * u.y;
+                    in2[2] += a * u.z;
+                    in2[3] += a * u.w;
+                }
+            });
+        } else {
+            const int nb = p.nb;
+            const std::int64_t ldv = p.ldv;
+            visit(std::true_type{}, [&](int j, T a, T) {
+#pragma unroll
+                for (int c = 0; c < NB; ++c) {
+                    if (c >= nb) {
+                        break;
+                    }
+                    const std::int64_t k = j + c * ldv;
+                    if constexpr (MODE == kIluThird) {
+                        in2[c] += a * ax[k];
+                    } else {
+                        in[c] += a * xs[k];
+                        if constexpr (MODE == kIluSecond) {
+                            in2[c] += a * ax[k];
+                        }
+                    }
+                }
+            });
+        }
+    }
+}
+
+// rows of up to four molecules of one species (stencil_row.cuh)
+template <typename T, int NB, int MODE>
+__global__ void __launch_bounds__(kRowBlock) stencil_kernel(const __grid_constant__ RowParams<T> p) {
+    constexpr int NS = 1, TMAX = 4, RPT = kRowsPerThread<MODE>;
+    __shared__ SectorDesc s_sec;
+    const Tile tile = p.tiles[blockIdx.x];
+    copy_to_shared(p.sectors + tile.sector, s_sec);
+    __syncthreads();
+    const SectorDesc &sec = s_sec;
+    const int colour = pass_colour(MODE, p.colour);
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+        const int in_tile = static_cast<int>(threadIdx.x) * RPT + q;
+        if (in_tile >= tile.count) {
+            break;
+        }
+        const int local = static_cast<int>(tile.local0) + in_tile;
+        const int row = static_cast<int>(sec.begin) + local;
+        StencilState<NS, TMAX> st;
+        stencil_load<T, NS, TMAX>(sec, p.md, local, st);
+        if (colour >= 0 && stencil_colour<NS, TMAX>(st) != colour) {
+            continue;
+        }
+        T exit = T(0), leak = T(0);
+        T in[NB], in2[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            in[c] = T(0);
+            in2[c] = T(0);
+        }
+        accumulate_terms<T, NB, MODE>(
+            p,
+            [&](auto want_in, auto &&acc) {
+                stencil_visit<T, NS, TMAX, decltype(want_in)::value>(p.B, p.sectors, sec, p.md, st,
+                                                                     row, exit, leak, acc);
+            },
+            in, in2);
+        finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
+    }
+}
+
+// the molecules and voxel masks of one pair or single-molecule row
+struct PairState {
+    int u0 = 0, u1 = 0;
+    unsigned m0 = 0U, m1 = 0U;
+};
+
+template <int NS, typename T>
+__device__ __forceinline__ PairState pair_load(const StencilSector<T> &ss, const ModelView<T> &md,
+                                               int local) {
+    PairState s;
+    const int V = md.V;
+    if constexpr (NS == 1) {
+        const int t = ss.total[0];
+        if (t == 2) {
+            unrank_pair(local, s.u0, s.u1);
+            s.m1 = load_ro(md.vmask + (V - 1 - s.u1));
+        } else {
+            s.u0 = local;
+        }
+        if (t >= 1) {
+            s.m0 = load_ro(md.vmask + (V - 1 - s.u0));
+        }
+    } else {
+        // species 0's rank is the quotient by stride0 (one molecule: rank = u)
+        if (ss.total[0] && ss.total[1]) {
+            s.u0 = div_small(local, ss.stride0, 1.0f / static_cast<float>(ss.stride0));
+            s.u1 = local - s.u0 * ss.stride0;
+        } else {
+            s.u0 = s.u1 = local;
+        }
+        if (ss.total[0]) {
+            s.m0 = load_ro(md.vmask + (V - 1 - s.u0));
+        }
+        if (ss.total[1]) {
+            s.m1 = load_ro(md.vmask + (V - 1 - s.u1));
+        }
+    }
+    return s;
+}
+
+// rows of one species of at most two molecules (NS = 1) or two species of at most one (NS = 2)
+template <typename T, int NS, int NB, int MODE>
+__global__ void __launch_bounds__(kRowBlock) pair_kernel(const __grid_constant__ RowParams<T> p) {
+    constexpr int RPT = kRowsPerThread<MODE>;
+    __shared__ StencilSector<T> s_ss;
+    const Tile tile = p.tiles[blockIdx.x];
+    copy_to_shared(p.sv.sectors + tile.sector, s_ss);
+    __syncthreads();
+    const StencilSector<T> &ss = s_ss;
+    const int colour = pass_colour(MODE, p.colour);
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+        const int in_tile = static_cast<int>(threadIdx.x) * RPT + q;
+        if (in_tile >= tile.count) {
+            break;
+        }
+        const int local = static_cast<int>(tile.local0) + in_tile;
+        const int row = ss.begin + local;
+        const PairState s = pair_load<NS>(ss, p.md, local);
+        if (colour >= 0 && static_cast<int>(((s.m0 ^ s.m1) >> kVoxelColourBit) & 1U) != colour) {
+            continue;
+        }
+        T exit = T(0), leak = T(0);
+        T in[NB], in2[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            in[c] = T(0);
+            in2[c] = T(0);
+        }
+        accumulate_terms<T, NB, MODE>(
+            p,
+            [&](auto want_in, auto &&acc) {
+                constexpr bool W = decltype(want_in)::value;
+                if constexpr (NS == 1) {
+                    pair_row<T, W>(p.md, p.sv, ss, ss.total[0], s.u0, s.u1, s.m0, s.m1, row, exit,
+                                   leak, acc);
+                } else {
+                    singles_row<T, W>(p.md, p.sv, ss, s.u0, s.u1, s.m0, s.m1, row, exit, leak, acc);
+                }
+            },
+            in, in2);
+        finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
+    }
+}
+
+// Rows of one species whose in-jumps come from every voxel (tile kind 1: a warp per row, kind 2:
+// the block), in the operator passes: lane 0 takes the row's light terms, every lane a share of
+// the voxels; sums in a fixed order.
+template <typename T, int NB, int MODE>
+__global__ void __launch_bounds__(kRowBlock) pair_heavy_kernel(const __grid_constant__ RowParams<T> p) {
+    __shared__ StencilSector<T> s_ss;
+    __shared__ T s_red[2 + NB][kRowBlock / 32];
+    const Tile tile = p.tiles[blockIdx.x];
+    copy_to_shared(p.sv.sectors + tile.sector, s_ss);
+    __syncthreads();
+    const StencilSector<T> &ss = s_ss;
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    int local, row_lane, row_lanes;
+    if (tile.kind == 1) {
+        if (warp >= tile.count) {
+            return;
+        }
+        local = static_cast<int>(tile.local0) + warp;
+        row_lane = lane;
+        row_lanes = 32;
+    } else {
+        local = static_cast<int>(tile.local0);
+        row_lane = static_cast<int>(threadIdx.x);
+        row_lanes = kRowBlock;
+    }
+    const int row = ss.begin + local;
+    const PairState s = pair_load<1>(ss, p.md, local);
+    const int t = ss.total[0];
+    T exit = T(0), leak = T(0);
+    T in[NB], in2[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] = T(0);
+        in2[c] = T(0);
+    }
+    accumulate_terms<T, NB, MODE>(
+        p,
+        [&](auto want_in, auto &&acc) {
+            constexpr bool W = decltype(want_in)::value;
+            if (row_lane == 0) {
+                pair_row<T, W>(p.md, p.sv, ss, t, s.u0, s.u1, s.m0, s.m1, row, exit, leak, acc);
+            }
+            if constexpr (W) {
+                pair_heavy_terms<T>(ss, p.md.V, t, s.u0, row_lane, row_lanes, acc);
+            }
+        },
+        in, in2);
+    exit = warp_sum(exit);
+    leak = warp_sum(leak);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] = warp_sum(in[c]);
+    }
+    if (tile.kind == 1) {
+        if (lane == 0) {
+            finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
+        }
+        return;
+    }
+    if (lane == 0) {
+        s_red[0][warp] = exit;
+        s_red[1][warp] = leak;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            s_red[2 + c][warp] = in[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        exit = leak = T(0);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            in[c] = T(0);
+        }
+        for (int w = 0; w < kRowBlock / 32; ++w) {
+            exit += s_red[0][w];
+            leak += s_red[1][w];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                in[c] += s_red[2 + c][w];
+            }
+        }
+        finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
+    }
+}
+
+template <typename T, int NB, int MODE>
+cudaError_t launch_light(const RowParams<T> &p, int S, int cap, cudaStream_t stream) {
+    const int threads = kRowBlock / kRowsPerThread<MODE>;
+    if (pair_shape(S, cap)) {
+        if (!p.sv.sectors) {
+            return cudaErrorInvalidValue;
+        }
+        if (S == 1) {
+            pair_kernel<T, 1, NB, MODE><<<p.n_tiles, threads, 0, stream>>>(p);
+        } else {
+            pair_kernel<T, 2, NB, MODE><<<p.n_tiles, threads, 0, stream>>>(p);
+        }
+    } else {
+        stencil_kernel<T, NB, MODE><<<p.n_tiles, threads, 0, stream>>>(p);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace
+
+template <typename T, int NB>
+cudaError_t launch_stencil(const RowParams<T> &p, int S, int cap, cudaStream_t stream) {
+    if (p.n_tiles == 0) {
+        return cudaSuccess;
+    }
+    count_launches(1);
+    switch (p.mode) {
+    case kApplyQ:
+        return launch_light<T, NB, kApplyQ>(p, S, cap, stream);
+    case kApplyShifted:
+        return launch_light<T, NB, kApplyShifted>(p, S, cap, stream);
+    case kResidual:
+        return launch_light<T, NB, kResidual>(p, S, cap, stream);
+    case kJacobiZero:
+        return launch_light<T, NB, kJacobiZero>(p, S, cap, stream);
+    case kJacobi:
+        return launch_light<T, NB, kJacobi>(p, S, cap, stream);
+    case kGaussSeidel:
+        return launch_light<T, NB, kGaussSeidel>(p, S, cap, stream);
+    case kIluFirst:
+        return launch_light<T, NB, kIluFirst>(p, S, cap, stream);
+    case kIluSecond:
+        return launch_light<T, NB, kIluSecond>(p, S, cap, stream);
+    case kIluThird:
+        return launch_light<T, NB, kIluThird>(p, S, cap, stream);
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T, int NB>
+cudaError_t launch_pair_heavy(const RowParams<T> &p, cudaStream_t stream) {
+    if (p.n_tiles == 0) {
+        return cudaSuccess;
+    }
+    if (!p.sv.sectors) {
+        return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    switch (p.mode) {
+    case kApplyQ:
+        pair_heavy_kernel<T, NB, kApplyQ><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kApplyShifted:
+        pair_heavy_kernel<T, NB, kApplyShifted><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kResidual:
+        pair_heavy_kernel<T, NB, kResidual><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_stencil<MK_T, MK_NB>(const RowParams<MK_T> &, int, int, cudaStream_t);
+template cudaError_t launch_pair_heavy<MK_T, MK_NB>(const RowParams<MK_T> &, cudaStream_t);
+
+} // namespace mkb::detail

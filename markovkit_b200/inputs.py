@@ -75,17 +75,20 @@ def fsp_batch_instances(seed: int = 3, count: int = 512, final_time: float = 2.0
     return out
 
 
-def fsp_instance_line(inst: dict, krylov_tol: float = 1e-8, krylov_dim: int = 30) -> str:
-    """One instance in the line format of the oracle's Krylov-FSP driver."""
+def fsp_instance_line(inst: dict, krylov_tol: float = 1e-8, krylov_dim: int = 30,
+                      max_steps: int | None = None) -> str:
+    """One instance in the line format of the oracle's Krylov-FSP driver (max_steps: the
+    attempt cap of krylov_fsp_options, default the reference's)."""
     g = lambda x: repr(float(x))  # noqa: E731 - shortest round-trip decimal
+    tail = [] if max_steps is None else [f"max_steps={int(max_steps)}"]
     if inst["family"] == "birth_death":
         return " ".join(["birth_death", g(inst["birth"]), g(inst["death"]), str(inst["bounds"][0]),
                          g(inst["final_time"]), g(inst["tolerance"]), g(krylov_tol), str(krylov_dim),
-                         str(inst["initial"][0])])
+                         str(inst["initial"][0]), *tail])
     return " ".join(["toggle", g(inst["a1"]), g(inst["a2"]), g(inst["n1"]), g(inst["n2"]),
                      str(inst["bounds"][0]), str(inst["bounds"][1]), g(inst["final_time"]),
                      g(inst["tolerance"]), g(krylov_tol), str(krylov_dim), str(inst["initial"][0]),
-                     str(inst["initial"][1])])
+                     str(inst["initial"][1]), *tail])
 
 
 SERVING_MODELS = ("cfg0", "cfg1", "cfg2", "bd1d")

@@ -6,6 +6,7 @@
 //   birth_death <birth> <death> <bound> <T> <tol> <krylov_tol> <krylov_dim> <x0>
 //   toggle <a1> <a2> <n1> <n2> <bound_x> <bound_y> <T> <tol> <krylov_tol> <krylov_dim> <x0> <y0>
 //   table <key>=<value> ...
+// The birth_death and toggle lines may end in <key>=<value> options as the table line takes.
 // Birth-death: {+1} at rate birth, {-1} at rate death * x. Toggle switch: {+1,0} at
 // a1 / (1 + y^n1), {0,+1} at a2 / (1 + x^n2), unit degradation {-1,0} at x and {0,-1} at y.
 // Table: any network whose propensities are tabulated over the box, read from path=<file>
@@ -30,6 +31,21 @@
 #include <vector>
 
 using namespace markovkit;
+
+namespace {
+
+// the <key>=<value> tokens left on an instance line
+void read_options(std::istringstream &in, std::map<std::string, std::string> &o) {
+    std::string tok;
+    while (in >> tok) {
+        const auto eq = tok.find('=');
+        if (eq != std::string::npos) {
+            o[tok.substr(0, eq)] = tok.substr(eq + 1);
+        }
+    }
+}
+
+} // namespace
 
 int main(int argc, char **argv) {
     std::map<std::string, std::string> kv;
@@ -66,6 +82,7 @@ int main(int argc, char **argv) {
                                {{-1}, [=](const state &s) { return d * s[0]; }}};
             bounds = {bound};
             x0 = {x};
+            read_options(in, extra);
         } else if (family == "toggle") {
             double a1, a2, n1, n2;
             int bx, by, x, y;
@@ -77,6 +94,7 @@ int main(int argc, char **argv) {
                 {{0, -1}, [](const state &s) { return double(s[1]); }}};
             bounds = {bx, by};
             x0 = {x, y};
+            read_options(in, extra);
         } else if (family == "table") {
             std::map<std::string, std::string> o;
             std::string tok;

@@ -4,8 +4,12 @@
 // the multigrid transfer against the reference's golden vectors before any kernel runs.
 // Built by tests/cpu_emulator.py with g++ into a small shared library.
 #include "host_model.hpp"
+#include "pair_rows.cuh"
+#include "stencil_row.cuh"
 
 #include <cstdint>
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -63,6 +67,9 @@ Problem make(int dim, const std::int64_t *dims, const double *spacing, int S, co
 constexpr int kCap = 64;
 using State = RowState<kMaxSpecies, kCap>; // the generic shape: any species count up to 4
 
+// the shapes the stencil kernel serves (stencil_shape in row_kernels.cu)
+bool stencil_shape_host(int S, int cap) { return (S == 1 && cap <= 4) || (S == 2 && cap <= 1); }
+
 } // namespace
 
 extern "C" {
@@ -104,6 +111,163 @@ std::int64_t emu_generator(int dim, const std::int64_t *dims, const double *spac
             return 0;
         });
         return p.n;
+    } catch (const std::exception &e) {
+        write_err(err, e.what());
+        return -1;
+    }
+}
+
+// The stencil row forms (stencil_row.cuh) against the general row visit on every light row of
+// a stencil-shaped space: the same in-jumps (source and rate, bit for bit) in the same order, the
+// same exit and leak bits, the same colour. Returns the rows compared (-1 with err on the first
+// difference; 0 when the space has no stencil shape).
+std::int64_t emu_stencil_check(int dim, const std::int64_t *dims, const double *spacing, int S,
+                               const double *D, int R, const int *change, const int *tmax,
+                               const double *rates, int is_box, const int *limits, int absorbing,
+                               char *err) {
+    try {
+        Problem p = make(dim, dims, spacing, S, D, R, change, tmax, rates, is_box, limits, absorbing);
+        const int cap = max_species_total(p.sectors);
+        if (!stencil_shape_host(S, cap) || !p.t.view.vmask) {
+            return 0;
+        }
+        std::int64_t rows = 0;
+        // the pair and single-molecule forms: the same in-jumps (as a multiset: reactions may
+        // come in another order) and the same exit and leak to rounding
+        std::vector<StencilSector<double>> tabs;
+        std::vector<double> ddeg;
+        StencilView<double> sv;
+        if (build_stencil_tables<double>(p.sectors, S, cap, p.t.view, p.t.rate, p.t.deg_coef, tabs,
+                                         ddeg, sv)) {
+            sv.sectors = tabs.data();
+            sv.ddeg = ddeg.data();
+            with_shape(S, cap, [&]<int NS, int TMAX>() {
+                for (std::size_t k = 0; k < p.sectors.size(); ++k) {
+                    const SectorDesc &sec = p.sectors[k];
+                    const StencilSector<double> &ss = tabs[k];
+                    if (sec.heavy && S == 1 && ss.fast && ss.heavy_ok) {
+                        // rows with in-jumps from every voxel: the pair-form heavy terms
+                        for (std::int64_t local = 0; local < sec.size; ++local) {
+                            RowState<NS, TMAX> st;
+                            load_state<NS, TMAX>(p.B, sec, S, p.model->V, local, st);
+                            std::vector<std::pair<std::int64_t, double>> a, b;
+                            double e1 = 0, l1 = 0;
+                            visit_row<double, NS, TMAX>(p.B, p.sectors.data(), sec, p.t.view, local, st,
+                                                        false, 0, 1, e1, l1,
+                                                        [&](std::int64_t j, double r, double) { a.emplace_back(j, r); });
+                            pair_heavy_terms<double>(ss, p.model->V, ss.total[0], static_cast<int>(local), 0, 1,
+                                                     [&](int j, double r, double) { b.emplace_back(j, r); });
+                            std::sort(a.begin(), a.end());
+                            std::sort(b.begin(), b.end());
+                            if (a != b) {
+                                throw Error(kEInval, "pair heavy terms differ at row " +
+                                                         std::to_string(sec.begin + local) + " (" +
+                                                         std::to_string(a.size()) + " vs " +
+                                                         std::to_string(b.size()) + ")");
+                            }
+                            ++rows;
+                        }
+                        continue;
+                    }
+                    if (sec.heavy || !ss.fast) {
+                        continue;
+                    }
+                    for (std::int64_t local = 0; local < sec.size; ++local) {
+                        RowState<NS, TMAX> st;
+                        load_state<NS, TMAX>(p.B, sec, S, p.model->V, local, st);
+                        std::vector<std::pair<std::int64_t, double>> a, b;
+                        double e1 = 0, l1 = 0, e2 = 0, l2 = 0;
+                        visit_row<double, NS, TMAX>(p.B, p.sectors.data(), sec, p.t.view, local, st,
+                                                    true, 0, 1, e1, l1,
+                                                    [&](std::int64_t j, double r, double) { a.emplace_back(j, r); });
+                        const int row = static_cast<int>(sec.begin + local);
+                        const int V = p.model->V;
+                        int u0 = 0, u1 = 0;
+                        unsigned m0 = 0, m1 = 0;
+                        auto acc = [&](int j, double r, double) { b.emplace_back(j, r); };
+                        if (S == 1) {
+                            const int t = ss.total[0];
+                            if (t == 2) {
+                                unrank_pair(static_cast<int>(local), u0, u1);
+                                m1 = p.t.vmask[V - 1 - u1];
+                            } else {
+                                u0 = static_cast<int>(local);
+                            }
+                            if (t >= 1) {
+                                m0 = p.t.vmask[V - 1 - u0];
+                            }
+                            for (int q = 0; q < t; ++q) {
+                                if ((q == 0 ? u0 : u1) != st.u[0][q]) {
+                                    throw Error(kEInval, "pair unrank differs at row " + std::to_string(row));
+                                }
+                            }
+                            pair_row<double, true>(p.t.view, sv, ss, t, u0, u1, m0, m1, row, e2, l2, acc);
+                        } else {
+                            if (ss.total[0] && ss.total[1]) {
+                                u0 = static_cast<int>(local) / ss.stride0;
+                                u1 = static_cast<int>(local) - u0 * ss.stride0;
+                            } else {
+                                u0 = u1 = static_cast<int>(local);
+                            }
+                            if (ss.total[0]) {
+                                m0 = p.t.vmask[V - 1 - u0];
+                            }
+                            if (ss.total[1]) {
+                                m1 = p.t.vmask[V - 1 - u1];
+                            }
+                            singles_row<double, true>(p.t.view, sv, ss, u0, u1, m0, m1, row, e2, l2, acc);
+                        }
+                        std::sort(a.begin(), a.end());
+                        std::sort(b.begin(), b.end());
+                        const double tol = 1e-14 * (std::abs(e1) + 1e-300);
+                        if (a != b || std::abs(e1 - e2) > tol || std::abs(l1 - l2) > 1e-14 * (std::abs(l1) + 1e-300) + 1e-300 ||
+                            ((((m0 ^ m1) >> kVoxelColourBit) & 1U) != static_cast<unsigned>(state_colour<double, NS, TMAX>(p.t.view, sec, st)))) {
+                            throw Error(kEInval, "pair row differs at row " + std::to_string(row) + " (" +
+                                                     std::to_string(a.size()) + " vs " + std::to_string(b.size()) +
+                                                     " in-jumps, exit " + std::to_string(e1) + " vs " + std::to_string(e2) + ")");
+                        }
+                        ++rows;
+                    }
+                }
+                return 0;
+            });
+        }
+        with_stencil_shape(S, cap, [&]<int NS, int TMAX>() {
+            for (const SectorDesc &sec : p.sectors) {
+                if (sec.heavy) {
+                    continue;
+                }
+                for (std::int64_t local = 0; local < sec.size; ++local) {
+                    RowState<NS, TMAX> st;
+                    load_state<NS, TMAX>(p.B, sec, S, p.model->V, local, st);
+                    StencilState<NS, TMAX> ss;
+                    stencil_load<double, NS, TMAX>(sec, p.t.view, static_cast<int>(local), ss);
+                    for (int s2 = 0; s2 < NS; ++s2) {
+                        for (int q = 0; q < (s2 < S ? sec.total[s2] : 0); ++q) {
+                            if (st.u[s2][q] != ss.rs.u[s2][q]) {
+                                throw Error(kEInval, "unrank differs at row " + std::to_string(sec.begin + local));
+                            }
+                        }
+                    }
+                    std::vector<std::pair<std::int64_t, double>> a, b;
+                    double e1 = 0, l1 = 0, e2 = 0, l2 = 0;
+                    visit_row<double, NS, TMAX>(p.B, p.sectors.data(), sec, p.t.view, local, st, true, 0,
+                                                1, e1, l1, [&](std::int64_t j, double r, double) { a.emplace_back(j, r); });
+                    const int row = static_cast<int>(sec.begin + local);
+                    stencil_visit<double, NS, TMAX, true>(p.B, p.sectors.data(), sec, p.t.view, ss, row,
+                                                          e2, l2, [&](int j, double r, double) { b.emplace_back(j, r); });
+                    if (a != b || e1 != e2 || l1 != l2 ||
+                        state_colour<double, NS, TMAX>(p.t.view, sec, st) != stencil_colour<NS, TMAX>(ss)) {
+                        throw Error(kEInval, "stencil row differs at row " + std::to_string(row) + " (" +
+                                                 std::to_string(a.size()) + " vs " + std::to_string(b.size()) +
+                                                 " in-jumps)");
+                    }
+                    ++rows;
+                }
+            }
+            return 0;
+        });
+        return rows;
     } catch (const std::exception &e) {
         write_err(err, e.what());
         return -1;

@@ -147,3 +147,26 @@ def transfer(dim, dims, spacing, totals, c, g):
     if r < 0:
         raise ValueError(err.value.decode())
     return Pc, Rg
+
+
+def stencil_check(dim, dims, spacing, D, reactions, limits, is_box=True, absorbing=True):
+    """Rows compared by emu_stencil_check (stencil forms == general visit, bit for bit)."""
+    L = lib()
+    S = len(D)
+    dims_a = np.array(list(dims) + [1] * (3 - dim), dtype=np.int64)
+    sp_a = np.array(list(spacing) + [1.0] * (3 - dim), dtype=np.float64)
+    D_a = np.array(D, dtype=np.float64)
+    lim = np.array(limits, dtype=np.int32)
+    R = len(reactions)
+    change = np.array([c for ch, _ in reactions for c in ch] or [0], dtype=np.int32)
+    tmax = np.array(limits, dtype=np.int32)
+    vol = float(np.prod(spacing))
+    rates = rate_table(reactions, list(limits), vol).ravel() if R else np.zeros(1)
+    err = C.create_string_buffer(256)
+    fn = L.emu_stencil_check
+    fn.restype = C.c_int64
+    n = fn(C.c_int(dim), _d(dims_a), _d(sp_a), C.c_int(S), _d(D_a), C.c_int(R), _d(change), _d(tmax), _d(rates),
+           C.c_int(int(is_box)), _d(lim), C.c_int(int(absorbing)), err)
+    if n < 0:
+        raise ValueError(err.value.decode())
+    return int(n)
