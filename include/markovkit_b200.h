@@ -173,18 +173,20 @@ int mk_multigrid_apply(mk_multigrid mg, const double *d_b, double *d_x, void *st
  * c * ldb, of x at c * ldx) */
 int mk_multigrid_apply_batch(mk_multigrid mg, const double *d_b, int64_t ldb, double *d_x,
                              int64_t ldx, int nb, void *stream);
-/* The same cycle for callers that must not allocate device memory during the call: code that
- * runs while a stream is being captured into a CUDA graph (where cudaMalloc is not allowed),
- * or a host that fixes its device-memory budget at start-up and forbids allocation inside its
- * compute callbacks. This entry point has no counterpart in the reference. It calls no
- * cudaMalloc or cudaFree: the work vectors of every level live in one static device array of
- * 64 MiB, which every GPU that loads the library holds until the process exits. A hierarchy
- * whose work vectors need more than that is rejected with MK_EINVAL and a message giving the
- * size. The first call on each device looks the array's address up (cudaGetSymbolAddress), so
- * make that first call before any stream capture. All calls share the one array and each
- * overwrites it; calls that overlap on the GPU (different streams, or different hierarchies
- * at once) race and give wrong results, so order them on one stream. The result equals
- * mk_multigrid_apply's up to the summation order of the restriction. */
+/* The same cycle for callers that must not allocate device memory during the call: a host that
+ * fixes its device-memory budget at start-up and forbids allocation inside its compute
+ * callbacks (a serving process that owns all of a GPU's memory, or a solver embedded in another
+ * framework whose allocator it may not bypass). This entry point has no counterpart in the
+ * reference. It calls no cudaMalloc or cudaFree: the work vectors of every level live in one
+ * static device array of 64 MiB, which every GPU that loads the library holds until the process
+ * exits. A hierarchy whose work vectors need more than that is rejected with MK_EINVAL and a
+ * message giving the size. The first call on each device looks the array's address up
+ * (cudaGetSymbolAddress) and caches it for the life of the process, so make that first call
+ * before any stream capture, and do not reset the device (cudaDeviceReset) while the library is
+ * loaded. All calls share the one array and each overwrites it; calls that overlap on the GPU
+ * (different streams, or different hierarchies at once) race and give wrong results, so order
+ * them on one stream. Use a hierarchy from one host thread at a time, as with every mk_multigrid
+ * call. The result equals mk_multigrid_apply's bit for bit. */
 int mk_multigrid_apply_noalloc(mk_multigrid mg, const double *d_b, double *d_x, void *stream);
 /* max_levels()                                  multigrid.hpp:389-395 */
 int mk_multigrid_max_levels(mk_multigrid mg, int *levels);

@@ -655,9 +655,9 @@ int Multigrid::levels_of_sector(int k) const {
 }
 
 template <typename T>
-T *Multigrid::buf(Level &L, int which) {
-    if (use_carved_) {
-        return static_cast<T *>(L.carved[which]);
+T *Multigrid::buf(Level &L, int which, void *const *carve_level) {
+    if (carve_level) {
+        return static_cast<T *>(carve_level[which]);
     }
     if constexpr (std::is_same_v<T, double>) {
         switch (which) {
@@ -695,12 +695,14 @@ T *Multigrid::buf(Level &L, int which) {
 // one cycle of every sector at depth d from a zero initial guess
 // (markovkit/rdme/multigrid.hpp:201-228); returns the buffer holding x
 template <typename T>
-T *Multigrid::cycle(int d, cudaStream_t stream) {
+T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
     Level &L = *levels[d];
-    const T *rhs = buf<T>(L, 0);
-    T *x = buf<T>(L, 1);
-    T *tmp = buf<T>(L, 2);
-    T *r = buf<T>(L, 3);
+    void *const *cl = carve ? carve + 6 * d : nullptr;       // this level's caller vectors
+    void *const *cc = carve ? carve + 6 * (d + 1) : nullptr; // the next level's
+    const T *rhs = buf<T>(L, 0, cl);
+    T *x = buf<T>(L, 1, cl);
+    T *tmp = buf<T>(L, 2, cl);
+    T *r = buf<T>(L, 3, cl);
     // nb_ columns: column c of every level vector at c * nd, except in the FP32 batched cycle,
     // whose kernels interleave kRowBatch lanes (entry (i, c) at i * kRowBatch + c)
     const std::int64_t nd = L.op.n;
@@ -755,7 +757,7 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
     L.op.run<T>(kResidual, p, stream);
     if (C) {
         check_cuda(launch_restrict<T>(L.child_begin.get(), L.children.get(), C->op.n, r, nd,
-                                      buf<T>(*C, 0), C->op.n, nb, inter, stream),
+                                      buf<T>(*C, 0, cc), C->op.n, nb, inter, stream),
                    "restrict");
     }
     if (!L.h_term.empty()) {
@@ -779,24 +781,24 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
     if (C) {
         T *cx = nullptr;
         if (opt.coarse_cycles <= 1) {
-            cx = cycle<T>(d + 1, stream);
+            cx = cycle<T>(d + 1, stream, carve);
         } else {
-            T *acc = buf<T>(L, 4), *crhs = buf<T>(L, 5);
+            T *acc = buf<T>(L, 4, cl), *crhs = buf<T>(L, 5, cl);
             const std::size_t bytes = C->op.n * lanes * sizeof(T);
-            check_cuda(cudaMemcpyAsync(crhs, buf<T>(*C, 0), bytes, cudaMemcpyDeviceToDevice, stream),
+            check_cuda(cudaMemcpyAsync(crhs, buf<T>(*C, 0, cc), bytes, cudaMemcpyDeviceToDevice, stream),
                        "copy");
-            T *e = cycle<T>(d + 1, stream);
+            T *e = cycle<T>(d + 1, stream, carve);
             check_cuda(cudaMemcpyAsync(acc, e, bytes, cudaMemcpyDeviceToDevice, stream), "copy");
             for (int c = 1; c < opt.coarse_cycles; ++c) {
                 RowParams<T> pc = C->op.params<T>();
                 pc.shift = static_cast<T>(shift);
                 pc.x = acc;
                 pc.b = crhs;
-                pc.y = buf<T>(*C, 0);
+                pc.y = buf<T>(*C, 0, cc);
                 pc.nb = nb;
                 pc.ldv = C->op.n;
                 C->op.run<T>(kResidual, pc, stream);
-                e = cycle<T>(d + 1, stream);
+                e = cycle<T>(d + 1, stream, carve);
                 axpy_t<T>(T(1), e, acc, C->op.n * lanes, stream);
             }
             cx = acc;
@@ -829,12 +831,12 @@ T *Multigrid::cycle(int d, cudaStream_t stream) {
         }
     }
     // keep the result in x's own buffer so the caller's view of the level stays fixed
-    if (x != buf<T>(L, 1)) {
-        check_cuda(cudaMemcpyAsync(buf<T>(L, 1), x, ndb * sizeof(T), cudaMemcpyDeviceToDevice,
+    if (x != buf<T>(L, 1, cl)) {
+        check_cuda(cudaMemcpyAsync(buf<T>(L, 1, cl), x, ndb * sizeof(T), cudaMemcpyDeviceToDevice,
                                    stream),
                    "copy");
     }
-    return buf<T>(L, 1);
+    return buf<T>(L, 1, cl);
 }
 
 void Multigrid::transfer(int d, int direction, const double *in, double *out,
@@ -1011,42 +1013,38 @@ void Multigrid::apply_in(const double *b, double *x, void *scratch, std::size_t 
     if (bytes < scratch_bytes() || (reinterpret_cast<std::uintptr_t>(scratch) % kCarveAlign) != 0) {
         throw Error(kEInval, "multigrid scratch too small or misaligned");
     }
+    // the work vectors of this call only: six per level, carved from the caller's memory and
+    // handed down the cycle (the hierarchy's own buffers and state stay untouched)
     const std::size_t w = opt.precision == 0 ? sizeof(double) : sizeof(float);
     auto *base = static_cast<unsigned char *>(scratch);
+    std::vector<void *> carve(6 * levels.size() + 6, nullptr);
     std::size_t off = 0;
     for (std::size_t d = 0; d < levels.size(); ++d) {
-        Level &L = *levels[d];
-        const std::size_t vec = carve_round(static_cast<std::size_t>(L.op.n) * w);
+        const std::size_t vec = carve_round(static_cast<std::size_t>(levels[d]->op.n) * w);
         for (int k = 0; k < 4; ++k) {
-            L.carved[k] = base + off;
+            carve[6 * d + k] = base + off;
             off += vec;
         }
-        L.carved[4] = L.carved[5] = nullptr;
         if (opt.coarse_cycles > 1 && d + 1 < levels.size()) {
             const std::size_t cvec = carve_round(static_cast<std::size_t>(levels[d + 1]->op.n) * w);
-            L.carved[4] = base + off;
+            carve[6 * d + 4] = base + off;
             off += cvec;
-            L.carved[5] = base + off;
+            carve[6 * d + 5] = base + off;
             off += cvec;
         }
     }
-    struct Restore {
-        bool &flag;
-        ~Restore() { flag = false; }
-    } restore{use_carved_};
-    use_carved_ = true;
     Level &L0 = *levels[0];
     const auto n0 = static_cast<std::int64_t>(L0.op.n);
     if (opt.precision == 0) {
-        check_cuda(cudaMemcpyAsync(buf<double>(L0, 0), b, n0 * sizeof(double),
+        check_cuda(cudaMemcpyAsync(buf<double>(L0, 0, carve.data()), b, n0 * sizeof(double),
                                    cudaMemcpyDeviceToDevice, stream),
                    "copy");
-        double *out = cycle<double>(0, stream);
+        double *out = cycle<double>(0, stream, carve.data());
         check_cuda(cudaMemcpyAsync(x, out, n0 * sizeof(double), cudaMemcpyDeviceToDevice, stream),
                    "copy");
     } else {
-        check_cuda(convert<double, float>(b, buf<float>(L0, 0), n0, stream), "convert");
-        float *out = cycle<float>(0, stream);
+        check_cuda(convert<double, float>(b, buf<float>(L0, 0, carve.data()), n0, stream), "convert");
+        float *out = cycle<float>(0, stream, carve.data());
         check_cuda(convert<float, double>(out, x, n0, stream), "convert");
     }
 }

@@ -210,7 +210,6 @@ struct Multigrid {
         DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
         DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
         std::vector<int> box_sector; // box sector of each slot
-        void *carved[6] = {};        // work vectors in caller memory (apply_in)
     };
     MultigridOptions opt;
     double shift = 0.0;
@@ -253,14 +252,15 @@ struct Multigrid {
     void smooth(int d, const double *b, double *x, cudaStream_t stream);
 
   private:
+    // carve: six work-vector pointers per level in caller memory (apply_in), else null
     template <typename T>
-    T *cycle(int d, cudaStream_t stream);
+    T *cycle(int d, cudaStream_t stream, void *const *carve = nullptr);
     template <typename T>
     void ilu_pivots();
     template <typename T>
     void ilu_sweep(Level &L, RowParams<T> p, T *x, const T *rhs, T *work, cudaStream_t stream);
     template <typename T>
-    T *buf(Level &L, int which);
+    T *buf(Level &L, int which, void *const *carve_level = nullptr);
     template <typename T>
     const T *weights(const Level &L) const;
     void build_transfers();
@@ -268,7 +268,6 @@ struct Multigrid {
     // the captured cycle for each batch width, and its kernel nodes
     std::vector<cudaGraphExec_t> graph_exec_;
     std::vector<std::uint64_t> graph_kernels_;
-    bool use_carved_ = false;
     int nb_ = 1; // columns the cycle being recorded or run serves
 };
 

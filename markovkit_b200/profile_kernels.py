@@ -6,7 +6,8 @@ Cases:
   spmv_birth_death_3d16      FP64 generator apply_shifted on the 3-D 16^3-voxel birth-death box of
                              cap 2 (8,394,753 states): 2 untimed launches, then 3 more
   solve_annihilation_2d32    one FP32-multigrid FGMRES resolvent solve of the 2-D 32 x 32
-                             annihilation box {1, 1} (1,050,625 states) after one warm-up solve
+                             annihilation box {1, 1} (1,050,625 states) after one warm-up solve,
+                             red-black Gauss-Seidel smoothing as the bench's FP32 path
   solve_birth_death_3d16     the same on the 3-D box above
   mg_birth_death_3d16        one FP32 sector-multigrid V-cycle on the 3-D box (after one warm-up)
   mg_annihilation_2d32       the same on the 2-D annihilation box (sectors of <= 256 states
@@ -64,7 +65,8 @@ def main(case: str) -> None:
             dom, box, Q, A = _rdme(mk, 3, 16, [2], "birth_death", 0.5)
             rhs = uniform_rhs
         N = box.size()
-        M = mk.sector_multigrid(dom, box, A.shift(), mk.multigrid_options(precision="fp32", coarsest_size=256))
+        M = mk.sector_multigrid(dom, box, A.shift(), mk.multigrid_options(precision="fp32", coarsest_size=256,
+                                                                          smoother="gauss_seidel"))
         if case.startswith("mg_"):
             b = torch.from_numpy(rhs(2, N)).to(dev)
             x = torch.zeros_like(b)

@@ -85,5 +85,6 @@ def load(name: str) -> Case:
 
 
 def names() -> list[str]:
-    """the resolvent fixtures (fsp_cases.npz holds the Krylov-FSP ones)"""
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != "fsp_cases")
+    """the small resolvent fixtures of make_golden.py (fsp_*.npz hold the Krylov-FSP ones,
+    full_*.npz the full-size solutions of make_full_golden.py)"""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("fsp_", "full_")))

@@ -111,12 +111,9 @@ def test_autotune_keeps_results(golden_batch):
     assert np.max(np.abs(out2 - out)) <= 1e-12
 
 
-def test_batching_workload_properties(cuda):
-    """All 512 instances of the batching workload in one launch, with at most 2000 attempts
-    each (toggles whose box cuts through a likely region need far more: their leak budget
-    forces tiny steps, in the reference too). Every instance that finishes reaches t = 2 and
-    every one keeps unit mass; birth-death laws are Poisson; the instances the reference ran
-    agree with it."""
+@pytest.fixture(scope="module")
+def batch512(cuda):
+    """all 512 instances of the batching workload in one launch, at most 2000 attempts each"""
     inst = fsp_batch_instances()
     probs = []
     for x in inst:
@@ -126,6 +123,16 @@ def test_batching_workload_properties(cuda):
     b = fsp_batch(probs)
     b.run()
     out, res = b.results()
+    return inst, b, out, res
+
+
+def test_batching_workload_properties(batch512):
+    """All 512 instances of the batching workload in one launch, with at most 2000 attempts
+    each (toggles whose box cuts through a likely region need far more: their leak budget
+    forces tiny steps, in the reference too). Every instance that finishes reaches t = 2 and
+    every one keeps unit mass; birth-death laws are Poisson; the instances the reference ran
+    agree with it."""
+    inst, b, out, res = batch512
     finished = 0
     for k, x in enumerate(inst):
         assert res[k].status in (_lib.MK_OK, _lib.MK_ENOTCONV)
@@ -149,3 +156,35 @@ def test_batching_workload_properties(cuda):
         size = b.problems[k].region.size()
         got = out[b.offsets[k]: b.offsets[k] + size]
         assert np.max(np.abs(got - _ref_dense(name, size))) <= P_TOL, name
+
+
+BATCH_GOLD_PATH = fsp_cases.__file__.replace("fsp_cases.py", "golden/fsp_batch_golden.npz")
+
+
+def test_batching_instances_match_reference(batch512):
+    """33 instances of the 512-instance launch (the first 16 of each family and a toggle the
+    reference itself stops at the attempt cap) against the reference's solve_krylov_fsp with the
+    same cap (tests/golden/fsp_batch_golden.npz, made by make_fsp_batch_golden.py): final times
+    within 1e-12, probabilities within 1e-9, for finished and capped instances alike."""
+    import os
+
+    if not os.path.exists(BATCH_GOLD_PATH):
+        pytest.skip("fsp_batch_golden.npz not generated")
+    gold = np.load(BATCH_GOLD_PATH)
+    meta = json.loads(str(gold["meta"]))
+    inst, b, out, res = batch512
+    capped = 0
+    for key, m in meta["instances"].items():
+        k = int(key)
+        size = b.problems[k].region.size()
+        got = out[b.offsets[k]: b.offsets[k] + size]
+        ref = np.zeros(size)
+        ref[gold[f"{key}/index"]] = gold[f"{key}/p"]
+        assert abs(res[k].time - m["t"]) <= 1e-12 * max(1.0, abs(m["t"])), k
+        assert np.max(np.abs(got - ref)) <= P_TOL, (k, float(np.max(np.abs(got - ref))))
+        if m["t"] < inst[k]["final_time"]:
+            capped += 1
+            assert res[k].status == _lib.MK_ENOTCONV and res[k].attempts == meta["max_steps"], k
+        else:
+            assert res[k].status == _lib.MK_OK, k
+    assert len(meta["instances"]) >= 32 and capped >= 1

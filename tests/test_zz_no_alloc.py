@@ -1,8 +1,9 @@
 """mk_multigrid_apply_noalloc: the multigrid apply for callers that cannot allocate device
-memory during the call (for example code running under CUDA stream capture, or a host with a
-fixed device-memory budget). Its work vectors live in a static 64 MiB device array; the result
-must match mk_multigrid_apply's on two calls in a row (the array keeps the previous call's
-contents, so the second call checks that nothing stale leaks in).
+memory during the call (a host with a fixed device-memory budget that forbids allocation inside
+its compute callbacks). Its work vectors live in a static 64 MiB device array; the result must
+equal mk_multigrid_apply's bit for bit on two calls in a row (the array keeps the previous
+call's contents, so the second call checks that nothing stale leaks in), the multigrid's
+transfers summing in a fixed order.
 
 This file is named to be collected last, so a run that stops at the first failure has run every
 other test first; it also passes alone in a fresh process.
@@ -19,14 +20,6 @@ from markovkit_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 
-# the tolerance the multigrid apply tests use: same operations, another restriction order
-REL_TOL = 1e-11
-
-
-def _relmax(a, b):
-    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
-
-
 @pytest.mark.parametrize("name", ["cfg0_birth_death_1d16", "annihilation_2d8", "birth_death_3d4_cap2"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_noalloc_apply_matches_apply_twice(cuda, name, precision):
@@ -41,12 +34,11 @@ def test_noalloc_apply_matches_apply_twice(cuda, name, precision):
     b = torch.as_tensor(c.data["b"], device=cuda)
     ref = torch.empty_like(b)
     _lib.check(lib.mk_multigrid_apply(M._h, C.c_void_p(b.data_ptr()), C.c_void_p(ref.data_ptr()), stream))
-    tol = REL_TOL if precision == "fp64" else 1e-5
     for _ in range(2):
         out = torch.full_like(b, float("nan"))
         _lib.check(lib.mk_multigrid_apply_noalloc(M._h, C.c_void_p(b.data_ptr()), C.c_void_p(out.data_ptr()), stream))
         torch.cuda.synchronize()
-        assert _relmax(out.cpu().numpy(), ref.cpu().numpy()) < tol
+        assert torch.equal(out, ref)
 
 
 def test_noalloc_rejects_hierarchy_beyond_static_scratch(cuda):
