@@ -28,7 +28,15 @@ MK_HD int tri(int k) {
 
 // the pair (u0 <= u1) of rank r < 2^31
 MK_HD void unrank_pair(int r, int &u0, int &u1) {
-    int k = static_cast<int>((sqrtf(8.0f * static_cast<float>(r) + 1.0f) - 1.0f) * 0.5f);
+    const float q = 8.0f * static_cast<float>(r) + 1.0f;
+    float root;
+#if defined(__CUDA_ARCH__)
+    // an approximate root is enough: the integer correction below makes k exact
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(root) : "f"(q));
+#else
+    root = sqrtf(q);
+#endif
+    int k = static_cast<int>((root - 1.0f) * 0.5f);
     const auto tri64 = [](int q) { return (static_cast<unsigned long long>(q) * (q + 1)) >> 1; };
     k += tri64(k + 1) <= static_cast<unsigned long long>(r) ? 1 : 0;
     k -= tri64(k) > static_cast<unsigned long long>(r) ? 1 : 0;
@@ -40,7 +48,9 @@ MK_HD bool has_lower(unsigned mask, int a) { return ((mask >> (2 * a)) & 1U) != 
 MK_HD bool has_upper(unsigned mask, int a) { return ((mask >> (2 * a + 1)) & 1U) != 0; }
 
 // One species, t <= 2 molecules (u0 <= u1; u0 alone when t = 1), masks m0 and m1 of their
-// voxels. acc(source, rate, 0) per in-jump in visit_row's order.
+// voxels. acc(source, rate, on) per candidate in-jump in visit_row's order: the in-jump exists
+// when on, and the caller reads the source only then (the sum takes rate * 0 otherwise, so
+// that lanes of a warp at different boundaries do not diverge).
 template <typename T, bool WANT_IN, typename Acc>
 MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const StencilSector<T> &ss,
                     int t, int u0, int u1, unsigned m0, unsigned m1, int row, T &exit, T &leak,
@@ -78,16 +88,12 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
                 }
                 const int g = md.gstride[a];
                 const T D = sv.da[0][a];
-                if (has_lower(m0, a)) {
-                    acc(row + g, D, T(0));
-                }
-                if (has_upper(m0, a)) {
-                    acc(row - g, D, T(0));
-                }
+                acc(row + g, D, has_lower(m0, a));
+                acc(row - g, D, has_upper(m0, a));
             }
             for (int k = 0; k < ss.n_in; ++k) {
                 if (ss.in_copies[k] == 1 && ss.rin[k][1] > T(0)) {
-                    acc(ss.in_src[k], ss.rin[k][1], T(0));
+                    acc(ss.in_src[k], ss.rin[k][1], true);
                 }
             }
             return;
@@ -103,12 +109,8 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
                 }
                 const int g = md.gstride[a];
                 const T D = sv.da[0][a];
-                if (has_lower(m0, a)) {
-                    acc(row + g, D, T(0));
-                }
-                if (has_upper(m0, a)) {
-                    acc(row - g, D, T(0));
-                }
+                acc(row + g, D, has_lower(m0, a));
+                acc(row - g, D, has_upper(m0, a));
             }
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -117,12 +119,8 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
                 }
                 const int g = md.gstride[a];
                 const T D = sv.da[0][a];
-                if (has_lower(m1, a)) {
-                    acc(row + g * u1 + tri(g), D, T(0));
-                }
-                if (has_upper(m1, a)) {
-                    acc(row - g * u1 + tri(g - 1), D, T(0));
-                }
+                acc(row + g * u1 + tri(g), D, has_lower(m1, a));
+                acc(row - g * u1 + tri(g - 1), D, has_upper(m1, a));
             }
         } else {
             const int base = row - u0 - tu1; // first row of the sector
@@ -137,14 +135,12 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
                 if (has_lower(m0, a) && !same) {
                     const int uw = u0 + g;
                     if (uw <= u1) {
-                        acc(base + uw + tu1, uw == u1 ? D + D : D, T(0));
+                        acc(base + uw + tu1, uw == u1 ? D + D : D, true);
                     } else {
-                        acc(base + u1 + tri(uw), D, T(0));
+                        acc(base + u1 + tri(uw), D, true);
                     }
                 }
-                if (has_upper(m0, a)) {
-                    acc(row - g, D, T(0));
-                }
+                acc(row - g, D, has_upper(m0, a));
             }
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -153,15 +149,13 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
                 }
                 const int g = md.gstride[a];
                 const T D = sv.da[0][a];
-                if (has_lower(m1, a)) {
-                    acc(base + u0 + tri(u1 + g), D, T(0));
-                }
+                acc(base + u0 + tri(u1 + g), D, has_lower(m1, a));
                 if (has_upper(m1, a) && !same) {
                     const int uw = u1 - g;
                     if (uw >= u0) {
-                        acc(base + u0 + tri(uw), uw == u0 ? D + D : D, T(0));
+                        acc(base + u0 + tri(uw), uw == u0 ? D + D : D, true);
                     } else {
-                        acc(base + uw + tri(u0), D, T(0));
+                        acc(base + uw + tri(u0), D, true);
                     }
                 }
             }
@@ -172,13 +166,13 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
             if (same) {
                 const T a = ss.rin[k][2];
                 if (a > T(0)) {
-                    acc(ss.in_src[k] + (c == 1 ? u0 : 0), a, T(0));
+                    acc(ss.in_src[k] + (c == 1 ? u0 : 0), a, true);
                 }
             } else if (c == 1) {
                 const T a = ss.rin[k][1];
                 if (a > T(0)) {
-                    acc(ss.in_src[k] + u1, a, T(0)); // voxel of u0 loses its copy: {u1} is left
-                    acc(ss.in_src[k] + u0, a, T(0));
+                    acc(ss.in_src[k] + u1, a, true); // voxel of u0 loses its copy: {u1} is left
+                    acc(ss.in_src[k] + u0, a, true);
                 }
             }
         }
@@ -188,7 +182,7 @@ MK_HD void pair_row(const ModelView<T> &md, const StencilView<T> &sv, const Sten
 // The in-jumps of a row's heavy reactions from the voxels w = lane, lane + nlanes, ... (the row
 // holds t <= 1 molecule u; the source holds c more copies of w, at most two molecules): source
 // rank w (one molecule), w + T(w) (two in w) or min + T(max) of {u, w}; rate by the row's count
-// in w. acc(source, rate, 0) per in-jump.
+// in w. acc(source, rate, on) per candidate in-jump (on: the rate is positive).
 template <typename T, typename Acc>
 MK_HD void pair_heavy_terms(const StencilSector<T> &ss, int V, int t, int u, int lane, int nlanes,
                             Acc &&acc) {
@@ -209,9 +203,7 @@ MK_HD void pair_heavy_terms(const StencilSector<T> &ss, int V, int t, int u, int
             } else {
                 rank = u + tri(w);
             }
-            if (a > T(0)) {
-                acc(src + rank, a, T(0));
-            }
+            acc(src + rank, a, a > T(0));
         }
     }
 }
@@ -260,12 +252,8 @@ MK_HD void singles_row(const ModelView<T> &md, const StencilView<T> &sv,
                 }
                 const int step = md.gstride[a] * stride;
                 const T D = sv.da[s][a];
-                if (has_lower(m, a)) {
-                    acc(row + step, D, T(0));
-                }
-                if (has_upper(m, a)) {
-                    acc(row - step, D, T(0));
-                }
+                acc(row + step, D, has_lower(m, a));
+                acc(row - step, D, has_upper(m, a));
             }
         }
     }

@@ -38,13 +38,42 @@ __device__ __forceinline__ void copy_to_shared(const S *src, S &dst) {
     }
 }
 
+// the value at p, read only when on (a bool: the read is predicated, the sum gets 0 otherwise);
+// an `on` of another type is a visitor's reverse rate and the read always happens
+template <typename T, typename On>
+__device__ __forceinline__ T fetch(On on, const T *p) {
+    if constexpr (std::is_same_v<On, bool>) {
+        T v = T(0);
+        if (on) {
+            v = *p;
+        }
+        return v;
+    } else {
+        return *p;
+    }
+}
+
+template <typename On>
+__device__ __forceinline__ float4 fetch4(On on, const float *p) {
+    if constexpr (std::is_same_v<On, bool>) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (on) {
+            v = *reinterpret_cast<const float4 *>(p);
+        }
+        return v;
+    } else {
+        return *reinterpret_cast<const float4 *>(p);
+    }
+}
+
 // The in-jump sums of one row for pass MODE (row_terms for any row visitor):
-// visit(std::bool_constant<WANT_IN>, acc) runs the row with acc(source, rate, reverse_rate).
+// visit(std::bool_constant<WANT_IN>, acc) runs the row with acc(source, rate, on), where `on`
+// is a bool for visitors that name candidate in-jumps (see fetch) and a reverse rate otherwise.
 template <typename T, int NB, int MODE, typename Visit>
 __device__ __forceinline__ void accumulate_terms(const RowParams<T> &p, Visit &&visit, T (&in)[NB],
                                                  T (&in2)[NB]) {
     if constexpr (MODE == kJacobiZero) {
-        visit(std::false_type{}, [](int, T, T) {});
+        visit(std::false_type{}, [](int, T, auto) {});
         return;
     } else {
         // Gauss-Seidel and the ILU passes update x (= y) in place: rows of one colour read only
@@ -53,28 +82,28 @@ __device__ __forceinline__ void accumulate_terms(const RowParams<T> &p, Visit &&
         const T *ax = p.aux;
         if constexpr (NB == 1) {
             if constexpr (MODE == kIluThird) {
-                visit(std::true_type{}, [&](int j, T a, T) { in2[0] += a * ax[j]; });
+                visit(std::true_type{}, [&](int j, T a, auto on) { in2[0] += a * fetch(on, ax + j); });
             } else if constexpr (MODE == kIluSecond) {
-                visit(std::true_type{}, [&](int j, T a, T) {
-                    in[0] += a * xs[j];
-                    in2[0] += a * ax[j];
+                visit(std::true_type{}, [&](int j, T a, auto on) {
+                    in[0] += a * fetch(on, xs + j);
+                    in2[0] += a * fetch(on, ax + j);
                 });
             } else {
-                visit(std::true_type{}, [&](int j, T a, T) { in[0] += a * xs[j]; });
+                visit(std::true_type{}, [&](int j, T a, auto on) { in[0] += a * fetch(on, xs + j); });
             }
         } else if constexpr (kInterleaved<T, NB>) {
             // the kRowBatch source values of an in-jump in one 16-byte load
-            visit(std::true_type{}, [&](int j, T a, T) {
+            visit(std::true_type{}, [&](int j, T a, auto on) {
                 const std::int64_t k = static_cast<std::int64_t>(j) * NB;
                 if constexpr (MODE != kIluThird) {
-                    const float4 v = *reinterpret_cast<const float4 *>(xs + k);
+                    const float4 v = fetch4(on, xs + k);
                     in[0] += a * v.x;
                     in[1] += a * v.y;
                     in[2] += a * v.z;
                     in[3] += a * v.w;
                 }
                 if constexpr (MODE == kIluSecond || MODE == kIluThird) {
-                    const float4 u = *reinterpret_cast<const float4 *>(ax + k);
+                    const float4 u = fetch4(on, ax + k);
                     in2[0] += a * u.x;
                     in2[1] += a * u.y;
                     in2[2] += a * u.z;
@@ -84,7 +113,7 @@ __device__ __forceinline__ void accumulate_terms(const RowParams<T> &p, Visit &&
         } else {
             const int nb = p.nb;
             const std::int64_t ldv = p.ldv;
-            visit(std::true_type{}, [&](int j, T a, T) {
+            visit(std::true_type{}, [&](int j, T a, auto on) {
 #pragma unroll
                 for (int c = 0; c < NB; ++c) {
                     if (c >= nb) {
@@ -92,11 +121,11 @@ __device__ __forceinline__ void accumulate_terms(const RowParams<T> &p, Visit &&
                     }
                     const std::int64_t k = j + c * ldv;
                     if constexpr (MODE == kIluThird) {
-                        in2[c] += a * ax[k];
+                        in2[c] += a * fetch(on, ax + k);
                     } else {
-                        in[c] += a * xs[k];
+                        in[c] += a * fetch(on, xs + k);
                         if constexpr (MODE == kIluSecond) {
-                            in2[c] += a * ax[k];
+                            in2[c] += a * fetch(on, ax + k);
                         }
                     }
                 }

@@ -156,7 +156,11 @@ std::int64_t emu_stencil_check(int dim, const std::int64_t *dims, const double *
                                                         false, 0, 1, e1, l1,
                                                         [&](std::int64_t j, double r, double) { a.emplace_back(j, r); });
                             pair_heavy_terms<double>(ss, p.model->V, ss.total[0], static_cast<int>(local), 0, 1,
-                                                     [&](int j, double r, double) { b.emplace_back(j, r); });
+                                                     [&](int j, double r, bool on) {
+                                                         if (on) {
+                                                             b.emplace_back(j, r);
+                                                         }
+                                                     });
                             std::sort(a.begin(), a.end());
                             std::sort(b.begin(), b.end());
                             if (a != b) {
@@ -184,7 +188,11 @@ std::int64_t emu_stencil_check(int dim, const std::int64_t *dims, const double *
                         const int V = p.model->V;
                         int u0 = 0, u1 = 0;
                         unsigned m0 = 0, m1 = 0;
-                        auto acc = [&](int j, double r, double) { b.emplace_back(j, r); };
+                        auto acc = [&](int j, double r, bool on) {
+                            if (on) {
+                                b.emplace_back(j, r);
+                            }
+                        };
                         if (S == 1) {
                             const int t = ss.total[0];
                             if (t == 2) {
