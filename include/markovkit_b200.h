@@ -157,7 +157,8 @@ typedef struct {
     int coarse_cycles;
     int sweep_growth;
     int smoother;  /* 0 weighted Jacobi (reference default), 1 red-black Gauss-Seidel,
-                      2 red-black ILU(0) (block ILU of rdme_full_multigrid.cpp:204-296 in colour order) */
+                      2 red-black ILU(0) (block ILU of rdme_full_multigrid.cpp:204-296 in colour order),
+                      3 aggregate blocks (relaxation::aggregate_block, multigrid.hpp:239-341; batch 1) */
     int precision; /* 0 FP64, 1 FP32 (use inside flexible GMRES) */
     int batch;     /* right-hand sides one cycle can serve at once (1..4), for batch solvers */
 } mk_multigrid_options;

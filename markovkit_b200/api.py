@@ -396,7 +396,7 @@ def multigrid_options(**kw) -> MultigridOptions:
     load().mk_multigrid_options_default(C.byref(o))
     for k, v in kw.items():
         if k == "smoother" and isinstance(v, str):
-            v = {"jacobi": 0, "gauss_seidel": 1, "ilu0": 2}[v]
+            v = {"jacobi": 0, "gauss_seidel": 1, "ilu0": 2, "aggregate_block": 3}[v]
         if k == "precision" and isinstance(v, str):
             v = {"fp64": 0, "fp32": 1}[v]
         setattr(o, k, v)

@@ -451,8 +451,11 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     if (model.V != space.V || model.S != space.S) {
         throw Error(kEInval, "model and space disagree on voxels or species");
     }
-    if (opt.smoother < 0 || opt.smoother > 2 || opt.precision < 0 || opt.precision > 1) {
+    if (opt.smoother < 0 || opt.smoother > 3 || opt.precision < 0 || opt.precision > 1) {
         throw Error(kEInval, "unknown smoother or precision");
+    }
+    if (opt.smoother == 3 && opt.batch != 1) {
+        throw Error(kEInval, "the aggregate-block smoother serves one right-hand side at a time");
     }
     if (opt.batch < 1 || opt.batch > kRowBatch) {
         throw Error(kEInval, "multigrid batch must be in 1.." + std::to_string(kRowBatch));
@@ -517,13 +520,21 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
         L->op.finalize(*grid_model, false);
 
         // dense inverses of the terminal blocks, from the same matrix-free rows
-        std::vector<double> inv_all, A, inv;
+        std::vector<double> inv_all, A, inv, dense_all;
         for (std::size_t k = 0; k < L->op.sectors.size(); ++k) {
             const SectorDesc &sec = L->op.sectors[k];
             if (sec.terminal < 0) {
                 continue;
             }
             assemble_terminal(L->op, static_cast<int>(k), shift, A);
+            if (opt.smoother == 3) {
+                DenseBlock db;
+                db.begin = sec.begin;
+                db.a_offset = static_cast<std::int64_t>(dense_all.size());
+                db.n = static_cast<int>(sec.size);
+                L->h_dense.push_back(db);
+                dense_all.insert(dense_all.end(), A.begin(), A.end());
+            }
             if (!invert_dense(A, static_cast<int>(sec.size), inv)) {
                 throw Error(kESingular, "population_multigrid: singular block");
             }
@@ -534,6 +545,11 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
         L->inv64.upload(inv_all);
         std::vector<float> inv_f(inv_all.begin(), inv_all.end());
         L->inv32.upload(inv_f);
+        if (opt.smoother == 3) {
+            L->d_dense.upload(L->h_dense);
+            L->dense64.upload(dense_all);
+            L->dense32.upload(std::vector<float>(dense_all.begin(), dense_all.end()));
+        }
 
         if (!next_totals.empty()) {
             // parent voxel of every fine voxel (multigrid.hpp:56-65)
@@ -542,6 +558,11 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
             parent_map(model.dim, dims, cdims, parent, log_children);
             L->parent.upload(parent);
             L->log_children.upload(log_children);
+            if (opt.smoother == 3) {
+                build_aggregates(*L, parent, static_cast<int>(log_children.size()));
+            }
+        } else if (opt.smoother == 3) {
+            L->agg_ptr.assign(1, 0);
         }
         levels.push_back(std::move(L));
         totals = next_totals;
@@ -644,6 +665,166 @@ void Multigrid::ilu_sweep(Level &L, RowParams<T> p, T *x, const T *rhs, T *work,
     L.op.run<T>(kIluThird, p, stream);
 }
 
+// The blocks of the aggregate-block smoother on one level (population_multigrid::build_blocks,
+// markovkit/rdme/multigrid.hpp:266-299): for each coarse voxel a, the states of the non-terminal
+// sectors grouped by their molecules outside a's fine voxels; groups of one state are skipped.
+// Per block: its states (ascending), the rows of A = shift I - Q of those states and the dense
+// inverse of A restricted to them (the reference factors the same matrix, multigrid.hpp:247-264).
+void Multigrid::build_aggregates(Level &L, const std::vector<int> &parent, int coarse_voxels) {
+    const OperatorLevel &op = L.op;
+    const int V = op.V, S = op.S;
+    const BinomTable B = op.binom->host_view();
+    auto st = std::make_unique<RowState<kMaxSpecies, 64>>();
+    // key: per species the count inside the coarse voxel, then the outside molecules
+    std::vector<std::map<std::vector<int>, std::vector<std::int64_t>>> groups(
+        static_cast<std::size_t>(coarse_voxels));
+    for (const SectorDesc &sec : op.sectors) {
+        if (sec.coarse < 0) {
+            continue;
+        }
+        for (std::int64_t local = 0; local < sec.size; ++local) {
+            load_state<kMaxSpecies, 64>(B, sec, S, V, local, *st);
+            std::vector<int> seen;
+            for (int s = 0; s < S; ++s) {
+                for (int q = 0; q < sec.total[s]; ++q) {
+                    const int a = parent[V - 1 - st->u[s][q]];
+                    if (std::find(seen.begin(), seen.end(), a) != seen.end()) {
+                        continue;
+                    }
+                    seen.push_back(a);
+                    std::vector<int> key;
+                    for (int s2 = 0; s2 < S; ++s2) {
+                        int inside = 0;
+                        for (int q2 = 0; q2 < sec.total[s2]; ++q2) {
+                            inside += parent[V - 1 - st->u[s2][q2]] == a ? 1 : 0;
+                        }
+                        key.push_back(inside);
+                        for (int q2 = 0; q2 < sec.total[s2]; ++q2) {
+                            if (parent[V - 1 - st->u[s2][q2]] != a) {
+                                key.push_back(st->u[s2][q2]);
+                            }
+                        }
+                        key.push_back(-1);
+                    }
+                    groups[a][key].push_back(sec.begin + local);
+                }
+            }
+        }
+    }
+    std::vector<AggBlock> blocks;
+    std::vector<int> states, row_col;
+    std::vector<std::int64_t> row_ptr{0};
+    std::vector<double> row_val, inv_all, A, inv;
+    L.agg_ptr.assign(1, 0);
+    for (int a = 0; a < coarse_voxels; ++a) {
+        for (auto &[key, members] : groups[a]) {
+            if (members.size() < 2) {
+                continue;
+            }
+            const int n = static_cast<int>(members.size());
+            AggBlock blk;
+            blk.state0 = static_cast<std::int64_t>(states.size());
+            blk.inv0 = static_cast<std::int64_t>(inv_all.size());
+            blk.n = n;
+            A.assign(static_cast<std::size_t>(n) * n, 0.0);
+            for (int k = 0; k < n; ++k) {
+                const std::int64_t i = members[k];
+                const int slot = [&] {
+                    int q = 0;
+                    while (q + 1 < static_cast<int>(op.sectors.size()) && op.sectors[q + 1].begin <= i) {
+                        ++q;
+                    }
+                    return q;
+                }();
+                const SectorDesc &sec = op.sectors[slot];
+                load_state<kMaxSpecies, 64>(B, sec, S, V, i - sec.begin, *st);
+                double exit = 0.0, leak = 0.0;
+                std::vector<std::pair<std::int64_t, double>> in;
+                visit_row<double, kMaxSpecies, 64>(B, op.sectors.data(), sec, op.t64.host, i - sec.begin, *st,
+                                                   true, 0, 1, exit, leak,
+                                                   [&](std::int64_t j, double rate, double) { in.emplace_back(j, rate); });
+                A[static_cast<std::size_t>(k) * n + k] += shift + exit;
+                row_col.push_back(static_cast<int>(i));
+                row_val.push_back(shift + exit);
+                for (const auto &[j, rate] : in) {
+                    row_col.push_back(static_cast<int>(j));
+                    row_val.push_back(-rate);
+                    const auto it = std::lower_bound(members.begin(), members.end(), j);
+                    if (it != members.end() && *it == j) {
+                        A[static_cast<std::size_t>(k) * n + (it - members.begin())] -= rate;
+                    }
+                }
+                row_ptr.push_back(static_cast<std::int64_t>(row_col.size()));
+                states.push_back(static_cast<int>(i));
+            }
+            if (!invert_dense(A, n, inv)) {
+                throw Error(kESingular, "population_multigrid: singular block");
+            }
+            inv_all.insert(inv_all.end(), inv.begin(), inv.end());
+            blocks.push_back(blk);
+        }
+        L.agg_ptr.push_back(static_cast<int>(blocks.size()));
+    }
+    L.agg_blocks.upload(blocks);
+    L.agg_states.upload(states);
+    L.agg_row_ptr.upload(row_ptr);
+    L.agg_row_col.upload(row_col);
+    if (opt.precision == 0) {
+        L.agg_val64.upload(row_val);
+        L.agg_inv64.upload(inv_all);
+        L.agg_r64.resize(states.size());
+        L.agg_e64.resize(states.size());
+    } else {
+        L.agg_val32.upload(std::vector<float>(row_val.begin(), row_val.end()));
+        L.agg_inv32.upload(std::vector<float>(inv_all.begin(), inv_all.end()));
+        L.agg_r32.resize(states.size());
+        L.agg_e32.resize(states.size());
+    }
+}
+
+// `sweeps` sweeps of the aggregate-block smoother on (rhs, x) (population_multigrid::smooth,
+// markovkit/rdme/multigrid.hpp:319-341): block Gauss-Seidel over the coarse voxels in order
+// (backwards when reverse), the blocks of one coarse voxel solved from the same residual; the
+// terminal sectors take weighted Jacobi sweeps on their dense blocks (multigrid.hpp:309-317)
+template <typename T>
+void Multigrid::aggregate_smooth(Level &L, const T *rhs, T *x, T *scratch, int sweeps, bool reverse,
+                                 bool from_zero, cudaStream_t stream) {
+    const T *dense;
+    AggView<T> v;
+    v.blocks = L.agg_blocks.get();
+    v.states = L.agg_states.get();
+    v.row_ptr = L.agg_row_ptr.get();
+    v.row_col = L.agg_row_col.get();
+    if constexpr (std::is_same_v<T, double>) {
+        dense = L.dense64.get();
+        v.row_val = L.agg_val64.get();
+        v.inv = L.agg_inv64.get();
+        v.r = L.agg_r64.get();
+        v.e = L.agg_e64.get();
+    } else {
+        dense = L.dense32.get();
+        v.row_val = L.agg_val32.get();
+        v.inv = L.agg_inv32.get();
+        v.r = L.agg_r32.get();
+        v.e = L.agg_e32.get();
+    }
+    check_cuda(launch_dense_jacobi<T>(L.d_dense.get(), static_cast<int>(L.h_dense.size()), dense, rhs, x,
+                                      scratch, static_cast<T>(opt.jacobi_weight), sweeps, from_zero, stream),
+               "dense Jacobi");
+    const int aggregates = static_cast<int>(L.agg_ptr.size()) - 1;
+    for (int sweep = 0; sweep < sweeps; ++sweep) {
+        for (int step = 0; step < aggregates; ++step) {
+            const int a = reverse ? aggregates - 1 - step : step;
+            const int b0 = L.agg_ptr[a], b1 = L.agg_ptr[a + 1];
+            if (b1 <= b0) {
+                continue;
+            }
+            check_cuda(launch_aggregate_solve<T>(v, b0, b1, rhs, x, stream), "aggregate solve");
+            check_cuda(launch_aggregate_update<T>(v, b0, b1, x, stream), "aggregate update");
+        }
+    }
+}
+
 int Multigrid::levels_of_sector(int k) const {
     int count = 0;
     for (const auto &L : levels) {
@@ -741,11 +922,14 @@ T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
                 L.op.run<T>(kGaussSeidel, p, stream);
             }
         }
-    } else {
+    } else if (opt.smoother == 2) {
         check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
         for (int k = 0; k < L.pre; ++k) {
             ilu_sweep<T>(L, p, x, rhs, tmp, stream);
         }
+    } else {
+        check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
+        aggregate_smooth<T>(L, rhs, x, tmp, L.pre, false, true, stream);
     }
 
     // r = b - A x on every row; the coarse right-hand side is its restriction, summed in a
@@ -825,10 +1009,12 @@ T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
                 L.op.run<T>(kGaussSeidel, p, stream);
             }
         }
-    } else {
+    } else if (opt.smoother == 2) {
         for (int k = 0; k < L.post; ++k) {
             ilu_sweep<T>(L, p, x, rhs, tmp, stream);
         }
+    } else {
+        aggregate_smooth<T>(L, rhs, x, tmp, L.post, true, false, stream);
     }
     // keep the result in x's own buffer so the caller's view of the level stays fixed
     if (x != buf<T>(L, 1, cl)) {
@@ -936,8 +1122,10 @@ void Multigrid::smooth(int d, const double *b, double *x, cudaStream_t stream) {
             p.colour = c;
             L.op.run<double>(kGaussSeidel, p, stream);
         }
-    } else {
+    } else if (opt.smoother == 2) {
         ilu_sweep<double>(L, p, x, b, tmp, stream);
+    } else {
+        aggregate_smooth<double>(L, b, x, tmp, 1, false, false, stream);
     }
 }
 

@@ -3,6 +3,7 @@
 // memory and launches the sm_100a kernels of row_kernels.cu and krylov.cu on a caller stream.
 #pragma once
 
+#include "aggregate.cuh"
 #include "host_model.hpp"
 #include "krylov.cuh"
 #include "launch_count.hpp"
@@ -180,7 +181,7 @@ struct MultigridOptions {
     int coarse_cycles = 1;
     int sweep_growth = 0;
     int smoother = 0;  // 0 weighted Jacobi (the reference's default), 1 red-black Gauss-Seidel,
-                       // 2 red-black ILU(0)
+                       // 2 red-black ILU(0), 3 aggregate blocks (relaxation::aggregate_block)
     int precision = 0; // 0 FP64, 1 FP32 preconditioner
     int batch = 1;     // right-hand sides one cycle can serve at once (work vectors per level)
 };
@@ -206,6 +207,18 @@ struct Multigrid {
         // red-black ILU(0) pivots (smoother 2): diagonal on colour 0, modified on colour 1
         DeviceArray<double> piv64;
         DeviceArray<float> piv32;
+        // aggregate-block smoother (smoother 3): the blocks of coarse voxel a are
+        // [agg_ptr[a], agg_ptr[a + 1]); the terminal sectors keep Jacobi on their dense blocks
+        std::vector<int> agg_ptr;
+        DeviceArray<AggBlock> agg_blocks;
+        DeviceArray<int> agg_states, agg_row_col;
+        DeviceArray<std::int64_t> agg_row_ptr;
+        DeviceArray<double> agg_val64, agg_inv64, agg_r64, agg_e64;
+        DeviceArray<float> agg_val32, agg_inv32, agg_r32, agg_e32;
+        std::vector<DenseBlock> h_dense;
+        DeviceArray<DenseBlock> d_dense;
+        DeviceArray<double> dense64;
+        DeviceArray<float> dense32;
         // work vectors (precision of the preconditioner)
         DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
         DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
@@ -263,6 +276,10 @@ struct Multigrid {
     T *buf(Level &L, int which, void *const *carve_level = nullptr);
     template <typename T>
     const T *weights(const Level &L) const;
+    void build_aggregates(Level &L, const std::vector<int> &parent, int coarse_voxels);
+    template <typename T>
+    void aggregate_smooth(Level &L, const T *rhs, T *x, T *scratch, int sweeps, bool reverse,
+                          bool from_zero, cudaStream_t stream);
     void build_transfers();
     void ensure_graph(int nb);
     // the captured cycle for each batch width, and its kernel nodes

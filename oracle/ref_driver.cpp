@@ -205,6 +205,9 @@ int run(const args &a) {
     mgo.max_levels = static_cast<int>(a.integer("max_levels", 32));
     mgo.coarse_cycles = static_cast<int>(a.integer("cycles", 1));
     mgo.sweep_growth = static_cast<int>(a.integer("growth", 0));
+    if (a.get("smoother", "jacobi") == "aggregate") {
+        mgo.smoother = relaxation::aggregate_block;
+    }
 
     if (a.integer("do_mg", 1)) {
         t0 = clock_type::now();
