@@ -263,7 +263,10 @@ int mk_batch_solver_solve(mk_batch_solver solver, const double *d_b, double *d_x
 
 /* ---- Krylov FSP: solve_krylov_fsp(model, initial, final_time, options), markovkit/fsp.hpp ---- */
 /* krylov_fsp_options (fsp.hpp:190-202) with inside = box(bounds) (fsp.hpp:26-35); save_every
- * has no counterpart: only the final distribution is kept */
+ * has no counterpart: only the final distribution is kept. method 1 runs solve_adaptive_fsp
+ * instead (fsp.hpp:108-188) with adaptive_fsp_options' step_scale, prune_fraction,
+ * flux_tolerance and min_probability (layers, max_steps (steps), krylov_dim and krylov_tol as
+ * named; sampled_expansion is not offered) */
 typedef struct {
     double tolerance;        /* the probability that may leak by final_time */
     double initial_step;
@@ -272,8 +275,13 @@ typedef struct {
     double drop_derivative;
     int layers;
     int krylov_dim;          /* 1..30 */
-    int64_t max_steps;       /* attempts */
+    int64_t max_steps;       /* attempts (method 1: steps) */
     double krylov_tol;
+    int method;              /* 0 solve_krylov_fsp, 1 solve_adaptive_fsp */
+    double step_scale;       /* method 1: each step expects about this many jumps */
+    double prune_fraction;   /* method 1: the least likely fraction of states may be pruned ... */
+    double flux_tolerance;   /* ... if its probability flux is below this share of the total */
+    double min_probability;  /* method 1: also prune any state below this probability */
 } mk_fsp_options;
 void mk_fsp_options_default(mk_fsp_options *opt);
 /* One instance. A reaction_network (markovkit/reaction_network.hpp:11-39) restricted to the

@@ -13,7 +13,8 @@
 //   num::gmres_options, num::solver_result,
 //   num::gmres(A, [M], b, x, options)          call sites tests/test_rdme.cpp:238-249
 //   reaction_network, box, krylov_fsp_options,
-//   fsp_solution, solve_krylov_fsp             markovkit/reaction_network.hpp, fsp.hpp:26-254
+//   adaptive_fsp_options, fsp_solution,
+//   solve_krylov_fsp, solve_adaptive_fsp       markovkit/reaction_network.hpp, fsp.hpp:26-254
 // Differences: the voxel graph is a structured grid (grid<1..3>); a region for FSP is a box;
 // krylov_dim <= 30; fsp_solution keeps the initial and final snapshots only.
 #pragma once
@@ -625,6 +626,22 @@ struct krylov_fsp_options {
     real krylov_tol = 1e-8;
 };
 
+// adaptive_fsp_options (fsp.hpp:108-121); sampled_expansion has no device counterpart
+struct adaptive_fsp_options {
+    region inside;
+    real step_scale = 1.0;
+    real prune_fraction = 0.1;
+    real flux_tolerance = 1e-6;
+    real min_probability = 0.0;
+    int layers = 1;
+    bool sampled_expansion = false;
+    unsigned seed = 42;
+    int save_every = 1000; // accepted for source compatibility; only the final state is saved
+    int max_steps = 1 << 28;
+    int krylov_dim = 30;
+    real krylov_tol = 1e-8;
+};
+
 class distribution {
   public:
     distribution() = default;
@@ -675,8 +692,8 @@ struct fsp_tables {
     idx box = 1;
 };
 
-inline fsp_tables tabulate(const reaction_network &model, const state &initial,
-                           const krylov_fsp_options &o) {
+// the network's propensities over the region of the options (krylov_ or adaptive_fsp_options)
+inline fsp_tables tabulate(const reaction_network &model, const state &initial, const auto &o) {
     fsp_tables t;
     t.bounds = o.inside.bounds;
     const idx S = t.bounds.size();
@@ -732,11 +749,35 @@ inline mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model
     return p;
 }
 
-} // namespace detail
+inline mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model, real T,
+                              const adaptive_fsp_options &o) {
+    if (o.sampled_expansion) {
+        throw std::invalid_argument("solve_adaptive_fsp: the device expands every neighbour");
+    }
+    mk_fsp_problem p{};
+    p.n_species = static_cast<int>(t.bounds.size());
+    p.n_reactions = static_cast<int>(model.reactions.size());
+    p.bounds = t.bounds.data();
+    p.change = t.change.data();
+    p.rates = t.rates.data();
+    p.initial = t.initial.data();
+    p.final_time = T;
+    mk_fsp_options_default(&p.options);
+    p.options.method = 1;
+    p.options.step_scale = o.step_scale;
+    p.options.prune_fraction = o.prune_fraction;
+    p.options.flux_tolerance = o.flux_tolerance;
+    p.options.min_probability = o.min_probability;
+    p.options.layers = o.layers;
+    p.options.krylov_dim = o.krylov_dim;
+    p.options.max_steps = o.max_steps;
+    p.options.krylov_tol = o.krylov_tol;
+    return p;
+}
 
-// solve_krylov_fsp for several instances in one launch
-inline array<fsp_solution> solve_krylov_fsp_batch(
-    const array<std::tuple<reaction_network, state, real, krylov_fsp_options>> &instances) {
+// every instance in one launch of the batched FSP kernel
+template <typename Options>
+array<fsp_solution> solve_batch(const array<std::tuple<reaction_network, state, real, Options>> &instances) {
     array<detail::fsp_tables> tables;
     array<mk_fsp_problem> problems;
     tables.reserve(instances.size());
@@ -785,6 +826,26 @@ inline array<fsp_solution> solve_krylov_fsp_batch(
         off += t.box;
     }
     return sols;
+}
+
+} // namespace detail
+
+// solve_krylov_fsp for several instances in one launch
+inline array<fsp_solution> solve_krylov_fsp_batch(
+    const array<std::tuple<reaction_network, state, real, krylov_fsp_options>> &instances) {
+    return detail::solve_batch(instances);
+}
+
+// solve_adaptive_fsp for several instances in one launch
+inline array<fsp_solution> solve_adaptive_fsp_batch(
+    const array<std::tuple<reaction_network, state, real, adaptive_fsp_options>> &instances) {
+    return detail::solve_batch(instances);
+}
+
+// FSP with flux-controlled steps on the GPU (fsp.hpp:123-188)
+inline fsp_solution solve_adaptive_fsp(const reaction_network &model, const state &initial,
+                                       real final_time, const adaptive_fsp_options &options = {}) {
+    return solve_adaptive_fsp_batch({{model, initial, final_time, options}}).front();
 }
 
 // the Krylov FSP of Vo and Sidje on the GPU (fsp.hpp:207-254)

@@ -75,6 +75,11 @@ class FspOptions(C.Structure):
         ("krylov_dim", C.c_int),
         ("max_steps", C.c_int64),
         ("krylov_tol", C.c_double),
+        ("method", C.c_int),
+        ("step_scale", C.c_double),
+        ("prune_fraction", C.c_double),
+        ("flux_tolerance", C.c_double),
+        ("min_probability", C.c_double),
     ]
 
 

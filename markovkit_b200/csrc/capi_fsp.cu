@@ -80,6 +80,11 @@ void check_options(const mk_fsp_options &o) {
                    std::isfinite(o.step_growth) && std::isfinite(o.krylov_tol) &&
                    o.krylov_tol > 0.0,
                "fsp: options must be finite, krylov_tol > 0");
+    MK_REQUIRE(o.method == 0 || o.method == 1, "fsp: method must be 0 (Krylov) or 1 (adaptive)");
+    MK_REQUIRE(std::isfinite(o.step_scale) && o.step_scale > 0.0 && std::isfinite(o.prune_fraction) &&
+                   o.prune_fraction >= 0.0 && std::isfinite(o.flux_tolerance) &&
+                   std::isfinite(o.min_probability),
+               "fsp: adaptive options must be finite, step_scale > 0, prune_fraction >= 0");
 }
 
 int sm_count() {
@@ -151,6 +156,11 @@ void mk_fsp_options_default(mk_fsp_options *opt) {
     opt->krylov_dim = 30;
     opt->max_steps = std::int64_t(1) << 28;
     opt->krylov_tol = 1e-8;
+    opt->method = 0;
+    opt->step_scale = 1.0;
+    opt->prune_fraction = 0.1;
+    opt->flux_tolerance = 1e-6;
+    opt->min_probability = 0.0;
 }
 
 int mk_fsp_box_size(int n_species, const int *bounds, int64_t *size) {
@@ -221,6 +231,11 @@ int mk_fsp_batch_create(int n, const mk_fsp_problem *problems, mk_fsp_batch *out
             I.drop_probability = p.options.drop_probability;
             I.drop_derivative = p.options.drop_derivative;
             I.krylov_tol = p.options.krylov_tol;
+            I.method = p.options.method;
+            I.step_scale = p.options.step_scale;
+            I.prune_fraction = p.options.prune_fraction;
+            I.flux_tolerance = p.options.flux_tolerance;
+            I.min_probability = p.options.min_probability;
             rate_offset[k] = rate_total;
             I.rate_offset = rate_total;
             rate_total += box * p.n_reactions;

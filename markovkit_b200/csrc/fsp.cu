@@ -77,6 +77,8 @@ struct Shared {
     double h1[kE];                   // first projections, kept for the Hessenberg column
     int i[8];
     int scan[kMaxWarps + 1];
+    int hist[256];            // radix-select histogram of the adaptive pruning
+    unsigned long long key;   // the select's prefix, broadcast
 };
 
 struct Ctx {
@@ -294,8 +296,10 @@ __device__ void place(Ctx &c, int n, int m) {
 // Q on the support (generator.hpp:27-44, absorbing): for slot k and reaction r the source
 // slot and rate of the jump into k (coefficient 0 and the slot itself when there is none),
 // and the exit rate of k over every valid positive jump
+// With `reflecting` (the adaptive FSP's generator, boundary::reflecting), the exit rate counts
+// only the jumps that land in the support.
 template <int NT>
-__device__ void assemble(const Ctx &c, int n) {
+__device__ void assemble(const Ctx &c, int n, bool reflecting = false) {
     const FspInstance &in = *c.in;
     for (int k = threadIdx.x; k < n; k += NT) {
         const int i = c.s2b[k];
@@ -303,20 +307,22 @@ __device__ void assemble(const Ctx &c, int n) {
         coords(in, i, xi);
         double ex = 0.0;
         for (int r = 0; r < in.R; ++r) {
-            bool valid = true, inside = true;
-            int j = i;
+            bool valid = true, inside = true, lands = true;
+            int j = i, to = i;
 #pragma unroll
             for (int s = 0; s < kFspMaxSpecies; ++s) {
                 if (s < in.S) {
                     const int ch = in.change[r][s];
                     valid = valid && xi[s] + ch >= 0;
+                    lands = lands && xi[s] + ch <= in.bound[s];
                     const int xs = xi[s] - ch;
                     inside = inside && xs >= 0 && xs <= in.bound[s];
                     j -= ch * in.stride[s];
+                    to += ch * in.stride[s];
                 }
             }
             const double a = c.rate[static_cast<std::int64_t>(r) * in.box + i];
-            if (a > 0.0 && valid) {
+            if (a > 0.0 && valid && (!reflecting || (lands && c.b2s[to] >= 0))) {
                 ex += a;
             }
             int sl = k;
@@ -816,6 +822,120 @@ __device__ int expand(Shared &sh, const Ctx &c, int n) {
     return f1;
 }
 
+// ---- adaptive FSP (fsp.hpp:108-188) ---------------------------------------------------------
+
+// the rate out of slot k over every existing jump (the reflecting generator's exit plus leak)
+__device__ __forceinline__ double out_rate(const Ctx &c, int k) {
+    const FspInstance &in = *c.in;
+    const int i = c.s2b[k];
+    int xi[kFspMaxSpecies];
+    coords(in, i, xi);
+    double out = 0.0;
+    for (int r = 0; r < in.R; ++r) {
+        bool valid = true;
+#pragma unroll
+        for (int s = 0; s < kFspMaxSpecies; ++s) {
+            if (s < in.S) {
+                valid = valid && xi[s] + in.change[r][s] >= 0;
+            }
+        }
+        const double a = c.rate[static_cast<std::int64_t>(r) * in.box + i];
+        if (a > 0.0 && valid) {
+            out += a;
+        }
+    }
+    return out;
+}
+
+// probabilities are non-negative: their bit patterns order like the values (-0 counts as 0)
+__device__ __forceinline__ unsigned long long prob_key(double p) {
+    return p > 0.0 ? static_cast<unsigned long long>(__double_as_longlong(p)) : 0ULL;
+}
+
+// flag[k] = 1 for the `count` slots of smallest probability, ties broken by slot (the order of
+// num::smallest_indices), else 0: a radix select over the keys, eight bits per pass, then the
+// first ties of the selected key in slot order
+template <int NT>
+__device__ void mark_smallest(Shared &sh, Ctx &c, int n, int count, double *flag) {
+    for (int k = threadIdx.x; k < n; k += NT) {
+        flag[k] = 0.0;
+    }
+    __syncthreads();
+    if (count <= 0) {
+        return;
+    }
+    unsigned long long prefix = 0ULL;
+    int want = count; // rank of the key sought within the keys that share the prefix so far
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int b = threadIdx.x; b < 256; b += NT) {
+            sh.hist[b] = 0;
+        }
+        __syncthreads();
+        const unsigned long long high = shift == 56 ? 0ULL : (~0ULL << (shift + 8));
+        for (int k = threadIdx.x; k < n; k += NT) {
+            const unsigned long long key = prob_key(c.prob[k]);
+            if ((key & high) == (prefix & high)) {
+                atomicAdd(&sh.hist[(key >> shift) & 255ULL], 1);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0, b = 0;
+            for (; b < 255 && acc + sh.hist[b] < want; ++b) {
+                acc += sh.hist[b];
+            }
+            sh.key = prefix | (static_cast<unsigned long long>(b) << shift);
+            sh.i[4] = want - acc;
+        }
+        __syncthreads();
+        prefix = sh.key;
+        want = sh.i[4];
+        __syncthreads();
+    }
+    compact<NT>(
+        sh, n, [&](int k) { return prob_key(c.prob[k]) == prefix; },
+        [&](int k, int dest) {
+            if (dest < want) {
+                flag[k] = 1.0;
+            }
+        });
+    for (int k = threadIdx.x; k < n; k += NT) {
+        if (prob_key(c.prob[k]) < prefix) {
+            flag[k] = 1.0;
+        }
+    }
+    __syncthreads();
+}
+
+// keep the slots with keep(k), in order, and renormalise to total probability one
+template <int NT, typename Keep>
+__device__ int keep_and_normalise(Shared &sh, Ctx &c, int n, Keep keep) {
+    const int kept = compact<NT>(sh, n, keep, [&](int k, int dest) {
+        c.buf0[dest] = c.prob[k];
+        c.itmp[dest] = c.s2b[k];
+    });
+    for (int k = threadIdx.x; k < n; k += NT) {
+        c.b2s[c.s2b[k]] = -1;
+    }
+    __syncthreads();
+    double tot = 0.0;
+    for (int k = threadIdx.x; k < kept; k += NT) {
+        const int j = c.itmp[k];
+        c.s2b[k] = j;
+        c.b2s[j] = k;
+        c.prob[k] = c.buf0[k];
+        tot += c.buf0[k];
+    }
+    const double total = block_reduce<NT, false>(sh, c, tot);
+    if (total > 0.0) {
+        for (int k = threadIdx.x; k < kept; k += NT) {
+            c.prob[k] /= total;
+        }
+    }
+    __syncthreads();
+    return kept;
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchView v) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -878,7 +998,57 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
         Counters cnt;
         int status = 0;
         const std::int64_t limit = in.max_steps < kAttemptLimit ? in.max_steps : kAttemptLimit;
-        for (; t < in.final_time && attempt < limit; ++attempt) {
+        // adaptive FSP: every step is taken (fsp.hpp:133-181)
+        for (; in.method == 1 && t < in.final_time && attempt < limit; ++attempt) {
+            n = expand<NT>(sh, c, n);
+            const int m = min(max(in.krylov_dim, 1), n);
+            place(c, n, m);
+            double act = 0.0;
+            for (int k = threadIdx.x; k < n; k += NT) {
+                c.w[k] = c.prob[k];
+            }
+            assemble<NT>(c, n, true);
+            for (int k = threadIdx.x; k < n; k += NT) {
+                act += c.prob[k] * c.diag[k];
+            }
+            const double activity = block_reduce<NT, false>(sh, c, act);
+            const double dt = activity > 0.0 ? fmin(in.step_scale / activity, in.final_time - t)
+                                             : in.final_time - t;
+            status = expv<NT>(sh, c, n, m, dt, in.krylov_tol, cnt);
+            if (status != 0) {
+                break;
+            }
+            for (int k = threadIdx.x; k < n; k += NT) {
+                c.prob[k] = fmax(0.0, c.w[k]);
+            }
+            __syncthreads();
+            // prune the unlikely states whose probability flux is negligible
+            double *drop = c.buf1;
+            if (n > 1) {
+                double fl = 0.0;
+                for (int k = threadIdx.x; k < n; k += NT) {
+                    c.tmp[k] = c.prob[k] * out_rate(c, k);
+                    fl += c.tmp[k];
+                }
+                const double total_flux = block_reduce<NT, false>(sh, c, fl);
+                const int candidates = min(static_cast<int>(llround(in.prune_fraction * static_cast<double>(n))), n - 1);
+                mark_smallest<NT>(sh, c, n, candidates, drop);
+                for (int k = threadIdx.x; k < n; k += NT) {
+                    const bool d = (drop[k] != 0.0 && c.tmp[k] < in.flux_tolerance * total_flux) ||
+                                   c.prob[k] < in.min_probability;
+                    drop[k] = d ? 1.0 : 0.0;
+                }
+            } else {
+                for (int k = threadIdx.x; k < n; k += NT) {
+                    drop[k] = 0.0;
+                }
+            }
+            __syncthreads();
+            n = keep_and_normalise<NT>(sh, c, n, [&](int k) { return drop[k] == 0.0; });
+            t += dt;
+            ++accepted;
+        }
+        for (; in.method == 0 && t < in.final_time && attempt < limit; ++attempt) {
             tau = fmin(tau, in.final_time - t);
             n = expand<NT>(sh, c, n);
             const int m = min(max(in.krylov_dim, 1), n);

@@ -31,6 +31,13 @@ struct FspInstance {
     double tolerance = 1e-6, initial_step = 1.0, step_growth = 2.0;
     double drop_probability = 1e-10, drop_derivative = 1e-16;
     double krylov_tol = 1e-8;
+    // 0: solve_krylov_fsp (fsp.hpp:190-254); 1: solve_adaptive_fsp (fsp.hpp:108-188), whose steps
+    // take step_scale / (expected jump rate) and prune the least likely prune_fraction of the
+    // support where their flux is below flux_tolerance of the total, and any state below
+    // min_probability
+    int method = 0;
+    int pad = 0;
+    double step_scale = 1.0, prune_fraction = 0.1, flux_tolerance = 1e-6, min_probability = 0.0;
 };
 
 // per-instance outcome

@@ -1,4 +1,4 @@
-"""Python mirror of MarkovKit's Krylov finite state projection over the C ABI.
+"""Python mirror of MarkovKit's Krylov and adaptive finite state projection over the C ABI.
 
 Names and argument meaning follow markovkit/fsp.hpp and markovkit/reaction_network.hpp:
 reaction_network{reactions: [reaction{change, rate}]}, krylov_fsp_options (fsp.hpp:190-202)
@@ -90,6 +90,41 @@ class krylov_fsp_options:
 
 
 @dataclass
+class adaptive_fsp_options:
+    """adaptive_fsp_options (fsp.hpp:108-121) with inside = box(bounds). sampled_expansion (and
+    its seed) has no device counterpart: only the full ring expansion runs."""
+
+    inside: Optional[box] = None
+    step_scale: float = 1.0
+    prune_fraction: float = 0.1
+    flux_tolerance: float = 1e-6
+    min_probability: float = 0.0
+    layers: int = 1
+    sampled_expansion: bool = False
+    seed: int = 42
+    save_every: int = 1000
+    max_steps: int = 1 << 28
+    krylov_dim: int = 30
+    krylov_tol: float = 1e-8
+
+    def _c(self) -> FspOptions:
+        if self.sampled_expansion:
+            raise ValueError("adaptive FSP on the device expands every neighbour (sampled_expansion = False)")
+        o = FspOptions()
+        load().mk_fsp_options_default(C.byref(o))
+        o.method = 1
+        o.step_scale = self.step_scale
+        o.prune_fraction = self.prune_fraction
+        o.flux_tolerance = self.flux_tolerance
+        o.min_probability = self.min_probability
+        o.layers = self.layers
+        o.max_steps = self.max_steps
+        o.krylov_dim = self.krylov_dim
+        o.krylov_tol = self.krylov_tol
+        return o
+
+
+@dataclass
 class distribution:
     """The supported states (rows, box order) and their probabilities (distribution.hpp)."""
 
@@ -145,7 +180,7 @@ def tabulate(model: reaction_network, region: box) -> tuple[np.ndarray, np.ndarr
 class _Problem:
     """one instance, with the arrays its mk_fsp_problem points at kept alive"""
 
-    def __init__(self, model, initial, final_time, options: krylov_fsp_options):
+    def __init__(self, model, initial, final_time, options):
         if options.inside is None:
             raise ValueError("the device FSP needs a box region (options.inside = box(bounds))")
         self.region = options.inside
@@ -264,3 +299,13 @@ def solve_krylov_fsp_batch(problems, stream=None, autotune: bool = False) -> lis
         b.autotune(stream=stream)
     b.run(stream)
     return b.solutions(stream)
+
+
+def solve_adaptive_fsp(model: reaction_network, initial: Sequence[int], final_time: float,
+                       options: Optional[adaptive_fsp_options] = None, stream=None) -> fsp_solution:
+    """solve_adaptive_fsp (fsp.hpp:123-188) on the GPU: flux-controlled steps of expand,
+    expv on the reflecting generator of the support, prune and renormalise."""
+    options = options or adaptive_fsp_options()
+    b = fsp_batch([(model, initial, final_time, options)])
+    b.run(stream)
+    return b.solutions(stream)[0]

@@ -7,6 +7,8 @@
 //   toggle <a1> <a2> <n1> <n2> <bound_x> <bound_y> <T> <tol> <krylov_tol> <krylov_dim> <x0> <y0>
 //   table <key>=<value> ...
 // The birth_death and toggle lines may end in <key>=<value> options as the table line takes.
+// adaptive=1 runs solve_adaptive_fsp (fsp.hpp:123-188) instead, with the keys scale, prune, flux
+// and minp for adaptive_fsp_options' step_scale, prune_fraction, flux_tolerance, min_probability.
 // Birth-death: {+1} at rate birth, {-1} at rate death * x. Toggle switch: {+1,0} at
 // a1 / (1 + y^n1), {0,+1} at a2 / (1 + x^n2), unit degradation {-1,0} at x and {0,-1} at y.
 // Table: any network whose propensities are tabulated over the box, read from path=<file>
@@ -173,7 +175,32 @@ int main(int argc, char **argv) {
             opt.max_steps = std::stoi(extra["max_steps"]);
         }
         const auto t0 = std::chrono::steady_clock::now();
-        const fsp_solution sol = solve_krylov_fsp(model, x0, T, opt);
+        fsp_solution sol;
+        if (extra.count("adaptive") && extra["adaptive"] == "1") {
+            // solve_adaptive_fsp (fsp.hpp:123-188) with adaptive_fsp_options from the keys
+            // scale, prune, flux, minp (and layers, max_steps, kdim, ktol as above)
+            adaptive_fsp_options ao;
+            ao.inside = box(bounds);
+            ao.krylov_dim = kdim;
+            ao.krylov_tol = ktol;
+            ao.layers = opt.layers;
+            ao.max_steps = opt.max_steps;
+            if (extra.count("scale")) {
+                ao.step_scale = std::stod(extra["scale"]);
+            }
+            if (extra.count("prune")) {
+                ao.prune_fraction = std::stod(extra["prune"]);
+            }
+            if (extra.count("flux")) {
+                ao.flux_tolerance = std::stod(extra["flux"]);
+            }
+            if (extra.count("minp")) {
+                ao.min_probability = std::stod(extra["minp"]);
+            }
+            sol = solve_adaptive_fsp(model, x0, T, ao);
+        } else {
+            sol = solve_krylov_fsp(model, x0, T, opt);
+        }
         const double ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         const distribution &p = sol.snapshots.back();

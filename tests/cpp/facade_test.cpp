@@ -152,6 +152,16 @@ void krylov_fsp() {
            "extinction probability");
 }
 
+// the reference's adaptive test (tests/test_fsp.cpp:68-77), written as the reference writes it
+void adaptive_fsp() {
+    const reaction_network birth_death{{{{1}, [](const state &) { return 5.0; }},
+                                        {{-1}, [](const state &x) { return 0.1 * x[0]; }}}};
+    const auto solution = solve_adaptive_fsp(birth_death, {0}, 2.0, {.inside = box({100}), .step_scale = 0.1});
+    expect(solution.times.size() > 1, "adaptive FSP saves snapshots");
+    const real exact = (5.0 / 0.1) * (1.0 - std::exp(-0.1 * 2.0));
+    expect(std::abs(solution.means().back()[0] - exact) < 0.1, "adaptive FSP matches the birth-death mean");
+}
+
 } // namespace
 
 int main() {
@@ -160,6 +170,7 @@ int main() {
         resolvent();
         annihilation_transform();
         krylov_fsp();
+        adaptive_fsp();
     } catch (const std::exception &e) {
         std::printf("FAILED with exception: %s\n", e.what());
         return 1;
