@@ -31,9 +31,10 @@ extern "C" {
 #define MK_ENOMEM 4     /* device allocation failed */
 #define MK_ENOTCONV 5   /* solver stopped at max_iterations (result still returned) */
 #define MK_ENAN 6       /* non-finite residual */
-#define MK_ETIMEOUT 7   /* a bounded device wait gave up */
+#define MK_ETIMEOUT 7   /* a bounded wait gave up (mk_server_wait_for) */
 #define MK_ECUDA 8      /* any other CUDA error */
 #define MK_ETOLERANCE 9 /* std::runtime_error ("expv: the requested tolerance is too high") */
+#define MK_ECANCELED 10 /* a queued server request was cancelled */
 
 typedef struct mk_space_s *mk_space;
 typedef struct mk_model_s *mk_model;
@@ -127,6 +128,13 @@ int mk_generator_apply_shifted_f32(mk_generator gen, float shift, const float *d
                                    void *stream);
 /* n_jumps(): the jumps between states of the space     generator.hpp:48 */
 int mk_generator_n_jumps(mk_generator gen, int64_t *n_jumps, void *stream);
+/* generator::jumps(j) (markovkit/generator.hpp:50-53): the jumps out of state j that stay in
+ * the space, as (to, rate) in the reference's order (diffusion by voxel, edge, species; then
+ * reactions by voxel and reaction). Computed on the host from the generator's model. *count is
+ * the number of jumps; the first min(count, capacity) are written (capacity 0 with NULL arrays
+ * asks for the count). */
+int mk_generator_jumps(mk_generator gen, int64_t j, int64_t *h_to, double *h_rate,
+                       int64_t capacity, int64_t *count);
 
 /* ---- the assembled generator: generator.hpp:84-107 ----
  * A CSR matrix in device memory owned by the handle: row_ptr[rows + 1], col[nonzeros] and
@@ -245,6 +253,39 @@ int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
  * that does not converge and returns its status. */
 int mk_solver_time_steps(mk_solver solver, int integrator, int steps, double rel_tolerance,
                          double *d_p, mk_solver_result *results, void *stream);
+
+/* ---- Preconditioners: the right preconditioner M of num::gmres(A, M, b, x, options) as any
+ * operator, not only a multigrid (examples/rdme_multigrid_benchmark.cpp:82-115):
+ *   diagonal   num::jacobi_preconditioner(inverse_diagonal): z = d .* v
+ *   ilu0       num::ilu0_preconditioner(A): ILU(0) of a CSR matrix in its natural row order,
+ *              factored on the device over level sets of rows (Saad, Alg. 10.4), applied as
+ *              level-scheduled triangular solves
+ *   multigrid  a sector multigrid as a preconditioner handle
+ *   host       any other operator: z = fn(ctx, v) on the host, v and z host arrays of n
+ * A solver made with mk_solver_create_pc uses flexible GMRES when the preconditioner varies
+ * (an FP32 multigrid). The handle must outlive the solvers that use it. ---- */
+typedef struct mk_precond_s *mk_precond;
+typedef int (*mk_precond_host_fn)(void *ctx, const double *v, double *z, int64_t n);
+int mk_precond_create_diagonal(int64_t n, const double *h_inverse_diagonal, mk_precond *out);
+/* row_ptr[n + 1]; each row's columns strictly ascending with the diagonal present (MK_EINVAL
+ * otherwise); MK_ESINGULAR on a zero or non-finite pivot */
+int mk_precond_create_ilu0(int64_t n, const int64_t *h_row_ptr, const int64_t *h_col,
+                           const double *h_val, void *stream, mk_precond *out);
+int mk_precond_create_multigrid(mk_space space, mk_model model, double shift,
+                                const mk_multigrid_options *opt, mk_precond *out);
+/* fn returns 0 on success; anything else fails the solve with MK_EINVAL */
+int mk_precond_create_host(int64_t n, mk_precond_host_fn fn, void *ctx, mk_precond *out);
+void mk_precond_destroy(mk_precond pc);
+int mk_precond_size(mk_precond pc, int64_t *n);
+/* z = M v on device vectors */
+int mk_precond_apply(mk_precond pc, const double *d_v, double *d_z, void *stream);
+/* an ILU(0) preconditioner's level sets: depth of the forward and backward sweeps, and the
+ * kernel launches one application takes (runs of thin levels share a launch) */
+int mk_precond_ilu0_schedule(mk_precond pc, int64_t *lower_levels, int64_t *upper_levels,
+                             int64_t *launches_per_apply);
+/* a resident solver for shift I - Q preconditioned by pc (NULL: plain GMRES) */
+int mk_solver_create_pc(mk_generator gen, double shift, mk_precond pc,
+                        const mk_gmres_options *opt, mk_solver *out);
 
 /* Several resolvent solves of one system at once (no counterpart in the reference; each column
  * is num::gmres(A, M, b, x)): flexible GMRES advancing up to `width` right-hand sides in
@@ -389,6 +430,12 @@ int mk_server_submit(mk_server server, int problem, double shift, const double *
                      int64_t *ticket);
 /* blocks until the request is done; returns its status */
 int mk_server_wait(mk_server server, int64_t ticket, mk_server_result *result);
+/* the same, giving up with MK_ETIMEOUT after timeout_ms (the request stays queued or running) */
+int mk_server_wait_for(mk_server server, int64_t ticket, double timeout_ms,
+                       mk_server_result *result);
+/* removes a request that no worker has taken yet; its result then carries MK_ECANCELED.
+ * MK_EINVAL when it has already started or finished. */
+int mk_server_cancel(mk_server server, int64_t ticket);
 /* blocks until every submitted request is done */
 int mk_server_drain(mk_server server);
 int mk_server_stats_get(mk_server server, mk_server_stats *stats);

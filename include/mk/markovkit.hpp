@@ -11,7 +11,11 @@
 //   boundary, generator, shifted_generator     markovkit/generator.hpp:11-133
 //   multigrid_options, sector_multigrid        markovkit/rdme/multigrid.hpp:125-134,364-408
 //   num::gmres_options, num::solver_result,
-//   num::gmres(A, [M], b, x, options)          call sites tests/test_rdme.cpp:238-249
+//   num::gmres(A, [M], b, x, options),
+//   num::jacobi_preconditioner,
+//   num::ilu0_preconditioner                   call sites tests/test_rdme.cpp:238-249,
+//                                              examples/rdme_multigrid_benchmark.cpp:82-115
+//   generator::jumps(j), exit_rates()          markovkit/generator.hpp:22-59
 //   reaction_network, box, krylov_fsp_options,
 //   adaptive_fsp_options, fsp_solution,
 //   solve_krylov_fsp, solve_adaptive_fsp       markovkit/reaction_network.hpp, fsp.hpp:26-254
@@ -21,6 +25,7 @@
 
 #include "../markovkit_b200.h"
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <concepts>
@@ -46,6 +51,18 @@ using array = std::vector<T>;
 template <typename T>
 using view = std::span<T>;
 using state = std::vector<int>;
+
+// the numerics library's names the reference's programs use through `num::`
+namespace num {
+using markovkit::real;
+using markovkit::idx;
+template <typename T>
+using vec = std::vector<T>;
+template <typename T>
+using array = std::vector<T>;
+template <typename T, std::size_t N>
+using static_array = std::array<T, N>;
+} // namespace num
 
 namespace detail {
 
@@ -369,7 +386,17 @@ class generator {
         n_ = static_cast<idx>(n);
         x_ = std::make_shared<detail::device_vector>(n_);
         y_ = std::make_shared<detail::device_vector>(n_);
+        detail::check(mk_generator_exit_leak(h, x_->get(), y_->get(), nullptr));
+        auto rates = std::make_shared<std::pair<array<real>, array<real>>>(array<real>(n_), array<real>(n_));
+        x_->download(rates->first.data());
+        y_->download(rates->second.data());
+        rates_ = std::move(rates);
     }
+    // a jump out of a state: the target's index and the rate (markovkit/generator.hpp:22-25)
+    struct jump {
+        idx to;
+        real rate;
+    };
     [[nodiscard]] idx rows() const { return n_; }
     [[nodiscard]] idx cols() const { return n_; }
     // y = Q x
@@ -385,8 +412,22 @@ class generator {
         detail::check(mk_generator_apply_shifted(h_.get(), shift, x_->get(), y_->get(), nullptr));
         y_->download(y.data());
     }
-    [[nodiscard]] array<real> exit_rates() const { return exit_leak().first; }
-    [[nodiscard]] array<real> leak_rates() const { return exit_leak().second; }
+    // the total rate out of each state, and the part of it that leaves the space
+    [[nodiscard]] const array<real> &exit_rates() const { return rates_->first; }
+    [[nodiscard]] const array<real> &leak_rates() const { return rates_->second; }
+    // the jumps out of state j that stay in the space, in the reference's order
+    [[nodiscard]] array<jump> jumps(idx j) const {
+        int64_t count = 0;
+        detail::check(mk_generator_jumps(h_.get(), static_cast<int64_t>(j), nullptr, nullptr, 0, &count));
+        std::vector<int64_t> to(static_cast<std::size_t>(count));
+        std::vector<real> rate(static_cast<std::size_t>(count));
+        detail::check(mk_generator_jumps(h_.get(), static_cast<int64_t>(j), to.data(), rate.data(), count, &count));
+        array<jump> out(static_cast<std::size_t>(count));
+        for (std::size_t k = 0; k < out.size(); ++k) {
+            out[k] = {static_cast<idx>(to[k]), rate[k]};
+        }
+        return out;
+    }
     [[nodiscard]] idx n_jumps() const {
         int64_t n = 0;
         detail::check(mk_generator_n_jumps(h_.get(), &n, nullptr));
@@ -408,14 +449,8 @@ class generator {
     [[nodiscard]] mk_model model_handle() const { return model_.get(); }
 
   private:
-    [[nodiscard]] std::pair<array<real>, array<real>> exit_leak() const {
-        detail::check(mk_generator_exit_leak(h_.get(), x_->get(), y_->get(), nullptr));
-        array<real> e(n_), l(n_);
-        x_->download(e.data());
-        y_->download(l.data());
-        return {e, l};
-    }
     std::shared_ptr<mk_model_s> model_;
+    std::shared_ptr<const std::pair<array<real>, array<real>>> rates_; // exit, leak
     std::shared_ptr<mk_generator_s> h_;
     std::shared_ptr<detail::device_vector> x_, y_;
     idx n_ = 0;
@@ -456,27 +491,28 @@ struct multigrid_options {
     int precision = 0; // 0 FP64, 1 FP32 (use with flexible GMRES)
 };
 
+// The reference's sector_multigrid<Graph> (markovkit/rdme/multigrid.hpp:364-408), over a
+// grid<D> domain; CTAD takes D from the domain. Copies share one device hierarchy.
+template <int D>
 class sector_multigrid {
   public:
     using domain_type = vec<real>;
     using codomain_type = vec<real>;
 
-    template <int D>
     sector_multigrid(const voxel_domain<D> &domain, const population_box &box, real shift,
                      const multigrid_options &options = {}) {
         init(reaction_diffusion<D>{domain, {}}, box, shift, options);
     }
-    template <int D>
     sector_multigrid(const voxel_domain<D> &domain, const population_sector &sector, real shift,
                      const multigrid_options &options = {}) {
         init(reaction_diffusion<D>{domain, {}}, sector, shift, options);
     }
     [[nodiscard]] idx rows() const { return n_; }
     [[nodiscard]] idx cols() const { return n_; }
-    [[nodiscard]] int max_levels() const {
+    [[nodiscard]] std::size_t max_levels() const {
         int l = 0;
         detail::check(mk_multigrid_max_levels(h_.get(), &l));
-        return l;
+        return static_cast<std::size_t>(l);
     }
     // one cycle per sector from a zero initial guess: x = M b
     void apply(const vec<real> &b, vec<real> &x) const {
@@ -489,7 +525,6 @@ class sector_multigrid {
     [[nodiscard]] bool fp32() const { return fp32_; }
 
   private:
-    template <int D>
     void init(const reaction_diffusion<D> &m, const population_space &space, real shift,
               const multigrid_options &o) {
         auto model = detail::make_model(m, space.limits());
@@ -518,19 +553,85 @@ class sector_multigrid {
     bool fp32_ = false;
 };
 
-// ---- GMRES --------------------------------------------------------------------------------
+// ---- preconditioners and GMRES -------------------------------------------------------------
 
 namespace num {
-
-using markovkit::idx;
-using markovkit::real;
-using markovkit::vec;
 
 template <typename Op, typename X, typename Y>
 concept linear_operator = requires(const Op &A, const X &x, Y &y) {
     { A.rows() } -> std::convertible_to<idx>;
     { A.cols() } -> std::convertible_to<idx>;
     A.apply(x, y);
+};
+
+namespace detail {
+
+// a preconditioner handle of the C ABI shared by copies, with a host apply(x, y)
+class device_preconditioner {
+  public:
+    [[nodiscard]] idx rows() const { return n_; }
+    [[nodiscard]] idx cols() const { return n_; }
+    void apply(const vec<real> &x, vec<real> &y) const {
+        if (x.size() != n_) {
+            throw std::invalid_argument("preconditioner: vector size differs from the operator's");
+        }
+        x_->upload(x.data());
+        markovkit::detail::check(mk_precond_apply(h_.get(), x_->get(), y_->get(), nullptr));
+        y.resize(n_);
+        y_->download(y.data());
+    }
+    [[nodiscard]] mk_precond precond_handle() const { return h_.get(); }
+
+  protected:
+    void adopt(mk_precond h) {
+        h_.reset(h, [](mk_precond p) { mk_precond_destroy(p); });
+        int64_t n = 0;
+        markovkit::detail::check(mk_precond_size(h, &n));
+        n_ = static_cast<idx>(n);
+        x_ = std::make_shared<markovkit::detail::device_vector>(n_);
+        y_ = std::make_shared<markovkit::detail::device_vector>(n_);
+    }
+
+  private:
+    std::shared_ptr<mk_precond_s> h_;
+    std::shared_ptr<markovkit::detail::device_vector> x_, y_;
+    idx n_ = 0;
+};
+
+} // namespace detail
+
+// z = d .* v with d the given inverse diagonal (num::jacobi_preconditioner)
+class jacobi_preconditioner : public detail::device_preconditioner {
+  public:
+    explicit jacobi_preconditioner(vec<real> inverse_diagonal) {
+        mk_precond h = nullptr;
+        markovkit::detail::check(mk_precond_create_diagonal(
+            static_cast<int64_t>(inverse_diagonal.size()), inverse_diagonal.data(), &h));
+        adopt(h);
+    }
+};
+
+// ILU(0) of an assembled matrix in its row order (num::ilu0_preconditioner), factored and
+// applied on the device
+class ilu0_preconditioner : public detail::device_preconditioner {
+  public:
+    explicit ilu0_preconditioner(const spmat &A) {
+        if (A.rows() != A.cols()) {
+            throw std::invalid_argument("ilu0_preconditioner: the matrix must be square");
+        }
+        const std::vector<int64_t> ptr(A.row_ptr().begin(), A.row_ptr().end());
+        const std::vector<int64_t> col(A.columns().begin(), A.columns().end());
+        mk_precond h = nullptr;
+        markovkit::detail::check(mk_precond_create_ilu0(static_cast<int64_t>(A.rows()), ptr.data(),
+                                                        col.data(), A.values().data(), nullptr, &h));
+        adopt(h);
+    }
+    // depth of the forward and backward level sets, and launches per application
+    [[nodiscard]] std::array<idx, 3> schedule() const {
+        int64_t lo = 0, up = 0, launches = 0;
+        markovkit::detail::check(mk_precond_ilu0_schedule(precond_handle(), &lo, &up, &launches));
+        return {static_cast<idx>(lo), static_cast<idx>(up), static_cast<idx>(launches)};
+    }
 };
 
 struct gmres_options {
@@ -547,8 +648,8 @@ struct solver_result {
 
 namespace detail {
 
-inline solver_result run(const shifted_generator &A, const sector_multigrid *M, const vec<real> &b,
-                         vec<real> &x, const gmres_options &o) {
+inline solver_result run(const shifted_generator &A, mk_multigrid mg, mk_precond pc,
+                         const vec<real> &b, vec<real> &x, const gmres_options &o) {
     if (b.size() != A.rows() || x.size() != A.rows()) {
         throw std::invalid_argument("gmres: vector sizes differ from the operator's");
     }
@@ -557,10 +658,12 @@ inline solver_result run(const shifted_generator &A, const sector_multigrid *M, 
     c.tolerance = o.tolerance;
     c.max_iterations = static_cast<int64_t>(o.max_iterations);
     c.restart = static_cast<int>(std::min<idx>(o.restart, 1u << 30));
-    c.flexible = (M && M->fp32()) ? 1 : 0;
     mk_solver h = nullptr;
-    markovkit::detail::check(
-        mk_solver_create(A.base().handle(), A.shift(), M ? M->handle() : nullptr, &c, &h));
+    if (pc) {
+        markovkit::detail::check(mk_solver_create_pc(A.base().handle(), A.shift(), pc, &c, &h));
+    } else {
+        markovkit::detail::check(mk_solver_create(A.base().handle(), A.shift(), mg, &c, &h));
+    }
     std::unique_ptr<mk_solver_s, void (*)(mk_solver)> solver(h, [](mk_solver p) { mk_solver_destroy(p); });
     mk_solver_result r{};
     const int rc = mk_solver_solve_host(h, b.data(), x.data(), &r, nullptr);
@@ -570,18 +673,59 @@ inline solver_result run(const shifted_generator &A, const sector_multigrid *M, 
     return {static_cast<idx>(r.iterations), r.residual, r.converged != 0};
 }
 
+// a host operator as a preconditioner handle: each application copies v out, calls
+// M.apply(v, z) on the calling thread and copies z back
+template <typename M>
+int host_apply(void *ctx, const double *v, double *z, int64_t n) {
+    try {
+        const auto &op = *static_cast<const M *>(ctx);
+        const vec<real> in(v, v + n);
+        vec<real> out(static_cast<std::size_t>(n), 0.0);
+        op.apply(in, out);
+        if (out.size() != static_cast<std::size_t>(n)) {
+            return 1;
+        }
+        std::copy(out.begin(), out.end(), z);
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
 } // namespace detail
 
 // restarted GMRES on A = shift I - Q; x holds the initial guess and the solution
 inline solver_result gmres(const shifted_generator &A, const vec<real> &b, vec<real> &x,
                            const gmres_options &options = {}) {
-    return detail::run(A, nullptr, b, x, options);
+    return detail::run(A, nullptr, nullptr, b, x, options);
 }
 
 // right-preconditioned by a sector multigrid (flexible GMRES when it runs in FP32)
-inline solver_result gmres(const shifted_generator &A, const sector_multigrid &M,
-                           const vec<real> &b, vec<real> &x, const gmres_options &options = {}) {
-    return detail::run(A, &M, b, x, options);
+template <int D>
+solver_result gmres(const shifted_generator &A, const sector_multigrid<D> &M, const vec<real> &b,
+                    vec<real> &x, const gmres_options &options = {}) {
+    return detail::run(A, M.handle(), nullptr, b, x, options);
+}
+
+// right-preconditioned by a device preconditioner (jacobi_preconditioner, ilu0_preconditioner)
+// or by any other operator with rows() and apply(x, y), applied on the host
+template <typename M>
+    requires linear_operator<M, vec<real>, vec<real>>
+solver_result gmres(const shifted_generator &A, const M &pre, const vec<real> &b, vec<real> &x,
+                    const gmres_options &options = {}) {
+    if constexpr (requires { pre.precond_handle(); }) {
+        return detail::run(A, nullptr, pre.precond_handle(), b, x, options);
+    } else {
+        if (pre.rows() != A.rows()) {
+            throw std::invalid_argument("gmres: preconditioner size differs from the operator's");
+        }
+        mk_precond h = nullptr;
+        markovkit::detail::check(mk_precond_create_host(static_cast<int64_t>(A.rows()),
+                                                        &detail::host_apply<M>,
+                                                        const_cast<M *>(&pre), &h));
+        std::unique_ptr<mk_precond_s, void (*)(mk_precond)> hold(h, [](mk_precond p) { mk_precond_destroy(p); });
+        return detail::run(A, nullptr, h, b, x, options);
+    }
 }
 
 } // namespace num

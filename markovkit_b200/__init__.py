@@ -9,6 +9,10 @@ from .api import (  # noqa: F401
     gmres,
     gmres_options,
     grid,
+    host_preconditioner,
+    ilu0_preconditioner,
+    jacobi_preconditioner,
+    jump,
     local_reaction,
     multigrid_options,
     population_box,

@@ -21,6 +21,7 @@ MK_ENAN = 6
 MK_ETIMEOUT = 7
 MK_ECUDA = 8
 MK_ETOLERANCE = 9
+MK_ECANCELED = 10
 
 
 class MkError(RuntimeError):
@@ -163,6 +164,8 @@ I64 = C.c_int64
 I64P = C.POINTER(C.c_int64)
 IP = C.POINTER(C.c_int)
 DP = C.POINTER(C.c_double)
+# int (*)(void *ctx, const double *v, double *z, int64_t n)
+PRECOND_HOST_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, DP, DP, C.c_int64)
 
 # name: (restype, argtypes)
 SIGNATURES = {
@@ -203,6 +206,7 @@ SIGNATURES = {
     "mk_generator_apply_f32": (C.c_int, [P, P, P, P]),
     "mk_generator_apply_shifted_f32": (C.c_int, [P, C.c_float, P, P, P]),
     "mk_generator_n_jumps": (C.c_int, [P, I64P, P]),
+    "mk_generator_jumps": (C.c_int, [P, I64, I64P, DP, I64, I64P]),
     "mk_generator_matrix": (C.c_int, [P, C.POINTER(P), P]),
     "mk_generator_characteristic_matrix": (C.c_int, [P, C.c_double, C.POINTER(P), P]),
     "mk_csr_size": (C.c_int, [P, I64P, I64P]),
@@ -229,6 +233,15 @@ SIGNATURES = {
     "mk_solver_solve": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
     "mk_solver_solve_host": (C.c_int, [P, P, P, C.POINTER(SolverResult), P]),
     "mk_solver_time_steps": (C.c_int, [P, C.c_int, C.c_int, C.c_double, P, C.POINTER(SolverResult), P]),
+    "mk_solver_create_pc": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.POINTER(P)]),
+    "mk_precond_create_diagonal": (C.c_int, [I64, DP, C.POINTER(P)]),
+    "mk_precond_create_ilu0": (C.c_int, [I64, I64P, I64P, DP, P, C.POINTER(P)]),
+    "mk_precond_create_multigrid": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
+    "mk_precond_create_host": (C.c_int, [I64, PRECOND_HOST_FN, P, C.POINTER(P)]),
+    "mk_precond_destroy": (None, [P]),
+    "mk_precond_size": (C.c_int, [P, I64P]),
+    "mk_precond_apply": (C.c_int, [P, P, P, P]),
+    "mk_precond_ilu0_schedule": (C.c_int, [P, I64P, I64P, I64P]),
     "mk_batch_solver_create": (C.c_int, [P, C.c_double, P, C.POINTER(GmresOptions), C.c_int, C.POINTER(P)]),
     "mk_batch_solver_destroy": (None, [P]),
     "mk_batch_solver_solve": (C.c_int, [P, P, P, I64, C.c_int, DP, C.POINTER(SolverResult), P]),
@@ -251,6 +264,8 @@ SIGNATURES = {
     "mk_server_footprint": (C.c_int, [P, C.c_int, C.POINTER(C.c_size_t)]),
     "mk_server_submit": (C.c_int, [P, C.c_int, C.c_double, P, P, I64P]),
     "mk_server_wait": (C.c_int, [P, I64, C.POINTER(ServerResult)]),
+    "mk_server_wait_for": (C.c_int, [P, I64, C.c_double, C.POINTER(ServerResult)]),
+    "mk_server_cancel": (C.c_int, [P, I64]),
     "mk_server_drain": (C.c_int, [P]),
     "mk_server_stats_get": (C.c_int, [P, C.POINTER(ServerStats)]),
 }

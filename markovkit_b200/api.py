@@ -302,6 +302,18 @@ class generator(_Handle):
         check(load().mk_generator_n_jumps(self._h, C.byref(n), None))
         return n.value
 
+    def jumps(self, j: int) -> list:
+        """The jumps out of state j that stay in the space, as (to, rate) pairs in the
+        reference's order (generator.hpp:50-53): diffusion by voxel, edge and species, then
+        reactions by voxel and reaction. Computed on the host from the model."""
+        lib = load()
+        count = C.c_int64()
+        check(lib.mk_generator_jumps(self._h, int(j), None, None, 0, C.byref(count)))
+        to = (C.c_int64 * max(count.value, 1))()
+        rate = (C.c_double * max(count.value, 1))()
+        check(lib.mk_generator_jumps(self._h, int(j), to, rate, count.value, C.byref(count)))
+        return [jump(int(to[k]), float(rate[k])) for k in range(count.value)]
+
     def matrix(self, device: bool = False):
         """Q assembled (generator.hpp:84): a scipy.sparse CSR matrix on the host, or with
         device=True a csr_matrix of device tensors."""
@@ -310,6 +322,13 @@ class generator(_Handle):
     def characteristic_matrix(self, shift: float, device: bool = False):
         """shift I - Q assembled (generator.hpp:87-90)."""
         return csr_matrix._assemble(self, float(shift), device)
+
+
+@dataclass(frozen=True)
+class jump:
+    """a jump out of a state (generator.hpp:22-25)"""
+    to: int
+    rate: float
 
 
 class csr_matrix(_Handle):
@@ -461,6 +480,85 @@ class sector_multigrid(_Handle):
         return x
 
 
+class _Preconditioner(_Handle):
+    """A right preconditioner handle of the C ABI (mk_precond): z = M v on device vectors."""
+
+    _destroy = "mk_precond_destroy"
+
+    def rows(self) -> int:
+        n = C.c_int64()
+        check(load().mk_precond_size(self._h, C.byref(n)))
+        return n.value
+
+    def cols(self) -> int:
+        return self.rows()
+
+    def apply(self, v, z, stream=None):
+        check(load().mk_precond_apply(self._h, _ptr(v), _ptr(z), _stream(stream)))
+        return z
+
+
+class jacobi_preconditioner(_Preconditioner):
+    """num::jacobi_preconditioner(inverse_diagonal): z = d .* v
+    (examples/rdme_multigrid_benchmark.cpp:109-114)."""
+
+    def __init__(self, inverse_diagonal):
+        super().__init__()
+        d = np.ascontiguousarray(np.asarray(inverse_diagonal, dtype=np.float64))
+        check(load().mk_precond_create_diagonal(d.size, d.ctypes.data_as(C.POINTER(C.c_double)), C.byref(self._h)))
+
+
+class ilu0_preconditioner(_Preconditioner):
+    """num::ilu0_preconditioner(A): ILU(0) of an assembled matrix (a scipy.sparse CSR matrix,
+    e.g. shifted_generator.matrix()) in its row order, factored and applied on the device
+    (examples/rdme_multigrid_benchmark.cpp:115)."""
+
+    def __init__(self, A, stream=None):
+        super().__init__()
+        import scipy.sparse as sp
+
+        A = sp.csr_matrix(A)
+        A.sort_indices()
+        if A.shape[0] != A.shape[1]:
+            raise ValueError("ilu0_preconditioner: the matrix must be square")
+        ptr = np.ascontiguousarray(A.indptr, dtype=np.int64)
+        col = np.ascontiguousarray(A.indices, dtype=np.int64)
+        val = np.ascontiguousarray(A.data, dtype=np.float64)
+        I64P = C.POINTER(C.c_int64)
+        check(load().mk_precond_create_ilu0(A.shape[0], ptr.ctypes.data_as(I64P), col.ctypes.data_as(I64P),
+                                            val.ctypes.data_as(C.POINTER(C.c_double)), _stream(stream),
+                                            C.byref(self._h)))
+
+    def schedule(self) -> dict:
+        """depth of the forward and backward level sets and kernel launches per application"""
+        lo, up, launches = C.c_int64(), C.c_int64(), C.c_int64()
+        check(load().mk_precond_ilu0_schedule(self._h, C.byref(lo), C.byref(up), C.byref(launches)))
+        return {"lower_levels": lo.value, "upper_levels": up.value, "launches_per_apply": launches.value}
+
+
+class host_preconditioner(_Preconditioner):
+    """Any operator as a preconditioner: fn(v) -> z on host float64 arrays of n entries, called
+    on the solving thread for every application (v is copied out of and z back into device
+    memory). An exception in fn fails the solve with MK_EINVAL."""
+
+    def __init__(self, n: int, fn):
+        super().__init__()
+        self._fn = fn
+
+        def trampoline(ctx, v, z, m):
+            try:
+                out = np.asarray(fn(np.ctypeslib.as_array(v, shape=(m,)).copy()), dtype=np.float64)
+                if out.shape != (m,):
+                    return 1
+                np.ctypeslib.as_array(z, shape=(m,))[:] = out
+                return 0
+            except Exception:  # noqa: BLE001 - reported through the solve's status
+                return 1
+
+        self._cb = _lib.PRECOND_HOST_FN(trampoline)
+        check(load().mk_precond_create_host(int(n), self._cb, None, C.byref(self._h)))
+
+
 def kernel_launches() -> int:
     """Kernels the library has launched in this process (graph launches count their nodes)."""
     v = C.c_uint64()
@@ -497,11 +595,15 @@ class solver(_Handle):
 
     _destroy = "mk_solver_destroy"
 
-    def __init__(self, A: shifted_generator, M: Optional[sector_multigrid] = None, options: Optional[GmresOptions] = None):
+    def __init__(self, A: shifted_generator, M=None, options: Optional[GmresOptions] = None):
         super().__init__()
         self.A, self.M = A, M
         opts = options if options is not None else gmres_options()
-        check(load().mk_solver_create(A.Q._h, A.shift(), M._h if M is not None else None, C.byref(opts), C.byref(self._h)))
+        if isinstance(M, _Preconditioner):
+            check(load().mk_solver_create_pc(A.Q._h, A.shift(), M._h, C.byref(opts), C.byref(self._h)))
+        else:
+            check(load().mk_solver_create(A.Q._h, A.shift(), M._h if M is not None else None, C.byref(opts),
+                                          C.byref(self._h)))
 
     def set_tolerance(self, tolerance: float) -> None:
         check(load().mk_solver_set_tolerance(self._h, float(tolerance)))
@@ -560,7 +662,7 @@ class batch_solver(_Handle):
 
 def gmres(A: shifted_generator, *args, **kw) -> solver_result:
     """num::gmres(A, [M], b, x, options): x holds the initial guess and gets the solution."""
-    if len(args) >= 3 and isinstance(args[0], sector_multigrid):
+    if len(args) >= 3 and isinstance(args[0], (sector_multigrid, _Preconditioner)):
         M, b, x = args[0], args[1], args[2]
         rest = args[3:]
     else:

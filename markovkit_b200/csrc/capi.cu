@@ -11,6 +11,7 @@ using mkb::capi::as_stream;
 using mkb::capi::fail;
 using mkb::capi::g_last_error;
 using mkb::capi::guarded;
+using mkb::capi::preconditioner_of;
 
 extern "C" {
 
@@ -270,7 +271,8 @@ int mk_generator_create(mk_space space, mk_model model, int absorbing, mk_genera
         auto h = std::make_unique<mk_generator_s>();
         const Space &sp = *space->space;
         h->space = Space::make(sp.V, sp.limits, sp.is_box);
-        h->gen = std::make_unique<Generator>(*h->space, *model->model, absorbing != 0);
+        h->model = std::make_unique<Model>(*model->model);
+        h->gen = std::make_unique<Generator>(*h->space, *h->model, absorbing != 0);
         *out = h.release();
     });
 }
@@ -531,13 +533,14 @@ void mk_gmres_options_default(mk_gmres_options *opt) {
     opt->flexible = d.flexible;
 }
 
-int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,
-                     const mk_gmres_options *opt, mk_solver *out) {
+static int create_solver(mk_generator gen, double shift, mk_multigrid mg, mk_precond pc,
+                         const mk_gmres_options *opt, mk_solver *out) {
     return guarded([&] {
         MK_REQUIRE(gen && out, "null argument");
         auto h = std::make_unique<mk_solver_s>();
         h->gen = gen;
         h->mg = mg;
+        h->pc = pc;
         h->shift = shift;
         if (opt) {
             MK_REQUIRE(opt->restart >= 1 && opt->max_iterations >= 0 && opt->tolerance >= 0.0,
@@ -547,13 +550,24 @@ int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,
             h->opt.restart = opt->restart;
             h->opt.flexible = opt->flexible;
         }
-        const bool flexible = h->opt.flexible || (mg && mg->mg->opt.precision != 0);
+        const Preconditioner *M = preconditioner_of(*h);
+        const bool flexible = h->opt.flexible || (M && M->varies());
         const int64_t n = gen->gen->op.n;
-        MK_REQUIRE(!mg || mg->mg->n == n, "preconditioner size does not match the system");
+        MK_REQUIRE(!M || M->n == n, "preconditioner size does not match the system");
         const int m = static_cast<int>(std::min<int64_t>(h->opt.restart, std::max<int64_t>(n, 1)));
         h->ws = std::make_unique<Krylov>(n, m, flexible);
         *out = h.release();
     });
+}
+
+int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,
+                     const mk_gmres_options *opt, mk_solver *out) {
+    return create_solver(gen, shift, mg, nullptr, opt, out);
+}
+
+int mk_solver_create_pc(mk_generator gen, double shift, mk_precond pc,
+                        const mk_gmres_options *opt, mk_solver *out) {
+    return create_solver(gen, shift, nullptr, pc, opt, out);
 }
 
 void mk_solver_destroy(mk_solver solver) { delete solver; }
@@ -587,7 +601,7 @@ int mk_solver_solve(mk_solver solver, const double *d_b, double *d_x, mk_solver_
     SolverResult r;
     const int rc = guarded([&] {
         MK_REQUIRE(solver && d_b && d_x, "null argument");
-        r = gmres(*solver->gen->gen, solver->shift, solver->mg ? solver->mg->mg.get() : nullptr,
+        r = gmres(*solver->gen->gen, solver->shift, preconditioner_of(*solver),
                   d_b, d_x, solver->opt, *solver->ws, as_stream(stream));
     });
     if (rc != MK_OK) {
@@ -633,7 +647,7 @@ int mk_solver_time_steps(mk_solver solver, int integrator, int steps, double rel
             check_cuda(cudaStreamSynchronize(st), "sync");
             GmresOptions o = solver->opt;
             o.tolerance = rel_tolerance * std::sqrt(nr2);
-            const SolverResult r = gmres(A, s, solver->mg ? solver->mg->mg.get() : nullptr, rhs, x,
+            const SolverResult r = gmres(A, s, preconditioner_of(*solver), rhs, x,
                                          o, *solver->ws, st);
             check_cuda(cudaMemcpyAsync(d_p, x, bytes, cudaMemcpyDeviceToDevice, st), "step");
             check_cuda(cudaStreamSynchronize(st), "sync");
@@ -660,7 +674,7 @@ int mk_solver_solve_host(mk_solver solver, const double *h_b, double *h_x,
         const std::size_t bytes = static_cast<std::size_t>(n) * sizeof(double);
         check_cuda(cudaMemcpyAsync(solver->b.get(), h_b, bytes, cudaMemcpyHostToDevice, s), "h2d");
         check_cuda(cudaMemcpyAsync(solver->x.get(), h_x, bytes, cudaMemcpyHostToDevice, s), "h2d");
-        r = gmres(*solver->gen->gen, solver->shift, solver->mg ? solver->mg->mg.get() : nullptr,
+        r = gmres(*solver->gen->gen, solver->shift, preconditioner_of(*solver),
                   solver->b.get(), solver->x.get(), solver->opt, *solver->ws, s);
         check_cuda(cudaMemcpyAsync(h_x, solver->x.get(), bytes, cudaMemcpyDeviceToHost, s), "d2h");
         check_cuda(cudaStreamSynchronize(s), "sync");

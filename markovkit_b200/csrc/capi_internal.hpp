@@ -17,6 +17,7 @@ struct mk_model_s {
 };
 struct mk_generator_s {
     std::unique_ptr<mkb::Space> space; // private copy of the geometry the generator indexes
+    std::unique_ptr<mkb::Model> model; // private copy of the model (jumps on the host)
     std::unique_ptr<mkb::Generator> gen;
 };
 struct mk_csr_s {
@@ -25,9 +26,13 @@ struct mk_csr_s {
 struct mk_multigrid_s {
     std::unique_ptr<mkb::Multigrid> mg;
 };
+struct mk_precond_s {
+    std::unique_ptr<mkb::Preconditioner> pc;
+};
 struct mk_solver_s {
     mk_generator gen = nullptr;
     mk_multigrid mg = nullptr;
+    mk_precond pc = nullptr; // used when mg is null
     double shift = 0.0;
     mkb::GmresOptions opt;
     std::unique_ptr<mkb::Krylov> ws;
@@ -67,6 +72,14 @@ int guarded(F &&f) {
 }
 
 inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+// the right preconditioner of a resident solver, or null for plain GMRES
+inline Preconditioner *preconditioner_of(const mk_solver_s &s) {
+    if (s.mg) {
+        return s.mg->mg.get();
+    }
+    return s.pc ? s.pc->pc.get() : nullptr;
+}
 
 } // namespace mkb::capi
 

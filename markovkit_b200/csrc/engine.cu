@@ -440,7 +440,7 @@ void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vec
 
 Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
                      const MultigridOptions &o)
-    : opt(o), shift(shift_), n(space.n), binom(space.binom) {
+    : Preconditioner(space.n), opt(o), shift(shift_), binom(space.binom) {
     if (!(shift > 0.0)) {
         throw Error(kEInval, "population_multigrid: shift must be positive");
     }
@@ -1444,8 +1444,8 @@ void read_report(const Krylov &ws, cudaStream_t stream) {
 
 } // namespace
 
-SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double *b, double *x,
-                   const GmresOptions &opt, Krylov &ws, cudaStream_t stream) {
+SolverResult gmres(const Generator &A, double shift, Preconditioner *M, const double *b,
+                   double *x, const GmresOptions &opt, Krylov &ws, cudaStream_t stream) {
     SolverResult res;
     const std::int64_t n = A.op.n;
     if (ws.n != n) {
@@ -1454,7 +1454,7 @@ SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double 
     if (M && M->n != n) {
         throw Error(kEInval, "preconditioner size does not match the system");
     }
-    const bool flexible = opt.flexible || (M && M->opt.precision != 0);
+    const bool flexible = opt.flexible || (M && M->varies());
     if (flexible && !ws.flexible) {
         throw Error(kEInval, "flexible GMRES needs a flexible workspace");
     }

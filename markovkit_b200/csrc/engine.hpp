@@ -186,9 +186,26 @@ struct MultigridOptions {
     int batch = 1;     // right-hand sides one cycle can serve at once (work vectors per level)
 };
 
+// A right preconditioner z = M v of gmres(): FP64 in and out, device vectors of n entries,
+// enqueued on `stream`. The reference takes any linear operator with apply(x, y) as num::gmres's
+// preconditioner (examples/rdme_multigrid_benchmark.cpp:82-115): the multigrid below, the
+// diagonal and ILU(0) ones of precond.cuh, or a host callback.
+struct Preconditioner {
+    std::int64_t n = 0;
+    Preconditioner() = default;
+    explicit Preconditioner(std::int64_t n_) : n(n_) {}
+    virtual ~Preconditioner() = default;
+    Preconditioner(const Preconditioner &) = delete;
+    Preconditioner &operator=(const Preconditioner &) = delete;
+    virtual void apply(const double *v, double *z, cudaStream_t stream) = 0;
+    // true when M is not one fixed linear map (FP32 arithmetic inside): GMRES must then keep
+    // the preconditioned basis (flexible GMRES)
+    [[nodiscard]] virtual bool varies() const { return false; }
+};
+
 // sector_multigrid (markovkit/rdme/multigrid.hpp:136-408): one geometric V-cycle per
 // population sector on the diffusion-only operator, all sectors of a depth in one launch.
-struct Multigrid {
+struct Multigrid : Preconditioner {
     struct Level {
         OperatorLevel op;
         int pre = 2, post = 2;
@@ -226,18 +243,16 @@ struct Multigrid {
     };
     MultigridOptions opt;
     double shift = 0.0;
-    std::int64_t n = 0;
     int max_depth = 0;
     std::vector<std::unique_ptr<Level>> levels;
     DeviceArray<double> lgf;
     std::shared_ptr<Binomials> binom;
 
     Multigrid(const Space &space, const Model &model, double shift, const MultigridOptions &opt);
-    ~Multigrid();
-    Multigrid(const Multigrid &) = delete;
-    Multigrid &operator=(const Multigrid &) = delete;
+    ~Multigrid() override;
     // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
-    void apply(const double *b, double *x, cudaStream_t stream);
+    void apply(const double *b, double *x, cudaStream_t stream) override;
+    [[nodiscard]] bool varies() const override { return opt.precision != 0; }
     // the same for nb <= opt.batch right-hand sides at once: column c of b at b + c * ldb,
     // of x at x + c * ldx; one cycle serves all columns
     void apply_batch(const double *b, std::int64_t ldb, double *x, std::int64_t ldx, int nb,
@@ -319,8 +334,8 @@ struct Krylov {
 
 // right-preconditioned restarted GMRES (Saad Alg. 9.5) or FGMRES (Alg. 9.6) on
 // A = shift I - Q with classical Gram-Schmidt and one re-orthogonalisation
-SolverResult gmres(const Generator &A, double shift, Multigrid *M, const double *b, double *x,
-                   const GmresOptions &opt, Krylov &ws, cudaStream_t stream);
+SolverResult gmres(const Generator &A, double shift, Preconditioner *M, const double *b,
+                   double *x, const GmresOptions &opt, Krylov &ws, cudaStream_t stream);
 
 // Workspace of FGMRES for nb right-hand sides advanced in lockstep. Basis vector j of column
 // c sits at V + (j * nb + c) * ld (and Z likewise), so step j of every column is one strided

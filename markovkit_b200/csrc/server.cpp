@@ -451,6 +451,51 @@ int mk_server_wait(mk_server server, int64_t ticket, mk_server_result *result) {
     return status;
 }
 
+int mk_server_wait_for(mk_server server, int64_t ticket, double timeout_ms,
+                       mk_server_result *result) {
+    int status = MK_OK;
+    const int rc = mkb::capi::guarded([&] {
+        MK_REQUIRE(server && result, "null argument");
+        MK_REQUIRE(timeout_ms >= 0.0 && std::isfinite(timeout_ms), "server: timeout must be finite and >= 0");
+        std::unique_lock<std::mutex> lock(server->mu);
+        MK_REQUIRE(ticket >= 1 && ticket < server->next_ticket, "server: unknown ticket");
+        const auto limit = std::chrono::duration<double, std::milli>(timeout_ms);
+        if (!server->cv_done.wait_for(lock, limit, [&] { return server->done.count(ticket) > 0; })) {
+            throw mkb::Error(MK_ETIMEOUT, "server: request " + std::to_string(ticket) +
+                                              " not done within the timeout");
+        }
+        *result = server->done[ticket];
+        status = result->status;
+    });
+    if (rc != MK_OK) {
+        return rc;
+    }
+    if (status != MK_OK) {
+        mkb::capi::g_last_error = "server: request " + std::to_string(ticket) + " ended with status " +
+                                  std::to_string(status);
+    }
+    return status;
+}
+
+int mk_server_cancel(mk_server server, int64_t ticket) {
+    return mkb::capi::guarded([&] {
+        MK_REQUIRE(server, "null argument");
+        std::lock_guard<std::mutex> lock(server->mu);
+        MK_REQUIRE(ticket >= 1 && ticket < server->next_ticket, "server: unknown ticket");
+        auto it = std::find_if(server->queue.begin(), server->queue.end(),
+                               [&](const Request &rq) { return rq.ticket == ticket; });
+        MK_REQUIRE(it != server->queue.end(), "server: the request has already started or finished");
+        mk_server_result r{};
+        r.ticket = ticket;
+        r.status = MK_ECANCELED;
+        r.latency_ms = r.queue_ms = ms_between(it->submitted, Clock::now());
+        server->queue.erase(it);
+        server->done[ticket] = r;
+        --server->in_flight;
+        server->cv_done.notify_all();
+    });
+}
+
 int mk_server_drain(mk_server server) {
     return mkb::capi::guarded([&] {
         MK_REQUIRE(server, "null argument");

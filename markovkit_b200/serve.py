@@ -98,13 +98,24 @@ class server:
         self._pending[t.value] = (b, x)
         return t.value
 
-    def wait(self, ticket: int):
+    def wait(self, ticket: int, timeout_ms: float | None = None, allow: tuple = ()):
+        """Block until the request is done (at most timeout_ms: MkError MK_ETIMEOUT, the request
+        stays pending) and return (x, request_result). A request that ended with a status other
+        than MK_OK or MK_ENOTCONV raises MkError, unless the status is in `allow`."""
         r = ServerResult()
-        rc = load().mk_server_wait(self._h, int(ticket), C.byref(r))
-        check(rc, allow=(MK_ENOTCONV,))
+        if timeout_ms is None:
+            rc = load().mk_server_wait(self._h, int(ticket), C.byref(r))
+        else:
+            rc = load().mk_server_wait_for(self._h, int(ticket), float(timeout_ms), C.byref(r))
+        check(rc, allow=(MK_ENOTCONV, *allow))
         b, x = self._pending.pop(ticket, (None, None))
         return x, request_result(r.ticket, r.status, r.iterations, r.residual, r.latency_ms, r.queue_ms, r.solve_ms,
                                  r.batched)
+
+    def cancel(self, ticket: int) -> None:
+        """Remove a request that no worker has taken yet; waiting on it then gives status
+        MK_ECANCELED. MkError MK_EINVAL once it has started or finished."""
+        check(load().mk_server_cancel(self._h, int(ticket)))
 
     def drain(self) -> None:
         check(load().mk_server_drain(self._h))

@@ -185,6 +185,22 @@ int run(const args &a) {
         dump("Am", A.matrix());
     }
 
+    // generator::jumps(j) for every j in the reference's order (generator.hpp:50-53):
+    // jumps_first = offsets (N + 1), jumps_to, jumps_rate
+    if (a.integer("dump_jumps", 0)) {
+        std::vector<double> first{0.0}, to, rate;
+        for (idx j = 0; j < N; ++j) {
+            for (const auto &e : Q.jumps(j)) {
+                to.push_back(static_cast<double>(e.to));
+                rate.push_back(e.rate);
+            }
+            first.push_back(static_cast<double>(to.size()));
+        }
+        write_f64(out + "/jumps_first.f64", first);
+        write_f64(out + "/jumps_to.f64", to);
+        write_f64(out + "/jumps_rate.f64", rate);
+    }
+
     const std::string rhs_kind = a.get("rhs", "uniform");
     const std::uint64_t seed = static_cast<std::uint64_t>(a.integer("seed", 0));
     vec<real> b;

@@ -4,6 +4,7 @@
 // tests/test_facade.py; run on a GPU it prints "facade: N checks passed" or exits 1.
 #include "mk/markovkit.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <numeric>
@@ -111,6 +112,75 @@ void resolvent() {
     expect(s32.converged && d32 < 1e-8 * norm(x_mg), "FP32 multigrid in flexible GMRES agrees");
 }
 
+// the reference's benchmark flow (examples/rdme_multigrid_benchmark.cpp:72-121): plain, Jacobi,
+// ILU(0) and multigrid preconditioners through one generic num::gmres, and a host operator
+template <std::size_t D>
+void preconditioners() {
+    num::static_array<num::idx, D> dims{};
+    dims.fill(4);
+    num::static_array<double, D> spacing{};
+    spacing.fill(0.25);
+    const reaction_diffusion model{voxel_domain(grid<D>(dims, spacing), {4.0}), birth_death(0.05, 0.02)};
+    const population_box box(model.n_voxels(), {2});
+    const generator Q(box, model, boundary::absorbing);
+    constexpr real shift = 0.5;
+    const shifted_generator system(Q, shift);
+    vec<real> rhs(Q.rows());
+    for (idx i = 0; i < rhs.size(); ++i) {
+        rhs[i] = 1.0 + 0.1 * std::cos(static_cast<double>(i));
+    }
+    const num::gmres_options options{.tolerance = 1e-10 * norm(rhs), .max_iterations = 2000,
+                                     .restart = std::min<idx>(50, Q.rows())};
+    vec<real> inverse_diagonal(Q.rows());
+    for (idx i = 0; i < Q.rows(); ++i) {
+        inverse_diagonal[i] = 1.0 / (shift + Q.exit_rates()[i]);
+    }
+    const num::jacobi_preconditioner jacobi(inverse_diagonal);
+    const num::ilu0_preconditioner ilu(system.matrix());
+    const sector_multigrid<D> mg(model.domain, box, shift);
+    expect(mg.max_levels() >= 2, "sector_multigrid<D> builds a hierarchy");
+    // any operator with rows(), cols() and apply(x, y) preconditions too (applied on the host)
+    struct diagonal_scaling {
+        const vec<real> *d;
+        [[nodiscard]] idx rows() const { return d->size(); }
+        [[nodiscard]] idx cols() const { return d->size(); }
+        void apply(const vec<real> &x, vec<real> &y) const {
+            y.resize(x.size());
+            for (idx i = 0; i < x.size(); ++i) {
+                y[i] = (*d)[i] * x[i];
+            }
+        }
+    } host{&inverse_diagonal};
+    vec<real> xp(Q.rows(), 0.0), xj(Q.rows(), 0.0), xi(Q.rows(), 0.0), xm(Q.rows(), 0.0), xh(Q.rows(), 0.0);
+    const auto rp = num::gmres(system, rhs, xp, options);
+    const auto rj = num::gmres(system, jacobi, rhs, xj, options);
+    const auto ri = num::gmres(system, ilu, rhs, xi, options);
+    const auto rm = num::gmres(system, mg, rhs, xm, options);
+    const auto rh = num::gmres(system, host, rhs, xh, options);
+    expect(rp.converged && rj.converged && ri.converged && rm.converged && rh.converged,
+           "plain, jacobi, ilu0, multigrid and host-operator GMRES converge");
+    expect(ri.iterations < rj.iterations, "ILU(0) takes fewer iterations than Jacobi");
+    expect(rh.iterations == rj.iterations && xh == xj, "a host d .* v gives the Jacobi iterates");
+    real diff = 0.0, scale = 0.0;
+    for (idx i = 0; i < Q.rows(); ++i) {
+        diff = std::max({diff, std::abs(xj[i] - xm[i]), std::abs(xi[i] - xm[i]), std::abs(xp[i] - xm[i])});
+        scale = std::max(scale, std::abs(xm[i]));
+    }
+    expect(diff <= 1e-8 * scale, "every preconditioner reaches the same solution");
+    // generator::jumps(j): in-space jumps plus the leak make up the exit rate
+    real worst = 0.0;
+    idx total = 0;
+    for (idx j = 0; j < Q.rows(); ++j) {
+        real out = Q.leak_rates()[j];
+        for (const auto &e : Q.jumps(j)) {
+            out += e.rate;
+            ++total;
+        }
+        worst = std::max(worst, std::abs(out - Q.exit_rates()[j]) / std::max(Q.exit_rates()[j], 1.0));
+    }
+    expect(worst < 1e-14 && total == Q.n_jumps(), "jumps(j) and leak_rates() add up to exit_rates()");
+}
+
 void annihilation_transform() {
     // A + B -> nothing at rate 2 a b / V; E[exp(-sT)] + s S_hat(s) = 1 for the annihilation time
     const reaction_diffusion<1> model{
@@ -168,6 +238,9 @@ int main() {
     try {
         spaces();
         resolvent();
+        preconditioners<1>();
+        preconditioners<2>();
+        preconditioners<3>();
         annihilation_transform();
         krylov_fsp();
         adaptive_fsp();

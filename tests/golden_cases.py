@@ -87,5 +87,7 @@ def load(name: str) -> Case:
 def names() -> list[str]:
     """the small resolvent fixtures of make_golden.py (fsp_*.npz hold the Krylov-FSP ones,
     full_*.npz the full-size solutions of make_full_golden.py, aggregate_golden.npz the
-    aggregate-block smoother's of make_aggregate_golden.py)"""
-    return sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("fsp_", "full_", "aggregate_")))
+    aggregate-block smoother's of make_aggregate_golden.py, jumps_golden.npz the generator's
+    jumps of make_jumps_golden.py)"""
+    return sorted(p.stem for p in GOLDEN.glob("*.npz")
+                  if not p.stem.startswith(("fsp_", "full_", "aggregate_", "jumps_")))
