@@ -1,5 +1,6 @@
 // Host side of the B200 resolvent engine (see engine.hpp).
 #include "engine.hpp"
+#include "dense_inverse.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -372,52 +373,6 @@ void axpy_t(T a, const T *x, T *y, std::int64_t n, cudaStream_t stream) {
     check_cuda(cudaGetLastError(), "axpy");
 }
 
-// dense inverse by Gauss-Jordan with partial pivoting; false when singular
-bool invert_dense(std::vector<double> &A, int n, std::vector<double> &inv) {
-    inv.assign(static_cast<std::size_t>(n) * n, 0.0);
-    for (int i = 0; i < n; ++i) {
-        inv[static_cast<std::size_t>(i) * n + i] = 1.0;
-    }
-    for (int k = 0; k < n; ++k) {
-        int p = k;
-        for (int i = k + 1; i < n; ++i) {
-            if (std::abs(A[static_cast<std::size_t>(i) * n + k]) >
-                std::abs(A[static_cast<std::size_t>(p) * n + k])) {
-                p = i;
-            }
-        }
-        if (A[static_cast<std::size_t>(p) * n + k] == 0.0) {
-            return false;
-        }
-        if (p != k) {
-            for (int j = 0; j < n; ++j) {
-                std::swap(A[static_cast<std::size_t>(k) * n + j], A[static_cast<std::size_t>(p) * n + j]);
-                std::swap(inv[static_cast<std::size_t>(k) * n + j],
-                          inv[static_cast<std::size_t>(p) * n + j]);
-            }
-        }
-        const double d = A[static_cast<std::size_t>(k) * n + k];
-        for (int j = 0; j < n; ++j) {
-            A[static_cast<std::size_t>(k) * n + j] /= d;
-            inv[static_cast<std::size_t>(k) * n + j] /= d;
-        }
-        for (int i = 0; i < n; ++i) {
-            if (i == k) {
-                continue;
-            }
-            const double f = A[static_cast<std::size_t>(i) * n + k];
-            if (f == 0.0) {
-                continue;
-            }
-            for (int j = 0; j < n; ++j) {
-                A[static_cast<std::size_t>(i) * n + j] -= f * A[static_cast<std::size_t>(k) * n + j];
-                inv[static_cast<std::size_t>(i) * n + j] -= f * inv[static_cast<std::size_t>(k) * n + j];
-            }
-        }
-    }
-    return true;
-}
-
 // the terminal block of one sector, dense, from the same matrix-free rows (host, generic shape)
 void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vector<double> &A) {
     const SectorDesc &sec = op.sectors[slot];
@@ -519,8 +474,11 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
         }
         L->op.finalize(*grid_model, false);
 
-        // dense inverses of the terminal blocks, from the same matrix-free rows
-        std::vector<double> inv_all, A, inv, dense_all;
+        // dense inverses of the terminal blocks, from the same matrix-free rows, all of a level
+        // at once (on the device when they are large)
+        std::vector<double> inv_all, A, A_all, dense_all;
+        std::vector<std::int64_t> term_offset;
+        std::vector<int> term_n;
         for (std::size_t k = 0; k < L->op.sectors.size(); ++k) {
             const SectorDesc &sec = L->op.sectors[k];
             if (sec.terminal < 0) {
@@ -535,11 +493,13 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
                 L->h_dense.push_back(db);
                 dense_all.insert(dense_all.end(), A.begin(), A.end());
             }
-            if (!invert_dense(A, static_cast<int>(sec.size), inv)) {
-                throw Error(kESingular, "population_multigrid: singular block");
-            }
-            L->h_term[sec.terminal].inv_offset = static_cast<std::int64_t>(inv_all.size());
-            inv_all.insert(inv_all.end(), inv.begin(), inv.end());
+            L->h_term[sec.terminal].inv_offset = static_cast<std::int64_t>(A_all.size());
+            term_offset.push_back(static_cast<std::int64_t>(A_all.size()));
+            term_n.push_back(static_cast<int>(sec.size));
+            A_all.insert(A_all.end(), A.begin(), A.end());
+        }
+        if (!invert_dense_blocks(A_all, term_offset, term_n, inv_all)) {
+            throw Error(kESingular, "population_multigrid: singular block");
         }
         L->d_term.upload(L->h_term);
         L->inv64.upload(inv_all);

@@ -505,7 +505,10 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
             }
             const SectorDesc &ss = sectors[sec.src[r]];
             // the source gains |change| molecules in the visited voxel; species with one more
-            // molecule use per-row insertion coefficients, others the general re-rank
+            // molecule use per-row insertion coefficients (lists of up to three, or of four
+            // with one species: the source then holds at most four, as a list of four has no
+            // source sector), others the general re-rank
+            constexpr bool kInsert = TMAX <= 3 || (TMAX == 4 && NS == 1);
             std::int64_t A[NS][TMAX], Bc[NS][TMAX];
             int fixed = static_cast<int>(ss.begin);
 #pragma unroll
@@ -513,11 +516,16 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                 if (md.change[r][s] == 0) {
                     fixed += st.rank[s] * static_cast<int>(ss.stride[s]);
                 }
-                if constexpr (TMAX <= 3) {
+                if constexpr (kInsert) {
                     static_for<TMAX>([&](auto I) {
                         constexpr int i = decltype(I)::value;
                         A[s][i] = binom_j<i + 1>(st.u[s][i] + i);
-                        Bc[s][i] = binom_j<i + 2>(st.u[s][i] + i + 1);
+                        // molecule i moves up a place only when i < t <= 3
+                        if constexpr (i + 2 <= 4) {
+                            Bc[s][i] = binom_j<i + 2>(st.u[s][i] + i + 1);
+                        } else {
+                            Bc[s][i] = 0;
+                        }
                     });
                 }
             }
@@ -550,8 +558,9 @@ MK_HD void visit_row(const BinomTable &B, const SectorDesc *sectors, const Secto
                         continue;
                     }
                     std::int64_t rs;
-                    if constexpr (TMAX <= 3) {
-                        rs = c == -1 ? rank_inserted<TMAX>(st.u[s], sec.total[s], A[s], Bc[s], uu)
+                    if constexpr (kInsert) {
+                        rs = c == -1 && sec.total[s] < 4
+                                 ? rank_inserted<TMAX>(st.u[s], sec.total[s], A[s], Bc[s], uu)
                                      : rank_modified<TMAX>(B, st.u[s], sec.total[s], uu, -c);
                     } else {
                         rs = rank_modified<TMAX>(B, st.u[s], sec.total[s], uu, -c);

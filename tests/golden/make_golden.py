@@ -6,7 +6,7 @@ seeded problems and stores its inputs and outputs as .npz. Inputs (x, b) are gen
 with markovkit_b200.inputs and handed to the driver as files, so both sides see identical
 bytes.
 
-usage: python tests/golden/make_golden.py
+usage: python tests/golden/make_golden.py [case ...]
 """
 
 from __future__ import annotations
@@ -42,6 +42,10 @@ CASES = {
     "annihilation_1d6_cap2": dict(dim=1, cells=6, cap="2,2", model="annihilation", k=3.0, D=0.5, D2=2.0, shift=0.7, rhs="uniform", seed=7, transfer=True, states=True),
     "birth_death_2d4_reflecting": dict(dim=2, cells=4, cap="2", model="birth_death", birth=0.4, death=0.3, D=2.0, shift=0.3, rhs="uniform", seed=9, boundary="reflecting", transfer=True),
     "diffusion_1d8_cap4": dict(dim=1, cells=8, cap="4", model="diffusion", D=1.5, shift=1.0, rhs="uniform", seed=11, transfer=True, states=True),
+    # lists of four molecules with births and deaths (sources of the death in-jumps in every voxel)
+    # an odd grid that cannot coarsen: every sector is a dense terminal block (up to 1820 states)
+    "birth_death_1d13_cap4": dict(dim=1, cells=13, cap="4", model="birth_death", birth=0.6, death=0.3, D=1.2, shift=0.8, rhs="uniform", seed=13, transfer=True),
+    "birth_death_1d10_cap4": dict(dim=1, cells=10, cap="4", model="birth_death", birth=0.6, death=0.3, D=1.2, shift=0.8, rhs="uniform", seed=12, transfer=True, states=True),
 }
 
 
@@ -85,7 +89,10 @@ def run_case(name: str, spec: dict, work: Path) -> dict:
 def main() -> None:
     if not DRIVER.exists():
         sys.exit("oracle/_ref/ref_driver is not built (make -C oracle)")
+    only = set(sys.argv[1:])  # case names to regenerate (default: all)
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         with tempfile.TemporaryDirectory() as tmp:
             data = run_case(name, spec, Path(tmp))
         np.savez_compressed(OUT / f"{name}.npz", **data)
