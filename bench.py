@@ -73,6 +73,7 @@ SECONDARY_WORKLOAD = "annihilation_2d32"
 REL_TOL = 1e-10
 RESTART = 30
 FP32_SMOOTHER = "gauss_seidel"
+MIX_SMOOTHER = "auto"  # the serving mix: the server picks the smoother per problem
 FP32_COARSEST = 256
 L2_FLUSH_BYTES = 256 << 20
 METRIC = "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)"
@@ -521,7 +522,7 @@ def serve_mix_measure(mk) -> dict:
     bs = [rhs_of({"rhs": "dirichlet"}, r["rhs_seed"], sizes[(r["model"], r["voxels"], r["cap"])]) for r in reqs]
     out = {}
     kw = dict(precision="fp32", slots=SERVE_SLOTS, batch=4, coarsest_size=FP32_COARSEST, restart=RESTART,
-              smoother=FP32_SMOOTHER)
+              smoother=MIX_SMOOTHER)
     with server(rel_tolerance=REL_TOL, **kw) as srv:
         pids = {k: srv.register(*problems[k]) for k in keys}
         t0 = time.perf_counter()
@@ -581,8 +582,9 @@ def serve_mix_measure(mk) -> dict:
     out["fp32_over_plain_fp64_path"] = round(out["fp32"]["value"] / out["plain_fp64_path"]["value"], 3)
     out["requests"] = len(reqs)
     out["largest_states"] = max(sizes.values())
-    out["note"] = (f"Poisson arrivals at {MIX_RATE}/s, seed 4; fp32: {SERVE_SLOTS} slots, batch 4 across shifts, "
-                   f"FGMRES({RESTART}), smoother {FP32_SMOOTHER}, dense solve of sectors <= {FP32_COARSEST} "
+    out["note"] = (f"Poisson arrivals at {MIX_RATE}/s, seed 4; fp32: {SERVE_SLOTS} slots, batch 4 (same problem and shift), "
+                   f"FGMRES({RESTART}), smoother {MIX_SMOOTHER} (Gauss-Seidel for one species of at most two "
+                   f"molecules per state, Jacobi otherwise), dense solve of sectors <= {FP32_COARSEST} "
                    "states; plain fp64: one request at a time, GMRES(30), the reference's multigrid options, "
                    "generator and multigrid set-up inside each latency; 1-D boxes use configuration 0's "
                    "voxel size 1/16")

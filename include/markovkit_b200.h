@@ -190,9 +190,8 @@ int mk_multigrid_apply_batch(mk_multigrid mg, const double *d_b, int64_t ldb, do
  * static device array of 64 MiB, which every GPU that loads the library holds until the process
  * exits. A hierarchy whose work vectors need more than that is rejected with MK_EINVAL and a
  * message giving the size. The first call on each device looks the array's address up
- * (cudaGetSymbolAddress) and caches it for the life of the process, so make that first call
- * before any stream capture, and do not reset the device (cudaDeviceReset) while the library is
- * loaded. All calls share the one array and each overwrites it; calls that overlap on the GPU
+ * (cudaGetSymbolAddress) and caches it for the life of the process, so do not reset the device
+ * (cudaDeviceReset) while the library is loaded. All calls share the one array and each overwrites it; calls that overlap on the GPU
  * (different streams, or different hierarchies at once) race and give wrong results, so order
  * them on one stream. Use a hierarchy from one host thread at a time, as with every mk_multigrid
  * call. The result equals mk_multigrid_apply's bit for bit. */
@@ -390,7 +389,9 @@ typedef struct {
     int slots;               /* concurrent solves (worker threads and streams), 1..64 */
     size_t hbm_budget;       /* bytes for resident solvers; 0 = 80 % of the free memory */
     int precision;           /* 1: FP32 multigrid inside FP64 flexible GMRES; 0: all FP64 */
-    int smoother;            /* multigrid smoother: 0 Jacobi, 1 red-black Gauss-Seidel, 2 ILU(0) */
+    int smoother;            /* multigrid smoother: 0 Jacobi, 1 red-black Gauss-Seidel, 2 ILU(0);
+                              * -1 per problem: Gauss-Seidel for one species of at most two
+                              * molecules per state, Jacobi otherwise */
     int restart;             /* GMRES restart, 1..64 */
     int64_t max_iterations;
     double rel_tolerance;    /* stop at ||b - A x|| <= rel_tolerance * ||b|| */

@@ -101,6 +101,36 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// one level over a grid, a warp per row: the lanes stride the row's entries and the partial
+// sums meet by shuffles (triangular solves only)
+template <int SWEEP>
+__global__ void __launch_bounds__(kThreads)
+    warp_level_kernel(const IluView a, const int *__restrict__ order,
+                      const std::int64_t *__restrict__ level_ptr, std::int64_t l,
+                      const double *in, double *out) {
+    static_assert(SWEEP == kLower || SWEEP == kUpper, "solves only");
+    const std::int64_t b = level_ptr[l], e = level_ptr[l + 1];
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    const std::int64_t warps = static_cast<std::int64_t>(gridDim.x) * (blockDim.x / 32);
+    for (std::int64_t t = b + (blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x) / 32;
+         t < e; t += warps) {
+        const int i = order[t];
+        const std::int64_t di = a.diag[i];
+        const std::int64_t p0 = SWEEP == kLower ? a.ptr[i] : di + 1;
+        const std::int64_t p1 = SWEEP == kLower ? di : a.ptr[i + 1];
+        double s = 0.0;
+        for (std::int64_t p = p0 + lane; p < p1; p += 32) {
+            s = fma(a.val[p], out[a.col[p]], s);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffU, s, o);
+        }
+        if (lane == 0) {
+            out[i] = SWEEP == kLower ? in[i] - s : (in[i] - s) / a.val[di];
+        }
+    }
+}
+
 // levels [l0, l1) in one block, a barrier after each so the next level sees its rows
 template <int SWEEP>
 __global__ void __launch_bounds__(kNarrowThreads)
@@ -166,21 +196,26 @@ void build_schedule(std::int64_t n, const std::vector<std::int64_t> &ptr,
     }
     std::vector<int> order(static_cast<std::size_t>(n));
     std::vector<std::int64_t> fill(s.h_level_ptr.begin(), s.h_level_ptr.end() - 1);
+    std::vector<std::int64_t> work(static_cast<std::size_t>(depth), 0), longest(work);
     for (std::int64_t i = 0; i < n; ++i) {
         order[fill[lev[i]]++] = static_cast<int>(i);
+        const std::int64_t len = lower_sweep ? diag[i] - ptr[i] : ptr[i + 1] - diag[i] - 1;
+        work[lev[i]] += len + 1;
+        longest[lev[i]] = std::max(longest[lev[i]], len);
     }
     s.order.upload(order);
     s.level_ptr.upload(s.h_level_ptr);
     s.segments.clear();
     for (std::int64_t l = 0; l < depth; ++l) {
         const std::int64_t rows = s.h_level_ptr[l + 1] - s.h_level_ptr[l];
-        if (rows > Ilu0Preconditioner::kNarrowRows) {
-            s.segments.push_back({l, l + 1, rows, true});
+        if (rows > Ilu0Preconditioner::kNarrowRows || work[l] > Ilu0Preconditioner::kNarrowWork) {
+            s.segments.push_back({l, l + 1, rows, true,
+                                  longest[l] > Ilu0Preconditioner::kWarpRowLength});
         } else if (!s.segments.empty() && !s.segments.back().wide) {
             s.segments.back().l1 = l + 1;
             s.segments.back().rows += rows;
         } else {
-            s.segments.push_back({l, l + 1, rows, false});
+            s.segments.push_back({l, l + 1, rows, false, false});
         }
     }
 }
@@ -189,6 +224,13 @@ template <int SWEEP>
 void run_schedule(const IluView a, const LevelSchedule &s, const double *in, double *out,
                   cudaStream_t stream) {
     for (const auto &g : s.segments) {
+        if constexpr (SWEEP != kFactor) {
+            if (g.warp) {
+                warp_level_kernel<SWEEP><<<grid_for(32 * g.rows), kThreads, 0, stream>>>(
+                    a, s.order.get(), s.level_ptr.get(), g.l0, in, out);
+                continue;
+            }
+        }
         if (g.wide) {
             wide_level_kernel<SWEEP><<<grid_for(g.rows), kThreads, 0, stream>>>(
                 a, s.order.get(), s.level_ptr.get(), g.l0, in, out);

@@ -14,7 +14,9 @@
 // levels; the backward solve U z = y uses the mirrored ones. Runs of consecutive levels of at
 // most kNarrowRows rows go to one CUDA block that steps through them between block barriers,
 // so a deep, thin schedule costs one launch per run instead of one per level; a level wider
-// than that gets its own grid. Every update is a fused multiply-add (fma(-l, u, a)).
+// than that, or with more entries than kNarrowWork, gets its own grid, and in the triangular
+// solves a warp per row when its rows are long (the one-molecule rows of a box hold an entry
+// per voxel). Every update is a fused multiply-add (fma(-l, u, a)).
 #pragma once
 
 #include "engine.hpp"
@@ -37,6 +39,7 @@ struct LevelSchedule {
         std::int64_t l0 = 0, l1 = 0; // levels [l0, l1)
         std::int64_t rows = 0;
         bool wide = false;           // one level over a grid, else one block steps the levels
+        bool warp = false;           // wide, with rows long enough for a warp each (solves)
     };
     DeviceArray<int> order;                // rows by level
     DeviceArray<std::int64_t> level_ptr;   // level l: order[level_ptr[l] .. level_ptr[l + 1])
@@ -48,7 +51,10 @@ struct LevelSchedule {
 };
 
 struct Ilu0Preconditioner final : Preconditioner {
-    static constexpr int kNarrowRows = 4096; // levels at most this wide share one block
+    static constexpr int kNarrowRows = 4096;     // levels at most this wide share one block,
+    static constexpr int kNarrowWork = 1 << 16;  // if their entries are at most this many
+    static constexpr int kWarpRowLength = 32;    // a wide level whose longest row is longer
+                                                 // than this runs a warp per row
     // the factors in A's pattern (each row's columns ascending): L strictly below the diagonal
     // (unit diagonal implied), U on and above it
     DeviceArray<std::int64_t> ptr, diag;

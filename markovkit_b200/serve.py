@@ -44,7 +44,7 @@ class server:
         o.slots = int(slots)
         o.hbm_budget = int(hbm_budget)
         o.precision = {"fp64": 0, "fp32": 1}[precision]
-        o.smoother = {"jacobi": 0, "gauss_seidel": 1, "ilu0": 2, "aggregate_block": 3}[smoother]
+        o.smoother = {"auto": -1, "jacobi": 0, "gauss_seidel": 1, "ilu0": 2, "aggregate_block": 3}[smoother]
         o.restart = int(restart)
         o.max_iterations = int(max_iterations)
         o.rel_tolerance = float(rel_tolerance)
