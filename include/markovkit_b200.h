@@ -376,6 +376,51 @@ int mk_fsp_batch_results(mk_fsp_batch batch, double *h_out, mk_fsp_result *resul
 int mk_fsp_krylov_batch(int n, const mk_fsp_problem *problems, double *h_out,
                         mk_fsp_result *results, void *stream);
 
+/* ---- Batched SSA: gillespie(model, x, final_time, random, max_jumps) and tau_leaping(model, x,
+ * final_time, random, leap_options) (markovkit/ssa.hpp:42-113), `paths` independent paths in one
+ * launch, one per thread. The network is described as for mk_fsp_problem: propensities
+ * tabulated over the box 0 <= x_s <= bounds[s]; a transition exists when its rate is > 0 and
+ * its result has no negative count (reaction_network::transitions). A path whose next state
+ * would leave the box stops there with status MK_EOVERFLOW (mk_ssa_run then returns
+ * MK_EOVERFLOW): widen the box and run again; path i is a function of (seed, i) alone, so a
+ * rerun replays it exactly. Random numbers: Philox4x32-10 keyed by the seed (the reference
+ * draws from a host generator, so paths agree with it in distribution, not sample by sample).
+ * Per path the outputs hold the final state, the state at each observation time (the state
+ * occupied at t, trajectory::indices_at), the jumps (or leaps) taken and a status, and when
+ * record > 0 the first `record` entries (times, states) of the path as the reference's
+ * trajectory holds them, with the full count. ---- */
+typedef struct {
+    int n_species;                  /* 1..4 */
+    int n_reactions;                /* 0..16 */
+    const int *bounds;              /* n_species */
+    const int *change;              /* n_reactions x n_species */
+    const double *rates;            /* n_reactions x box_size, host memory (as mk_fsp_problem) */
+    const int *initial;             /* n_species, inside the box */
+    double final_time;
+    int method;                     /* 0 Gillespie's direct method, 1 Poisson tau-leaping */
+    int64_t max_jumps;              /* Gillespie: jumps per path (ssa.hpp:44) */
+    double leap_step;               /* tau-leaping leap_options: step (0: from epsilon), */
+    double leap_epsilon;            /* epsilon and */
+    double leap_min_step;           /* min_step (ssa.hpp:77-81) */
+    int64_t paths;
+    uint64_t seed;
+    int n_observations;
+    const double *observation_times; /* sorted, within [0, final_time] */
+    int record;                     /* trajectory entries kept per path; 0: none */
+} mk_ssa_problem;
+typedef struct {                    /* host arrays; observed and record_* may be NULL when unused */
+    int *final_state;               /* paths x n_species */
+    int *observed;                  /* paths x n_observations x n_species */
+    int64_t *steps;                 /* paths: jumps (Gillespie) or leaps (tau-leaping) */
+    int *status;                    /* paths: MK_OK, MK_EOVERFLOW (left the box), MK_ENOTCONV */
+    double *record_times;           /* paths x record */
+    int *record_states;             /* paths x record x n_species */
+    int *record_count;              /* paths: entries of the whole trajectory */
+} mk_ssa_output;
+/* defaults: max_jumps unlimited, leap_epsilon 0.03, leap_min_step 1e-6, one path */
+void mk_ssa_problem_default(mk_ssa_problem *problem);
+int mk_ssa_run(const mk_ssa_problem *problem, mk_ssa_output *out, void *stream);
+
 /* ---- Serving: a request loop of resolvent solves (no counterpart in the reference; each
  * request is the reference's shifted_generator + sector_multigrid + num::gmres solve,
  * tests/test_rdme.cpp:225-251, on a resident solver) ----

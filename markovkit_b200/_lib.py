@@ -97,6 +97,40 @@ class FspProblem(C.Structure):
     ]
 
 
+class SsaProblem(C.Structure):
+    _fields_ = [
+        ("n_species", C.c_int),
+        ("n_reactions", C.c_int),
+        ("bounds", C.POINTER(C.c_int)),
+        ("change", C.POINTER(C.c_int)),
+        ("rates", C.POINTER(C.c_double)),
+        ("initial", C.POINTER(C.c_int)),
+        ("final_time", C.c_double),
+        ("method", C.c_int),
+        ("max_jumps", C.c_int64),
+        ("leap_step", C.c_double),
+        ("leap_epsilon", C.c_double),
+        ("leap_min_step", C.c_double),
+        ("paths", C.c_int64),
+        ("seed", C.c_uint64),
+        ("n_observations", C.c_int),
+        ("observation_times", C.POINTER(C.c_double)),
+        ("record", C.c_int),
+    ]
+
+
+class SsaOutput(C.Structure):
+    _fields_ = [
+        ("final_state", C.POINTER(C.c_int)),
+        ("observed", C.POINTER(C.c_int)),
+        ("steps", C.POINTER(C.c_int64)),
+        ("status", C.POINTER(C.c_int)),
+        ("record_times", C.POINTER(C.c_double)),
+        ("record_states", C.POINTER(C.c_int)),
+        ("record_count", C.POINTER(C.c_int)),
+    ]
+
+
 class FspResult(C.Structure):
     _fields_ = [
         ("time", C.c_double),
@@ -257,6 +291,8 @@ SIGNATURES = {
     "mk_fsp_batch_device_output": (C.c_int, [P, C.POINTER(P)]),
     "mk_fsp_batch_results": (C.c_int, [P, DP, C.POINTER(FspResult), P]),
     "mk_fsp_krylov_batch": (C.c_int, [C.c_int, C.POINTER(FspProblem), DP, C.POINTER(FspResult), P]),
+    "mk_ssa_problem_default": (None, [C.POINTER(SsaProblem)]),
+    "mk_ssa_run": (C.c_int, [C.POINTER(SsaProblem), C.POINTER(SsaOutput), P]),
     "mk_server_options_default": (None, [C.POINTER(ServerOptions)]),
     "mk_server_create": (C.c_int, [C.POINTER(ServerOptions), C.POINTER(P)]),
     "mk_server_destroy": (None, [P]),
