@@ -22,7 +22,8 @@ two-particle annihilation box of 1,050,625 states); `served` (requests of the wo
 request loop, batched four wide); `served_mix` (the seeded serving workload of
 markovkit_b200.inputs.serving_requests against the plain FP64 path on the same arrivals);
 `fsp_batch` (512 Krylov-FSP propagations in one persistent launch, with its CPU baseline);
-`roofline` (the generator SpMV of the workload) and `cpu_baseline`.
+`ssa_batch` (2^20 Gillespie paths of a toggle switch in one launch, with the reference's own
+gillespie on the host cores beside it); `roofline` (the generator SpMV of the workload) and `cpu_baseline`.
 
 Multi-GPU: independent replicas (one resident solver per rank, each solving its own
 right-hand sides; no collective on the data path), weak scaling. `--gpus N` outside torchrun
@@ -308,6 +309,7 @@ def run_ours(args) -> dict | None:
     served = None if args.no_serve else serve_measure(mk, box, model, w, host_b, W, K)
     served_mix = serve_mix_measure(mk) if world == 1 and not args.no_serve_mix else None
     fsp = fsp_batch_measure(rank == 0 and world == 1 and not args.no_cpu_baseline) if not args.no_fsp else None
+    ssa = ssa_measure(rank == 0 and world == 1 and not args.no_cpu_baseline) if not args.no_ssa else None
     dist_teardown(world)
     if rank != 0:
         return None
@@ -362,6 +364,7 @@ def run_ours(args) -> dict | None:
         "served": served,
         "served_mix": served_mix,
         "fsp_batch": fsp,
+        "ssa_batch": ssa,
         "roofline": roof,
         "gpu_launches": r32["launches"],
         "clocks": r32["clocks"],
@@ -678,6 +681,67 @@ def fsp_cpu_baseline(inst) -> dict:
                       f"seconds per instance ({mean:.3f} s)"}
 
 
+SSA_PATHS = 1 << 20
+SSA_TOGGLE = (30.0, 25.0, 2.0, 2.5)  # a1, a2, n1, n2: a toggle switch of the FSP batch's family
+SSA_CPU_PATHS = 20000                 # paths per host core in the CPU baseline
+
+
+def ssa_measure(with_cpu: bool) -> dict:
+    """The batched SSA: SSA_PATHS Gillespie paths of a toggle switch from (0, 0) to t = 2 in one
+    launch, through the public call (markovkit_b200.ssa.simulate: propensity table built and
+    uploaded, the launch, final states, jumps and statuses copied back), timed by wall clock
+    after an untimed run of the same seed that sizes the propensity box. The CPU baseline runs
+    the reference's own gillespie (oracle/_ref/ref_ssa), one process per host core."""
+    from markovkit_b200.fsp_models import toggle
+    from markovkit_b200.ssa import simulate
+
+    model = toggle(*SSA_TOGGLE)
+    sized = simulate(model, [0, 0], 2.0, SSA_PATHS, seed=3)
+    t0 = time.perf_counter()
+    ens = simulate(model, [0, 0], 2.0, SSA_PATHS, seed=3, bounds=sized.bounds)
+    sec = time.perf_counter() - t0
+    jumps = int(ens.steps.sum())
+    out = {
+        "metric": "Gillespie paths/sec to t = 2 (toggle switch a1 30, a2 25, n1 2, n2 2.5), one launch",
+        "value": round(SSA_PATHS / sec, 1),
+        "unit": "paths/s",
+        "ms": round(1e3 * sec, 3),
+        "paths": SSA_PATHS,
+        "jumps_per_s": round(jumps / sec, 1),
+        "mean_final": [round(float(v), 4) for v in ens.final_means()],
+        "box": ens.bounds,
+        "timing": "wall clock around the public call (host table, upload, launch, copies out)",
+    }
+    if with_cpu:
+        out["cpu_baseline"] = ssa_cpu_baseline()
+    return out
+
+
+def ssa_cpu_baseline() -> dict:
+    from concurrent.futures import ThreadPoolExecutor
+
+    driver = ROOT / "oracle" / "_ref" / "ref_ssa"
+    if not driver.exists():
+        return {"value": None, "unit": "paths/s", "cores": None, "kind": "reference",
+                "sample": "oracle/_ref/ref_ssa not built"}
+    cores = os.cpu_count() or 1
+    a1, a2, n1, n2 = SSA_TOGGLE
+
+    def one(k):
+        args = [str(driver), "model=toggle", f"paths={SSA_CPU_PATHS}", "T=2", f"seed={k + 1}",
+                f"a1={a1}", f"a2={a2}", f"n1={n1}", f"n2={n2}"]
+        p = subprocess.run(args, capture_output=True, text=True, timeout=600)
+        return p.returncode
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        rcs = list(ex.map(one, range(cores)))
+    wall = time.perf_counter() - t0
+    ok = sum(1 for rc in rcs if rc == 0)
+    return {"value": round(ok * SSA_CPU_PATHS / wall, 1), "unit": "paths/s", "cores": cores, "kind": "reference",
+            "sample": f"{SSA_CPU_PATHS} paths per core, one ref_ssa process per core, {wall:.2f} s wall"}
+
+
 def _uuid(dev) -> str | None:
     import torch
 
@@ -884,6 +948,7 @@ def main() -> None:
     ap.add_argument("--no-serve", action="store_true", help="skip the served line")
     ap.add_argument("--no-serve-mix", action="store_true", help="skip the mixed serving workload")
     ap.add_argument("--no-fsp", action="store_true", help="skip the Krylov-FSP batch line")
+    ap.add_argument("--no-ssa", action="store_true", help="skip the batched SSA line")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 2-D secondary workload")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -31,9 +31,11 @@
 #include <concepts>
 #include <cstdint>
 #include <functional>
+#include <limits>
 #include <map>
 #include <memory>
 #include <optional>
+#include <random>
 #include <span>
 #include <stdexcept>
 #include <string>
@@ -62,6 +64,21 @@ template <typename T>
 using array = std::vector<T>;
 template <typename T, std::size_t N>
 using static_array = std::array<T, N>;
+
+// a seeded uniform random bit generator, the numerics library's num::rng as MarkovKit's
+// programs use it (tests/test_ssa.cpp:27): here it only seeds the device streams of
+// gillespie and tau_leaping
+class rng {
+  public:
+    using result_type = std::uint64_t;
+    explicit rng(std::uint64_t seed = 0) : engine_(seed) {}
+    static constexpr result_type min() { return std::mt19937_64::min(); }
+    static constexpr result_type max() { return std::mt19937_64::max(); }
+    result_type operator()() { return engine_(); }
+
+  private:
+    std::mt19937_64 engine_;
+};
 } // namespace num
 
 namespace detail {
@@ -737,8 +754,36 @@ struct reaction {
     std::function<real(const state &)> rate;
 };
 
+// a jump out of a state (chain.hpp:33-36)
+struct transition {
+    state to;
+    real rate;
+};
+
 struct reaction_network {
     array<reaction> reactions;
+
+    // every reaction with a positive rate whose result has no negative count
+    // (reaction_network.hpp:20-37); host-side, for callers that enumerate jumps
+    [[nodiscard]] array<transition> transitions(const state &x) const {
+        array<transition> result;
+        for (const reaction &r : reactions) {
+            const real rate = r.rate(x);
+            if (!(rate > 0.0)) {
+                continue;
+            }
+            state y = x;
+            bool valid = true;
+            for (idx s = 0; s < y.size(); ++s) {
+                y[s] += r.change[s];
+                valid = valid && y[s] >= 0;
+            }
+            if (valid) {
+                result.push_back({std::move(y), rate});
+            }
+        }
+        return result;
+    }
 };
 
 // box(bounds): 0 <= x[s] <= bounds[s]; the only region the device FSP supports
@@ -996,6 +1041,203 @@ inline fsp_solution solve_adaptive_fsp(const reaction_network &model, const stat
 inline fsp_solution solve_krylov_fsp(const reaction_network &model, const state &initial,
                                      real final_time, const krylov_fsp_options &options) {
     return solve_krylov_fsp_batch({{model, initial, final_time, options}}).front();
+}
+
+// ---- stochastic simulation ----------------------------------------------------------------
+
+// a piecewise-constant path: the chain is in states[k] from times[k] until times[k + 1]
+// (ssa.hpp:14-39)
+struct trajectory {
+    array<real> times;
+    array<state> states;
+    [[nodiscard]] vec<real> component(idx species) const {
+        vec<real> out(states.size());
+        for (idx k = 0; k < states.size(); ++k) {
+            out[k] = states[k][species];
+        }
+        return out;
+    }
+    [[nodiscard]] array<idx> indices_at(view<const real> observation_times) const {
+        array<idx> out;
+        idx k = 0;
+        for (real t : observation_times) {
+            while (k + 1 < times.size() && times[k + 1] <= t) {
+                ++k;
+            }
+            out.push_back(k);
+        }
+        return out;
+    }
+};
+
+struct leap_options {
+    real step = 0.0;     // a fixed leap; zero chooses each leap from epsilon
+    real epsilon = 0.03; // expected number of jumps per leap
+    real min_step = 1e-6;
+};
+
+// many paths of one network, run on the device at once (mk_ssa_run)
+struct ssa_ensemble {
+    idx paths = 0, species = 0;
+    array<int> final_states;      // paths x species
+    array<int> observed;          // paths x observation times x species
+    array<std::int64_t> steps;    // jumps (Gillespie) or leaps per path
+    array<int> bounds;            // the propensity box used
+    array<real> observation_times;
+    array<trajectory> paths_kept; // with record > 0: each path as the reference returns it
+    // mean state at each observation time
+    [[nodiscard]] array<vec<real>> means() const {
+        const idx n = observation_times.size();
+        array<vec<real>> out(n, vec<real>(species, 0.0));
+        for (idx p = 0; p < paths; ++p) {
+            for (idx k = 0; k < n; ++k) {
+                for (idx s = 0; s < species; ++s) {
+                    out[k][s] += observed[(p * n + k) * species + s];
+                }
+            }
+        }
+        for (auto &m : out) {
+            for (real &v : m) {
+                v /= static_cast<real>(paths);
+            }
+        }
+        return out;
+    }
+};
+
+namespace detail {
+
+struct ssa_box {
+    region inside;
+};
+
+// mk_ssa_run over a box that doubles until no path leaves it (path i depends on (seed, i)
+// alone, so every rerun replays the same paths)
+inline ssa_ensemble simulate(const reaction_network &model, const state &initial, real final_time,
+                             idx paths, std::uint64_t seed, int method, std::int64_t max_jumps,
+                             const leap_options &leap, const array<real> &obs, int record) {
+    const idx S = initial.size();
+    array<int> bounds(S);
+    for (idx s = 0; s < S; ++s) {
+        bounds[s] = std::max(2 * initial[s], initial[s] + 64);
+    }
+    for (;;) {
+        const fsp_tables t = tabulate(model, initial, ssa_box{box(bounds)});
+        mk_ssa_problem q{};
+        mk_ssa_problem_default(&q);
+        q.n_species = static_cast<int>(S);
+        q.n_reactions = static_cast<int>(model.reactions.size());
+        q.bounds = t.bounds.data();
+        q.change = t.change.data();
+        q.rates = t.rates.data();
+        q.initial = t.initial.data();
+        q.final_time = final_time;
+        q.method = method;
+        q.max_jumps = max_jumps;
+        q.leap_step = leap.step;
+        q.leap_epsilon = leap.epsilon;
+        q.leap_min_step = leap.min_step;
+        q.paths = static_cast<int64_t>(paths);
+        q.seed = seed;
+        q.n_observations = static_cast<int>(obs.size());
+        q.observation_times = obs.data();
+        q.record = record;
+        ssa_ensemble e;
+        e.paths = paths;
+        e.species = S;
+        e.bounds = bounds;
+        e.observation_times = obs;
+        e.final_states.resize(paths * S);
+        e.observed.resize(paths * obs.size() * S);
+        e.steps.resize(paths);
+        array<int> status(paths), rec_states(paths * static_cast<idx>(record) * S), rec_n(record ? paths : 0);
+        array<real> rec_times(paths * static_cast<idx>(record));
+        mk_ssa_output out{e.final_states.data(), obs.empty() ? nullptr : e.observed.data(),
+                          e.steps.data(),        status.data(),
+                          record ? rec_times.data() : nullptr,
+                          record ? rec_states.data() : nullptr,
+                          record ? rec_n.data() : nullptr};
+        const int rc = mk_ssa_run(&q, &out, nullptr);
+        if (rc == MK_EOVERFLOW) {
+            idx size = 1;
+            for (int &b : bounds) {
+                b = 2 * b + 1;
+                size *= static_cast<idx>(b) + 1;
+            }
+            if (size > (idx(1) << 26)) {
+                throw std::overflow_error("ssa: the paths leave every propensity box of at most 2^26 states");
+            }
+            continue;
+        }
+        check(rc);
+        for (idx p = 0; p < (record ? paths : 0); ++p) {
+            const idx n = static_cast<idx>(rec_n[p]);
+            if (n > static_cast<idx>(record)) {
+                e.paths_kept.push_back({});
+                continue;
+            }
+            trajectory tr;
+            for (idx k = 0; k < n; ++k) {
+                tr.times.push_back(rec_times[p * record + k]);
+                const int *x = rec_states.data() + (p * record + k) * S;
+                tr.states.emplace_back(x, x + S);
+            }
+            e.paths_kept.push_back(std::move(tr));
+        }
+        return e;
+    }
+}
+
+template <std::uniform_random_bit_generator Rng>
+std::uint64_t seed_from(Rng &random) {
+    std::uint64_t s = 0;
+    for (int k = 0; k < 4; ++k) {
+        s = (s << 16) ^ static_cast<std::uint64_t>(random());
+    }
+    return s;
+}
+
+inline trajectory single_path(const reaction_network &model, const state &x, real final_time,
+                              std::uint64_t seed, int method, std::int64_t max_jumps,
+                              const leap_options &leap) {
+    for (int record = 1024;;) {
+        auto e = simulate(model, x, final_time, 1, seed, method, max_jumps, leap, {}, record);
+        if (!e.paths_kept.front().states.empty()) {
+            return std::move(e.paths_kept.front());
+        }
+        record *= 4;
+    }
+}
+
+} // namespace detail
+
+// `paths` independent paths in one device launch: Gillespie (method 0) or tau-leaping (1),
+// with the states at the observation times (sorted, within [0, final_time])
+inline ssa_ensemble simulate_paths(const reaction_network &model, const state &initial, real final_time,
+                                   idx paths, std::uint64_t seed, int method = 0,
+                                   array<real> observation_times = {},
+                                   std::int64_t max_jumps = std::numeric_limits<std::int64_t>::max(),
+                                   const leap_options &leap = {}) {
+    return detail::simulate(model, initial, final_time, paths, seed, method, max_jumps, leap,
+                            observation_times, 0);
+}
+
+// Gillespie's direct method (ssa.hpp:42-74) on the device; `random` seeds the path's stream
+template <std::uniform_random_bit_generator Rng>
+trajectory gillespie(const reaction_network &model, state x, real final_time, Rng &random,
+                     idx max_jumps = std::numeric_limits<idx>::max()) {
+    const auto cap = max_jumps > static_cast<idx>(std::numeric_limits<std::int64_t>::max())
+                         ? std::numeric_limits<std::int64_t>::max()
+                         : static_cast<std::int64_t>(max_jumps);
+    return detail::single_path(model, x, final_time, detail::seed_from(random), 0, cap, {});
+}
+
+// Poisson tau-leaping (ssa.hpp:83-111) on the device
+template <std::uniform_random_bit_generator Rng>
+trajectory tau_leaping(const reaction_network &model, state x, real final_time, Rng &random,
+                       leap_options options = {}) {
+    return detail::single_path(model, x, final_time, detail::seed_from(random), 1,
+                               std::numeric_limits<std::int64_t>::max(), options);
 }
 
 } // namespace markovkit

@@ -4,7 +4,8 @@ compiles against it with g++ and links the in-tree library (CPU), and runs corre
 compares plain, Jacobi, ILU(0) and multigrid-preconditioned GMRES) compiles unchanged against
 the facade with -I include/mk where the reference tree is at hand (MK_REFERENCE_ROOT, else a
 `reference` folder beside the repository); the binary lands in tests/cpp/_build and runs on a
-B200 with --quick."""
+B200 with --quick. The reference's own tests/test_ssa.cpp builds the same way and passes on the
+device SSA."""
 
 import os
 import subprocess
@@ -33,6 +34,9 @@ def _build() -> Path:
 REF = Path(os.environ.get("MK_REFERENCE_ROOT", ROOT.parent / "reference"))
 REF_BENCH = REF / "examples" / "rdme_multigrid_benchmark.cpp"
 REF_BENCH_OUT = ROOT / "tests" / "cpp" / "_build" / "rdme_multigrid_benchmark"
+# the reference's own SSA test (gillespie, tau_leaping, trajectory, reaction_network::transitions)
+REF_SSA = REF / "tests" / "test_ssa.cpp"
+REF_SSA_OUT = ROOT / "tests" / "cpp" / "_build" / "reference_test_ssa"
 
 
 def test_facade_program_compiles_and_links():
@@ -48,6 +52,27 @@ def test_reference_benchmark_compiles_against_facade():
     proc = subprocess.run(cmd, capture_output=True, text=True)
     assert proc.returncode == 0, proc.stderr[-4000:]
     assert REF_BENCH_OUT.exists()
+
+
+def test_reference_ssa_test_compiles_against_facade():
+    if not REF_SSA.exists():
+        pytest.skip("the reference tree is not here")
+    _build()
+    cmd = ["g++", "-std=c++20", "-O2", f"-I{ROOT / 'include' / 'mk'}", f"-I{REF / 'tests'}", str(REF_SSA),
+           f"-L{LIBDIR}", "-lmarkovkit_b200", f"-Wl,-rpath,{LIBDIR}", "-o", str(REF_SSA_OUT)]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    assert proc.returncode == 0, proc.stderr[-4000:]
+
+
+@pytest.mark.gpu
+def test_reference_ssa_test_runs(cuda):
+    """the reference's tests/test_ssa.cpp, unchanged, on the device SSA: every check passes
+    (its exit status counts the failed checks)"""
+    if not REF_SSA_OUT.exists():
+        pytest.skip("the reference SSA test was not built against the facade")
+    proc = subprocess.run([str(REF_SSA_OUT)], capture_output=True, text=True, timeout=600,
+                          env={**os.environ, "LD_LIBRARY_PATH": str(LIBDIR)})
+    assert proc.returncode == 0, proc.stdout + proc.stderr
 
 
 @pytest.mark.gpu
