@@ -227,6 +227,23 @@ typedef struct {
     int status;
 } mk_solver_result;
 void mk_gmres_options_default(mk_gmres_options *opt);
+/* The full-operator multigrid of the paper driver (rdme/cpp/rdme_full_multigrid.cpp:348-560,
+ * 819-850; no counterpart in the library): every level is the whole box on the grid coarsened
+ * d times, with the diffusivities doubled per level and the reactions of level_models[d],
+ * tabulated by the caller at that level's voxel volume (level_models[0] is the fine model; the
+ * grids must be those coarsen() gives). Transfers as sector_multigrid's; the level where the grid
+ * stops coarsening (or n_levels is reached) is inverted densely as one block (at most 8192
+ * states). Smoother 0 (weighted Jacobi) only; coarse_cycles 2 gives the W-cycle. Use it as a
+ * GMRES preconditioner (mk_solver_create) or as a solver of its own: */
+int mk_multigrid_create_full(mk_space space, const mk_model *level_models, int n_levels, double shift,
+                             const mk_multigrid_options *opt, mk_multigrid *out);
+/* the stationary iteration x <- x + M (b - A x), A = shift I - Q of gen with the multigrid's
+ * shift, from the x given, until ||b - A x||_2 <= tolerance (MK_ENOTCONV after max_cycles);
+ * result->iterations counts the cycles */
+int mk_multigrid_stationary(mk_multigrid mg, mk_generator gen, const double *d_b, double *d_x,
+                            double tolerance, int64_t max_cycles, mk_solver_result *result,
+                            void *stream);
+
 /* a resident solver for A = shift I - Q (shifted_generator, generator.hpp:116-133),
  * preconditioned by mg (NULL: plain GMRES); it keeps the Krylov workspace on the device */
 int mk_solver_create(mk_generator gen, double shift, mk_multigrid mg,

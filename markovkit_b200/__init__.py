@@ -5,6 +5,7 @@ include/markovkit_b200.h). This package is the Python mirror of the reference AP
 """
 
 from .api import (  # noqa: F401
+    full_multigrid,
     generator,
     gmres,
     gmres_options,

@@ -249,6 +249,8 @@ SIGNATURES = {
     "mk_csr_destroy": (None, [P]),
     "mk_multigrid_options_default": (None, [C.POINTER(MultigridOptions)]),
     "mk_multigrid_create": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
+    "mk_multigrid_create_full": (C.c_int, [P, C.POINTER(P), C.c_int, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
+    "mk_multigrid_stationary": (C.c_int, [P, P, P, P, C.c_double, I64, C.POINTER(SolverResult), P]),
     "mk_multigrid_destroy": (None, [P]),
     "mk_multigrid_apply": (C.c_int, [P, P, P, P]),
     "mk_multigrid_apply_batch": (C.c_int, [P, P, I64, P, I64, C.c_int, P]),

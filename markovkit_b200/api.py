@@ -559,6 +559,60 @@ class host_preconditioner(_Preconditioner):
         check(load().mk_precond_create_host(int(n), self._cb, None, C.byref(self._h)))
 
 
+def _coarsened(dims: Sequence[int]):
+    """coarsen() of the reference (multigrid.hpp:25-42): every axis longer than one cell halved,
+    None when an axis is odd or none is longer than one"""
+    if all(d == 1 for d in dims):
+        return None
+    out = []
+    for d in dims:
+        if d == 1:
+            out.append(1)
+        elif d % 2:
+            return None
+        else:
+            out.append(d // 2)
+    return out
+
+
+class full_multigrid(sector_multigrid):
+    """The paper driver's full-operator multigrid (rdme/cpp/rdme_full_multigrid.cpp:348-560,
+    819-850): every level is the whole space on a coarser grid, reactions included, with the
+    diffusivities doubled per level and the reactions re-tabulated at each level's voxel volume;
+    the coarsest level is solved densely. Weighted Jacobi smoothing; coarse_cycles=2 for the
+    W-cycle. A GMRES preconditioner (mk.solver(A, M)) or a solver of its own (stationary)."""
+
+    def __init__(self, model: reaction_diffusion, space: _Space, shift: float,
+                 options: Optional[MultigridOptions] = None):
+        _Handle.__init__(self)
+        self.space = space
+        self._shift = float(shift)
+        opts = options if options is not None else multigrid_options()
+        self.options = opts
+        g = model.domain.graph
+        dims, spacing = list(g.dimensions), list(g.spacing)
+        self._models = []
+        while True:
+            dom = voxel_domain(grid(dims, spacing), list(model.domain.diffusivities))
+            self._models.append(_Model(reaction_diffusion(dom, model.reactions), tuple_max=list(space.limits)))
+            coarse = _coarsened(dims)
+            if coarse is None or len(self._models) >= opts.max_levels:
+                break
+            spacing = [h * 2.0 if d > 1 else h for d, h in zip(dims, spacing)]
+            dims = coarse
+        self.model = self._models[0]
+        handles = (C.c_void_p * len(self._models))(*[m._h.value for m in self._models])
+        check(load().mk_multigrid_create_full(space._h, handles, len(self._models), float(shift), C.byref(opts),
+                                              C.byref(self._h)))
+
+    def stationary(self, Q: "generator", b, x, tolerance: float, max_cycles: int = 1000, stream=None) -> "solver_result":
+        """x <- x + M (b - A x) with A = shift I - Q until ||b - A x||_2 <= tolerance"""
+        r = SolverResult()
+        check(load().mk_multigrid_stationary(self._h, Q._h, _ptr(b), _ptr(x), float(tolerance), int(max_cycles),
+                                             C.byref(r), _stream(stream)), allow=(_lib.MK_ENOTCONV,))
+        return solver_result(r.iterations, r.residual, bool(r.converged), r.status)
+
+
 def kernel_launches() -> int:
     """Kernels the library has launched in this process (graph launches count their nodes)."""
     v = C.c_uint64()

@@ -417,31 +417,69 @@ void mk_multigrid_options_default(mk_multigrid_options *opt) {
     opt->batch = d.batch;
 }
 
+static int fill_result(const SolverResult &r, mk_solver_result *out);
+
+static MultigridOptions multigrid_options_of(const mk_multigrid_options *opt) {
+    MultigridOptions o;
+    if (opt) {
+        MK_REQUIRE(opt->pre_sweeps >= 0 && opt->post_sweeps >= 0 && opt->coarse_cycles >= 1 &&
+                       opt->sweep_growth >= 0 && opt->max_levels >= 1 && opt->coarsest_size >= 0,
+                   "bad multigrid options");
+        o.pre_sweeps = opt->pre_sweeps;
+        o.post_sweeps = opt->post_sweeps;
+        o.jacobi_weight = opt->jacobi_weight;
+        o.coarsest_size = opt->coarsest_size;
+        o.max_levels = opt->max_levels;
+        o.coarse_cycles = opt->coarse_cycles;
+        o.sweep_growth = opt->sweep_growth;
+        o.smoother = opt->smoother;
+        o.precision = opt->precision;
+        o.batch = opt->batch;
+    }
+    return o;
+}
+
 int mk_multigrid_create(mk_space space, mk_model model, double shift,
                         const mk_multigrid_options *opt, mk_multigrid *out) {
     return guarded([&] {
         MK_REQUIRE(space && model && out, "null argument");
-        MultigridOptions o;
-        if (opt) {
-            MK_REQUIRE(opt->pre_sweeps >= 0 && opt->post_sweeps >= 0 && opt->coarse_cycles >= 1 &&
-                           opt->sweep_growth >= 0 && opt->max_levels >= 1 &&
-                           opt->coarsest_size >= 0,
-                       "bad multigrid options");
-            o.pre_sweeps = opt->pre_sweeps;
-            o.post_sweeps = opt->post_sweeps;
-            o.jacobi_weight = opt->jacobi_weight;
-            o.coarsest_size = opt->coarsest_size;
-            o.max_levels = opt->max_levels;
-            o.coarse_cycles = opt->coarse_cycles;
-            o.sweep_growth = opt->sweep_growth;
-            o.smoother = opt->smoother;
-            o.precision = opt->precision;
-            o.batch = opt->batch;
-        }
+        const MultigridOptions o = multigrid_options_of(opt);
         auto h = std::make_unique<mk_multigrid_s>();
         h->mg = std::make_unique<Multigrid>(*space->space, *model->model, shift, o);
         *out = h.release();
     });
+}
+
+int mk_multigrid_create_full(mk_space space, const mk_model *level_models, int n_levels, double shift,
+                             const mk_multigrid_options *opt, mk_multigrid *out) {
+    return guarded([&] {
+        MK_REQUIRE(space && level_models && out && n_levels >= 1, "null argument");
+        std::vector<const Model *> models;
+        for (int d = 0; d < n_levels; ++d) {
+            MK_REQUIRE(level_models[d], "null level model");
+            models.push_back(level_models[d]->model.get());
+        }
+        const MultigridOptions o = multigrid_options_of(opt);
+        auto h = std::make_unique<mk_multigrid_s>();
+        h->mg = std::make_unique<Multigrid>(*space->space, models, shift, o);
+        *out = h.release();
+    });
+}
+
+int mk_multigrid_stationary(mk_multigrid mg, mk_generator gen, const double *d_b, double *d_x,
+                            double tolerance, int64_t max_cycles, mk_solver_result *result,
+                            void *stream) {
+    SolverResult r;
+    const int rc = guarded([&] {
+        MK_REQUIRE(mg && gen && d_b && d_x, "null argument");
+        MK_REQUIRE(tolerance >= 0.0 && max_cycles >= 0, "bad stationary-iteration options");
+        r = stationary(*gen->gen, mg->mg->shift, *mg->mg, d_b, d_x, tolerance, max_cycles,
+                       as_stream(stream));
+    });
+    if (rc != MK_OK) {
+        return rc;
+    }
+    return fill_result(r, result);
 }
 
 void mk_multigrid_destroy(mk_multigrid mg) { delete mg; }

@@ -373,6 +373,27 @@ void axpy_t(T a, const T *x, T *y, std::int64_t n, cudaStream_t stream) {
     check_cuda(cudaGetLastError(), "axpy");
 }
 
+// a whole level (every sector, reactions included) as one dense block, from the same
+// matrix-free rows (host, generic shape)
+void assemble_level(const OperatorLevel &op, double shift, std::vector<double> &A) {
+    const auto n = static_cast<std::size_t>(op.n);
+    A.assign(n * n, 0.0);
+    const BinomTable B = op.binom->host_view();
+    auto st = std::make_unique<RowState<kMaxSpecies, 64>>();
+    for (const SectorDesc &sec : op.sectors) {
+        for (std::int64_t i = 0; i < sec.size; ++i) {
+            load_state<kMaxSpecies, 64>(B, sec, op.S, op.V, i, *st);
+            double exit = 0.0, leak = 0.0;
+            const std::size_t row = static_cast<std::size_t>(sec.begin + i);
+            visit_row<double, kMaxSpecies, 64>(B, op.sectors.data(), sec, op.t64.host, i, *st, true, 0,
+                                               1, exit, leak, [&](std::int64_t j, double a, double) {
+                                                   A[row * n + static_cast<std::size_t>(j)] -= a;
+                                               });
+            A[row * n + row] += shift + exit;
+        }
+    }
+}
+
 // the terminal block of one sector, dense, from the same matrix-free rows (host, generic shape)
 void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vector<double> &A) {
     const SectorDesc &sec = op.sectors[slot];
@@ -393,9 +414,27 @@ void assemble_terminal(const OperatorLevel &op, int slot, double shift, std::vec
 
 } // namespace
 
+namespace {
+const Model &fine_model(const std::vector<const Model *> &level_models) {
+    if (level_models.empty() || !level_models[0]) {
+        throw Error(kEInval, "full-operator multigrid: no level models");
+    }
+    return *level_models[0];
+}
+} // namespace
+
+Multigrid::Multigrid(const Space &space, const std::vector<const Model *> &level_models,
+                     double shift_, const MultigridOptions &o)
+    : Multigrid(space, fine_model(level_models), shift_, o, &level_models) {}
+
 Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
                      const MultigridOptions &o)
-    : Preconditioner(space.n), opt(o), shift(shift_), binom(space.binom) {
+    : Multigrid(space, model, shift_, o, nullptr) {}
+
+Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
+                     const MultigridOptions &o, const std::vector<const Model *> *level_models)
+    : Preconditioner(space.n), opt(o), shift(shift_), full_(level_models != nullptr),
+      binom(space.binom) {
     if (!(shift > 0.0)) {
         throw Error(kEInval, "population_multigrid: shift must be positive");
     }
@@ -411,6 +450,9 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     }
     if (opt.smoother == 3 && opt.batch != 1) {
         throw Error(kEInval, "the aggregate-block smoother serves one right-hand side at a time");
+    }
+    if (full_ && opt.smoother != 0) {
+        throw Error(kEInval, "the full-operator multigrid smooths by weighted Jacobi (smoother 0)");
     }
     if (opt.batch < 1 || opt.batch > kRowBatch) {
         throw Error(kEInval, "multigrid batch must be in 1.." + std::to_string(kRowBatch));
@@ -435,12 +477,30 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     for (int d = 0; !totals.empty(); ++d) {
         auto L = std::make_unique<Level>();
         auto grid_model = Model::grid(model.dim, dims, spacing, model.diff);
+        if (full_) {
+            // this level's reactions, tabulated by the caller at its voxel volume
+            if (d >= static_cast<int>(level_models->size()) || !(*level_models)[d]) {
+                throw Error(kEInval, "full-operator multigrid: no model for level " + std::to_string(d));
+            }
+            const Model &lm = *(*level_models)[d];
+            if (lm.V != grid_model->V || lm.S != S) {
+                throw Error(kEInval, "full-operator multigrid: level " + std::to_string(d) +
+                                         "'s model is not on the coarsened grid");
+            }
+            grid_model->R = lm.R;
+            grid_model->change = lm.change;
+            grid_model->tmax = lm.tmax;
+            grid_model->nvc = lm.nvc;
+            grid_model->vclass = lm.vclass;
+            grid_model->rates = lm.rates;
+            grid_model->validate();
+        }
         L->op.V = grid_model->V;
         L->op.S = S;
         L->op.binom = binom;
         L->op.sectors = layout_sectors(grid_model->V, S, totals, binom->host_view(), &L->op.n);
-        L->op.t64.build(*grid_model, scale, false, true);
-        L->op.t32.build(*grid_model, scale, false, true);
+        L->op.t64.build(*grid_model, scale, full_, true);
+        L->op.t32.build(*grid_model, scale, full_, true);
         L->pre = opt.pre_sweeps + d * opt.sweep_growth;
         L->post = opt.post_sweeps + d * opt.sweep_growth;
         L->box_sector = box_of;
@@ -453,8 +513,29 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
 
         std::vector<std::vector<int>> next_totals;
         std::vector<int> next_box;
+        // the full operator couples the sectors: the level coarsens or stops as a whole
+        const bool whole_terminal = full_ && (L->op.n <= opt.coarsest_size || levels_left <= 1 ||
+                                              !can_coarsen ||
+                                              d + 1 >= static_cast<int>(level_models->size()));
+        if (whole_terminal) {
+            if (L->op.n > 8192) {
+                throw Error(kEInval, "full-operator multigrid: coarsest level larger than 8192 states");
+            }
+            TerminalBlock tb;
+            tb.begin = 0;
+            tb.n = static_cast<int>(L->op.n);
+            L->h_term.push_back(tb);
+        }
         for (std::size_t k = 0; k < totals.size(); ++k) {
             SectorDesc &sec = L->op.sectors[k];
+            if (full_) {
+                if (!whole_terminal) {
+                    sec.coarse = static_cast<int>(next_totals.size());
+                    next_totals.push_back(totals[k]);
+                    next_box.push_back(box_of[k]);
+                }
+                continue;
+            }
             const bool terminal =
                 sec.size <= opt.coarsest_size || levels_left <= 1 || !can_coarsen;
             if (terminal) {
@@ -472,14 +553,19 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
                 next_box.push_back(box_of[k]);
             }
         }
-        L->op.finalize(*grid_model, false);
+        L->op.finalize(*grid_model, full_);
 
         // dense inverses of the terminal blocks, from the same matrix-free rows, all of a level
         // at once (on the device when they are large)
         std::vector<double> inv_all, A, A_all, dense_all;
         std::vector<std::int64_t> term_offset;
         std::vector<int> term_n;
-        for (std::size_t k = 0; k < L->op.sectors.size(); ++k) {
+        if (whole_terminal) {
+            assemble_level(L->op, shift, A_all);
+            term_offset.push_back(0);
+            term_n.push_back(static_cast<int>(L->op.n));
+        }
+        for (std::size_t k = 0; k < L->op.sectors.size() && !full_; ++k) {
             const SectorDesc &sec = L->op.sectors[k];
             if (sec.terminal < 0) {
                 continue;
@@ -1403,6 +1489,40 @@ void read_report(const Krylov &ws, cudaStream_t stream) {
 }
 
 } // namespace
+
+SolverResult stationary(const Generator &A, double shift, Preconditioner &M, const double *b,
+                        double *x, double tol, std::int64_t max_cycles, cudaStream_t stream) {
+    SolverResult res;
+    const std::int64_t n = A.op.n;
+    if (M.n != n) {
+        throw Error(kEInval, "preconditioner size does not match the system");
+    }
+    DeviceArray<double> r(static_cast<std::size_t>(n)), z(static_cast<std::size_t>(n));
+    DeviceArray<double> partials(kDotBlocks), norm2(1);
+    for (std::int64_t it = 0;; ++it) {
+        A.apply<double>(kResidual, shift, x, b, r.get(), nullptr, stream);
+        check_cuda(dot(r.get(), r.get(), n, partials.get(), norm2.get(), stream), "dot");
+        double h = 0.0;
+        check_cuda(cudaMemcpyAsync(&h, norm2.get(), sizeof h, cudaMemcpyDeviceToHost, stream), "norm");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        res.residual = std::sqrt(h);
+        res.iterations = it;
+        if (!std::isfinite(res.residual)) {
+            res.status = kENan;
+            return res;
+        }
+        if (res.residual <= tol) {
+            res.converged = 1;
+            return res;
+        }
+        if (it >= max_cycles) {
+            res.status = kENotConv;
+            return res;
+        }
+        M.apply(r.get(), z.get(), stream);
+        check_cuda(axpy(1.0, z.get(), x, n, stream), "update");
+    }
+}
 
 SolverResult gmres(const Generator &A, double shift, Preconditioner *M, const double *b,
                    double *x, const GmresOptions &opt, Krylov &ws, cudaStream_t stream) {

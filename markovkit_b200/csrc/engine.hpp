@@ -244,11 +244,27 @@ struct Multigrid : Preconditioner {
     MultigridOptions opt;
     double shift = 0.0;
     int max_depth = 0;
+    bool full_ = false;
     std::vector<std::unique_ptr<Level>> levels;
     DeviceArray<double> lgf;
     std::shared_ptr<Binomials> binom;
 
     Multigrid(const Space &space, const Model &model, double shift, const MultigridOptions &opt);
+    // The full-operator hierarchy of the paper driver (rdme/cpp/rdme_full_multigrid.cpp:348-560,
+    // 819-850): every level is the whole box on a grid coarsened d times, with diffusivities
+    // doubled per level and the reactions of level_models[d] (the caller tabulates the rates at
+    // that level's voxel volume; level_models[0] is the fine model); the coarsest level, where
+    // the grid stops coarsening, is solved densely as one block. Weighted Jacobi smoothing only:
+    // reactions couple states of one checkerboard colour, so a red-black pass would race.
+    Multigrid(const Space &space, const std::vector<const Model *> &level_models, double shift,
+              const MultigridOptions &opt);
+    [[nodiscard]] bool full_operator() const { return full_; }
+
+  private:
+    Multigrid(const Space &space, const Model &model, double shift, const MultigridOptions &opt,
+              const std::vector<const Model *> *level_models);
+
+  public:
     ~Multigrid() override;
     // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
     void apply(const double *b, double *x, cudaStream_t stream) override;
@@ -331,6 +347,12 @@ struct Krylov {
     Krylov(const Krylov &) = delete;
     Krylov &operator=(const Krylov &) = delete;
 };
+
+// the stationary iteration x <- x + M (b - A x) on A = shift I - Q (the paper driver's
+// multigrid method, rdme/cpp/rdme_full_multigrid.cpp:1190-1215) until ||b - A x||_2 <= tol;
+// iterations = cycles applied
+SolverResult stationary(const Generator &A, double shift, Preconditioner &M, const double *b,
+                        double *x, double tol, std::int64_t max_cycles, cudaStream_t stream);
 
 // right-preconditioned restarted GMRES (Saad Alg. 9.5) or FGMRES (Alg. 9.6) on
 // A = shift I - Q with classical Gram-Schmidt and one re-orthogonalisation

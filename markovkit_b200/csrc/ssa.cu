@@ -106,8 +106,8 @@ __device__ std::int64_t poisson(Philox &rng, double mu) {
 
 // the propensities of the listed transitions of x (reaction_network::transitions: a reaction is
 // listed when its result has no negative count and its rate is > 0), 0 for the others
-__device__ double propensities(const SsaParams &p, const int (&x)[kSsaMaxSpecies],
-                               double (&a)[kSsaMaxReactions]) {
+template <int NR>
+__device__ double propensities(const SsaParams &p, const int (&x)[kSsaMaxSpecies], double (&a)[NR]) {
     std::int64_t idx = 0;
 #pragma unroll
     for (int s = 0; s < kSsaMaxSpecies; ++s) {
@@ -117,7 +117,7 @@ __device__ double propensities(const SsaParams &p, const int (&x)[kSsaMaxSpecies
     }
     double total = 0.0;
 #pragma unroll
-    for (int r = 0; r < kSsaMaxReactions; ++r) {
+    for (int r = 0; r < NR; ++r) {
         a[r] = 0.0;
         if (r >= p.R) {
             continue;
@@ -142,6 +142,8 @@ __device__ void write_state(int *dst, const int (&x)[kSsaMaxSpecies], int S) {
     }
 }
 
+// NR: the reactions' count rounded up to 4, 8 or 16 (the propensities stay in registers)
+template <int NR>
 __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
     const std::int64_t path = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x;
     if (path >= p.paths) {
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
         }
     };
     record(0.0);
-    double a[kSsaMaxReactions];
+    double a[NR];
     double t = 0.0;
     std::int64_t steps = 0;
     int status = kOk;
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
                 status = p.max_jumps > cap ? kENotConv : kOk;
                 break;
             }
-            const double total = propensities(p, x, a);
+            const double total = propensities<NR>(p, x, a);
             if (!(total > 0.0)) {
                 break;
             }
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
             double acc = 0.0;
             int chosen = -1;
 #pragma unroll
-            for (int r = 0; r < kSsaMaxReactions; ++r) {
+            for (int r = 0; r < NR; ++r) {
                 if (a[r] > 0.0) {
                     acc += a[r];
                     if (chosen < 0 && target < acc) {
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
             }
             if (chosen < 0) { // rounding at the top end: the last listed transition
 #pragma unroll
-                for (int r = 0; r < kSsaMaxReactions; ++r) {
+                for (int r = 0; r < NR; ++r) {
                     chosen = a[r] > 0.0 ? r : chosen;
                 }
             }
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
                 status = kENotConv;
                 break;
             }
-            const double total = propensities(p, x, a);
+            const double total = propensities<NR>(p, x, a);
             if (!(total > 0.0)) {
                 break;
             }
@@ -248,7 +250,7 @@ __global__ void __launch_bounds__(kSsaThreads) ssa_kernel(const SsaParams p) {
                 next[s] = x[s];
             }
 #pragma unroll
-            for (int r = 0; r < kSsaMaxReactions; ++r) {
+            for (int r = 0; r < NR; ++r) {
                 if (!(a[r] > 0.0)) {
                     continue;
                 }
@@ -298,7 +300,14 @@ cudaError_t launch_ssa(const SsaParams &p, cudaStream_t stream) {
         return cudaErrorInvalidValue;
     }
     count_launches(1);
-    ssa_kernel<<<static_cast<unsigned>(blocks), kSsaThreads, 0, stream>>>(p);
+    const auto grid = static_cast<unsigned>(blocks);
+    if (p.R <= 4) {
+        ssa_kernel<4><<<grid, kSsaThreads, 0, stream>>>(p);
+    } else if (p.R <= 8) {
+        ssa_kernel<8><<<grid, kSsaThreads, 0, stream>>>(p);
+    } else {
+        ssa_kernel<kSsaMaxReactions><<<grid, kSsaThreads, 0, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 
