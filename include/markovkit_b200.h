@@ -169,6 +169,9 @@ typedef struct {
                       3 aggregate blocks (relaxation::aggregate_block, multigrid.hpp:239-341; batch 1) */
     int precision; /* 0 FP64, 1 FP32 (use inside flexible GMRES) */
     int batch;     /* right-hand sides one cycle can serve at once (1..4), for batch solvers */
+    int cycle_type; /* 0 V or W (coarse_cycles); 1 K-cycle of the full-operator multigrid
+                       (rdme_full_multigrid.cpp:851-878; FP64, batch 1; a nonlinear cycle:
+                       flexible GMRES when used as a preconditioner) */
 } mk_multigrid_options;
 void mk_multigrid_options_default(mk_multigrid_options *opt);
 /* sector_multigrid(domain, box, shift, options) multigrid.hpp:377-384; a single-sector

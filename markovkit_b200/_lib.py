@@ -53,6 +53,7 @@ class MultigridOptions(C.Structure):
         ("smoother", C.c_int),
         ("precision", C.c_int),
         ("batch", C.c_int),
+        ("cycle_type", C.c_int),
     ]
 
 

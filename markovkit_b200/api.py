@@ -418,6 +418,8 @@ def multigrid_options(**kw) -> MultigridOptions:
             v = {"jacobi": 0, "gauss_seidel": 1, "ilu0": 2, "aggregate_block": 3}[v]
         if k == "precision" and isinstance(v, str):
             v = {"fp64": 0, "fp32": 1}[v]
+        if k == "cycle_type" and isinstance(v, str):
+            v = {"standard": 0, "k": 1}[v]
         setattr(o, k, v)
     return o
 

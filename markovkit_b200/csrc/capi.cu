@@ -415,6 +415,7 @@ void mk_multigrid_options_default(mk_multigrid_options *opt) {
     opt->smoother = d.smoother;
     opt->precision = d.precision;
     opt->batch = d.batch;
+    opt->cycle_type = d.cycle_type;
 }
 
 static int fill_result(const SolverResult &r, mk_solver_result *out);
@@ -435,6 +436,7 @@ static MultigridOptions multigrid_options_of(const mk_multigrid_options *opt) {
         o.smoother = opt->smoother;
         o.precision = opt->precision;
         o.batch = opt->batch;
+        o.cycle_type = opt->cycle_type;
     }
     return o;
 }

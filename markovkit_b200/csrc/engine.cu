@@ -454,6 +454,10 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     if (full_ && opt.smoother != 0) {
         throw Error(kEInval, "the full-operator multigrid smooths by weighted Jacobi (smoother 0)");
     }
+    if (opt.cycle_type != 0 && (opt.cycle_type != 1 || !full_ || opt.precision != 0 || opt.batch != 1)) {
+        throw Error(kEInval, "the K-cycle belongs to the full-operator multigrid, in FP64, one "
+                             "right-hand side at a time");
+    }
     if (opt.batch < 1 || opt.batch > kRowBatch) {
         throw Error(kEInval, "multigrid batch must be in 1.." + std::to_string(kRowBatch));
     }
@@ -650,6 +654,18 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
                 L.acc32.resize(nc);
                 L.crhs32.resize(nc);
             }
+        }
+    }
+    if (opt.cycle_type == 1) {
+        for (std::size_t d = 0; d + 2 < levels.size(); ++d) {
+            Level &L = *levels[d];
+            const std::size_t nc = static_cast<std::size_t>(levels[d + 1]->op.n);
+            for (DeviceArray<double> *v : {&L.kg, &L.kv1, &L.kw1, &L.kv2, &L.kw2, &L.kr, &L.ke}) {
+                v->resize(nc);
+            }
+            L.kdots.resize(8);
+            L.kcoef.resize(4);
+            L.kpartials.resize(kDotBlocks);
         }
     }
     build_transfers();
@@ -1010,7 +1026,14 @@ T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
     }
     if (C) {
         T *cx = nullptr;
-        if (opt.coarse_cycles <= 1) {
+        if constexpr (std::is_same_v<T, double>) {
+            if (opt.cycle_type == 1 && d + 2 < max_depth) {
+                cx = kcycle_coarse(d, stream);
+            }
+        }
+        if (cx) {
+            // the K-cycle's correction
+        } else if (opt.coarse_cycles <= 1) {
             cx = cycle<T>(d + 1, stream, carve);
         } else {
             T *acc = buf<T>(L, 4, cl), *crhs = buf<T>(L, 5, cl);
@@ -1069,6 +1092,98 @@ T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
                    "copy");
     }
     return buf<T>(L, 1, cl);
+}
+
+namespace {
+
+// The K-cycle's step coefficients from its dot products, on the device so that the cycle stays
+// one captured graph (the reference's early returns become zero coefficients):
+//   dots: 0 g.g, 1 w1.w1, 2 w1.g, 3 r.r, 4 w2.w1, 5 w2.w2, 6 w2.r
+//   coef: 0 a1, 1 beta, 2 a2, 3 whether the second step is taken
+__global__ void kcycle_coef_kernel(int phase, const double *dots, double *coef) {
+    const bool first = dots[0] > 0.0 && dots[1] > 0.0;
+    if (phase == 0) {
+        coef[0] = first ? dots[2] / dots[1] : 0.0;
+        coef[1] = coef[2] = coef[3] = 0.0;
+    } else if (phase == 1) {
+        const bool second = first && !(dots[3] <= 0.0625 * dots[0]);
+        coef[3] = second ? 1.0 : 0.0;
+        coef[1] = second ? dots[4] / dots[1] : 0.0;
+    } else {
+        coef[2] = coef[3] != 0.0 && dots[5] > 0.0 ? dots[6] / dots[5] : 0.0;
+    }
+}
+
+// y = sign * coef[k] * x (init) or y += sign * coef[k] * x
+__global__ void kcycle_axpy_kernel(const double *coef, int k, double sign, const double *x,
+                                   double *y, std::int64_t n, bool init) {
+    const double a = sign * coef[k];
+    const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
+    for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += stride) {
+        y[i] = init ? a * x[i] : y[i] + a * x[i];
+    }
+}
+
+void kcycle_axpy(const double *coef, int k, double sign, const double *x, double *y,
+                 std::int64_t n, bool init, cudaStream_t stream) {
+    const auto blocks = static_cast<unsigned>(std::clamp<std::int64_t>((n + 255) / 256, 1, 148 * 8));
+    count_launches(1);
+    kcycle_axpy_kernel<<<blocks, 256, 0, stream>>>(coef, k, sign, x, y, n, init);
+    check_cuda(cudaGetLastError(), "K-cycle update");
+}
+
+} // namespace
+
+// The K-cycle coarse solve of the paper driver (rdme/cpp/rdme_full_multigrid.cpp:851-878, after
+// Notay and Vassilevski, in nonsymmetric GCR form): on A_c e = g at depth d + 1, at most two
+// minimal-residual steps, each preconditioned by one recursive coarse cycle; the second step is
+// skipped when the first reduces ||g|| by the factor 0.25 (here: taken with coefficient zero).
+double *Multigrid::kcycle_coarse(int d, cudaStream_t stream) {
+    Level &L = *levels[d];
+    Level &C = *levels[d + 1];
+    const std::int64_t n = C.op.n;
+    const std::size_t bytes = static_cast<std::size_t>(n) * sizeof(double);
+    double *g = buf<double>(C, 0, nullptr);
+    double *dots = L.kdots.get(), *coef = L.kcoef.get(), *part = L.kpartials.get();
+    auto apply_c = [&](const double *v, double *w) {
+        RowParams<double> p = C.op.params<double>();
+        p.shift = shift;
+        p.x = v;
+        p.y = w;
+        C.op.run<double>(kApplyShifted, p, stream);
+    };
+    auto dot_into = [&](const double *a, const double *b, int k) {
+        check_cuda(dot(a, b, n, part, dots + k, stream), "K-cycle dot");
+    };
+    auto copy = [&](double *dst, const double *src) {
+        check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream), "copy");
+    };
+    copy(L.kg.get(), g);
+    dot_into(L.kg.get(), L.kg.get(), 0);
+    copy(L.kv1.get(), cycle<double>(d + 1, stream, nullptr));
+    apply_c(L.kv1.get(), L.kw1.get());
+    dot_into(L.kw1.get(), L.kw1.get(), 1);
+    dot_into(L.kw1.get(), L.kg.get(), 2);
+    count_launches(3);
+    kcycle_coef_kernel<<<1, 1, 0, stream>>>(0, dots, coef);
+    kcycle_axpy(coef, 0, 1.0, L.kv1.get(), L.ke.get(), n, true, stream);
+    copy(L.kr.get(), L.kg.get());
+    kcycle_axpy(coef, 0, -1.0, L.kw1.get(), L.kr.get(), n, false, stream);
+    dot_into(L.kr.get(), L.kr.get(), 3);
+    copy(g, L.kr.get());
+    copy(L.kv2.get(), cycle<double>(d + 1, stream, nullptr));
+    apply_c(L.kv2.get(), L.kw2.get());
+    dot_into(L.kw2.get(), L.kw1.get(), 4);
+    kcycle_coef_kernel<<<1, 1, 0, stream>>>(1, dots, coef);
+    kcycle_axpy(coef, 1, -1.0, L.kv1.get(), L.kv2.get(), n, false, stream);
+    kcycle_axpy(coef, 1, -1.0, L.kw1.get(), L.kw2.get(), n, false, stream);
+    dot_into(L.kw2.get(), L.kw2.get(), 5);
+    dot_into(L.kw2.get(), L.kr.get(), 6);
+    kcycle_coef_kernel<<<1, 1, 0, stream>>>(2, dots, coef);
+    check_cuda(cudaGetLastError(), "K-cycle coefficients");
+    kcycle_axpy(coef, 2, 1.0, L.kv2.get(), L.ke.get(), n, false, stream);
+    return L.ke.get();
 }
 
 void Multigrid::transfer(int d, int direction, const double *in, double *out,
@@ -1246,6 +1361,9 @@ void Multigrid::apply_in(const double *b, double *x, void *scratch, std::size_t 
                          cudaStream_t stream) {
     if (bytes < scratch_bytes() || (reinterpret_cast<std::uintptr_t>(scratch) % kCarveAlign) != 0) {
         throw Error(kEInval, "multigrid scratch too small or misaligned");
+    }
+    if (opt.cycle_type == 1) {
+        throw Error(kEInval, "the K-cycle keeps its vectors in the hierarchy");
     }
     // the work vectors of this call only: six per level, carved from the caller's memory and
     // handed down the cycle (the hierarchy's own buffers and state stay untouched)

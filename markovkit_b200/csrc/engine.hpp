@@ -184,6 +184,7 @@ struct MultigridOptions {
                        // 2 red-black ILU(0), 3 aggregate blocks (relaxation::aggregate_block)
     int precision = 0; // 0 FP64, 1 FP32 preconditioner
     int batch = 1;     // right-hand sides one cycle can serve at once (work vectors per level)
+    int cycle_type = 0; // 0 V/W cycles (coarse_cycles), 1 K-cycle (full-operator hierarchy, FP64)
 };
 
 // A right preconditioner z = M v of gmres(): FP64 in and out, device vectors of n entries,
@@ -240,6 +241,9 @@ struct Multigrid : Preconditioner {
         DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
         DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
         std::vector<int> box_sector; // box sector of each slot
+        // K-cycle coarse solve (cycle_type 1): vectors of the next level's size, the dot
+        // products and the step coefficients
+        DeviceArray<double> kg, kv1, kw1, kv2, kw2, kr, ke, kdots, kcoef, kpartials;
     };
     MultigridOptions opt;
     double shift = 0.0;
@@ -263,12 +267,14 @@ struct Multigrid : Preconditioner {
   private:
     Multigrid(const Space &space, const Model &model, double shift, const MultigridOptions &opt,
               const std::vector<const Model *> *level_models);
+    // the K-cycle's coarse correction at depth d + 1 (two GCR steps); returns its device vector
+    double *kcycle_coarse(int d, cudaStream_t stream);
 
   public:
     ~Multigrid() override;
     // x = M b (FP64 in and out; FP32 inside when opt.precision == 1)
     void apply(const double *b, double *x, cudaStream_t stream) override;
-    [[nodiscard]] bool varies() const override { return opt.precision != 0; }
+    [[nodiscard]] bool varies() const override { return opt.precision != 0 || opt.cycle_type == 1; }
     // the same for nb <= opt.batch right-hand sides at once: column c of b at b + c * ldb,
     // of x at x + c * ldx; one cycle serves all columns
     void apply_batch(const double *b, std::int64_t ldb, double *x, std::int64_t ldx, int nb,

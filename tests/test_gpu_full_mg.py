@@ -7,7 +7,10 @@
   1e-10 relative residual, so within 1e-6 relative: ||A^-1||_1 <= 1/s for s I - Q),
   on the paper's 1-D linear birth-death model (birth 2 vol, death n, D = 1, s = 0.5, cap 2) and on
   a 2-D two-species annihilation box.
-- The red-black smoothers are refused (reactions couple states of one colour)."""
+- The K-cycle (two GCR steps per coarse visit, the paper driver's :851-878) reaches the same
+  solution in no more cycles than the W-cycle.
+- The red-black smoothers are refused (reactions couple states of one colour), and so is a
+  K-cycle outside the full-operator FP64 hierarchy."""
 
 import numpy as np
 import pytest
@@ -94,3 +97,33 @@ def test_red_black_smoothers_are_refused(cuda):
     with pytest.raises(_lib.MkError) as e:
         mk.full_multigrid(model, box, 0.5, mk.multigrid_options(smoother="gauss_seidel"))
     assert e.value.code == _lib.MK_EINVAL
+
+
+@pytest.mark.parametrize("cells", [64, 256])
+def test_k_cycle_reaches_the_solution(cuda, cells):
+    import torch
+
+    dom, model, box = _paper_model(cells)
+    shift = 0.5
+    b = _rhs(box.size(), 4)
+    Q, A, x_ref = _reference_solution(dom, model, box, shift, b)
+    bt = torch.as_tensor(b, device=cuda)
+    tol = 1e-10 * float(np.linalg.norm(b))
+    its = {}
+    for kind, opts in (("w", dict(coarse_cycles=2)), ("k", dict(cycle_type="k"))):
+        M = mk.full_multigrid(model, box, shift, mk.multigrid_options(**opts))
+        x = torch.zeros_like(bt)
+        r = M.stationary(Q, bt, x, tolerance=tol, max_cycles=1000)
+        assert r.converged, (kind, r)
+        assert np.max(np.abs(x.cpu().numpy() - x_ref)) <= 1e-6 * np.max(np.abs(x_ref))
+        its[kind] = r.iterations
+    assert its["k"] <= its["w"], its
+
+
+def test_k_cycle_needs_the_full_fp64_hierarchy(cuda):
+    dom, model, box = _paper_model(8)
+    with pytest.raises(_lib.MkError):
+        mk.full_multigrid(model, box, 0.5, mk.multigrid_options(cycle_type="k", precision="fp32"))
+    with pytest.raises(_lib.MkError):
+        mk.sector_multigrid(dom, box, 0.5, mk.multigrid_options(cycle_type="k"))
+
