@@ -14,6 +14,8 @@ Cases:
                              solved densely)
   fsp_toggle                 one batched Krylov-FSP launch of 8 toggle-switch instances of the
                              batching workload (after one warm-up launch)
+  ssa_toggle                 two batched-SSA launches of 65,536 Gillespie paths of the bench's
+                             toggle switch to t = 2 (the second is the one to capture)
 
 Each prints one JSON line with what it ran. Nothing here is timed: profilers time the kernels.
 """
@@ -98,6 +100,14 @@ def main(case: str) -> None:
         b.run()
         _, res = b.results()
         print(json.dumps({"case": case, "instances": len(probs), "applies": int(sum(r.applies for r in res))}))
+    elif case == "ssa_toggle":
+        from markovkit_b200.fsp_models import toggle
+        from markovkit_b200.ssa import simulate
+
+        model = toggle(30.0, 25.0, 2.0, 2.5)
+        for seed in (1, 2):
+            ens = simulate(model, [0, 0], 2.0, 65536, seed=seed, bounds=[64, 64])
+        print(json.dumps({"case": case, "paths": 65536, "launches": 2, "jumps": int(ens.steps.sum())}))
     else:
         raise SystemExit(f"unknown case {case!r}; see the module docstring")
 
