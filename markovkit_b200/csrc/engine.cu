@@ -451,8 +451,9 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
     if (opt.smoother == 3 && opt.batch != 1) {
         throw Error(kEInval, "the aggregate-block smoother serves one right-hand side at a time");
     }
-    if (full_ && opt.smoother != 0) {
-        throw Error(kEInval, "the full-operator multigrid smooths by weighted Jacobi (smoother 0)");
+    if (full_ && opt.smoother != 0 && opt.smoother != 1) {
+        throw Error(kEInval, "the full-operator multigrid smooths by weighted Jacobi (0) or "
+                             "multicolour Gauss-Seidel (1)");
     }
     if (opt.cycle_type != 0 && (opt.cycle_type != 1 || !full_ || opt.precision != 0 || opt.batch != 1)) {
         throw Error(kEInval, "the K-cycle belongs to the full-operator multigrid, in FP64, one "
@@ -558,6 +559,30 @@ Multigrid::Multigrid(const Space &space, const Model &model, double shift_,
             }
         }
         L->op.finalize(*grid_model, full_);
+        if (full_) {
+            // Gauss-Seidel colour classes of the sectors: a greedy colouring of the graph whose
+            // edges are the reactions between sectors, so that no in-jump of a class's rows
+            // starts in the same class; with the checkerboard colour inside a sector (every
+            // diffusion jump flips it) no pass reads what it writes
+            auto &secs = L->op.sectors;
+            for (std::size_t k = 0; k < secs.size(); ++k) {
+                std::vector<bool> used(secs.size() + 1, false);
+                for (int r = 0; r < grid_model->R; ++r) {
+                    for (int nb : {secs[k].src[r], secs[k].dst[r]}) {
+                        if (nb >= 0 && static_cast<std::size_t>(nb) < k) {
+                            used[static_cast<std::size_t>(secs[nb].gs_class)] = true;
+                        }
+                    }
+                }
+                int c = 0;
+                while (used[static_cast<std::size_t>(c)]) {
+                    ++c;
+                }
+                secs[k].gs_class = c;
+                L->n_classes = std::max(L->n_classes, c + 1);
+            }
+            L->op.d_sectors.upload(secs);
+        }
 
         // dense inverses of the terminal blocks, from the same matrix-free rows, all of a level
         // at once (on the device when they are large)
@@ -977,13 +1002,17 @@ T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
     } else if (opt.smoother == 1) {
         check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
         for (int k = 0; k < L.pre; ++k) {
-            for (int c = 0; c < 2; ++c) {
-                p.b = rhs;
-                p.y = x;
-                p.colour = c;
-                L.op.run<T>(kGaussSeidel, p, stream);
+            for (int q = 0; q < L.n_classes; ++q) {
+                for (int c = 0; c < 2; ++c) {
+                    p.b = rhs;
+                    p.y = x;
+                    p.colour = c;
+                    p.sector_class = full_ ? q : -1;
+                    L.op.run<T>(kGaussSeidel, p, stream);
+                }
             }
         }
+        p.sector_class = -1;
     } else if (opt.smoother == 2) {
         check_cuda(cudaMemsetAsync(x, 0, ndb * sizeof(T), stream), "memset");
         for (int k = 0; k < L.pre; ++k) {
@@ -1071,13 +1100,17 @@ T *Multigrid::cycle(int d, cudaStream_t stream, void *const *carve) {
         }
     } else if (opt.smoother == 1) {
         for (int k = 0; k < L.post; ++k) {
-            for (int c = 1; c >= 0; --c) {
-                p.b = rhs;
-                p.y = x;
-                p.colour = c;
-                L.op.run<T>(kGaussSeidel, p, stream);
+            for (int q = L.n_classes - 1; q >= 0; --q) {
+                for (int c = 1; c >= 0; --c) {
+                    p.b = rhs;
+                    p.y = x;
+                    p.colour = c;
+                    p.sector_class = full_ ? q : -1;
+                    L.op.run<T>(kGaussSeidel, p, stream);
+                }
             }
         }
+        p.sector_class = -1;
     } else if (opt.smoother == 2) {
         for (int k = 0; k < L.post; ++k) {
             ilu_sweep<T>(L, p, x, rhs, tmp, stream);

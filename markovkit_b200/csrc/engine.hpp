@@ -241,6 +241,7 @@ struct Multigrid : Preconditioner {
         DeviceArray<double> rhs64, x64, tmp64, r64, acc64, crhs64;
         DeviceArray<float> rhs32, x32, tmp32, r32, acc32, crhs32;
         std::vector<int> box_sector; // box sector of each slot
+        int n_classes = 1;           // full-operator Gauss-Seidel: sector colour classes
         // K-cycle coarse solve (cycle_type 1): vectors of the next level's size, the dot
         // products and the step coefficients
         DeviceArray<double> kg, kv1, kw1, kv2, kw2, kr, ke, kdots, kcoef, kpartials;
@@ -258,8 +259,9 @@ struct Multigrid : Preconditioner {
     // 819-850): every level is the whole box on a grid coarsened d times, with diffusivities
     // doubled per level and the reactions of level_models[d] (the caller tabulates the rates at
     // that level's voxel volume; level_models[0] is the fine model); the coarsest level, where
-    // the grid stops coarsening, is solved densely as one block. Weighted Jacobi smoothing only:
-    // reactions couple states of one checkerboard colour, so a red-black pass would race.
+    // the grid stops coarsening, is solved densely as one block. Weighted Jacobi smoothing, or
+    // Gauss-Seidel over (sector colour class x checkerboard colour) passes: reactions couple
+    // states of one checkerboard colour, so the sectors they couple get different classes.
     Multigrid(const Space &space, const std::vector<const Model *> &level_models, double shift,
               const MultigridOptions &opt);
     [[nodiscard]] bool full_operator() const { return full_; }

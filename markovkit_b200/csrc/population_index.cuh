@@ -321,7 +321,7 @@ struct SectorDesc {
     int heavy = 0;                    // some in-jump reaction can start at an empty voxel
     int coarse = -1;                  // slot of the same totals on the next multigrid level
     int terminal = -1;                // dense terminal block of this sector, -1 if none
-    int pad = 0;
+    int gs_class = 0;                 // full-operator Gauss-Seidel: the sector's colour class
 };
 
 // q = floor(a / b) for 0 <= a < 2^52, b >= 1, from a * (1/b) in double and one correction

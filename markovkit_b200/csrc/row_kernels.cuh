@@ -69,6 +69,8 @@ struct RowParams {
     std::int64_t ldv = 0;
     // batched requests of one problem with different shifts: column c uses col_shift[c], and
     // with piv_per_col its ILU(0) pivots sit at column c of piv (laid out like x)
+    // Gauss-Seidel of the full operator: only sectors of this colour class (-1: all)
+    int sector_class = -1;
     int per_col_shift = 0;
     int piv_per_col = 0;
     T col_shift[kRowBatch] = {};

@@ -234,6 +234,9 @@ __global__ void __launch_bounds__(kRowBlock) row_kernel(const __grid_constant__ 
     }
     __syncthreads();
     const SectorDesc &sec = s_sec;
+    if (p.sector_class >= 0 && sec.gs_class != p.sector_class) {
+        return; // another colour class's pass (the whole block)
+    }
     const int warp = static_cast<int>(threadIdx.x) >> 5;
     const int lane = static_cast<int>(threadIdx.x) & 31;
 

@@ -140,6 +140,9 @@ __global__ void __launch_bounds__(kRowBlock) stencil_kernel(const __grid_constan
     constexpr int NS = 1, TMAX = 4, RPT = kRowsPerThread<MODE>;
     __shared__ SectorDesc s_sec;
     const Tile tile = p.tiles[blockIdx.x];
+    if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
+        return; // another colour class's pass (the whole block)
+    }
     copy_to_shared(p.sectors + tile.sector, s_sec);
     __syncthreads();
     const SectorDesc &sec = s_sec;
@@ -221,6 +224,9 @@ __global__ void __launch_bounds__(kRowBlock) pair_kernel(const __grid_constant__
     constexpr int RPT = kRowsPerThread<MODE>;
     __shared__ StencilSector<T> s_ss;
     const Tile tile = p.tiles[blockIdx.x];
+    if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
+        return; // another colour class's pass (the whole block)
+    }
     copy_to_shared(p.sv.sectors + tile.sector, s_ss);
     __syncthreads();
     const StencilSector<T> &ss = s_ss;
@@ -268,6 +274,9 @@ __global__ void __launch_bounds__(kRowBlock) pair_heavy_kernel(const __grid_cons
     __shared__ StencilSector<T> s_ss;
     __shared__ T s_red[2 + NB][kRowBlock / 32];
     const Tile tile = p.tiles[blockIdx.x];
+    if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
+        return; // another colour class's pass (the whole block)
+    }
     copy_to_shared(p.sv.sectors + tile.sector, s_ss);
     __syncthreads();
     const StencilSector<T> &ss = s_ss;

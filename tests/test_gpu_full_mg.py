@@ -9,8 +9,10 @@
   a 2-D two-species annihilation box.
 - The K-cycle (two GCR steps per coarse visit, the paper driver's :851-878) reaches the same
   solution in no more cycles than the W-cycle.
-- The red-black smoothers are refused (reactions couple states of one colour), and so is a
-  K-cycle outside the full-operator FP64 hierarchy."""
+- Gauss-Seidel runs over (sector colour class x checkerboard colour) passes: reactions couple
+  states of one checkerboard colour, so the sectors they couple get different classes. It is
+  deterministic and needs fewer cycles than Jacobi. ILU(0) smoothing and a K-cycle outside the
+  full-operator FP64 hierarchy are refused."""
 
 import numpy as np
 import pytest
@@ -92,11 +94,37 @@ def test_preconditioner_reaches_the_solution(cuda, case):
     assert np.max(np.abs(x - x_ref)) <= 1e-6 * np.max(np.abs(x_ref))
 
 
-def test_red_black_smoothers_are_refused(cuda):
+def test_ilu_smoother_is_refused(cuda):
     dom, model, box = _paper_model(8)
     with pytest.raises(_lib.MkError) as e:
-        mk.full_multigrid(model, box, 0.5, mk.multigrid_options(smoother="gauss_seidel"))
+        mk.full_multigrid(model, box, 0.5, mk.multigrid_options(smoother="ilu0"))
     assert e.value.code == _lib.MK_EINVAL
+
+
+@pytest.mark.parametrize("case", ["paper_1d256", "annihilation_2d8"])
+def test_multicolour_gauss_seidel(cuda, case):
+    """Gauss-Seidel passes over (sector colour class x checkerboard colour): deterministic (two
+    runs agree bit for bit), the same solution, and fewer W-cycles than weighted Jacobi"""
+    import torch
+
+    dom, model, box = _paper_model(256) if case == "paper_1d256" else _annihilation(8)
+    shift = 0.5
+    b = _rhs(box.size(), 5)
+    Q, A, x_ref = _reference_solution(dom, model, box, shift, b)
+    bt = torch.as_tensor(b, device=cuda)
+    tol = 1e-10 * float(np.linalg.norm(b))
+    its, xs = {}, []
+    for sm in ("jacobi", "gauss_seidel", "gauss_seidel"):
+        M = mk.full_multigrid(model, box, shift, mk.multigrid_options(coarse_cycles=2, smoother=sm))
+        x = torch.zeros_like(bt)
+        r = M.stationary(Q, bt, x, tolerance=tol, max_cycles=1000)
+        assert r.converged, (sm, r)
+        assert np.max(np.abs(x.cpu().numpy() - x_ref)) <= 1e-6 * np.max(np.abs(x_ref))
+        its[sm] = r.iterations
+        if sm == "gauss_seidel":
+            xs.append(x.cpu().numpy())
+    assert np.array_equal(xs[0], xs[1])
+    assert its["gauss_seidel"] < its["jacobi"], its
 
 
 @pytest.mark.parametrize("cells", [64, 256])
