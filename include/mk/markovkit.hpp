@@ -39,6 +39,8 @@
 #include <span>
 #include <stdexcept>
 #include <string>
+#include <tuple>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -225,11 +227,38 @@ class population_sector : public population_space {
 
 // ---- models -------------------------------------------------------------------------------
 
-// grid<D>(dims, spacing): a structured voxel grid (the reference's structured_grid_graph)
+// a jump out of a state (chain.hpp:33-36)
+struct transition {
+    state to;
+    real rate;
+};
+
+// a model lists every jump out of a state with a positive rate (chain.hpp:38-42)
+template <typename Model>
+concept markov_model = requires(const Model &model, const state &x) {
+    { model.transitions(x) } -> std::convertible_to<array<transition>>;
+};
+
+// a finite state space numbers its states 0, ..., size() - 1 (chain.hpp:44-50)
+template <typename Space>
+concept state_space = requires(const Space &space, const state &x, idx i) {
+    { space.size() } -> std::convertible_to<idx>;
+    { space[i] } -> std::convertible_to<const state &>;
+    { space.find(x) } -> std::convertible_to<std::optional<idx>>;
+};
+
+// grid<D>(dims, spacing): a structured voxel grid (the reference's structured_grid_graph):
+// vertex numbering with axis 0 fastest, closed boundary, neighbours axis by axis with the lower
+// one first, edge weight = face area / h
 template <int D>
 struct grid {
+    struct edge {
+        idx to;
+        real weight;
+    };
     std::array<idx, D> dims;
     std::array<real, D> spacing;
+    explicit grid(std::array<idx, D> d) : dims(d) { spacing.fill(1.0); }
     grid(std::array<idx, D> d, std::array<real, D> h) : dims(d), spacing(h) {}
     [[nodiscard]] idx n_vertices() const {
         idx n = 1;
@@ -245,18 +274,80 @@ struct grid {
         }
         return v;
     }
+    [[nodiscard]] array<edge> neighbors(idx v) const {
+        array<edge> out;
+        idx stride = 1, rem = v;
+        for (int a = 0; a < D; ++a) {
+            const idx c = rem % dims[a];
+            rem /= dims[a];
+            real face = 1.0;
+            for (int b = 0; b < D; ++b) {
+                if (b != a) {
+                    face *= spacing[b];
+                }
+            }
+            const real w = face / spacing[a];
+            if (c > 0) {
+                out.push_back({v - stride, w});
+            }
+            if (c + 1 < dims[a]) {
+                out.push_back({v + stride, w});
+            }
+            stride *= dims[a];
+        }
+        return out;
+    }
 };
 
-template <int D>
+namespace num {
+
+// an explicit undirected weighted graph (the numerics library's graph<W, I>):
+// add_edge(a, b, w) adds a -> b and b -> a
+template <typename W = double, typename I = idx>
+class graph {
+  public:
+    struct edge {
+        I to;
+        W weight;
+    };
+    explicit graph(I n = 0) : adj_(n) {}
+    void add_edge(I a, I b, W weight) {
+        adj_.at(a).push_back({b, weight});
+        adj_.at(b).push_back({a, weight});
+    }
+    [[nodiscard]] I n_vertices() const { return static_cast<I>(adj_.size()); }
+    [[nodiscard]] const array<edge> &neighbors(I v) const { return adj_.at(v); }
+
+  private:
+    array<array<edge>> adj_;
+};
+
+} // namespace num
+
+// voxel_domain(graph, [volumes,] diffusivities) (reaction_diffusion.hpp:23-56): a grid's
+// volumes are its cell volume
+template <typename Graph>
 struct voxel_domain {
-    grid<D> graph;
+    Graph graph;
     vec<real> diffusivities;
     vec<real> volumes;
-    voxel_domain(grid<D> g, vec<real> diff)
+    voxel_domain(Graph g, vec<real> diff)
+        requires requires(const Graph &x) { x.cell_volume(); }
         : graph(std::move(g)), diffusivities(std::move(diff)),
           volumes(graph.n_vertices(), graph.cell_volume()) {}
-    [[nodiscard]] idx n_voxels() const { return graph.n_vertices(); }
+    voxel_domain(Graph g, vec<real> vols, vec<real> diff)
+        : graph(std::move(g)), diffusivities(std::move(diff)), volumes(std::move(vols)) {
+        if (volumes.size() != static_cast<idx>(graph.n_vertices())) {
+            throw std::invalid_argument("voxel_domain: one volume per voxel");
+        }
+    }
+    [[nodiscard]] idx n_voxels() const { return static_cast<idx>(graph.n_vertices()); }
     [[nodiscard]] idx n_species() const { return diffusivities.size(); }
+    // the rate at which one molecule of a species hops along an edge out of a voxel
+    template <typename Edge>
+    [[nodiscard]] real jump_rate(idx species, idx from, const Edge &edge) const {
+        return diffusivities[species] * static_cast<real>(edge.weight) / volumes[from];
+    }
 };
 
 // a reaction inside one voxel: change vector and rate(counts, volume)
@@ -265,33 +356,94 @@ struct local_reaction {
     std::function<real(view<const int>, real)> rate;
 };
 
-template <int D>
+template <typename Graph>
 struct reaction_diffusion {
-    voxel_domain<D> domain;
+    voxel_domain<Graph> domain;
     array<local_reaction> reactions;
     [[nodiscard]] idx n_voxels() const { return domain.n_voxels(); }
     [[nodiscard]] idx n_species() const { return domain.n_species(); }
     [[nodiscard]] idx index(idx voxel, idx species) const { return voxel * n_species() + species; }
+    // every jump out of x (reaction_diffusion.hpp:82-118): diffusion by voxel, edge and species,
+    // then local reactions by voxel; a host-side enumeration for callers (the device kernels
+    // visit the same jumps)
+    [[nodiscard]] array<transition> transitions(const state &x) const {
+        array<transition> result;
+        const idx S = n_species();
+        for (idx v = 0; v < n_voxels(); ++v) {
+            for (const auto &edge : domain.graph.neighbors(v)) {
+                for (idx s = 0; s < S; ++s) {
+                    const int n = x[index(v, s)];
+                    if (n == 0) {
+                        continue;
+                    }
+                    state y = x;
+                    --y[index(v, s)];
+                    ++y[index(static_cast<idx>(edge.to), s)];
+                    result.push_back({std::move(y), n * domain.jump_rate(s, v, edge)});
+                }
+            }
+        }
+        for (idx v = 0; v < n_voxels(); ++v) {
+            const view<const int> counts(x.data() + index(v, 0), S);
+            for (const local_reaction &r : reactions) {
+                const real rate = r.rate(counts, domain.volumes[v]);
+                if (!(rate > 0.0)) {
+                    continue;
+                }
+                state y = x;
+                bool valid = true;
+                for (idx s = 0; s < S; ++s) {
+                    y[index(v, s)] += r.change[s];
+                    valid = valid && y[index(v, s)] >= 0;
+                }
+                if (valid) {
+                    result.push_back({std::move(y), rate});
+                }
+            }
+        }
+        return result;
+    }
 };
 
 namespace detail {
 
-// the model handle of a reaction-diffusion model with its local rates tabulated over the
-// count tuples a space allows (n_s <= limits[s])
+template <typename G>
+struct is_grid : std::false_type {};
 template <int D>
-std::shared_ptr<mk_model_s> make_model(const reaction_diffusion<D> &m, const array<int> &limits) {
-    std::array<int64_t, 3> dims{1, 1, 1};
-    std::array<double, 3> spacing{1.0, 1.0, 1.0};
-    for (int a = 0; a < D; ++a) {
-        dims[a] = static_cast<int64_t>(m.domain.graph.dims[a]);
-        spacing[a] = m.domain.graph.spacing[a];
-    }
+struct is_grid<grid<D>> : std::true_type {};
+
+// the model handle of a reaction-diffusion model with its local rates tabulated over the
+// count tuples a space allows (n_s <= limits[s]), one table per distinct voxel volume
+template <typename Graph>
+std::shared_ptr<mk_model_s> make_model(const reaction_diffusion<Graph> &m, const array<int> &limits) {
+    const auto &dom = m.domain;
+    const int S = static_cast<int>(m.n_species());
     mk_model h = nullptr;
-    check(mk_model_create_grid(D, dims.data(), spacing.data(), static_cast<int>(m.n_species()),
-                               m.domain.diffusivities.data(), &h));
+    if constexpr (is_grid<Graph>::value) {
+        constexpr int D = static_cast<int>(std::tuple_size_v<decltype(dom.graph.dims)>);
+        std::array<int64_t, 3> dims{1, 1, 1};
+        std::array<double, 3> spacing{1.0, 1.0, 1.0};
+        for (int a = 0; a < D; ++a) {
+            dims[a] = static_cast<int64_t>(dom.graph.dims[a]);
+            spacing[a] = dom.graph.spacing[a];
+        }
+        check(mk_model_create_grid(D, dims.data(), spacing.data(), S, dom.diffusivities.data(), &h));
+    } else {
+        const idx V = dom.n_voxels();
+        std::vector<int64_t> ptr{0}, nbr;
+        std::vector<double> w;
+        for (idx v = 0; v < V; ++v) {
+            for (const auto &e : dom.graph.neighbors(static_cast<decltype(dom.graph.n_vertices())>(v))) {
+                nbr.push_back(static_cast<int64_t>(e.to));
+                w.push_back(static_cast<double>(e.weight));
+            }
+            ptr.push_back(static_cast<int64_t>(nbr.size()));
+        }
+        check(mk_model_create_graph(static_cast<int64_t>(V), ptr.data(), nbr.data(), w.data(),
+                                    dom.volumes.data(), S, dom.diffusivities.data(), &h));
+    }
     std::shared_ptr<mk_model_s> model(h, [](mk_model p) { mk_model_destroy(p); });
     if (!m.reactions.empty()) {
-        const int S = static_cast<int>(m.n_species());
         if (static_cast<int>(limits.size()) != S) {
             throw std::invalid_argument("the space and the model have different species counts");
         }
@@ -299,27 +451,40 @@ std::shared_ptr<mk_model_s> make_model(const reaction_diffusion<D> &m, const arr
         for (int t : limits) {
             ntuple *= t + 1;
         }
+        // volume classes: the distinct voxel volumes, in order of first appearance
+        std::vector<double> classes;
+        std::vector<int> vclass(dom.n_voxels());
+        for (idx v = 0; v < dom.n_voxels(); ++v) {
+            const auto it = std::find(classes.begin(), classes.end(), dom.volumes[v]);
+            vclass[v] = static_cast<int>(it - classes.begin());
+            if (it == classes.end()) {
+                classes.push_back(dom.volumes[v]);
+            }
+        }
         const int R = static_cast<int>(m.reactions.size());
+        const int C = static_cast<int>(classes.size());
         std::vector<int> change;
-        std::vector<double> rates(static_cast<std::size_t>(R) * ntuple);
-        const real vol = m.domain.graph.cell_volume();
+        std::vector<double> rates(static_cast<std::size_t>(R) * C * ntuple);
         std::vector<int> counts(S);
         for (int r = 0; r < R; ++r) {
             if (static_cast<int>(m.reactions[r].change.size()) != S) {
                 throw std::invalid_argument("change vector length differs from the species count");
             }
             change.insert(change.end(), m.reactions[r].change.begin(), m.reactions[r].change.end());
-            for (int t = 0; t < ntuple; ++t) {
-                int rem = t;
-                for (int s = S - 1; s >= 0; --s) {
-                    counts[s] = rem % (limits[s] + 1);
-                    rem /= limits[s] + 1;
+            for (int c = 0; c < C; ++c) {
+                for (int t = 0; t < ntuple; ++t) {
+                    int rem = t;
+                    for (int s = S - 1; s >= 0; --s) {
+                        counts[s] = rem % (limits[s] + 1);
+                        rem /= limits[s] + 1;
+                    }
+                    rates[(static_cast<std::size_t>(r) * C + c) * ntuple + t] =
+                        m.reactions[r].rate(view<const int>(counts.data(), counts.size()), classes[c]);
                 }
-                rates[static_cast<std::size_t>(r) * ntuple + t] =
-                    m.reactions[r].rate(view<const int>(counts.data(), counts.size()), vol);
             }
         }
-        check(mk_model_set_reactions(h, R, change.data(), limits.data(), 1, nullptr, rates.data()));
+        check(mk_model_set_reactions(h, R, change.data(), limits.data(), C, C > 1 ? vclass.data() : nullptr,
+                                     rates.data()));
     }
     return model;
 }
@@ -390,8 +555,8 @@ class generator {
     using domain_type = vec<real>;
     using codomain_type = vec<real>;
 
-    template <int D>
-    generator(const population_space &space, const reaction_diffusion<D> &model,
+    template <typename Graph>
+    generator(const population_space &space, const reaction_diffusion<Graph> &model,
               boundary leaks = boundary::absorbing) {
         model_ = detail::make_model(model, space.limits());
         mk_generator h = nullptr;
@@ -496,6 +661,14 @@ class shifted_generator {
 
 // ---- multigrid ----------------------------------------------------------------------------
 
+// multigrid.hpp:120-123, with this library's two other smoothers after the reference's two
+enum class relaxation : std::uint8_t {
+    jacobi,          // weighted point Jacobi
+    aggregate_block, // exact solves on states that differ only inside one coarse voxel
+    gauss_seidel,    // red-black Gauss-Seidel
+    ilu0             // red-black ILU(0)
+};
+
 struct multigrid_options {
     int pre_sweeps = 2;
     int post_sweeps = 2;
@@ -504,28 +677,49 @@ struct multigrid_options {
     int max_levels = 32;
     int coarse_cycles = 1;
     int sweep_growth = 0;
-    int smoother = 0;  // 0 weighted Jacobi (the reference's), 1 red-black Gauss-Seidel
+    relaxation smoother = relaxation::jacobi;
     int precision = 0; // 0 FP64, 1 FP32 (use with flexible GMRES)
 };
 
-// The reference's sector_multigrid<Graph> (markovkit/rdme/multigrid.hpp:364-408), over a
-// grid<D> domain; CTAD takes D from the domain. Copies share one device hierarchy.
+namespace detail {
+
+inline mk_multigrid_options to_c(const multigrid_options &o) {
+    mk_multigrid_options c{};
+    mk_multigrid_options_default(&c);
+    c.pre_sweeps = o.pre_sweeps;
+    c.post_sweeps = o.post_sweeps;
+    c.jacobi_weight = o.jacobi_weight;
+    c.coarsest_size = static_cast<int64_t>(o.coarsest_size);
+    c.max_levels = o.max_levels;
+    c.coarse_cycles = o.coarse_cycles;
+    c.sweep_growth = o.sweep_growth;
+    static constexpr int kSmoother[] = {0, 3, 1, 2}; // the C ABI's numbering
+    c.smoother = kSmoother[static_cast<int>(o.smoother)];
+    c.precision = o.precision;
+    return c;
+}
+
+} // namespace detail
+
+// The reference's sector_multigrid<D> (markovkit/rdme/multigrid.hpp:364-408), over a grid<D>
+// domain; CTAD takes D from the domain. Copies share one device hierarchy.
 template <int D>
 class sector_multigrid {
   public:
     using domain_type = vec<real>;
     using codomain_type = vec<real>;
 
-    sector_multigrid(const voxel_domain<D> &domain, const population_box &box, real shift,
+    sector_multigrid(const voxel_domain<grid<D>> &domain, const population_box &box, real shift,
                      const multigrid_options &options = {}) {
-        init(reaction_diffusion<D>{domain, {}}, box, shift, options);
+        init(reaction_diffusion<grid<D>>{domain, {}}, box, shift, options);
     }
-    sector_multigrid(const voxel_domain<D> &domain, const population_sector &sector, real shift,
+    sector_multigrid(const voxel_domain<grid<D>> &domain, const population_sector &sector, real shift,
                      const multigrid_options &options = {}) {
-        init(reaction_diffusion<D>{domain, {}}, sector, shift, options);
+        init(reaction_diffusion<grid<D>>{domain, {}}, sector, shift, options);
     }
     [[nodiscard]] idx rows() const { return n_; }
     [[nodiscard]] idx cols() const { return n_; }
+    [[nodiscard]] idx n_sectors() const { return sectors_; }
     [[nodiscard]] std::size_t max_levels() const {
         int l = 0;
         detail::check(mk_multigrid_max_levels(h_.get(), &l));
@@ -541,34 +735,169 @@ class sector_multigrid {
     [[nodiscard]] mk_multigrid handle() const { return h_.get(); }
     [[nodiscard]] bool fp32() const { return fp32_; }
 
-  private:
-    void init(const reaction_diffusion<D> &m, const population_space &space, real shift,
+  protected:
+    sector_multigrid() = default;
+    void init(const reaction_diffusion<grid<D>> &m, const population_space &space, real shift,
               const multigrid_options &o) {
         auto model = detail::make_model(m, space.limits());
-        mk_multigrid_options c{};
-        mk_multigrid_options_default(&c);
-        c.pre_sweeps = o.pre_sweeps;
-        c.post_sweeps = o.post_sweeps;
-        c.jacobi_weight = o.jacobi_weight;
-        c.coarsest_size = static_cast<int64_t>(o.coarsest_size);
-        c.max_levels = o.max_levels;
-        c.coarse_cycles = o.coarse_cycles;
-        c.sweep_growth = o.sweep_growth;
-        c.smoother = o.smoother;
-        c.precision = o.precision;
+        const mk_multigrid_options c = detail::to_c(o);
         mk_multigrid h = nullptr;
         detail::check(mk_multigrid_create(space.handle(), model.get(), shift, &c, &h));
         h_.reset(h, [](mk_multigrid p) { mk_multigrid_destroy(p); });
         n_ = space.size();
+        sectors_ = space.n_sectors();
         fp32_ = o.precision == 1;
         b_ = std::make_shared<detail::device_vector>(n_);
         x_ = std::make_shared<detail::device_vector>(n_);
     }
     std::shared_ptr<mk_multigrid_s> h_;
     std::shared_ptr<detail::device_vector> b_, x_;
-    idx n_ = 0;
+    idx n_ = 0, sectors_ = 0;
     bool fp32_ = false;
 };
+
+// one depth of a population_multigrid hierarchy: y = A_d x
+class population_multigrid_level {
+  public:
+    population_multigrid_level(std::shared_ptr<mk_multigrid_s> h, int depth, idx n)
+        : h_(std::move(h)), depth_(depth), n_(n), x_(std::make_shared<detail::device_vector>(n)),
+          y_(std::make_shared<detail::device_vector>(n)) {}
+    [[nodiscard]] idx rows() const { return n_; }
+    [[nodiscard]] idx cols() const { return n_; }
+    void apply_system(view<const real> x, view<real> y) const {
+        x_->upload(x.data());
+        detail::check(mk_multigrid_apply_system(h_.get(), depth_, x_->get(), y_->get(), nullptr));
+        y_->download(y.data());
+    }
+
+  private:
+    std::shared_ptr<mk_multigrid_s> h_;
+    int depth_ = 0;
+    idx n_ = 0;
+    std::shared_ptr<detail::device_vector> x_, y_;
+};
+
+// population_transfer between depth d and d + 1 (multigrid.hpp:48-111)
+class population_transfer_view {
+  public:
+    population_transfer_view(std::shared_ptr<mk_multigrid_s> h, int depth, idx fine, idx coarse)
+        : h_(std::move(h)), depth_(depth), fine_(fine), coarse_(coarse),
+          f_(std::make_shared<detail::device_vector>(fine)),
+          c_(std::make_shared<detail::device_vector>(coarse)) {}
+    [[nodiscard]] idx fine_size() const { return fine_; }
+    [[nodiscard]] idx coarse_size() const { return coarse_; }
+    // coarse[c(i)] += fine[i], in a fixed order
+    void restrict(view<const real> fine, view<real> coarse) const {
+        f_->upload(fine.data());
+        detail::check(mk_multigrid_restrict(h_.get(), depth_, f_->get(), c_->get(), nullptr));
+        c_->download(coarse.data());
+    }
+    // fine[i] = w_i coarse[c(i)]
+    void prolong(view<const real> coarse, view<real> fine) const {
+        c_->upload(coarse.data());
+        detail::check(mk_multigrid_prolong(h_.get(), depth_, c_->get(), f_->get(), nullptr));
+        f_->download(fine.data());
+    }
+
+  private:
+    std::shared_ptr<mk_multigrid_s> h_;
+    int depth_ = 0;
+    idx fine_ = 0, coarse_ = 0;
+    std::shared_ptr<detail::device_vector> f_, c_;
+};
+
+// The reference's population_multigrid<D> (multigrid.hpp:136-361): the multigrid of one
+// population sector of a diffusion-only grid model, as its own object with its levels and
+// transfers exposed (the device hierarchy is the sector multigrid's, on that one sector)
+template <int D>
+class population_multigrid : public sector_multigrid<D> {
+  public:
+    population_multigrid(const voxel_domain<grid<D>> &domain, const array<int> &totals, real shift,
+                         multigrid_options options = {})
+        : domain_(domain), totals_(totals), shift_(shift) {
+        const population_sector space(domain.n_voxels(), totals);
+        this->init(reaction_diffusion<grid<D>>{domain, {}}, space, shift, options);
+        int depth = 0;
+        detail::check(mk_multigrid_depth(this->h_.get(), &depth));
+        for (int d = 0; d < depth; ++d) {
+            int64_t n = 0;
+            detail::check(mk_multigrid_level_size(this->h_.get(), d, &n));
+            sizes_.push_back(static_cast<idx>(n));
+        }
+        for (int d = 0; d < depth; ++d) {
+            levels_.push_back(std::make_shared<population_multigrid_level>(this->h_, d, sizes_[d]));
+            if (d + 1 < depth) {
+                transfers_.push_back(std::make_shared<population_transfer_view>(this->h_, d, sizes_[d],
+                                                                                sizes_[d + 1]));
+            }
+        }
+    }
+    [[nodiscard]] real shift() const { return shift_; }
+    [[nodiscard]] idx n_levels() const { return sizes_.size(); }
+    // y = (shift I - Q) x on this level's sector
+    void apply_system(view<const real> x, view<real> y) const { levels_.front()->apply_system(x, y); }
+    [[nodiscard]] const population_transfer_view &transfer() const {
+        if (transfers_.empty()) {
+            throw std::logic_error("population_multigrid: a single level has no transfer");
+        }
+        return *transfers_.front();
+    }
+    [[nodiscard]] const population_multigrid_level *coarse_level() const {
+        return levels_.size() > 1 ? levels_[1].get() : nullptr;
+    }
+    // states of every level over those of the finest
+    [[nodiscard]] real grid_complexity() const {
+        real total = 0.0;
+        for (idx n : sizes_) {
+            total += static_cast<real>(n);
+        }
+        return total / static_cast<real>(sizes_.front());
+    }
+    // entries (states plus jumps) of every level's operator over those of the finest; each
+    // level's jumps are counted on its own diffusion-only generator
+    [[nodiscard]] real operator_complexity() const {
+        real total = 0.0, fine = 0.0;
+        std::array<idx, D> dims = domain_.graph.dims;
+        std::array<real, D> spacing = domain_.graph.spacing;
+        for (idx d = 0; d < sizes_.size(); ++d) {
+            const voxel_domain<grid<D>> dom(grid<D>(dims, spacing), domain_.diffusivities);
+            const population_sector space(dom.n_voxels(), totals_);
+            const reaction_diffusion<grid<D>> model{dom, {}};
+            auto h = detail::make_model(model, space.limits());
+            mk_generator g = nullptr;
+            detail::check(mk_generator_create(space.handle(), h.get(), 1, &g));
+            std::unique_ptr<mk_generator_s, void (*)(mk_generator)> hold(g, mk_generator_destroy);
+            int64_t jumps = 0;
+            detail::check(mk_generator_n_jumps(g, &jumps, nullptr));
+            const real entries = static_cast<real>(space.size()) + static_cast<real>(jumps);
+            total += entries;
+            if (d == 0) {
+                fine = entries;
+            }
+            for (int a = 0; a < D; ++a) {
+                if (dims[a] > 1) {
+                    dims[a] /= 2;
+                    spacing[a] *= 2.0;
+                }
+            }
+        }
+        return total / fine;
+    }
+
+  private:
+    voxel_domain<grid<D>> domain_;
+    array<int> totals_;
+    real shift_ = 0.0;
+    array<idx> sizes_;
+    array<std::shared_ptr<population_multigrid_level>> levels_;
+    array<std::shared_ptr<population_transfer_view>> transfers_;
+};
+
+template <int D>
+population_multigrid(const voxel_domain<grid<D>> &, const array<int> &, real) -> population_multigrid<D>;
+template <int D>
+population_multigrid(const voxel_domain<grid<D>> &, const array<int> &, real, multigrid_options)
+    -> population_multigrid<D>;
 
 // ---- preconditioners and GMRES -------------------------------------------------------------
 
@@ -752,12 +1081,6 @@ solver_result gmres(const shifted_generator &A, const M &pre, const vec<real> &b
 struct reaction {
     state change;
     std::function<real(const state &)> rate;
-};
-
-// a jump out of a state (chain.hpp:33-36)
-struct transition {
-    state to;
-    real rate;
 };
 
 struct reaction_network {
@@ -1238,6 +1561,63 @@ trajectory tau_leaping(const reaction_network &model, state x, real final_time, 
                        leap_options options = {}) {
     return detail::single_path(model, x, final_time, detail::seed_from(random), 1,
                                std::numeric_limits<std::int64_t>::max(), options);
+}
+
+namespace detail {
+
+// an RDME model as a reaction network over its voxel-major counts: one reaction per (voxel, edge,
+// species) hop at n * jump_rate and one per (voxel, local reaction), in the order of
+// reaction_diffusion::transitions; the device paths hold at most four counts
+template <typename Graph>
+reaction_network as_network(const reaction_diffusion<Graph> &m) {
+    const idx V = m.n_voxels(), S = m.n_species(), N = V * S;
+    if (N > 4) {
+        throw std::invalid_argument("ssa: the device paths hold at most four counts; this model has " +
+                                    std::to_string(N) + " (voxels x species)");
+    }
+    reaction_network net;
+    for (idx v = 0; v < V; ++v) {
+        for (const auto &edge : m.domain.graph.neighbors(v)) {
+            for (idx s = 0; s < S; ++s) {
+                state change(N, 0);
+                const idx from = v * S + s, to = static_cast<idx>(edge.to) * S + s;
+                --change[from];
+                ++change[to];
+                const real hop = m.domain.jump_rate(s, v, edge);
+                net.reactions.push_back({change, [from, hop](const state &x) { return x[from] * hop; }});
+            }
+        }
+    }
+    for (idx v = 0; v < V; ++v) {
+        for (const local_reaction &r : m.reactions) {
+            state change(N, 0);
+            for (idx s = 0; s < S; ++s) {
+                change[v * S + s] = r.change[s];
+            }
+            const real volume = m.domain.volumes[v];
+            const auto rate = r.rate;
+            net.reactions.push_back({change, [v, S, volume, rate](const state &x) {
+                                         return rate(view<const int>(x.data() + v * S, S), volume);
+                                     }});
+        }
+    }
+    return net;
+}
+
+} // namespace detail
+
+// Gillespie's direct method on an RDME model (ssa.hpp:42-74 over reaction_diffusion, a
+// markov_model): the device paths of its reaction-network form
+template <typename Graph, std::uniform_random_bit_generator Rng>
+trajectory gillespie(const reaction_diffusion<Graph> &model, state x, real final_time, Rng &random,
+                     idx max_jumps = std::numeric_limits<idx>::max()) {
+    return gillespie(detail::as_network(model), std::move(x), final_time, random, max_jumps);
+}
+
+template <typename Graph, std::uniform_random_bit_generator Rng>
+trajectory tau_leaping(const reaction_diffusion<Graph> &model, state x, real final_time, Rng &random,
+                       leap_options options = {}) {
+    return tau_leaping(detail::as_network(model), std::move(x), final_time, random, options);
 }
 
 } // namespace markovkit

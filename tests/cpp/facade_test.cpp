@@ -46,7 +46,7 @@ void spaces() {
 }
 
 void resolvent() {
-    const reaction_diffusion<1> model{voxel_domain<1>(grid<1>({16}, {1.0 / 16}), {1.0}),
+    const reaction_diffusion<grid<1>> model{voxel_domain(grid<1>({16}, {1.0 / 16}), {1.0}),
                                       birth_death(0.05, 0.02)};
     population_box box(16, {3});
     const generator Q(box, model, boundary::absorbing);
@@ -183,8 +183,8 @@ void preconditioners() {
 
 void annihilation_transform() {
     // A + B -> nothing at rate 2 a b / V; E[exp(-sT)] + s S_hat(s) = 1 for the annihilation time
-    const reaction_diffusion<1> model{
-        voxel_domain<1>(grid<1>({4}, {0.25}), {1.0, 1.0}),
+    const reaction_diffusion<grid<1>> model{
+        voxel_domain(grid<1>({4}, {0.25}), {1.0, 1.0}),
         {{{-1, -1}, [](view<const int> n, real volume) { return 2.0 * n[0] * n[1] / volume; }}}};
     population_box box(4, {1, 1});
     const generator Q(box, model);

@@ -4,8 +4,8 @@ compiles against it with g++ and links the in-tree library (CPU), and runs corre
 compares plain, Jacobi, ILU(0) and multigrid-preconditioned GMRES) compiles unchanged against
 the facade with -I include/mk where the reference tree is at hand (MK_REFERENCE_ROOT, else a
 `reference` folder beside the repository); the binary lands in tests/cpp/_build and runs on a
-B200 with --quick. The reference's own tests/test_ssa.cpp builds the same way and passes on the
-device SSA."""
+B200 with --quick. The reference's own tests/test_ssa.cpp and tests/test_rdme.cpp build the same
+way and pass on the B200."""
 
 import os
 import subprocess
@@ -34,9 +34,13 @@ def _build() -> Path:
 REF = Path(os.environ.get("MK_REFERENCE_ROOT", ROOT.parent / "reference"))
 REF_BENCH = REF / "examples" / "rdme_multigrid_benchmark.cpp"
 REF_BENCH_OUT = ROOT / "tests" / "cpp" / "_build" / "rdme_multigrid_benchmark"
-# the reference's own SSA test (gillespie, tau_leaping, trajectory, reaction_network::transitions)
+# the reference's own tests: SSA (gillespie, tau_leaping, trajectory, transitions) and RDME
+# (voxel domains over grids and explicit graphs, population spaces, generator, population and
+# sector multigrid with transfers, resolvent solves, the annihilation transform)
 REF_SSA = REF / "tests" / "test_ssa.cpp"
 REF_SSA_OUT = ROOT / "tests" / "cpp" / "_build" / "reference_test_ssa"
+REF_RDME = REF / "tests" / "test_rdme.cpp"
+REF_RDME_OUT = ROOT / "tests" / "cpp" / "_build" / "reference_test_rdme"
 
 
 def test_facade_program_compiles_and_links():
@@ -54,23 +58,25 @@ def test_reference_benchmark_compiles_against_facade():
     assert REF_BENCH_OUT.exists()
 
 
-def test_reference_ssa_test_compiles_against_facade():
-    if not REF_SSA.exists():
+@pytest.mark.parametrize("src,out", [(REF_SSA, REF_SSA_OUT), (REF_RDME, REF_RDME_OUT)], ids=["ssa", "rdme"])
+def test_reference_test_compiles_against_facade(src, out):
+    if not src.exists():
         pytest.skip("the reference tree is not here")
     _build()
-    cmd = ["g++", "-std=c++20", "-O2", f"-I{ROOT / 'include' / 'mk'}", f"-I{REF / 'tests'}", str(REF_SSA),
-           f"-L{LIBDIR}", "-lmarkovkit_b200", f"-Wl,-rpath,{LIBDIR}", "-o", str(REF_SSA_OUT)]
+    cmd = ["g++", "-std=c++20", "-O2", f"-I{ROOT / 'include' / 'mk'}", f"-I{REF / 'tests'}", str(src),
+           f"-L{LIBDIR}", "-lmarkovkit_b200", f"-Wl,-rpath,{LIBDIR}", "-o", str(out)]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     assert proc.returncode == 0, proc.stderr[-4000:]
 
 
 @pytest.mark.gpu
-def test_reference_ssa_test_runs(cuda):
-    """the reference's tests/test_ssa.cpp, unchanged, on the device SSA: every check passes
-    (its exit status counts the failed checks)"""
-    if not REF_SSA_OUT.exists():
-        pytest.skip("the reference SSA test was not built against the facade")
-    proc = subprocess.run([str(REF_SSA_OUT)], capture_output=True, text=True, timeout=600,
+@pytest.mark.parametrize("out", [REF_SSA_OUT, REF_RDME_OUT], ids=["ssa", "rdme"])
+def test_reference_test_runs(cuda, out):
+    """the reference's tests/test_ssa.cpp and tests/test_rdme.cpp, unchanged, on the device:
+    every check passes (their exit status counts the failed checks)"""
+    if not out.exists():
+        pytest.skip("the reference test was not built against the facade")
+    proc = subprocess.run([str(out)], capture_output=True, text=True, timeout=600,
                           env={**os.environ, "LD_LIBRARY_PATH": str(LIBDIR)})
     assert proc.returncode == 0, proc.stdout + proc.stderr
 
