@@ -75,7 +75,10 @@ REL_TOL = 1e-10
 RESTART = 30
 FP32_SMOOTHER = "gauss_seidel"
 MIX_SMOOTHER = "auto"  # the serving mix: the server picks the smoother per problem
-FP32_COARSEST = 256
+MIX_COARSEST = 256     # the serving mix: dense solves of small sectors only (its 1-D boxes and
+                       # configuration 1 have many sectors near 4096 states on coarse levels)
+FP32_COARSEST = 4096
+FP32_SWEEPS = (2, 1)  # pre- and post-smoothing sweeps of the FP32 path
 L2_FLUSH_BYTES = 256 << 20
 METRIC = "resolvent solves/sec at 1e-10 relative true residual (FP32-MG / FP64-FGMRES)"
 
@@ -332,7 +335,8 @@ def run_ours(args) -> dict | None:
         "config": {
             "workload": w["workload"], "states": N, "voxels": box.n_voxels(), "shift": w["shift"],
             "gmres_restart": RESTART, "tolerance": "1e-10 relative true residual",
-            "fp32_multigrid": f"smoother {FP32_SMOOTHER}, dense solve of sectors <= {FP32_COARSEST} states",
+            "fp32_multigrid": f"smoother {FP32_SMOOTHER} {FP32_SWEEPS[0]}/{FP32_SWEEPS[1]}, dense solve of "
+                              f"sectors <= {FP32_COARSEST} states",
             "parallelism": f"replicas x{world}",
             "l2": f"inputs of {N * 8 / 1e6:.0f} MB per vector and L2 flushed between steps (256 MiB write)",
         },
@@ -391,7 +395,8 @@ PATHS = {"fp32": ("fp32", FP32_SMOOTHER, FP32_COARSEST), "fp64": ("fp64", "jacob
 
 
 def make_solver(mk, A, dom, box, shift, precision, smoother, coarsest, bnorm0):
-    mo = mk.multigrid_options(precision=precision, smoother=smoother, coarsest_size=coarsest)
+    sweeps = dict(pre_sweeps=FP32_SWEEPS[0], post_sweeps=FP32_SWEEPS[1]) if precision == "fp32" else {}
+    mo = mk.multigrid_options(precision=precision, smoother=smoother, coarsest_size=coarsest, **sweeps)
     M = mk.sector_multigrid(dom, box, shift, mo)
     opts = mk.gmres_options(tolerance=REL_TOL * bnorm0, max_iterations=2000, restart=RESTART,
                             flexible=(precision == "fp32"))
@@ -524,7 +529,7 @@ def serve_mix_measure(mk) -> dict:
     sizes = {k: problems[k][0].size() for k in keys}
     bs = [rhs_of({"rhs": "dirichlet"}, r["rhs_seed"], sizes[(r["model"], r["voxels"], r["cap"])]) for r in reqs]
     out = {}
-    kw = dict(precision="fp32", slots=SERVE_SLOTS, batch=4, coarsest_size=FP32_COARSEST, restart=RESTART,
+    kw = dict(precision="fp32", slots=SERVE_SLOTS, batch=4, coarsest_size=MIX_COARSEST, restart=RESTART,
               smoother=MIX_SMOOTHER)
     with server(rel_tolerance=REL_TOL, **kw) as srv:
         pids = {k: srv.register(*problems[k]) for k in keys}
@@ -587,7 +592,7 @@ def serve_mix_measure(mk) -> dict:
     out["largest_states"] = max(sizes.values())
     out["note"] = (f"Poisson arrivals at {MIX_RATE}/s, seed 4; fp32: {SERVE_SLOTS} slots, batch 4 (same problem and shift), "
                    f"FGMRES({RESTART}), smoother {MIX_SMOOTHER} (Gauss-Seidel for one species of at most two "
-                   f"molecules per state, Jacobi otherwise), dense solve of sectors <= {FP32_COARSEST} "
+                   f"molecules per state, Jacobi otherwise), dense solve of sectors <= {MIX_COARSEST} "
                    "states; plain fp64: one request at a time, GMRES(30), the reference's multigrid options, "
                    "generator and multigrid set-up inside each latency; 1-D boxes use configuration 0's "
                    "voxel size 1/16")
