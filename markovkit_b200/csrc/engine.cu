@@ -1556,6 +1556,7 @@ Krylov::Krylov(std::int64_t n_, int m_, bool flexible_) : n(n_), m(m_), flexible
     w.resize(ld);
     r.resize(ld);
     t.resize(ld);
+    skip.resize(1);
     partials.resize(static_cast<std::size_t>(kDotBlocks) * kMaxFusedBasis);
     const std::size_t H = static_cast<std::size_t>(m + 1) * m;
     small.resize(H + 6 * (m + 1) + 16);
@@ -1724,9 +1725,16 @@ SolverResult gmres(const Generator &A, double shift, Preconditioner *M, const do
             }
             A.apply<double>(kApplyShifted, shift, z, nullptr, ws.w.get(), nullptr, stream);
             const int K = j + 1;
-            gs_dots(ws, K, ws.w.get(), ws.st.h1, stream);
-            gs_update(ws, 1, K, ws.w.get(), ws.st.h1, ws.st.h2, stream);
-            gs_update(ws, 2, K, ws.w.get(), ws.st.h2, ws.st.hn, stream);
+            if (K < kMaxFusedBasis) {
+                // the second (re-orthogonalisation) pass only where the first lost too much
+                check_cuda(cgs_dgks(ws.V.get(), ws.ld, K, ws.w.get(), ws.n, ws.partials.get(),
+                                    ws.st.h1, ws.st.h2, ws.st.hn, ws.skip.get(), stream),
+                           "cgs");
+            } else {
+                gs_dots(ws, K, ws.w.get(), ws.st.h1, stream);
+                gs_update(ws, 1, K, ws.w.get(), ws.st.h1, ws.st.h2, stream);
+                gs_update(ws, 2, K, ws.w.get(), ws.st.h2, ws.st.hn, stream);
+            }
             check_cuda(arnoldi_column(ws.st, j, stream), "arnoldi");
             double *slot = ws.report_host + 4 * (1 + (j & 1));
             check_cuda(cudaMemcpyAsync(slot, ws.st.report, 4 * sizeof(double),

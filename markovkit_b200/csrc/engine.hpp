@@ -347,6 +347,7 @@ struct Krylov {
     int m = 0;
     bool flexible = false;
     DeviceArray<double> V, Z, w, r, t, partials, small;
+    DeviceArray<int> skip; // the selective re-orthogonalisation's decision
     ArnoldiState st;
     double *report_host = nullptr; // pinned, 3 slots of 4
     cudaEvent_t step_done[2] = {nullptr, nullptr};

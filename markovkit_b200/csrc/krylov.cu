@@ -45,7 +45,11 @@ __device__ __forceinline__ void block_partials(double (&acc)[KMAX], int K, doubl
 // once; left unbounded, KMAX 16 takes 145 registers and one block per SM.
 template <int KMAX, int MODE>
 constexpr int cgs_min_blocks() {
-    if constexpr (MODE == 1) {
+    if constexpr (MODE == 4) {
+        return cgs_min_blocks<KMAX, 0>();
+    } else if constexpr (MODE == 5) {
+        return cgs_min_blocks<KMAX, 1>();
+    } else if constexpr (MODE == 1) {
         return KMAX >= 32 ? 1 : (KMAX >= 16 ? 2 : (KMAX >= 8 ? 3 : 4));
     } else if constexpr (MODE == 2) {
         return KMAX >= 16 ? 2 : 4;
@@ -54,7 +58,9 @@ constexpr int cgs_min_blocks() {
     }
 }
 
-// mode 0: dots; mode 1: update then dots; mode 2: update then norm^2; mode 3: update only.
+// mode 0: dots; mode 1: update then dots; mode 2: update then norm^2; mode 3: update only;
+// modes 4 and 5: modes 0 and 1 with <w, w> after the K dots (entry K). A block returns at once
+// when skip is set (the selective re-orthogonalisation's second pass, not needed).
 // Each element's K basis values are loaded first (all in flight at once), then used. The update
 // coefficients sit in shared memory (a broadcast read per use), which leaves the registers to
 // the loaded values and the accumulators.
@@ -65,10 +71,13 @@ __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
     cgs_kernel(const double *__restrict__ V, std::int64_t ld, int K, double *__restrict__ w,
                std::int64_t n, const double *__restrict__ coef, double *__restrict__ partials,
                std::int64_t col, std::int64_t coef_stride, std::int64_t part_stride,
-               unsigned mask) {
-    if (!((mask >> blockIdx.y) & 1U)) {
+               unsigned mask, const int *skip = nullptr) {
+    if (!((mask >> blockIdx.y) & 1U) || (skip && *skip)) {
         return;
     }
+    constexpr bool kNorm = MODE == 4 || MODE == 5;
+    constexpr bool kDots = MODE == 0 || MODE == 1 || kNorm;
+    constexpr bool kUpdate = MODE == 1 || MODE == 2 || MODE == 3 || MODE == 5;
     V += col * blockIdx.y;
     w += col * blockIdx.y;
     if (coef) {
@@ -76,15 +85,15 @@ __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
     }
     partials += part_stride * blockIdx.y;
     __shared__ double c[KMAX];
-    if constexpr (MODE != 0) {
+    if constexpr (kUpdate) {
         if (static_cast<int>(threadIdx.x) < KMAX) {
             c[threadIdx.x] = static_cast<int>(threadIdx.x) < K ? coef[threadIdx.x] : 0.0;
         }
         __syncthreads();
     }
-    double acc[KMAX];
+    double acc[KMAX + 1];
 #pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
+    for (int k = 0; k <= KMAX; ++k) {
         acc[k] = 0.0;
     }
     const std::int64_t stride = static_cast<std::int64_t>(gridDim.x) * blockDim.x;
@@ -96,7 +105,7 @@ __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
             v[k] = k < K ? __ldcs(V + k * ld + i) : 0.0;
         }
         double wi = w[i];
-        if constexpr (MODE != 0) {
+        if constexpr (kUpdate) {
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {
                 wi -= c[k] * v[k];
@@ -105,23 +114,35 @@ __global__ void __launch_bounds__(kDotThreads, (cgs_min_blocks<KMAX, MODE>()))
         }
         if constexpr (MODE == 2) {
             acc[0] += wi * wi;
-        } else if constexpr (MODE == 0 || MODE == 1) {
+        } else if constexpr (kDots) {
 #pragma unroll
             for (int k = 0; k < KMAX; ++k) {
                 acc[k] += v[k] * wi;
             }
+            if constexpr (kNorm) {
+                acc[KMAX] += wi * wi;
+            }
         }
     }
-    if constexpr (MODE != 3) {
-        block_partials<KMAX>(acc, MODE == 2 ? 1 : K, partials);
+    if constexpr (kNorm) {
+        // the norm goes to entry K: move it down from the spare accumulator
+        double tmp[KMAX + 1];
+#pragma unroll
+        for (int k = 0; k <= KMAX; ++k) {
+            tmp[k] = k < K ? acc[k] : (k == K ? acc[KMAX] : 0.0);
+        }
+        block_partials<KMAX + 1>(tmp, K + 1, partials);
+    } else if constexpr (MODE != 3) {
+        block_partials<KMAX + 1>(acc, MODE == 2 ? 1 : K, partials);
     }
 }
 
 // out[k] = sum_b partials[k * nb + b], one warp per k, fixed order; block y serves column y of
 // a batch (partials + part_stride * y, out + out_stride * y)
 __global__ void finalize_kernel(const double *partials, int nb, int K, double *out,
-                                std::int64_t part_stride, std::int64_t out_stride, unsigned mask) {
-    if (!((mask >> blockIdx.x) & 1U)) {
+                                std::int64_t part_stride, std::int64_t out_stride, unsigned mask,
+                                const int *skip = nullptr) {
+    if (!((mask >> blockIdx.x) & 1U) || (skip && *skip)) {
         return;
     }
     partials += part_stride * blockIdx.x;
@@ -141,30 +162,46 @@ __global__ void finalize_kernel(const double *partials, int nb, int K, double *o
 
 template <int KMAX, int MODE>
 cudaError_t launch_cgs(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
-                       const double *coef, double *partials, double *out, cudaStream_t stream) {
+                       const double *coef, double *partials, double *out, cudaStream_t stream,
+                       const int *skip = nullptr) {
     count_launches(MODE != 3 ? 2 : 1);
-    cgs_kernel<KMAX, MODE>
-        <<<kDotBlocks, kDotThreads, 0, stream>>>(V, ld, K, w, n, coef, partials, 0, 0, 0, 1U);
+    cgs_kernel<KMAX, MODE><<<kDotBlocks, kDotThreads, 0, stream>>>(V, ld, K, w, n, coef, partials,
+                                                                   0, 0, 0, 1U, skip);
     if (MODE != 3) {
-        finalize_kernel<<<1, 1024, 0, stream>>>(partials, kDotBlocks, MODE == 2 ? 1 : K, out, 0, 0,
-                                                1U);
+        const int outs = MODE == 2 ? 1 : (MODE == 4 || MODE == 5 ? K + 1 : K);
+        finalize_kernel<<<1, 1024, 0, stream>>>(partials, kDotBlocks, outs, out, 0, 0, 1U, skip);
     }
     return cudaGetLastError();
 }
 
 template <int MODE>
 cudaError_t launch_cgs_k(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
-                         const double *coef, double *partials, double *out, cudaStream_t stream) {
+                         const double *coef, double *partials, double *out, cudaStream_t stream,
+                         const int *skip = nullptr) {
     if (K <= 4) {
-        return launch_cgs<4, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+        return launch_cgs<4, MODE>(V, ld, K, w, n, coef, partials, out, stream, skip);
     }
     if (K <= 8) {
-        return launch_cgs<8, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+        return launch_cgs<8, MODE>(V, ld, K, w, n, coef, partials, out, stream, skip);
     }
     if (K <= 16) {
-        return launch_cgs<16, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+        return launch_cgs<16, MODE>(V, ld, K, w, n, coef, partials, out, stream, skip);
     }
-    return launch_cgs<32, MODE>(V, ld, K, w, n, coef, partials, out, stream);
+    return launch_cgs<32, MODE>(V, ld, K, w, n, coef, partials, out, stream, skip);
+}
+
+// DGKS: after the first pass, w' = w - V h1; a second pass is needed only when
+// ||w'||^2 < ||w||^2 / 2. Otherwise h2 = 0, <w', w'> is the norm, and the second pass's
+// kernels return at once.
+__global__ void dgks_kernel(const double *h1, double *h2, int K, double *hn, int *skip) {
+    const bool enough = h2[K] >= 0.5 * h1[K];
+    *skip = enough ? 1 : 0;
+    if (enough) {
+        *hn = h2[K];
+        for (int k = 0; k < K; ++k) {
+            h2[k] = 0.0;
+        }
+    }
 }
 
 // one CGS pass for every selected column of a batch: grid (kDotBlocks, nb), then nb finalizes
@@ -334,6 +371,27 @@ __global__ void arnoldi_solve_kernel(ArnoldiState s, int k) {
 }
 
 } // namespace
+
+cudaError_t cgs_dgks(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
+                     double *partials, double *h1, double *h2, double *hn, int *skip,
+                     cudaStream_t stream) {
+    if (K < 1 || K >= kMaxFusedBasis) {
+        return cudaErrorInvalidValue;
+    }
+    cudaError_t e = launch_cgs_k<4>(V, ld, K, w, n, nullptr, partials, h1, stream);
+    if (e == cudaSuccess) {
+        e = launch_cgs_k<5>(V, ld, K, w, n, h1, partials, h2, stream);
+    }
+    if (e == cudaSuccess) {
+        count_launches(1);
+        dgks_kernel<<<1, 1, 0, stream>>>(h1, h2, K, hn, skip);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        e = launch_cgs_k<2>(V, ld, K, w, n, h2, partials, hn, stream, skip);
+    }
+    return e;
+}
 
 cudaError_t cgs_pass(int mode, const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
                      const double *coef, double *partials, double *out, cudaStream_t stream) {

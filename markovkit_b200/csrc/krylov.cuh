@@ -18,6 +18,15 @@ constexpr int kMaxFusedBasis = 32;  // basis vectors handled by the fused CGS ke
 //   mode 2: w -= sum_k coef[k] V_k, then out[0] = <w_new, w_new>
 //   mode 3: w -= sum_k coef[k] V_k only
 // K <= kMaxFusedBasis; longer bases are processed in chunks by the caller.
+// One Gram-Schmidt step with selective re-orthogonalisation (Daniel, Gragg, Kaufman, Stewart,
+// Math. Comp. 30, 1976): h1 = V^T w, w -= V h1; a second pass h2 = V^T w, w -= V h2 only when
+// ||w|| dropped below 1/sqrt(2) of its value, decided on the device (h2 = 0 and the second
+// pass's kernels return at once otherwise); hn = <w, w> after the step. K < kMaxFusedBasis
+// (h1 and h2 hold K + 1 entries: entry K is a norm); skip is one device int of scratch.
+cudaError_t cgs_dgks(const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
+                     double *partials, double *h1, double *h2, double *hn, int *skip,
+                     cudaStream_t stream);
+
 cudaError_t cgs_pass(int mode, const double *V, std::int64_t ld, int K, double *w, std::int64_t n,
                      const double *coef, double *partials, double *out, cudaStream_t stream);
 
