@@ -154,6 +154,12 @@ int mk_csr_device(mk_csr m, const int64_t **row_ptr, const int64_t **col, const 
 /* copies into host arrays of rows + 1, nonzeros and nonzeros elements */
 int mk_csr_copy_host(mk_csr m, int64_t *row_ptr, int64_t *col, double *val);
 void mk_csr_destroy(mk_csr m);
+/* a caller-given CSR matrix (host arrays, columns in range; duplicates are summed) on the device,
+ * e.g. the generator of an explicit state list such as an FSP support (generator.hpp:27-44) */
+int mk_csr_create_host(int64_t rows, const int64_t *row_ptr, const int64_t *col, const double *val,
+                       mk_csr *out);
+/* y = shift x + sign A x on device vectors (a warp per row): A x with (0, 1), s x - A x with (s, -1) */
+int mk_csr_apply(mk_csr m, double shift, double sign, const double *d_x, double *d_y, void *stream);
 
 /* ---- sector multigrid: markovkit/rdme/multigrid.hpp ---- */
 typedef struct {
@@ -368,6 +374,8 @@ typedef struct {
     int64_t substeps;        /* expv time steps over all attempts */
     int64_t applies;         /* operator applies over all attempts */
     int status;              /* MK_OK, MK_ENOTCONV (stopped before final_time), MK_ETOLERANCE, MK_ENAN */
+    int clipped;             /* bit s set when an expansion met a jump to a state above bounds[s]:
+                                the box, not the network, kept that state out of the support */
 } mk_fsp_result;
 typedef struct mk_fsp_batch_s *mk_fsp_batch;
 /* the number of states in box(bounds) */

@@ -532,6 +532,23 @@ class spmat {
     array<idx> ptr_;
 };
 
+// a dense row-major matrix (what fsp_solution::means() returns): m(i, j)
+template <typename T>
+class mat {
+  public:
+    mat() = default;
+    mat(idx rows, idx cols, T fill = T{}) : rows_(rows), cols_(cols), data_(rows * cols, fill) {}
+    [[nodiscard]] idx rows() const { return rows_; }
+    [[nodiscard]] idx cols() const { return cols_; }
+    T &operator()(idx i, idx j) { return data_[i * cols_ + j]; }
+    const T &operator()(idx i, idx j) const { return data_[i * cols_ + j]; }
+    [[nodiscard]] const array<T> &data() const { return data_; }
+
+  private:
+    idx rows_ = 0, cols_ = 0;
+    array<T> data_;
+};
+
 } // namespace num
 
 namespace detail {
@@ -554,6 +571,47 @@ class generator {
   public:
     using domain_type = vec<real>;
     using codomain_type = vec<real>;
+
+    // Q over any listed state space (an FSP support, a distribution) of any model that lists its
+    // jumps (generator.hpp:27-44): a jump into the space is an entry, one leaving it adds to the
+    // leak rate, and an absorbing boundary keeps the leak on the diagonal. The jumps are listed
+    // on the host; Q is kept on the device in CSR and applied there (mk_csr_apply).
+    template <state_space Space, markov_model Model>
+        requires(!std::derived_from<Space, population_space>)
+    generator(const Space &space, const Model &model, boundary leaks = boundary::absorbing) {
+        const idx n = space.size();
+        auto listed = std::make_shared<listed_jumps>();
+        listed->first.assign(n + 1, 0);
+        array<real> exit(n, 0.0), leak(n, 0.0);
+        for (idx j = 0; j < n; ++j) {
+            for (const transition &e : model.transitions(space[j])) {
+                if (const std::optional<idx> i = space.find(e.to)) {
+                    listed->jumps.push_back({*i, e.rate});
+                    exit[j] += e.rate;
+                } else {
+                    leak[j] += e.rate;
+                }
+            }
+            if (leaks == boundary::absorbing) {
+                exit[j] += leak[j];
+            }
+            listed->first[j + 1] = listed->jumps.size();
+        }
+        listed->Q = assemble_listed(n, listed->first, listed->jumps, exit);
+        const num::spmat &Q = listed->Q;
+        std::vector<int64_t> ptr(Q.row_ptr().begin(), Q.row_ptr().end());
+        std::vector<int64_t> col(Q.columns().begin(), Q.columns().end());
+        mk_csr m = nullptr;
+        detail::check(mk_csr_create_host(static_cast<int64_t>(n), ptr.data(), col.data(), Q.values().data(), &m));
+        csr_.reset(m, [](mk_csr c) { mk_csr_destroy(c); });
+        listed_ = std::move(listed);
+        rates_ = std::make_shared<std::pair<array<real>, array<real>>>(std::move(exit), std::move(leak));
+        n_ = n;
+        if (n_ > 0) {
+            x_ = std::make_shared<detail::device_vector>(n_);
+            y_ = std::make_shared<detail::device_vector>(n_);
+        }
+    }
 
     template <typename Graph>
     generator(const population_space &space, const reaction_diffusion<Graph> &model,
@@ -583,15 +641,23 @@ class generator {
     [[nodiscard]] idx cols() const { return n_; }
     // y = Q x
     void apply(const vec<real> &x, vec<real> &y) const {
-        x_->upload(x.data());
-        detail::check(mk_generator_apply(h_.get(), x_->get(), y_->get(), nullptr));
         y.resize(n_);
+        if (n_ == 0) {
+            return;
+        }
+        x_->upload(x.data());
+        detail::check(csr_ ? mk_csr_apply(csr_.get(), 0.0, 1.0, x_->get(), y_->get(), nullptr)
+                           : mk_generator_apply(h_.get(), x_->get(), y_->get(), nullptr));
         y_->download(y.data());
     }
     // y = shift x - Q x
     void apply_shifted(real shift, view<const real> x, view<real> y) const {
+        if (n_ == 0) {
+            return;
+        }
         x_->upload(x.data());
-        detail::check(mk_generator_apply_shifted(h_.get(), shift, x_->get(), y_->get(), nullptr));
+        detail::check(csr_ ? mk_csr_apply(csr_.get(), shift, -1.0, x_->get(), y_->get(), nullptr)
+                           : mk_generator_apply_shifted(h_.get(), shift, x_->get(), y_->get(), nullptr));
         y_->download(y.data());
     }
     // the total rate out of each state, and the part of it that leaves the space
@@ -599,6 +665,10 @@ class generator {
     [[nodiscard]] const array<real> &leak_rates() const { return rates_->second; }
     // the jumps out of state j that stay in the space, in the reference's order
     [[nodiscard]] array<jump> jumps(idx j) const {
+        if (listed_) {
+            return array<jump>(listed_->jumps.begin() + static_cast<std::ptrdiff_t>(listed_->first[j]),
+                               listed_->jumps.begin() + static_cast<std::ptrdiff_t>(listed_->first[j + 1]));
+        }
         int64_t count = 0;
         detail::check(mk_generator_jumps(h_.get(), static_cast<int64_t>(j), nullptr, nullptr, 0, &count));
         std::vector<int64_t> to(static_cast<std::size_t>(count));
@@ -611,26 +681,81 @@ class generator {
         return out;
     }
     [[nodiscard]] idx n_jumps() const {
+        if (listed_) {
+            return listed_->jumps.size();
+        }
         int64_t n = 0;
         detail::check(mk_generator_n_jumps(h_.get(), &n, nullptr));
         return static_cast<idx>(n);
     }
     // Q, assembled
     [[nodiscard]] num::spmat matrix() const {
+        if (listed_) {
+            return listed_->Q;
+        }
         mk_csr m = nullptr;
         detail::check(mk_generator_matrix(h_.get(), &m, nullptr));
         return detail::take_csr(m);
     }
     // shift I - Q, assembled
     [[nodiscard]] num::spmat characteristic_matrix(real shift) const {
+        if (listed_) {
+            const num::spmat &Q = listed_->Q;
+            array<real> v(Q.values().size());
+            for (idx i = 0; i < Q.rows(); ++i) {
+                for (idx k = Q.row_ptr()[i]; k < Q.row_ptr()[i + 1]; ++k) {
+                    v[k] = (Q.columns()[k] == i ? shift : 0.0) - Q.values()[k];
+                }
+            }
+            return num::spmat(Q.rows(), Q.cols(), std::move(v), Q.columns(), Q.row_ptr());
+        }
         mk_csr m = nullptr;
         detail::check(mk_generator_characteristic_matrix(h_.get(), shift, &m, nullptr));
         return detail::take_csr(m);
     }
+    // the device handle of a population-space generator (null for one over a listed space)
     [[nodiscard]] mk_generator handle() const { return h_.get(); }
     [[nodiscard]] mk_model model_handle() const { return model_.get(); }
+    // the device CSR of a generator over a listed space (null for a population-space one)
+    [[nodiscard]] mk_csr csr_handle() const { return csr_.get(); }
 
   private:
+    struct listed_jumps {
+        array<idx> first;  // jumps out of state j: [first[j], first[j + 1])
+        array<jump> jumps;
+        num::spmat Q;      // rows are targets: Q[to][from] = rate, Q[j][j] = -exit[j]
+    };
+
+    // Q in CSR from the jumps: each row's columns ascending, equal positions summed
+    static num::spmat assemble_listed(idx n, const array<idx> &first, const array<jump> &jumps,
+                                      const array<real> &exit) {
+        array<array<std::pair<idx, real>>> rows(n);
+        for (idx j = 0; j < n; ++j) {
+            rows[j].push_back({j, -exit[j]});
+            for (idx k = first[j]; k < first[j + 1]; ++k) {
+                rows[jumps[k].to].push_back({j, jumps[k].rate});
+            }
+        }
+        array<idx> ptr(n + 1, 0), col;
+        array<real> val;
+        for (idx i = 0; i < n; ++i) {
+            auto &r = rows[i];
+            std::stable_sort(r.begin(), r.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+            for (const auto &[c, v] : r) {
+                if (!col.empty() && static_cast<idx>(col.size()) > ptr[i] && col.back() == c) {
+                    val.back() += v;
+                } else {
+                    col.push_back(c);
+                    val.push_back(v);
+                }
+            }
+            ptr[i + 1] = col.size();
+        }
+        return num::spmat(n, n, std::move(val), std::move(col), std::move(ptr));
+    }
+
+    std::shared_ptr<const listed_jumps> listed_;
+    std::shared_ptr<mk_csr_s> csr_;
     std::shared_ptr<mk_model_s> model_;
     std::shared_ptr<const std::pair<array<real>, array<real>>> rates_; // exit, leak
     std::shared_ptr<mk_generator_s> h_;
@@ -1109,23 +1234,76 @@ struct reaction_network {
     }
 };
 
-// box(bounds): 0 <= x[s] <= bounds[s]; the only region the device FSP supports
-struct region {
-    array<int> bounds;
+// the states an FSP may add to its support (fsp.hpp:16-42): box(bounds), box(bound) and
+// everywhere() run on the device; a region made from any other predicate serves the host-side
+// expand() and generator only. The default region is everywhere(), as in the reference.
+class region {
+  public:
+    region() = default;
+    template <typename F>
+        requires(!std::same_as<std::decay_t<F>, region> && std::is_invocable_r_v<bool, const F &, const state &>)
+    region(F f) : kind_(kind::predicate), predicate_(std::move(f)) {}
+
+    static region bounded(array<int> bounds) {
+        region r;
+        r.kind_ = kind::box;
+        r.bounds_ = std::move(bounds);
+        return r;
+    }
+    static region uniform(int bound) {
+        region r;
+        r.kind_ = kind::uniform;
+        r.uniform_ = bound;
+        return r;
+    }
+
     [[nodiscard]] bool operator()(const state &x) const {
+        switch (kind_) {
+        case kind::everywhere:
+            return true;
+        case kind::predicate:
+            return predicate_(x);
+        case kind::uniform:
+            return std::all_of(x.begin(), x.end(), [&](int c) { return c >= 0 && c <= uniform_; });
+        case kind::box:
+            break;
+        }
         for (idx s = 0; s < x.size(); ++s) {
-            if (s >= bounds.size() || x[s] < 0 || x[s] > bounds[s]) {
+            if (s >= bounds_.size() || x[s] < 0 || x[s] > bounds_[s]) {
                 return false;
             }
         }
         return true;
     }
+    [[nodiscard]] bool is_everywhere() const { return kind_ == kind::everywhere; }
+    [[nodiscard]] bool is_box() const { return kind_ == kind::box || kind_ == kind::uniform; }
+    // the box's bounds over `species` species
+    [[nodiscard]] array<int> bounds(idx species) const {
+        if (kind_ == kind::uniform) {
+            return array<int>(species, uniform_);
+        }
+        if (kind_ != kind::box || bounds_.size() != species) {
+            throw std::invalid_argument("fsp: the region is not a box over every species");
+        }
+        return bounds_;
+    }
+
+  private:
+    enum class kind : std::uint8_t { everywhere, box, uniform, predicate };
+    kind kind_ = kind::everywhere;
+    array<int> bounds_;
+    int uniform_ = 0;
+    std::function<bool(const state &)> predicate_;
 };
 
-inline region box(array<int> bounds) { return region{std::move(bounds)}; }
+// 0 <= x[s] <= bounds[s] for every coordinate (fsp.hpp:26-35)
+inline region box(array<int> bounds) { return region::bounded(std::move(bounds)); }
+// 0 <= x[s] <= bound for every coordinate (fsp.hpp:37-42)
+inline region box(int bound) { return region::uniform(bound); }
+inline region everywhere() { return region{}; }
 
 struct krylov_fsp_options {
-    region inside;
+    region inside = everywhere();
     real tolerance = 1e-6;
     real initial_step = 1.0;
     real step_growth = 2.0;
@@ -1140,7 +1318,7 @@ struct krylov_fsp_options {
 
 // adaptive_fsp_options (fsp.hpp:108-121); sampled_expansion has no device counterpart
 struct adaptive_fsp_options {
-    region inside;
+    region inside = everywhere();
     real step_scale = 1.0;
     real prune_fraction = 0.1;
     real flux_tolerance = 1e-6;
@@ -1154,14 +1332,73 @@ struct adaptive_fsp_options {
     real krylov_tol = 1e-8;
 };
 
+// states, their probabilities and a lookup from state to index (distribution.hpp:10-88); a
+// state_space, so generator(p, model, boundary) lists Q over it
 class distribution {
   public:
     distribution() = default;
-    distribution(array<state> states, array<real> p) : states_(std::move(states)), p_(std::move(p)) {}
+    // the point mass at x
+    explicit distribution(const state &x) { add(x, 1.0); }
+    distribution(array<state> states, array<real> p) : states_(std::move(states)), p_(std::move(p)) {
+        for (idx i = 0; i < states_.size(); ++i) {
+            index_.emplace(states_[i], i);
+        }
+    }
     [[nodiscard]] idx size() const { return states_.size(); }
     [[nodiscard]] const state &operator[](idx i) const { return states_[i]; }
     [[nodiscard]] const array<state> &states() const { return states_; }
+    [[nodiscard]] array<real> &probabilities() { return p_; }
     [[nodiscard]] const array<real> &probabilities() const { return p_; }
+    [[nodiscard]] std::optional<idx> find(const state &x) const {
+        const auto it = index_.find(x);
+        return it == index_.end() ? std::nullopt : std::optional<idx>(it->second);
+    }
+    // x with probability `mass`, unless x is already present
+    void add(const state &x, real mass = 0.0) {
+        if (index_.emplace(x, states_.size()).second) {
+            states_.push_back(x);
+            p_.push_back(mass);
+        }
+    }
+    // drops every state i with remove(i); the others keep their order
+    template <typename Remove>
+    void remove_if(Remove remove) {
+        array<bool> gone(size());
+        for (idx i = 0; i < size(); ++i) {
+            gone[i] = static_cast<bool>(remove(i));
+        }
+        idx n = 0;
+        for (idx i = 0; i < size(); ++i) {
+            if (!gone[i]) {
+                if (n != i) {
+                    states_[n] = std::move(states_[i]);
+                    p_[n] = p_[i];
+                }
+                ++n;
+            }
+        }
+        states_.resize(n);
+        p_.resize(n);
+        index_.clear();
+        for (idx i = 0; i < n; ++i) {
+            index_.emplace(states_[i], i);
+        }
+    }
+    // negative entries (roundoff) become 0, then the total is scaled to 1; returns the total
+    // before scaling
+    real normalize() {
+        real total = 0.0;
+        for (real &v : p_) {
+            v = v < 0.0 ? 0.0 : v;
+            total += v;
+        }
+        if (total > 0.0) {
+            for (real &v : p_) {
+                v /= total;
+            }
+        }
+        return total;
+    }
     [[nodiscard]] vec<real> means() const {
         vec<real> m(states_.empty() ? 0 : states_.front().size(), 0.0);
         for (idx i = 0; i < size(); ++i) {
@@ -1182,15 +1419,39 @@ class distribution {
   private:
     array<state> states_;
     array<real> p_;
+    std::map<state, idx> index_;
 };
+
+// adds `layers` rings of neighbours inside the region; a ring after the first grows only from
+// the states the ring before added (fsp.hpp:44-59). Host-side, for callers that build a support.
+template <markov_model Model>
+void expand(distribution &p, const Model &model, const region &inside, int layers = 1) {
+    idx from = 0;
+    for (int layer = 0; layer < layers; ++layer) {
+        const idx to = p.size();
+        for (idx i = from; i < to; ++i) {
+            for (const transition &e : model.transitions(p[i])) {
+                if (inside(e.to)) {
+                    p.add(e.to);
+                }
+            }
+        }
+        from = to;
+    }
+}
 
 struct fsp_solution {
     array<real> times;
     array<distribution> snapshots;
-    [[nodiscard]] std::vector<vec<real>> means() const {
-        std::vector<vec<real>> m;
-        for (const auto &d : snapshots) {
-            m.push_back(d.means());
+    // means(k, s): the mean count of species s at times[k] (fsp.hpp:90-101)
+    [[nodiscard]] num::mat<real> means() const {
+        const idx species = snapshots.empty() || snapshots.front().size() == 0 ? 0 : snapshots.front()[0].size();
+        num::mat<real> m(snapshots.size(), species, 0.0);
+        for (idx k = 0; k < snapshots.size(); ++k) {
+            const vec<real> v = snapshots[k].means();
+            for (idx s = 0; s < species && s < v.size(); ++s) {
+                m(k, s) = v[s];
+            }
         }
         return m;
     }
@@ -1204,13 +1465,13 @@ struct fsp_tables {
     idx box = 1;
 };
 
-// the network's propensities over the region of the options (krylov_ or adaptive_fsp_options)
-inline fsp_tables tabulate(const reaction_network &model, const state &initial, const auto &o) {
+// the network's propensities over box(bounds), box order (species 0 most significant)
+inline fsp_tables tabulate(const reaction_network &model, const state &initial, const array<int> &bounds) {
     fsp_tables t;
-    t.bounds = o.inside.bounds;
+    t.bounds = bounds;
     const idx S = t.bounds.size();
     if (S == 0 || S != initial.size()) {
-        throw std::invalid_argument("fsp: the device FSP needs box(bounds) over every species");
+        throw std::invalid_argument("fsp: the box must bound every species");
     }
     for (int b : t.bounds) {
         t.box *= static_cast<idx>(b) + 1;
@@ -1238,34 +1499,35 @@ inline fsp_tables tabulate(const reaction_network &model, const state &initial, 
     return t;
 }
 
-inline mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model, real T,
-                              const krylov_fsp_options &o) {
-    mk_fsp_problem p{};
-    p.n_species = static_cast<int>(t.bounds.size());
-    p.n_reactions = static_cast<int>(model.reactions.size());
-    p.bounds = t.bounds.data();
-    p.change = t.change.data();
-    p.rates = t.rates.data();
-    p.initial = t.initial.data();
-    p.final_time = T;
-    mk_fsp_options_default(&p.options);
-    p.options.tolerance = o.tolerance;
-    p.options.initial_step = o.initial_step;
-    p.options.step_growth = o.step_growth;
-    p.options.drop_probability = o.drop_probability;
-    p.options.drop_derivative = o.drop_derivative;
-    p.options.layers = o.layers;
-    p.options.krylov_dim = o.krylov_dim;
-    p.options.max_steps = o.max_steps;
-    p.options.krylov_tol = o.krylov_tol;
-    return p;
+inline void fill_options(mk_fsp_options &c, const krylov_fsp_options &o) {
+    c.tolerance = o.tolerance;
+    c.initial_step = o.initial_step;
+    c.step_growth = o.step_growth;
+    c.drop_probability = o.drop_probability;
+    c.drop_derivative = o.drop_derivative;
+    c.layers = o.layers;
+    c.krylov_dim = o.krylov_dim;
+    c.max_steps = o.max_steps;
+    c.krylov_tol = o.krylov_tol;
 }
 
-inline mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model, real T,
-                              const adaptive_fsp_options &o) {
+inline void fill_options(mk_fsp_options &c, const adaptive_fsp_options &o) {
     if (o.sampled_expansion) {
         throw std::invalid_argument("solve_adaptive_fsp: the device expands every neighbour");
     }
+    c.method = 1;
+    c.step_scale = o.step_scale;
+    c.prune_fraction = o.prune_fraction;
+    c.flux_tolerance = o.flux_tolerance;
+    c.min_probability = o.min_probability;
+    c.layers = o.layers;
+    c.krylov_dim = o.krylov_dim;
+    c.max_steps = o.max_steps;
+    c.krylov_tol = o.krylov_tol;
+}
+
+template <typename Options>
+mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model, real T, const Options &o) {
     mk_fsp_problem p{};
     p.n_species = static_cast<int>(t.bounds.size());
     p.n_reactions = static_cast<int>(model.reactions.size());
@@ -1275,67 +1537,112 @@ inline mk_fsp_problem problem(const fsp_tables &t, const reaction_network &model
     p.initial = t.initial.data();
     p.final_time = T;
     mk_fsp_options_default(&p.options);
-    p.options.method = 1;
-    p.options.step_scale = o.step_scale;
-    p.options.prune_fraction = o.prune_fraction;
-    p.options.flux_tolerance = o.flux_tolerance;
-    p.options.min_probability = o.min_probability;
-    p.options.layers = o.layers;
-    p.options.krylov_dim = o.krylov_dim;
-    p.options.max_steps = o.max_steps;
-    p.options.krylov_tol = o.krylov_tol;
+    fill_options(p.options, o);
     return p;
 }
 
-// every instance in one launch of the batched FSP kernel
+// the box an everywhere() instance starts in
+inline array<int> first_box(const state &initial) {
+    array<int> b(initial.size());
+    for (idx s = 0; s < initial.size(); ++s) {
+        b[s] = std::max(2 * initial[s], initial[s] + 16);
+    }
+    return b;
+}
+
+constexpr idx kLargestAutoBox = idx(1) << 26;
+
+// Every instance in one launch of the batched FSP kernel. A region other than a box must be
+// everywhere(): such an instance runs in a box whose bounds double (2b + 1) on each species
+// an expansion would have crossed, and runs again until no expansion met the box; the support
+// then grew exactly as an unbounded region lets it, so the result is the everywhere() one.
 template <typename Options>
 array<fsp_solution> solve_batch(const array<std::tuple<reaction_network, state, real, Options>> &instances) {
-    array<detail::fsp_tables> tables;
-    array<mk_fsp_problem> problems;
-    tables.reserve(instances.size());
-    for (const auto &[model, initial, T, o] : instances) {
-        tables.push_back(detail::tabulate(model, initial, o));
-    }
-    for (idx k = 0; k < instances.size(); ++k) {
+    const idx n = instances.size();
+    array<array<int>> bounds(n);
+    array<bool> automatic(n, false);
+    for (idx k = 0; k < n; ++k) {
         const auto &[model, initial, T, o] = instances[k];
-        problems.push_back(detail::problem(tables[k], model, T, o));
-    }
-    idx total = 0;
-    for (const auto &t : tables) {
-        total += t.box;
-    }
-    array<real> out(total);
-    array<mk_fsp_result> results(instances.size());
-    const int rc = mk_fsp_krylov_batch(static_cast<int>(problems.size()), problems.data(),
-                                       out.data(), results.data(), nullptr);
-    if (rc != MK_OK && rc != MK_ENOTCONV) {
-        markovkit::detail::check(rc);
-    }
-    array<fsp_solution> sols;
-    idx off = 0;
-    for (idx k = 0; k < instances.size(); ++k) {
-        const auto &t = tables[k];
-        const idx S = t.bounds.size();
-        array<state> states;
-        array<real> p;
-        for (idx i = 0; i < t.box; ++i) {
-            if (out[off + i] != 0.0) {
-                state x(S);
-                idx rem = i;
-                for (idx s = S; s-- > 0;) {
-                    x[s] = static_cast<int>(rem % (t.bounds[s] + 1));
-                    rem /= t.bounds[s] + 1;
-                }
-                states.push_back(std::move(x));
-                p.push_back(out[off + i]);
-            }
+        if (o.inside.is_box()) {
+            bounds[k] = o.inside.bounds(initial.size());
+        } else if (o.inside.is_everywhere()) {
+            automatic[k] = true;
+            bounds[k] = first_box(initial);
+        } else {
+            throw std::invalid_argument("fsp: the device FSP takes box(...) or everywhere() as the region");
         }
-        fsp_solution sol;
-        sol.times = {0.0, results[k].time};
-        sol.snapshots.emplace_back(array<state>{t.initial}, array<real>{1.0});
-        sol.snapshots.emplace_back(std::move(states), std::move(p));
-        sols.push_back(std::move(sol));
-        off += t.box;
+    }
+    array<fsp_solution> sols(n);
+    array<idx> pending(n);
+    for (idx k = 0; k < n; ++k) {
+        pending[k] = k;
+    }
+    while (!pending.empty()) {
+        array<fsp_tables> tables;
+        array<mk_fsp_problem> problems;
+        tables.reserve(pending.size());
+        for (idx k : pending) {
+            const auto &[model, initial, T, o] = instances[k];
+            tables.push_back(tabulate(model, initial, bounds[k]));
+        }
+        for (idx q = 0; q < pending.size(); ++q) {
+            const auto &[model, initial, T, o] = instances[pending[q]];
+            problems.push_back(problem(tables[q], model, T, o));
+        }
+        idx total = 0;
+        for (const auto &t : tables) {
+            total += t.box;
+        }
+        array<real> out(total);
+        array<mk_fsp_result> results(pending.size());
+        const int rc = mk_fsp_krylov_batch(static_cast<int>(problems.size()), problems.data(), out.data(),
+                                           results.data(), nullptr);
+        if (rc != MK_OK && rc != MK_ENOTCONV) {
+            markovkit::detail::check(rc);
+        }
+        array<idx> again;
+        idx off = 0;
+        for (idx q = 0; q < pending.size(); ++q) {
+            const idx k = pending[q];
+            const auto &t = tables[q];
+            const idx S = t.bounds.size();
+            if (automatic[k] && results[q].clipped != 0) {
+                idx size = 1;
+                for (idx s = 0; s < S; ++s) {
+                    if (results[q].clipped & (1 << s)) {
+                        bounds[k][s] = 2 * bounds[k][s] + 1;
+                    }
+                    size *= static_cast<idx>(bounds[k][s]) + 1;
+                }
+                if (size > kLargestAutoBox) {
+                    throw std::runtime_error("fsp: the everywhere() support outgrew a box of 2^26 states");
+                }
+                again.push_back(k);
+                off += t.box;
+                continue;
+            }
+            array<state> states;
+            array<real> p;
+            for (idx i = 0; i < t.box; ++i) {
+                if (out[off + i] != 0.0) {
+                    state x(S);
+                    idx rem = i;
+                    for (idx s = S; s-- > 0;) {
+                        x[s] = static_cast<int>(rem % (t.bounds[s] + 1));
+                        rem /= t.bounds[s] + 1;
+                    }
+                    states.push_back(std::move(x));
+                    p.push_back(out[off + i]);
+                }
+            }
+            fsp_solution &sol = sols[k];
+            sol.times = {0.0, results[q].time};
+            sol.snapshots.clear();
+            sol.snapshots.emplace_back(array<state>{t.initial}, array<real>{1.0});
+            sol.snapshots.emplace_back(std::move(states), std::move(p));
+            off += t.box;
+        }
+        pending = std::move(again);
     }
     return sols;
 }
@@ -1362,7 +1669,7 @@ inline fsp_solution solve_adaptive_fsp(const reaction_network &model, const stat
 
 // the Krylov FSP of Vo and Sidje on the GPU (fsp.hpp:207-254)
 inline fsp_solution solve_krylov_fsp(const reaction_network &model, const state &initial,
-                                     real final_time, const krylov_fsp_options &options) {
+                                     real final_time, const krylov_fsp_options &options = {}) {
     return solve_krylov_fsp_batch({{model, initial, final_time, options}}).front();
 }
 
@@ -1430,10 +1737,6 @@ struct ssa_ensemble {
 
 namespace detail {
 
-struct ssa_box {
-    region inside;
-};
-
 // mk_ssa_run over a box that doubles until no path leaves it (path i depends on (seed, i)
 // alone, so every rerun replays the same paths)
 inline ssa_ensemble simulate(const reaction_network &model, const state &initial, real final_time,
@@ -1445,7 +1748,7 @@ inline ssa_ensemble simulate(const reaction_network &model, const state &initial
         bounds[s] = std::max(2 * initial[s], initial[s] + 64);
     }
     for (;;) {
-        const fsp_tables t = tabulate(model, initial, ssa_box{box(bounds)});
+        const fsp_tables t = tabulate(model, initial, bounds);
         mk_ssa_problem q{};
         mk_ssa_problem_default(&q);
         q.n_species = static_cast<int>(S);

@@ -141,6 +141,7 @@ class FspResult(C.Structure):
         ("substeps", C.c_int64),
         ("applies", C.c_int64),
         ("status", C.c_int),
+        ("clipped", C.c_int),
     ]
 
 
@@ -248,6 +249,8 @@ SIGNATURES = {
     "mk_csr_device": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "mk_csr_copy_host": (C.c_int, [P, I64P, I64P, C.POINTER(C.c_double)]),
     "mk_csr_destroy": (None, [P]),
+    "mk_csr_create_host": (C.c_int, [I64, I64P, I64P, DP, C.POINTER(P)]),
+    "mk_csr_apply": (C.c_int, [P, C.c_double, C.c_double, P, P, P]),
     "mk_multigrid_options_default": (None, [C.POINTER(MultigridOptions)]),
     "mk_multigrid_create": (C.c_int, [P, P, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),
     "mk_multigrid_create_full": (C.c_int, [P, C.POINTER(P), C.c_int, C.c_double, C.POINTER(MultigridOptions), C.POINTER(P)]),

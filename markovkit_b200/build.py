@@ -22,7 +22,7 @@ LIB = HERE / "libmarkovkit_b200.so"
 
 PLAIN = ["row_kernels.cu", "transfer.cu", "aggregate.cu", "krylov.cu", "engine.cu", "capi.cu", "noalloc.cu", "fsp.cu",
          "capi_fsp.cu", "server.cpp", "assemble.cu", "precond.cu", "capi_precond.cu", "dense_inverse.cu",
-         "ssa.cu", "capi_ssa.cu"]
+         "ssa.cu", "capi_ssa.cu", "csr_apply.cu"]
 PRECISIONS = {"f64": "double", "f32": "float"}
 N_SHAPES = 10  # the state shapes of with_shape (generator_row.cuh)
 

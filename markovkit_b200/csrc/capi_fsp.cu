@@ -402,6 +402,7 @@ int mk_fsp_batch_results(mk_fsp_batch batch, double *h_out, mk_fsp_result *resul
             r.substeps = outcome[k].substeps;
             r.applies = outcome[k].applies;
             r.status = status_code(outcome[k].status);
+            r.clipped = outcome[k].clipped;
             if (r.status != MK_OK && first_failure == MK_OK) {
                 first_failure = r.status;
                 mkb::capi::g_last_error =

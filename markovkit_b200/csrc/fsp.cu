@@ -79,6 +79,7 @@ struct Shared {
     int scan[kMaxWarps + 1];
     int hist[256];            // radix-select histogram of the adaptive pruning
     unsigned long long key;   // the select's prefix, broadcast
+    int clipped;              // species whose bound an expansion met (bit mask)
 };
 
 struct Ctx {
@@ -778,6 +779,30 @@ __device__ __forceinline__ bool new_neighbour(const Ctx &c, int k, int r, int &j
     return inside && c.b2s[j] < 0;
 }
 
+// when reaction r is a jump out of slot k (rate > 0, no count negative) whose target lies above
+// the box's bounds, a state the region box(bounds) keeps out of the support: the species it
+// crosses the bounds of, as a bit mask (0 otherwise)
+__device__ __forceinline__ int clipped_neighbour(const Ctx &c, int k, int r) {
+    const FspInstance &in = *c.in;
+    const int i = c.s2b[k];
+    if (!(c.rate[static_cast<std::int64_t>(r) * in.box + i] > 0.0)) {
+        return 0;
+    }
+    int xi[kFspMaxSpecies];
+    coords(in, i, xi);
+    bool valid = true;
+    int above = 0;
+#pragma unroll
+    for (int s = 0; s < kFspMaxSpecies; ++s) {
+        if (s < in.S) {
+            const int y = xi[s] + in.change[r][s];
+            valid = valid && y >= 0;
+            above |= y > in.bound[s] ? 1 << s : 0;
+        }
+    }
+    return valid ? above : 0;
+}
+
 // add `layers` rings of neighbours inside the box to slots [0, n), in the reference's order;
 // returns the new n
 template <int NT>
@@ -792,6 +817,8 @@ __device__ int expand(Shared &sh, const Ctx &c, int n) {
             int j;
             if (new_neighbour(c, f0 + q / R, q % R, j)) {
                 atomicMin(&c.owner[j], q);
+            } else if (const int mask = clipped_neighbour(c, f0 + q / R, q % R)) {
+                atomicOr(&sh.clipped, mask);
             }
         }
         __syncthreads();
@@ -990,6 +1017,7 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
             c.b2s[in.initial] = 0;
             c.s2b[0] = in.initial;
             c.prob[0] = 1.0;
+            sh.clipped = 0;
         }
         __syncthreads();
         int n = 1;
@@ -1131,6 +1159,7 @@ __global__ void __launch_bounds__(NT, 384 / NT + 1) fsp_kernel(const FspBatchVie
             o.substeps = cnt.substeps;
             o.applies = cnt.applies;
             o.status = status;
+            o.clipped = sh.clipped;
             v.outcome[in.index] = o;
         }
         __syncthreads();

@@ -49,7 +49,7 @@ struct FspOutcome {
     std::int64_t substeps = 0;  // expv time steps
     std::int64_t applies = 0;   // operator applies (Arnoldi steps and the extra ones)
     int status = 0; // 0 ok, 1 expv tolerance too high, 2 step limit, 3 non-finite
-    int pad = 0;
+    int clipped = 0; // bit s: an expansion met a jump to a state above bounds[s]
 };
 
 struct FspBatchView {

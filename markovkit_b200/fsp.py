@@ -5,14 +5,18 @@ reaction_network{reactions: [reaction{change, rate}]}, krylov_fsp_options (fsp.h
 with inside = box(bounds) (fsp.hpp:26-35), solve_krylov_fsp(model, initial, final_time,
 options) -> fsp_solution{times, snapshots} (fsp.hpp:86-107,207-254). The propensities are
 tabulated here over the box and the whole attempt loop runs on the GPU, many instances per
-launch (fsp_batch). Differences from the reference: the region must be a box containing the
-initial state, krylov_dim is at most 30, and only the initial and final distributions are
-saved (save_every has no counterpart).
+launch (fsp_batch). The region is box(bounds), box(bound) or everywhere() (the default, None):
+an everywhere() instance runs in a box whose bounds double (2b + 1) on each species an expansion
+would have crossed and runs again until no expansion met the box (mk_fsp_result.clipped), so its
+support grew exactly as an unbounded region lets it. Differences from the reference: krylov_dim
+is at most 30, and only the initial and final distributions are saved (save_every has no
+counterpart).
 """
 
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 from dataclasses import dataclass, field
 from typing import Callable, Optional, Sequence
 
@@ -41,9 +45,15 @@ class reaction_network:
 
 @dataclass
 class box:
-    """box(bounds): 0 <= x[s] <= bounds[s] (fsp.hpp:26-35)."""
+    """box(bounds): 0 <= x[s] <= bounds[s] (fsp.hpp:26-35); box(bound) with one int bounds every
+    species by it (fsp.hpp:37-42) once the species count is known (resolved)."""
 
     bounds: Sequence[int]
+
+    def resolved(self, species: int) -> "box":
+        if isinstance(self.bounds, (int, np.integer)):
+            return box([int(self.bounds)] * species)
+        return self
 
     def size(self) -> int:
         return int(np.prod([b + 1 for b in self.bounds], dtype=np.int64))
@@ -177,12 +187,26 @@ def tabulate(model: reaction_network, region: box) -> tuple[np.ndarray, np.ndarr
     return change, rates
 
 
+class everywhere:
+    """everywhere() (fsp.hpp:20-24): the region of every state; the device runs it in a box that
+    grows until no expansion meets it. options.inside = None means the same."""
+
+
+def _first_box(initial) -> box:
+    return box([max(2 * int(v), int(v) + 16) for v in initial])
+
+
+_LARGEST_AUTO_BOX = 1 << 26
+
+
 class _Problem:
     """one instance, with the arrays its mk_fsp_problem points at kept alive"""
 
     def __init__(self, model, initial, final_time, options):
-        if options.inside is None:
-            raise ValueError("the device FSP needs a box region (options.inside = box(bounds))")
+        if not isinstance(options.inside, box):
+            raise ValueError("an fsp_batch instance needs a box region (options.inside = box(bounds)); "
+                             "solve_krylov_fsp and solve_adaptive_fsp also take everywhere()")
+        options = dataclasses.replace(options, inside=options.inside.resolved(len(initial)))
         self.region = options.inside
         self.bounds = np.ascontiguousarray(options.inside.bounds, dtype=np.int32)
         self.change, self.rates = tabulate(model, options.inside)
@@ -283,29 +307,53 @@ class fsp_batch:
         return sols
 
 
+def _solve(problems, stream=None, autotune: bool = False) -> list:
+    """every (model, initial, final_time, options) in one launch; everywhere() instances run
+    again in grown boxes until no expansion met their box"""
+    problems = [tuple(p) for p in problems]
+    automatic = [not isinstance(p[3].inside, box) for p in problems]
+    for p, auto in zip(problems, automatic):
+        if auto and p[3].inside is not None and not isinstance(p[3].inside, everywhere):
+            raise ValueError("the device FSP takes box(...) or everywhere() as the region")
+    regions = [_first_box(p[1]) if auto else p[3].inside for p, auto in zip(problems, automatic)]
+    sols: list = [None] * len(problems)
+    pending = list(range(len(problems)))
+    while pending:
+        b = fsp_batch([(problems[k][0], problems[k][1], problems[k][2],
+                        dataclasses.replace(problems[k][3], inside=regions[k])) for k in pending])
+        if autotune:
+            b.autotune(stream=stream)
+        b.run(stream)
+        _, res = b.results(stream, with_output=False)
+        grown = []
+        for q, k in enumerate(pending):
+            if automatic[k] and res[q].clipped:
+                bounds = [2 * v + 1 if res[q].clipped >> s & 1 else v for s, v in enumerate(regions[k].bounds)]
+                regions[k] = box(bounds)
+                if regions[k].size() > _LARGEST_AUTO_BOX:
+                    raise ValueError("fsp: the everywhere() support outgrew a box of 2^26 states")
+                grown.append(k)
+        done = b.solutions(stream)
+        for q, k in enumerate(pending):
+            if k not in grown:
+                sols[k] = done[q]
+        pending = grown
+    return sols
+
+
 def solve_krylov_fsp(model: reaction_network, initial: Sequence[int], final_time: float,
                      options: Optional[krylov_fsp_options] = None, stream=None) -> fsp_solution:
     """solve_krylov_fsp (fsp.hpp:207-254) on the GPU."""
-    options = options or krylov_fsp_options()
-    b = fsp_batch([(model, initial, final_time, options)])
-    b.run(stream)
-    return b.solutions(stream)[0]
+    return _solve([(model, initial, final_time, options or krylov_fsp_options())], stream)[0]
 
 
 def solve_krylov_fsp_batch(problems, stream=None, autotune: bool = False) -> list:
     """solve_krylov_fsp for each (model, initial, final_time, options), in one launch."""
-    b = fsp_batch(problems)
-    if autotune:
-        b.autotune(stream=stream)
-    b.run(stream)
-    return b.solutions(stream)
+    return _solve(problems, stream, autotune)
 
 
 def solve_adaptive_fsp(model: reaction_network, initial: Sequence[int], final_time: float,
                        options: Optional[adaptive_fsp_options] = None, stream=None) -> fsp_solution:
     """solve_adaptive_fsp (fsp.hpp:123-188) on the GPU: flux-controlled steps of expand,
     expv on the reflecting generator of the support, prune and renormalise."""
-    options = options or adaptive_fsp_options()
-    b = fsp_batch([(model, initial, final_time, options)])
-    b.run(stream)
-    return b.solutions(stream)[0]
+    return _solve([(model, initial, final_time, options or adaptive_fsp_options())], stream)[0]

@@ -217,7 +217,8 @@ void krylov_fsp() {
     o.krylov_tol = 1e-12;
     const auto sol = solve_krylov_fsp(death, {5}, 1.0, o);
     expect(sol.times.back() == 1.0, "Krylov FSP reaches the final time");
-    expect(std::abs(sol.means().back()[0] - 5.0 * std::exp(-1.0)) < 1e-8, "pure-death mean");
+    const auto m = sol.means();
+    expect(m.rows() == 2 && std::abs(m(1, 0) - 5.0 * std::exp(-1.0)) < 1e-8, "pure-death mean");
     expect(std::abs(sol.snapshots.back().marginal(0).at(0) - std::pow(1.0 - std::exp(-1.0), 5)) < 1e-8,
            "extinction probability");
 }
@@ -229,7 +230,46 @@ void adaptive_fsp() {
     const auto solution = solve_adaptive_fsp(birth_death, {0}, 2.0, {.inside = box({100}), .step_scale = 0.1});
     expect(solution.times.size() > 1, "adaptive FSP saves snapshots");
     const real exact = (5.0 / 0.1) * (1.0 - std::exp(-0.1 * 2.0));
-    expect(std::abs(solution.means().back()[0] - exact) < 0.1, "adaptive FSP matches the birth-death mean");
+    const auto m = solution.means();
+    expect(std::abs(m(m.rows() - 1, 0) - exact) < 0.1, "adaptive FSP matches the birth-death mean");
+}
+
+// everywhere() (the default region): the device box grows until no expansion meets it, and the
+// result is the one of a box the support never reaches
+void fsp_everywhere() {
+    const reaction_network birth_death{{{{1}, [](const state &) { return 5.0; }},
+                                        {{-1}, [](const state &x) { return 0.1 * x[0]; }}}};
+    krylov_fsp_options o;
+    o.tolerance = 1e-8;
+    const auto grown = solve_krylov_fsp(birth_death, {0}, 2.0, o);
+    o.inside = box(400);
+    const auto boxed = solve_krylov_fsp(birth_death, {0}, 2.0, o);
+    const distribution &a = grown.snapshots.back(), &b = boxed.snapshots.back();
+    expect(a.size() == b.size() && a.size() > 17, "everywhere() grows past the first box");
+    real diff = 0.0;
+    for (idx i = 0; i < a.size() && i < b.size(); ++i) {
+        expect(a[i] == b[i], "the same support in the same order");
+        diff = std::max(diff, std::abs(a.probabilities()[i] - b.probabilities()[i]));
+    }
+    expect(diff <= 1e-14, "everywhere() matches a box the support never reaches");
+    const real exact = (5.0 / 0.1) * (1.0 - std::exp(-0.1 * 2.0));
+    expect(std::abs(grown.means()(1, 0) - exact) < 1e-6, "the birth-death mean");
+
+    // a listed generator over a support built on the host (generator.hpp:27-44)
+    distribution p(state{0});
+    expand(p, birth_death, box(10), 3);
+    expect(p.size() == 4, "three rings from {0}");
+    const generator Q(p, birth_death, boundary::reflecting);
+    vec<real> x{0.1, 0.2, 0.3, 0.4}, y, z;
+    Q.apply(x, y);
+    Q.matrix().apply(x, z);
+    real sum = 0.0;
+    for (idx i = 0; i < 4; ++i) {
+        expect(std::abs(y[i] - z[i]) < 1e-15, "device apply equals the assembled matrix");
+        sum += y[i];
+    }
+    expect(std::abs(sum) < 1e-15, "a reflecting generator conserves probability");
+    expect(Q.leak_rates()[3] == 5.0 && std::abs(Q.exit_rates()[3] - 0.3) < 1e-15, "the birth out of {3} leaks");
 }
 
 } // namespace
@@ -244,6 +284,7 @@ int main() {
         annihilation_transform();
         krylov_fsp();
         adaptive_fsp();
+        fsp_everywhere();
     } catch (const std::exception &e) {
         std::printf("FAILED with exception: %s\n", e.what());
         return 1;

@@ -4,8 +4,8 @@ compiles against it with g++ and links the in-tree library (CPU), and runs corre
 compares plain, Jacobi, ILU(0) and multigrid-preconditioned GMRES) compiles unchanged against
 the facade with -I include/mk where the reference tree is at hand (MK_REFERENCE_ROOT, else a
 `reference` folder beside the repository); the binary lands in tests/cpp/_build and runs on a
-B200 with --quick. The reference's own tests/test_ssa.cpp and tests/test_rdme.cpp build the same
-way and pass on the B200."""
+B200 with --quick. The reference's own tests/test_ssa.cpp, tests/test_rdme.cpp and
+tests/test_fsp.cpp build the same way and pass on the B200."""
 
 import os
 import subprocess
@@ -41,6 +41,10 @@ REF_SSA = REF / "tests" / "test_ssa.cpp"
 REF_SSA_OUT = ROOT / "tests" / "cpp" / "_build" / "reference_test_ssa"
 REF_RDME = REF / "tests" / "test_rdme.cpp"
 REF_RDME_OUT = ROOT / "tests" / "cpp" / "_build" / "reference_test_rdme"
+# FSP: distribution, expand, the generator over a listed support, adaptive and Krylov FSP
+# (the latter over everywhere(), the default region)
+REF_FSP = REF / "tests" / "test_fsp.cpp"
+REF_FSP_OUT = ROOT / "tests" / "cpp" / "_build" / "reference_test_fsp"
 
 
 def test_facade_program_compiles_and_links():
@@ -58,7 +62,8 @@ def test_reference_benchmark_compiles_against_facade():
     assert REF_BENCH_OUT.exists()
 
 
-@pytest.mark.parametrize("src,out", [(REF_SSA, REF_SSA_OUT), (REF_RDME, REF_RDME_OUT)], ids=["ssa", "rdme"])
+@pytest.mark.parametrize("src,out", [(REF_SSA, REF_SSA_OUT), (REF_RDME, REF_RDME_OUT), (REF_FSP, REF_FSP_OUT)],
+                         ids=["ssa", "rdme", "fsp"])
 def test_reference_test_compiles_against_facade(src, out):
     if not src.exists():
         pytest.skip("the reference tree is not here")
@@ -70,9 +75,9 @@ def test_reference_test_compiles_against_facade(src, out):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("out", [REF_SSA_OUT, REF_RDME_OUT], ids=["ssa", "rdme"])
+@pytest.mark.parametrize("out", [REF_SSA_OUT, REF_RDME_OUT, REF_FSP_OUT], ids=["ssa", "rdme", "fsp"])
 def test_reference_test_runs(cuda, out):
-    """the reference's tests/test_ssa.cpp and tests/test_rdme.cpp, unchanged, on the device:
+    """the reference's tests/test_ssa.cpp, test_rdme.cpp and test_fsp.cpp, unchanged, on the device:
     every check passes (their exit status counts the failed checks)"""
     if not out.exists():
         pytest.skip("the reference test was not built against the facade")

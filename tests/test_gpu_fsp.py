@@ -13,6 +13,7 @@ extinction probability within 1e-8 (tests/test_fsp.cpp:79-90), birth-death Poiss
 within 1e-7.
 """
 
+import dataclasses
 import json
 import math
 
@@ -188,3 +189,33 @@ def test_batching_instances_match_reference(batch512):
         else:
             assert res[k].status == _lib.MK_OK, k
     assert len(meta["instances"]) >= 32 and capped >= 1
+
+
+@pytest.mark.parametrize("name,big", [("birth_death_leaky_box", [400]), ("chain3", [40, 40, 40])])
+def test_everywhere_matches_a_box_the_support_never_reaches(cuda, name, big):
+    """everywhere() (the reference's default region): the device box grows on the species an
+    expansion crossed until no expansion meets it; the support and probabilities then equal
+    those of a box far beyond the support (which no expansion meets either)"""
+    from markovkit_b200.fsp import box, everywhere
+
+    net, init, T, opt = fsp_cases.cases()[name]
+    grown = solve_krylov_fsp(net, init, T, dataclasses.replace(opt, inside=everywhere()))
+    boxed = solve_krylov_fsp(net, init, T, dataclasses.replace(opt, inside=box(big)))
+    a, b = grown.snapshots[-1], boxed.snapshots[-1]
+    assert np.array_equal(a.states, b.states)
+    assert np.max(np.abs(a.probabilities - b.probabilities)) <= 1e-14
+    assert grown.times[-1] == boxed.times[-1] == T
+    # the default (inside=None) is everywhere() too
+    again = solve_krylov_fsp(net, init, T, dataclasses.replace(opt, inside=None))
+    assert np.array_equal(again.snapshots[-1].probabilities, a.probabilities)
+
+
+def test_clipped_reports_the_species_a_box_stopped(cuda):
+    cases = fsp_cases.cases()
+    names = ["birth_death_two_layers", "pure_death_5", "chain3"]
+    b = fsp_batch([cases[n] for n in names])
+    b.run()
+    _, res = b.results(with_output=False)
+    assert res[0].clipped == 1  # births out of box([10]): P(x > 10 at t = 0.5) > the tolerance
+    assert res[1].clipped == 0  # deaths only
+    assert res[2].clipped != 0 and res[2].clipped & ~0b111 == 0
