@@ -49,9 +49,13 @@ int mk_kernel_launches(uint64_t *count);
 
 /* Which kernel runs the rows of the solve passes (no reference counterpart; the reference has one
  * CPU code path): 0 (default) the stencil row kernel on the light rows of structured-grid levels
- * whose states hold one species of at most four molecules or two species of at most one, the
- * general row kernel elsewhere; 1 the general kernel everywhere. Both give bit-identical results;
- * the switch exists so that they can be compared. Process-wide; MK_EINVAL for other values. */
+ * whose states hold one species of at most four molecules or two species of at most one (and
+ * the pair-strip kernel, a block per pair of triangle rows, on the sectors of every pair of
+ * voxels of one species), the general row kernel elsewhere; 1 the general kernel everywhere;
+ * 2 as 0 without the pair-strip kernel. 0 and 2 give bit-identical results; 1 agrees with them
+ * bit for bit on the stencil forms and to rounding on the pair forms (their exit terms add in
+ * another order). The switch exists so that the paths can be compared. Process-wide; MK_EINVAL
+ * for other values. */
 int mk_set_row_path(int path);
 
 /* ---- device memory helpers (for callers without their own CUDA runtime) ---- */

@@ -624,9 +624,11 @@ def kernel_launches() -> int:
 
 def set_row_path(path: str = "stencil") -> None:
     """Which kernel runs the rows of the solve passes: "stencil" (default: the stencil row kernel
-    wherever a level allows it) or "general" (the general row kernel everywhere). Both give
-    bit-identical results; process-wide."""
-    check(load().mk_set_row_path({"stencil": 0, "general": 1}[path]))
+    wherever a level allows it, the pair-strip kernel on sectors of every pair of voxels of one
+    species), "general" (the general row kernel everywhere) or "no_strip" (as "stencil" without
+    the pair-strip kernel). "stencil" and "no_strip" agree bit for bit; "general" agrees with them
+    bit for bit on stencil forms and to rounding on pair forms. Process-wide."""
+    check(load().mk_set_row_path({"stencil": 0, "general": 1, "no_strip": 2}[path]))
 
 
 def gmres_options(tolerance: float = 1e-8, max_iterations: int = 1000, restart: int = 30, flexible: bool = False) -> GmresOptions:

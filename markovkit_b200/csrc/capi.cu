@@ -28,7 +28,8 @@ int mk_kernel_launches(uint64_t *count) {
 
 int mk_set_row_path(int path) {
     return guarded([&] {
-        MK_REQUIRE(path == 0 || path == 1, "row path must be 0 (stencil where possible) or 1 (general)");
+        MK_REQUIRE(path >= 0 && path <= 2,
+                   "row path must be 0 (stencil where possible), 1 (general) or 2 (stencil, no pair strips)");
         set_row_path(path);
     });
 }

@@ -166,7 +166,7 @@ namespace {
 std::atomic<int> g_row_path{0};
 } // namespace
 
-void set_row_path(int path) { g_row_path.store(path == 1 ? 1 : 0); }
+void set_row_path(int path) { g_row_path.store(path == 1 || path == 2 ? path : 0); }
 int row_path() { return g_row_path.load(); }
 
 void OperatorLevel::finalize(const Model &m, bool with_reactions) {
@@ -227,6 +227,32 @@ void OperatorLevel::finalize(const Model &m, bool with_reactions) {
             general_rest.clear();
         }
     }
+    // sectors of every pair u0 <= u1 of the V voxels: the pair-strip form, a tile per pair of
+    // triangle rows
+    strip_tiles.clear();
+    stencil_rest.clear();
+    if (pair && S == 1 && !stencil_tiles.empty()) {
+        const std::int64_t pairs = static_cast<std::int64_t>(V) * (V + 1) / 2;
+        std::vector<char> strip(sectors.size(), 0);
+        for (std::size_t k = 0; k < sectors.size(); ++k) {
+            const SectorDesc &sec = sectors[k];
+            strip[k] = !sec.heavy && h_ss64[k].fast && h_ss64[k].total[0] == 2 && sec.size == pairs ? 1 : 0;
+            for (int q = 0; strip[k] && q < (V + 1) / 2; ++q) {
+                Tile t;
+                t.local0 = q;
+                t.sector = static_cast<int>(k);
+                t.kind = 3;
+                strip_tiles.push_back(t);
+            }
+        }
+        for (const Tile &t : stencil_tiles) {
+            if (!strip[t.sector]) {
+                stencil_rest.push_back(t);
+            }
+        }
+    }
+    d_strip_tiles.upload(strip_tiles);
+    d_stencil_rest.upload(stencil_rest);
     d_heavy_tiles.upload(heavy_tiles);
     d_general_rest.upload(general_rest);
     ss64.upload(h_ss64);
@@ -289,8 +315,23 @@ void OperatorLevel::run(RowMode mode, const RowParams<T> &p, cudaStream_t stream
         q.n_tiles = static_cast<int>(general_tiles.size());
         check_cuda(launch_rows<T>(mode, S, mol_cap, q, stream), "row kernel launch");
     }
-    q.tiles = d_stencil_tiles.get();
-    q.n_tiles = static_cast<int>(stencil_tiles.size());
+    const bool strip = !strip_tiles.empty() && row_path() == 0;
+    if (strip) {
+        q.tiles = d_strip_tiles.get();
+        q.n_tiles = static_cast<int>(strip_tiles.size());
+        cudaError_t e;
+        if constexpr (std::is_same_v<T, double>) {
+            e = launch_pair_strip_rows_f64(q, stream);
+        } else {
+            e = launch_pair_strip_rows_f32(q, stream);
+        }
+        check_cuda(e, "pair strip row kernel launch");
+        if (stencil_rest.empty()) {
+            return;
+        }
+    }
+    q.tiles = strip ? d_stencil_rest.get() : d_stencil_tiles.get();
+    q.n_tiles = static_cast<int>(strip ? stencil_rest.size() : stencil_tiles.size());
     cudaError_t e;
     if constexpr (std::is_same_v<T, double>) {
         e = launch_stencil_rows_f64(q, S, mol_cap, stream);

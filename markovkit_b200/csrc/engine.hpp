@@ -140,6 +140,10 @@ struct OperatorLevel {
     // passes (then general_rest holds the general kernel's other rows)
     std::vector<Tile> heavy_tiles, general_rest;
     DeviceArray<Tile> d_heavy_tiles, d_general_rest;
+    // two-molecule sectors of one species in the pair-strip form (kind-3 tiles, a block per pair
+    // of triangle rows) and the stencil kernel's other rows; empty when no sector qualifies
+    std::vector<Tile> strip_tiles, stencil_rest;
+    DeviceArray<Tile> d_strip_tiles, d_stencil_rest;
     // tables of the pair and single-molecule row forms (stencil_tables.hpp), per precision
     std::vector<StencilSector<double>> h_ss64;
     DeviceArray<StencilSector<double>> ss64;

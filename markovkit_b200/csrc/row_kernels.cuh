@@ -99,6 +99,12 @@ bool pair_heavy_mode(int mode);
 cudaError_t launch_pair_heavy_rows_f64(const RowParams<double> &p, cudaStream_t stream);
 cudaError_t launch_pair_heavy_rows_f32(const RowParams<float> &p, cudaStream_t stream);
 
+// Rows of two-molecule sectors of one species (every pair u0 <= u1 of V voxels), a block per
+// pair of triangle rows (kind-3 tiles, local0 = the pair index), for the stencil passes; the
+// results equal the stencil kernel's bit for bit.
+cudaError_t launch_pair_strip_rows_f64(const RowParams<double> &p, cudaStream_t stream);
+cudaError_t launch_pair_strip_rows_f32(const RowParams<float> &p, cudaStream_t stream);
+
 namespace detail {
 // the general row kernel of one state shape (row_kernels_impl.cuh, instantiated per shape by
 // row_kernels_inst.cu)
@@ -110,6 +116,9 @@ cudaError_t launch_stencil(const RowParams<T> &p, int S, int cap, cudaStream_t s
 // the pair-form kernel for rows with in-jumps from every voxel (one species of cap <= 2)
 template <typename T, int NB>
 cudaError_t launch_pair_heavy(const RowParams<T> &p, cudaStream_t stream);
+// the pair-strip kernel for the rows of two-molecule sectors of one species
+template <typename T, int NB>
+cudaError_t launch_pair_strip(const RowParams<T> &p, cudaStream_t stream);
 } // namespace detail
 
 struct TerminalBlock {

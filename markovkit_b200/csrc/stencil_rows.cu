@@ -4,7 +4,8 @@
 // Rows of one species of at most two molecules or two species of at most one take the pair and
 // single-molecule forms (pair_rows.cuh); rows of up to four molecules of one species the stencil
 // forms (stencil_row.cuh). Rows whose in-jumps come from every voxel take pair_heavy_kernel in the
-// operator passes (a warp or a block per row). The build compiles this file once per (precision
+// operator passes (a warp or a block per row); the rows of two-molecule sectors of one species
+// take pair_strip_kernel (a block per pair of triangle rows). The build compiles this file once per (precision
 // MK_T, batch width MK_NB); the tiles each kernel gets list only rows its forms serve.
 #include "pair_rows.cuh"
 #include "row_kernels_impl.cuh"
@@ -356,6 +357,100 @@ __global__ void __launch_bounds__(kRowBlock) pair_heavy_kernel(const __grid_cons
     }
 }
 
+// Rows of a two-molecule sector of one species (u0 <= u1, rank u0 + T(u1): every pair of V
+// voxels) a block per pair of triangle rows u1 = w and V - 1 - w, so that every block takes
+// V + 1 rows and no row is unranked. A row outside the band u1 - u0 <= gmax has its sources at
+// offsets fixed per triangle row (computed once per row w); it visits the same in-jumps in the
+// same order as pair_row, whose other rows it calls, so the results equal pair_kernel's bit for
+// bit. p.tiles: kind-3 tiles, local0 = the pair index.
+template <typename T, int NB, int MODE>
+__global__ void __launch_bounds__(kRowBlock) pair_strip_kernel(const __grid_constant__ RowParams<T> p) {
+    __shared__ StencilSector<T> s_ss;
+    const Tile tile = p.tiles[blockIdx.x];
+    if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
+        return; // another colour class's pass (the whole block)
+    }
+    copy_to_shared(p.sv.sectors + tile.sector, s_ss);
+    __syncthreads();
+    const StencilSector<T> &ss = s_ss;
+    const int V = p.md.V;
+    const int colour = pass_colour(MODE, p.colour);
+    const int pair = static_cast<int>(tile.local0);
+    for (int h = 0; h < 2; ++h) {
+        const int w = h == 0 ? pair : V - 1 - pair;
+        if (h == 1 && w == pair) {
+            break;
+        }
+        const int tw = tri(w);
+        const unsigned m1 = load_ro(p.md.vmask + (V - 1 - w));
+        int up[3], down[3]; // molecule 1 from w + g and from w - g, relative to the row
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int g = p.md.gstride[a];
+            up[a] = g * w + tri(g);
+            down[a] = -g * w + tri(g - 1);
+        }
+        const int far_end = w - p.sv.gmax; // rows u0 < far_end are outside the band
+        for (int u0 = static_cast<int>(threadIdx.x); u0 <= w; u0 += kRowBlock) {
+            const int row = ss.begin + tw + u0;
+            const unsigned m0 = load_ro(p.md.vmask + (V - 1 - u0));
+            if (colour >= 0 && static_cast<int>(((m0 ^ m1) >> kVoxelColourBit) & 1U) != colour) {
+                continue;
+            }
+            const bool far = u0 < far_end;
+            T exit = T(0), leak = T(0);
+            T in[NB], in2[NB];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                in[c] = T(0);
+                in2[c] = T(0);
+            }
+            accumulate_terms<T, NB, MODE>(
+                p,
+                [&](auto want_in, auto &&acc) {
+                    constexpr bool W = decltype(want_in)::value;
+                    if (!far) {
+                        pair_row<T, W>(p.md, p.sv, ss, 2, u0, w, m0, m1, row, exit, leak, acc);
+                        return;
+                    }
+                    pair_row<T, false>(p.md, p.sv, ss, 2, u0, w, m0, m1, row, exit, leak, acc);
+                    if constexpr (W) {
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            if (a >= p.md.grid_dim) {
+                                continue;
+                            }
+                            const int g = p.md.gstride[a];
+                            const T D = p.sv.da[0][a];
+                            acc(row + g, D, has_lower(m0, a));
+                            acc(row - g, D, has_upper(m0, a));
+                        }
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            if (a >= p.md.grid_dim) {
+                                continue;
+                            }
+                            const T D = p.sv.da[0][a];
+                            acc(row + up[a], D, has_lower(m1, a));
+                            acc(row + down[a], D, has_upper(m1, a));
+                        }
+                        for (int k = 0; k < ss.n_in; ++k) {
+                            if (ss.in_copies[k] == 1) {
+                                const T a = ss.rin[k][1];
+                                if (a > T(0)) {
+                                    acc(ss.in_src[k] + w, a, true);
+                                    acc(ss.in_src[k] + u0, a, true);
+                                }
+                            }
+                        }
+                    }
+                },
+                in, in2);
+            finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
+        }
+    }
+}
+
 template <typename T, int NB, int MODE>
 cudaError_t launch_light(const RowParams<T> &p, int S, int cap, cudaStream_t stream) {
     const int threads = kRowBlock / kRowsPerThread<MODE>;
@@ -431,7 +526,51 @@ cudaError_t launch_pair_heavy(const RowParams<T> &p, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+template <typename T, int NB>
+cudaError_t launch_pair_strip(const RowParams<T> &p, cudaStream_t stream) {
+    if (p.n_tiles == 0) {
+        return cudaSuccess;
+    }
+    if (!p.sv.sectors) {
+        return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    switch (p.mode) {
+    case kApplyQ:
+        pair_strip_kernel<T, NB, kApplyQ><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kApplyShifted:
+        pair_strip_kernel<T, NB, kApplyShifted><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kResidual:
+        pair_strip_kernel<T, NB, kResidual><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kJacobiZero:
+        pair_strip_kernel<T, NB, kJacobiZero><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kJacobi:
+        pair_strip_kernel<T, NB, kJacobi><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kGaussSeidel:
+        pair_strip_kernel<T, NB, kGaussSeidel><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kIluFirst:
+        pair_strip_kernel<T, NB, kIluFirst><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kIluSecond:
+        pair_strip_kernel<T, NB, kIluSecond><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    case kIluThird:
+        pair_strip_kernel<T, NB, kIluThird><<<p.n_tiles, kRowBlock, 0, stream>>>(p);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 template cudaError_t launch_stencil<MK_T, MK_NB>(const RowParams<MK_T> &, int, int, cudaStream_t);
+template cudaError_t launch_pair_strip<MK_T, MK_NB>(const RowParams<MK_T> &, cudaStream_t);
 template cudaError_t launch_pair_heavy<MK_T, MK_NB>(const RowParams<MK_T> &, cudaStream_t);
 
 } // namespace mkb::detail

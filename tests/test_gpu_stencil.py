@@ -5,10 +5,13 @@ general kernel bit for bit; rows of one species of cap 2 or two of cap 1 (pair f
 exit terms in another order and agree to rounding (1e-14 relative here). Each path is bitwise
 reproducible, and so is every multigrid cycle."""
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
 import markovkit_b200 as mk
+from markovkit_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 
@@ -110,3 +113,43 @@ def test_cycle_matches_general_and_is_reproducible(cuda, general_after, name, sm
     else:
         scale = float(torch.max(torch.abs(outs[2])))
         assert float(torch.max(torch.abs(outs[0] - outs[2]))) <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("name", ["birth_death_3d16_cap2", "birth_death_3d8_cap2_reflecting"])
+def test_pair_strip_matches_pair_kernel_bitwise(cuda, general_after, name):
+    """The pair-strip kernel (a block per pair of triangle rows) on the two-molecule sectors
+    against the stencil kernel's pair form on the same rows: every operator pass, FP64 and
+    FP32, one and four right-hand sides, and V-cycles with each smoother, bit for bit."""
+    import torch
+
+    dom, _, box, Q = _problem(name)
+    n = box.size()
+    g = torch.Generator(device="cpu").manual_seed(5)
+    x = torch.rand(n, dtype=torch.float64, generator=g).to(cuda)
+    xb = torch.rand(4, n, dtype=torch.float64, generator=g).to(cuda)
+    outs = {}
+    for path in ("stencil", "no_strip"):
+        mk.set_row_path(path)
+        r = []
+        for dt in (torch.float64, torch.float32):
+            y = torch.empty(n, dtype=dt, device=cuda)
+            Q.apply_shifted(0.5, x.to(dt), y)
+            r.append(y.double().cpu())
+            qx = torch.empty(n, dtype=dt, device=cuda)
+            Q.apply(x.to(dt), qx)
+            r.append(qx.double().cpu())
+        yb = torch.empty_like(xb)
+        _lib.check(_lib.load().mk_generator_apply_shifted_batch(
+            Q._h, 0.5, C.c_void_p(xb.data_ptr()), C.c_void_p(yb.data_ptr()), n, 4,
+            C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        r.append(yb.cpu())
+        for smoother in ("jacobi", "gauss_seidel", "ilu0"):
+            for precision in ("fp64", "fp32"):
+                M = mk.sector_multigrid(dom, box, 0.7, mk.multigrid_options(smoother=smoother, precision=precision))
+                z = torch.empty_like(x)
+                M.apply(x, z)
+                r.append(z.cpu())
+        torch.cuda.synchronize()
+        outs[path] = r
+    for k, (a, b) in enumerate(zip(outs["stencil"], outs["no_strip"])):
+        assert torch.equal(a, b), k
