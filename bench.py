@@ -810,8 +810,9 @@ def roofline(mk, Q, dev, N, w) -> dict:
     algo = N * 16
     achieved = algo / (ms * 1e-3) / 1e9
     return {
-        "kernel": "generator apply_shifted, FP64 gather SpMV (pair_kernel<double,1> light rows + "
-                  "row_kernel<double,1,2> all-voxel rows)",
+        "kernel": "generator apply_shifted, FP64 gather SpMV (pair_strip_kernel: the two-molecule rows, a block "
+                  "per pair of triangle rows; pair_heavy_group_kernel: the one-molecule rows fed from every "
+                  "voxel, eight a block; pair_heavy_kernel: the empty state)",
         "bound": "hbm",
         "achieved": round(achieved, 1),
         "peak": pk["hbm_gbs"],

@@ -253,6 +253,36 @@ void OperatorLevel::finalize(const Model &m, bool with_reactions) {
     }
     d_strip_tiles.upload(strip_tiles);
     d_stencil_rest.upload(stencil_rest);
+    // heavy rows of one molecule fed by the pair sector: groups of eight rows
+    heavy_group_tiles.clear();
+    if (pair && S == 1 && !heavy_tiles.empty()) {
+        std::vector<char> grouped(sectors.size(), 0);
+        for (std::size_t k = 0; k < sectors.size(); ++k) {
+            const StencilSector<double> &ss = h_ss64[k];
+            bool ok = sectors[k].heavy && ss.fast && ss.heavy_ok && ss.total[0] == 1 && ss.n_heavy > 0 &&
+                      sectors[k].size == V;
+            for (int q = 0; ok && q < ss.n_heavy; ++q) {
+                ok = ss.heavy_copies[q] == 1;
+            }
+            grouped[k] = ok ? 1 : 0;
+            for (std::int64_t l = 0; ok && l < sectors[k].size; l += kHeavyGroupRows) {
+                Tile t;
+                t.local0 = l;
+                t.sector = static_cast<int>(k);
+                t.kind = 4;
+                t.count = static_cast<int>(std::min<std::int64_t>(kHeavyGroupRows, sectors[k].size - l));
+                heavy_group_tiles.push_back(t);
+            }
+        }
+        std::vector<Tile> rest;
+        for (const Tile &t : heavy_tiles) {
+            if (!grouped[t.sector]) {
+                rest.push_back(t);
+            }
+        }
+        heavy_tiles.swap(rest);
+    }
+    d_heavy_group_tiles.upload(heavy_group_tiles);
     d_heavy_tiles.upload(heavy_tiles);
     d_general_rest.upload(general_rest);
     ss64.upload(h_ss64);
@@ -294,17 +324,29 @@ void OperatorLevel::run(RowMode mode, const RowParams<T> &p, cudaStream_t stream
     }
     RowParams<T> q = p;
     q.mode = mode;
-    if (!heavy_tiles.empty() && pair_heavy_mode(mode)) {
+    if ((!heavy_tiles.empty() || !heavy_group_tiles.empty()) && pair_heavy_mode(mode)) {
         // rows with in-jumps from every voxel first (they read the whole next sector), then the rest
-        q.tiles = d_heavy_tiles.get();
-        q.n_tiles = static_cast<int>(heavy_tiles.size());
-        cudaError_t e;
-        if constexpr (std::is_same_v<T, double>) {
-            e = launch_pair_heavy_rows_f64(q, stream);
-        } else {
-            e = launch_pair_heavy_rows_f32(q, stream);
+        cudaError_t e = cudaSuccess;
+        if (!heavy_group_tiles.empty()) {
+            q.tiles = d_heavy_group_tiles.get();
+            q.n_tiles = static_cast<int>(heavy_group_tiles.size());
+            if constexpr (std::is_same_v<T, double>) {
+                e = launch_pair_heavy_group_rows_f64(q, stream);
+            } else {
+                e = launch_pair_heavy_group_rows_f32(q, stream);
+            }
+            check_cuda(e, "pair heavy group kernel launch");
         }
-        check_cuda(e, "pair heavy row kernel launch");
+        if (!heavy_tiles.empty()) {
+            q.tiles = d_heavy_tiles.get();
+            q.n_tiles = static_cast<int>(heavy_tiles.size());
+            if constexpr (std::is_same_v<T, double>) {
+                e = launch_pair_heavy_rows_f64(q, stream);
+            } else {
+                e = launch_pair_heavy_rows_f32(q, stream);
+            }
+            check_cuda(e, "pair heavy row kernel launch");
+        }
         if (!general_rest.empty()) {
             q.tiles = d_general_rest.get();
             q.n_tiles = static_cast<int>(general_rest.size());

@@ -144,6 +144,10 @@ struct OperatorLevel {
     // of triangle rows) and the stencil kernel's other rows; empty when no sector qualifies
     std::vector<Tile> strip_tiles, stencil_rest;
     DeviceArray<Tile> d_strip_tiles, d_stencil_rest;
+    // heavy rows of one molecule whose heavy sources are the pair sector, eight a block (kind-4
+    // tiles); heavy_tiles then holds the other heavy rows
+    std::vector<Tile> heavy_group_tiles;
+    DeviceArray<Tile> d_heavy_group_tiles;
     // tables of the pair and single-molecule row forms (stencil_tables.hpp), per precision
     std::vector<StencilSector<double>> h_ss64;
     DeviceArray<StencilSector<double>> ss64;

@@ -136,6 +136,22 @@ cudaError_t launch_pair_strip_rows_f32(const RowParams<float> &p, cudaStream_t s
                     : detail::launch_pair_strip<float, 1>(p, stream);
 }
 
+cudaError_t launch_pair_heavy_group_rows_f64(const RowParams<double> &p, cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch || !pair_heavy_mode(p.mode)) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? detail::launch_pair_heavy_group<double, kRowBatch>(p, stream)
+                    : detail::launch_pair_heavy_group<double, 1>(p, stream);
+}
+
+cudaError_t launch_pair_heavy_group_rows_f32(const RowParams<float> &p, cudaStream_t stream) {
+    if (p.nb < 1 || p.nb > kRowBatch || !pair_heavy_mode(p.mode)) {
+        return cudaErrorInvalidValue;
+    }
+    return p.nb > 1 ? detail::launch_pair_heavy_group<float, kRowBatch>(p, stream)
+                    : detail::launch_pair_heavy_group<float, 1>(p, stream);
+}
+
 namespace {
 
 constexpr int kTerminalThreads = 256;

@@ -19,6 +19,7 @@ struct Tile {
 };
 constexpr int kRowBlock = 256;
 constexpr int kWarpRows = kRowBlock / 32;
+constexpr int kHeavyGroupRows = 8; // rows of a kind-4 (grouped heavy) tile
 
 constexpr int kRowBatch = 4; // widest batch of the instantiated kernels
 
@@ -104,6 +105,11 @@ cudaError_t launch_pair_heavy_rows_f32(const RowParams<float> &p, cudaStream_t s
 // results equal the stencil kernel's bit for bit.
 cudaError_t launch_pair_strip_rows_f64(const RowParams<double> &p, cudaStream_t stream);
 cudaError_t launch_pair_strip_rows_f32(const RowParams<float> &p, cudaStream_t stream);
+// Rows of one molecule whose heavy in-jumps come from the pair sector, eight rows a block
+// (kind-4 tiles), in the operator passes: the sources of the group's rows for one voxel w sit
+// side by side, so the reads of the pair sector coalesce.
+cudaError_t launch_pair_heavy_group_rows_f64(const RowParams<double> &p, cudaStream_t stream);
+cudaError_t launch_pair_heavy_group_rows_f32(const RowParams<float> &p, cudaStream_t stream);
 
 namespace detail {
 // the general row kernel of one state shape (row_kernels_impl.cuh, instantiated per shape by
@@ -119,6 +125,9 @@ cudaError_t launch_pair_heavy(const RowParams<T> &p, cudaStream_t stream);
 // the pair-strip kernel for the rows of two-molecule sectors of one species
 template <typename T, int NB>
 cudaError_t launch_pair_strip(const RowParams<T> &p, cudaStream_t stream);
+// the grouped heavy-row kernel for rows of one molecule
+template <typename T, int NB>
+cudaError_t launch_pair_heavy_group(const RowParams<T> &p, cudaStream_t stream);
 } // namespace detail
 
 struct TerminalBlock {

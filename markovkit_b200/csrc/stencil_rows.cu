@@ -357,6 +357,60 @@ __global__ void __launch_bounds__(kRowBlock) pair_heavy_kernel(const __grid_cons
     }
 }
 
+// One row of pair_strip_kernel: FAR (outside the band) with its sources at the row's fixed
+// offsets, else pair_row's form; exit, leak and the sums stay in registers.
+template <typename T, int NB, int MODE, bool FAR>
+__device__ __forceinline__ void strip_row(const RowParams<T> &p, const StencilSector<T> &ss, int u0, int w,
+                                          unsigned m0, unsigned m1, int row, int up0, int up1, int up2,
+                                          int down0, int down1, int down2) {
+    T exit = T(0), leak = T(0);
+    T in[NB], in2[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] = T(0);
+        in2[c] = T(0);
+    }
+    accumulate_terms<T, NB, MODE>(
+        p,
+        [&](auto want_in, auto &&acc) {
+            constexpr bool W = decltype(want_in)::value;
+            if constexpr (!FAR) {
+                pair_row<T, W>(p.md, p.sv, ss, 2, u0, w, m0, m1, row, exit, leak, acc);
+            } else {
+                pair_row<T, false>(p.md, p.sv, ss, 2, u0, w, m0, m1, row, exit, leak, acc);
+                if constexpr (W) {
+                    // the axes in order, as pair_row; an axis past the grid's adds 0 (no read)
+                    const int gd = p.md.grid_dim;
+                    const int g0 = p.md.gstride[0], g1 = p.md.gstride[1], g2 = p.md.gstride[2];
+                    acc(row + g0, p.sv.da[0][0], gd > 0 && has_lower(m0, 0));
+                    acc(row - g0, p.sv.da[0][0], gd > 0 && has_upper(m0, 0));
+                    acc(row + g1, p.sv.da[0][1], gd > 1 && has_lower(m0, 1));
+                    acc(row - g1, p.sv.da[0][1], gd > 1 && has_upper(m0, 1));
+                    acc(row + g2, p.sv.da[0][2], gd > 2 && has_lower(m0, 2));
+                    acc(row - g2, p.sv.da[0][2], gd > 2 && has_upper(m0, 2));
+                    acc(row + up0, p.sv.da[0][0], gd > 0 && has_lower(m1, 0));
+                    acc(row + down0, p.sv.da[0][0], gd > 0 && has_upper(m1, 0));
+                    acc(row + up1, p.sv.da[0][1], gd > 1 && has_lower(m1, 1));
+                    acc(row + down1, p.sv.da[0][1], gd > 1 && has_upper(m1, 1));
+                    acc(row + up2, p.sv.da[0][2], gd > 2 && has_lower(m1, 2));
+                    acc(row + down2, p.sv.da[0][2], gd > 2 && has_upper(m1, 2));
+                    for (int k = 0; k < ss.n_in; ++k) {
+                        if (ss.in_copies[k] == 1) {
+                            const T a = ss.rin[k][1];
+                            if (a > T(0)) {
+                                acc(ss.in_src[k] + w, a, true);
+                                acc(ss.in_src[k] + u0, a, true);
+                            }
+                        }
+                    }
+                }
+            }
+        },
+        in, in2);
+    finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
+
+}
+
 // Rows of a two-molecule sector of one species (u0 <= u1, rank u0 + T(u1): every pair of V
 // voxels) a block per pair of triangle rows u1 = w and V - 1 - w, so that every block takes
 // V + 1 rows and no row is unranked. A row outside the band u1 - u0 <= gmax has its sources at
@@ -364,7 +418,7 @@ __global__ void __launch_bounds__(kRowBlock) pair_heavy_kernel(const __grid_cons
 // same order as pair_row, whose other rows it calls, so the results equal pair_kernel's bit for
 // bit. p.tiles: kind-3 tiles, local0 = the pair index.
 template <typename T, int NB, int MODE>
-__global__ void __launch_bounds__(kRowBlock) pair_strip_kernel(const __grid_constant__ RowParams<T> p) {
+__global__ void __launch_bounds__(kRowBlock, 4) pair_strip_kernel(const __grid_constant__ RowParams<T> p) {
     __shared__ StencilSector<T> s_ss;
     const Tile tile = p.tiles[blockIdx.x];
     if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
@@ -383,13 +437,10 @@ __global__ void __launch_bounds__(kRowBlock) pair_strip_kernel(const __grid_cons
         }
         const int tw = tri(w);
         const unsigned m1 = load_ro(p.md.vmask + (V - 1 - w));
-        int up[3], down[3]; // molecule 1 from w + g and from w - g, relative to the row
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int g = p.md.gstride[a];
-            up[a] = g * w + tri(g);
-            down[a] = -g * w + tri(g - 1);
-        }
+        // molecule 1 from w + g and from w - g, relative to the row, per axis
+        const int g0 = p.md.gstride[0], g1 = p.md.gstride[1], g2 = p.md.gstride[2];
+        const int up0 = g0 * w + tri(g0), up1 = g1 * w + tri(g1), up2 = g2 * w + tri(g2);
+        const int down0 = -g0 * w + tri(g0 - 1), down1 = -g1 * w + tri(g1 - 1), down2 = -g2 * w + tri(g2 - 1);
         const int far_end = w - p.sv.gmax; // rows u0 < far_end are outside the band
         for (int u0 = static_cast<int>(threadIdx.x); u0 <= w; u0 += kRowBlock) {
             const int row = ss.begin + tw + u0;
@@ -397,58 +448,115 @@ __global__ void __launch_bounds__(kRowBlock) pair_strip_kernel(const __grid_cons
             if (colour >= 0 && static_cast<int>(((m0 ^ m1) >> kVoxelColourBit) & 1U) != colour) {
                 continue;
             }
-            const bool far = u0 < far_end;
-            T exit = T(0), leak = T(0);
-            T in[NB], in2[NB];
-#pragma unroll
-            for (int c = 0; c < NB; ++c) {
-                in[c] = T(0);
-                in2[c] = T(0);
+            if (u0 < far_end) {
+                strip_row<T, NB, MODE, true>(p, ss, u0, w, m0, m1, row, up0, up1, up2, down0, down1, down2);
+            } else {
+                strip_row<T, NB, MODE, false>(p, ss, u0, w, m0, m1, row, up0, up1, up2, down0, down1, down2);
             }
-            accumulate_terms<T, NB, MODE>(
-                p,
-                [&](auto want_in, auto &&acc) {
-                    constexpr bool W = decltype(want_in)::value;
-                    if (!far) {
-                        pair_row<T, W>(p.md, p.sv, ss, 2, u0, w, m0, m1, row, exit, leak, acc);
-                        return;
-                    }
-                    pair_row<T, false>(p.md, p.sv, ss, 2, u0, w, m0, m1, row, exit, leak, acc);
-                    if constexpr (W) {
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            if (a >= p.md.grid_dim) {
-                                continue;
-                            }
-                            const int g = p.md.gstride[a];
-                            const T D = p.sv.da[0][a];
-                            acc(row + g, D, has_lower(m0, a));
-                            acc(row - g, D, has_upper(m0, a));
-                        }
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            if (a >= p.md.grid_dim) {
-                                continue;
-                            }
-                            const T D = p.sv.da[0][a];
-                            acc(row + up[a], D, has_lower(m1, a));
-                            acc(row + down[a], D, has_upper(m1, a));
-                        }
-                        for (int k = 0; k < ss.n_in; ++k) {
-                            if (ss.in_copies[k] == 1) {
-                                const T a = ss.rin[k][1];
-                                if (a > T(0)) {
-                                    acc(ss.in_src[k] + w, a, true);
-                                    acc(ss.in_src[k] + u0, a, true);
-                                }
-                            }
-                        }
-                    }
-                },
-                in, in2);
-            finish_row<T, NB, MODE>(p, row, exit, leak, in, in2);
         }
     }
+}
+
+constexpr int kHeavyGroup = kHeavyGroupRows;           // rows of a group tile
+constexpr int kHeavyThreads = 1024;                     // threads of a group's block
+constexpr int kHeavySlots = kHeavyThreads / kHeavyGroup; // threads per row of the group
+
+// Rows of one molecule (u = local) of one species whose heavy reactions come from the pair sector
+// (the source holds one more copy in any voxel w: {w, u} of rank min + T(max)), kHeavyGroup rows
+// u0 .. u0 + count - 1 a block (kind-4 tiles). Thread (slot, j) takes row j and the voxels
+// w = slot, slot + kHeavySlots, ...; the threads of one w read the sources of the group's rows
+// side by side: {u, w} for w > u sits at u + T(w), so the group's sources of one w are adjacent.
+// Per row the sums run over w in a fixed order and meet in a fixed tree; the row's own terms
+// (pair_row) come last. Operator passes only (kApplyQ, kApplyShifted, kResidual).
+template <typename T, int NB, int MODE>
+__global__ void __launch_bounds__(kHeavyThreads) pair_heavy_group_kernel(const __grid_constant__ RowParams<T> p) {
+    __shared__ StencilSector<T> s_ss;
+    __shared__ T s_red[kHeavyThreads / 32][kHeavyGroup][NB];
+    const Tile tile = p.tiles[blockIdx.x];
+    if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
+        return;
+    }
+    copy_to_shared(p.sv.sectors + tile.sector, s_ss);
+    __syncthreads();
+    const StencilSector<T> &ss = s_ss;
+    const int V = p.md.V;
+    const int j = static_cast<int>(threadIdx.x) % kHeavyGroup;
+    const int slot = static_cast<int>(threadIdx.x) / kHeavyGroup;
+    const int u0 = static_cast<int>(tile.local0);
+    const int u = u0 + j;
+    const bool active = j < tile.count;
+    T in[NB], in2[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] = T(0);
+        in2[c] = T(0);
+    }
+    accumulate_terms<T, NB, MODE>(
+        p,
+        [&](auto want_in, auto &&acc) {
+            if constexpr (decltype(want_in)::value) {
+                const int tu = tri(u);
+                for (int k = 0; k < ss.n_heavy; ++k) {
+                    const int src = ss.heavy_src[k];
+                    const T a0 = ss.rheavy[k][0], a1 = ss.rheavy[k][1];
+                    // {w, u} for w <= u: the run src + T(u) .. src + T(u) + u
+#pragma unroll 4
+                    for (int w = slot; w <= u; w += kHeavySlots) {
+                        const T a = w == u ? a1 : a0;
+                        acc(src + tu + w, a, active && a > T(0));
+                    }
+                    // {u, w} for w > u: src + u + T(w), the group's rows side by side
+#pragma unroll 4
+                    for (int w = u0 + 1 + slot; w < V; w += kHeavySlots) {
+                        acc(src + u + tri(w), a0, active && w > u && a0 > T(0));
+                    }
+                }
+            }
+        },
+        in, in2);
+    // the threads of row j: lanes j, j + 8, j + 16, j + 24 of each warp, then the warps in order
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        in[c] += __shfl_xor_sync(0xffffffffU, in[c], 8);
+        in[c] += __shfl_xor_sync(0xffffffffU, in[c], 16);
+    }
+    const int warp = static_cast<int>(threadIdx.x) >> 5;
+    const int lane = static_cast<int>(threadIdx.x) & 31;
+    if (lane < kHeavyGroup) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            s_red[warp][lane][c] = in[c];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x >= static_cast<unsigned>(tile.count)) {
+        return;
+    }
+    // thread j < count: the row's own terms, then the heavy sum
+    const int row = ss.begin + u;
+    const unsigned m = load_ro(p.md.vmask + (V - 1 - u));
+    T exit = T(0), leak = T(0);
+    T own[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        own[c] = T(0);
+    }
+    accumulate_terms<T, NB, MODE>(
+        p,
+        [&](auto want_in, auto &&acc) {
+            constexpr bool W = decltype(want_in)::value;
+            pair_row<T, W>(p.md, p.sv, ss, 1, u, 0, m, 0U, row, exit, leak, acc);
+        },
+        own, in2);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        T h = T(0);
+        for (int w = 0; w < kHeavyThreads / 32; ++w) {
+            h += s_red[w][j][c];
+        }
+        own[c] += h;
+    }
+    finish_row<T, NB, MODE>(p, row, exit, leak, own, in2);
 }
 
 template <typename T, int NB, int MODE>
@@ -527,6 +635,31 @@ cudaError_t launch_pair_heavy(const RowParams<T> &p, cudaStream_t stream) {
 }
 
 template <typename T, int NB>
+cudaError_t launch_pair_heavy_group(const RowParams<T> &p, cudaStream_t stream) {
+    if (p.n_tiles == 0) {
+        return cudaSuccess;
+    }
+    if (!p.sv.sectors) {
+        return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    switch (p.mode) {
+    case kApplyQ:
+        pair_heavy_group_kernel<T, NB, kApplyQ><<<p.n_tiles, kHeavyThreads, 0, stream>>>(p);
+        break;
+    case kApplyShifted:
+        pair_heavy_group_kernel<T, NB, kApplyShifted><<<p.n_tiles, kHeavyThreads, 0, stream>>>(p);
+        break;
+    case kResidual:
+        pair_heavy_group_kernel<T, NB, kResidual><<<p.n_tiles, kHeavyThreads, 0, stream>>>(p);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T, int NB>
 cudaError_t launch_pair_strip(const RowParams<T> &p, cudaStream_t stream) {
     if (p.n_tiles == 0) {
         return cudaSuccess;
@@ -571,6 +704,7 @@ cudaError_t launch_pair_strip(const RowParams<T> &p, cudaStream_t stream) {
 
 template cudaError_t launch_stencil<MK_T, MK_NB>(const RowParams<MK_T> &, int, int, cudaStream_t);
 template cudaError_t launch_pair_strip<MK_T, MK_NB>(const RowParams<MK_T> &, cudaStream_t);
+template cudaError_t launch_pair_heavy_group<MK_T, MK_NB>(const RowParams<MK_T> &, cudaStream_t);
 template cudaError_t launch_pair_heavy<MK_T, MK_NB>(const RowParams<MK_T> &, cudaStream_t);
 
 } // namespace mkb::detail
