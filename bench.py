@@ -800,8 +800,8 @@ def roofline(mk, Q, dev, N, w) -> dict:
     """The generator SpMV of the workload, the kernel the roofline target names: FP64
     apply_shifted, one compulsory read of x and write of y, 16 bytes per state (134 MB per apply
     on the 16^3 box, larger than L2), L2 flushed before each timed apply; every kernel of the
-    pass is inside the timed region (the pair-row kernel for the light rows and the general one
-    for the rows whose in-jumps come from every voxel)."""
+    pass is inside the timed region (the pair-strip kernel for the two-molecule rows, the
+    grouped and single heavy-row kernels for the rows whose in-jumps come from every voxel)."""
     import torch
 
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -820,7 +820,7 @@ def roofline(mk, Q, dev, N, w) -> dict:
         "unit": "GB/s",
         "frac": round(achieved / pk["hbm_gbs"], 4),
         "traffic": ncu_traffic(SPMV_PROFILE) if w["workload"].startswith("rdme_birth_death_3d_16") else None,
-        "traffic_source": f"profiles/{SPMV_PROFILE}.md (ncu dram bytes, both kernels of one apply)",
+        "traffic_source": f"profiles/{SPMV_PROFILE}.md (ncu dram bytes, the three kernels of one apply)",
         "us_per_apply": round(ms * 1e3, 3),
         "algorithmic_bytes_per_apply": algo,
     }
