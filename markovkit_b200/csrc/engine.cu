@@ -228,10 +228,12 @@ void OperatorLevel::finalize(const Model &m, bool with_reactions) {
         }
     }
     // sectors of every pair u0 <= u1 of the V voxels: the pair-strip form, a tile per pair of
-    // triangle rows
+    // triangle rows. On grids of fewer voxels a level's rows fit a few waves of one launch, and
+    // a second launch per pass would cost more than the form saves.
     strip_tiles.clear();
     stencil_rest.clear();
-    if (pair && S == 1 && !stencil_tiles.empty()) {
+    constexpr int kStripMinVoxels = 1024;
+    if (pair && S == 1 && !stencil_tiles.empty() && V >= kStripMinVoxels) {
         const std::int64_t pairs = static_cast<std::int64_t>(V) * (V + 1) / 2;
         std::vector<char> strip(sectors.size(), 0);
         for (std::size_t k = 0; k < sectors.size(); ++k) {

@@ -29,6 +29,9 @@ PROBLEMS = {
                           [1, 1], "absorbing"),
     "birth_death_1d128_cap4": ([128], [1.0], _birth_death(), [4], "absorbing"),
     "diffusion_2d6_cap4": ([6, 6], [0.8], [], [4], "absorbing"),
+    # grids of at least 1024 voxels take the pair-strip form on their two-molecule sectors
+    "birth_death_1d2048_cap2_reflecting": ([2048], [1.0], _birth_death(2.0, 1.0), [2], "reflecting"),
+    "birth_death_2d32_cap2": ([32, 32], [0.7], _birth_death(), [2], "absorbing"),
 }
 
 
@@ -46,7 +49,8 @@ def general_after():
     mk.set_row_path("stencil")
 
 
-PAIR_SHAPES = {"birth_death_3d16_cap2", "birth_death_3d8_cap2_reflecting", "annihilation_2d32"}
+PAIR_SHAPES = {"birth_death_3d16_cap2", "birth_death_3d8_cap2_reflecting", "annihilation_2d32",
+               "birth_death_1d2048_cap2_reflecting", "birth_death_2d32_cap2"}
 
 
 def _same(a, b, name, rel=1e-14):
@@ -115,11 +119,13 @@ def test_cycle_matches_general_and_is_reproducible(cuda, general_after, name, sm
         assert float(torch.max(torch.abs(outs[0] - outs[2]))) <= 1e-5 * scale
 
 
-@pytest.mark.parametrize("name", ["birth_death_3d16_cap2", "birth_death_3d8_cap2_reflecting"])
+@pytest.mark.parametrize("name", ["birth_death_3d16_cap2", "birth_death_1d2048_cap2_reflecting",
+                                  "birth_death_2d32_cap2"])
 def test_pair_strip_matches_pair_kernel_bitwise(cuda, general_after, name):
-    """The pair-strip kernel (a block per pair of triangle rows) on the two-molecule sectors
-    against the stencil kernel's pair form on the same rows: every operator pass, FP64 and
-    FP32, one and four right-hand sides, and V-cycles with each smoother, bit for bit."""
+    """The pair-strip kernel (a block per pair of triangle rows, on grids of at least 1024
+    voxels) on the two-molecule sectors against the stencil kernel's pair form on the same rows:
+    every operator pass, FP64 and FP32, one and four right-hand sides, and V-cycles with each
+    smoother, bit for bit; 1-, 2- and 3-D grids."""
     import torch
 
     dom, _, box, Q = _problem(name)
