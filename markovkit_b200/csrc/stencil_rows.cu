@@ -442,16 +442,26 @@ __global__ void __launch_bounds__(kRowBlock, 4) pair_strip_kernel(const __grid_c
         const int up0 = g0 * w + tri(g0), up1 = g1 * w + tri(g1), up2 = g2 * w + tri(g2);
         const int down0 = -g0 * w + tri(g0 - 1), down1 = -g1 * w + tri(g1 - 1), down2 = -g2 * w + tri(g2 - 1);
         const int far_end = w - p.sv.gmax; // rows u0 < far_end are outside the band
-        for (int u0 = static_cast<int>(threadIdx.x); u0 <= w; u0 += kRowBlock) {
-            const int row = ss.begin + tw + u0;
-            const unsigned m0 = load_ro(p.md.vmask + (V - 1 - u0));
-            if (colour >= 0 && static_cast<int>(((m0 ^ m1) >> kVoxelColourBit) & 1U) != colour) {
-                continue;
-            }
-            if (u0 < far_end) {
-                strip_row<T, NB, MODE, true>(p, ss, u0, w, m0, m1, row, up0, up1, up2, down0, down1, down2);
-            } else {
-                strip_row<T, NB, MODE, false>(p, ss, u0, w, m0, m1, row, up0, up1, up2, down0, down1, down2);
+        // colour passes: two consecutive rows per thread, of which mostly one has the pass's colour
+        // (the colours alternate along a grid line), so that few lanes idle
+        constexpr int RPT = kRowsPerThread<MODE>;
+        for (int base = RPT * static_cast<int>(threadIdx.x); base <= w; base += RPT * kRowBlock) {
+#pragma unroll
+            for (int q = 0; q < RPT; ++q) {
+                const int u0 = base + q;
+                if (u0 > w) {
+                    break;
+                }
+                const int row = ss.begin + tw + u0;
+                const unsigned m0 = load_ro(p.md.vmask + (V - 1 - u0));
+                if (colour >= 0 && static_cast<int>(((m0 ^ m1) >> kVoxelColourBit) & 1U) != colour) {
+                    continue;
+                }
+                if (u0 < far_end) {
+                    strip_row<T, NB, MODE, true>(p, ss, u0, w, m0, m1, row, up0, up1, up2, down0, down1, down2);
+                } else {
+                    strip_row<T, NB, MODE, false>(p, ss, u0, w, m0, m1, row, up0, up1, up2, down0, down1, down2);
+                }
             }
         }
     }
