@@ -418,7 +418,7 @@ __device__ __forceinline__ void strip_row(const RowParams<T> &p, const StencilSe
 // same order as pair_row, whose other rows it calls, so the results equal pair_kernel's bit for
 // bit. p.tiles: kind-3 tiles, local0 = the pair index.
 template <typename T, int NB, int MODE>
-__global__ void __launch_bounds__(kRowBlock, 4) pair_strip_kernel(const __grid_constant__ RowParams<T> p) {
+__global__ void __launch_bounds__(kRowBlock, NB == 1 ? 5 : 4) pair_strip_kernel(const __grid_constant__ RowParams<T> p) {
     __shared__ StencilSector<T> s_ss;
     const Tile tile = p.tiles[blockIdx.x];
     if (p.sector_class >= 0 && p.sectors[tile.sector].gs_class != p.sector_class) {
