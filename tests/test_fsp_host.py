@@ -102,3 +102,17 @@ def test_argument_errors_before_device_work():
     assert _lib.load().mk_fsp_box_size(2, (C.c_int * 2)(40000, 40000), C.byref(size)) == _lib.MK_EOVERFLOW
     assert _lib.load().mk_fsp_box_size(2, (C.c_int * 2)(3, 4), C.byref(size)) == _lib.MK_OK
     assert size.value == 20
+
+
+def test_regions_resolve_on_the_host():
+    """box(bound) bounds every species once their count is known; the device FSP takes a box or
+    everywhere() (None too) and refuses any other region before any device work."""
+    from markovkit_b200.fsp import _first_box, _solve, box, everywhere
+
+    assert box(7).resolved(3).bounds == [7, 7, 7]
+    assert box([1, 2]).resolved(2).bounds == [1, 2]
+    assert _first_box([0, 5]).bounds == [16, 21]
+    net, init, T, opt = fsp_cases.cases()["birth_death_two_layers"]
+    with pytest.raises(ValueError):
+        _solve([(net, init, T, krylov_fsp_options(inside=lambda x: True))])
+    assert isinstance(everywhere(), everywhere)
